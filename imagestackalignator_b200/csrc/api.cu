@@ -1,0 +1,987 @@
+// C ABI (include/isa.h): argument checks, the context that owns the fused
+// pipeline's buffers, and the pipeline itself, which issues the kernels in
+// the order of the reference controller (ImageStackAlignatorController.cs:
+// DeBayerBWGaussWB :2384-2418, TrackPatches :1601-1746, PrepareAccumulation
+// :1795-1926, Accumulate :1928-1987) on the caller's stream.
+#include "isa.h"
+#include "isa_internal.cuh"
+
+#include <cufft.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define ISA_CK(call)                                                                         \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) return fail(ISA_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define ISA_FFT(call)                                                              \
+    do {                                                                           \
+        cufftResult r_ = (call);                                                   \
+        if (r_ != CUFFT_SUCCESS) return fail(ISA_ECUDA, "%s: cufft error %d", #call, (int)r_); \
+    } while (0)
+#define ISA_TRY(call)            \
+    do {                         \
+        int s_ = (call);         \
+        if (s_ != ISA_OK) return s_; \
+    } while (0)
+
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+unsigned pack_cfa(const int cfa[4])
+{
+    unsigned v = 0;
+    for (int i = 0; i < 4; i++) v |= (unsigned)(cfa[i] & 3) << (2 * i);
+    return v;
+}
+
+bool cfa_ok(const int cfa[4])
+{
+    for (int i = 0; i < 4; i++)
+        if (cfa[i] < 0 || cfa[i] > 2) return false;
+    return true;
+}
+
+// gaussian_filter_1D (controller :2351-2382), float arithmetic as in C#.
+std::vector<float> gauss_taps(float sigma)
+{
+    if (sigma <= 0) {
+        std::vector<float> t(9, 0.f);
+        t[4] = 1.f;
+        return t;
+    }
+    int size = (int)(sigma / 0.6f - 0.4f) * 2 + 1 + 2;
+    size = std::min(size, 99);
+    std::vector<float> t(size);
+    int c = size / 2;
+    for (int i = 0; i < size; i++) {
+        int x = i - c;
+        t[i] = (float)std::exp((double)((float)(-(x * x)) / (2 * sigma * sigma)));
+    }
+    float sum = 0;
+    for (int i = 0; i < size; i++) sum += t[i];
+    for (int i = 0; i < size; i++) t[i] /= sum;
+    return t;
+}
+
+// ---- ShiftCollection bookkeeping (ShiftCollection.cs:100-512) -------------
+struct Strategy {
+    int n = 0, m = 0, n1 = 0;
+    std::vector<std::pair<int, int>> pairs;  // tracking order (FillShiftPairs)
+    std::vector<int> idx;                    // n x n -> measurement row (FillIndexTable)
+    std::vector<int> a, b, sign;             // row k of the incidence matrix = sign on [a, b)
+};
+
+int shift_count(int n, int strategy, int block)
+{
+    switch (strategy) {
+    case ISA_TRACK_FULL: return (int)((n - 1) * ((float)n / 2.0f));
+    case ISA_TRACK_ONLY_ON_REFERENCE: return n - 1;
+    case ISA_TRACK_ON_REFERENCE_BLOCK: return (int)((block - 1) * ((float)block / 2.0f)) + block * (n - block);
+    case ISA_TRACK_BLOCKS: return (int)(-0.5 * block * (block - 2 * n + 1));
+    }
+    return 0;
+}
+
+bool build_strategy(int n, int ref, int strategy, int block, Strategy& s)
+{
+    if (block >= n) block = n - 1;  // ShiftCollection constructor
+    s = Strategy();
+    s.n = n;
+    s.n1 = n - 1;
+    s.m = shift_count(n, strategy, block);
+    s.idx.assign((size_t)n * n, -1);
+    int first = 0, last = 0;
+    if (strategy == ISA_TRACK_ON_REFERENCE_BLOCK) {
+        if (ref < n / 2) { first = std::max(ref - block / 2, 0); last = first + block - 1; }
+        else { last = std::min(ref + block / 2, n - 1); first = last - block + 1; }
+    }
+    auto add_row = [&](int from, int to, int a, int b, int sg) {
+        s.idx[(size_t)from * n + to] = (int)s.a.size();
+        s.a.push_back(a); s.b.push_back(b); s.sign.push_back(sg);
+    };
+    // rows in FillIndexTable order with their incidence intervals
+    if (strategy == ISA_TRACK_FULL) {
+        for (int d = 1; d < n; d++)
+            for (int f = 0; f + d < n; f++) add_row(f, f + d, f, f + d, 1);
+        for (int r = 0; r < n; r++)
+            for (int t = r + 1; t < n; t++) s.pairs.push_back({r, t});
+    } else if (strategy == ISA_TRACK_ONLY_ON_REFERENCE) {
+        for (int t = 0; t < n; t++) {
+            if (t == ref) continue;
+            if (t < ref) add_row(ref, t, t, ref, -1);
+            else add_row(ref, t, ref, t, 1);
+            s.pairs.push_back({ref, t});
+        }
+    } else if (strategy == ISA_TRACK_ON_REFERENCE_BLOCK) {
+        for (int sh = 0; sh < block - 1; sh++) {
+            int count = block - 1 - sh;
+            for (int line = 0; line < count; line++) {
+                int f = line + first, t = line + first + block - count;
+                add_row(f, t, f, t, 1);
+                s.pairs.push_back({f, t});
+            }
+        }
+        for (int i = 0; i < first; i++)
+            for (int tb = first; tb <= last; tb++) { add_row(tb, i, i, tb, -1); s.pairs.push_back({tb, i}); }
+        for (int i = last + 1; i < n; i++)
+            for (int tb = first; tb <= last; tb++) { add_row(tb, i, tb, i, 1); s.pairs.push_back({tb, i}); }
+    } else if (strategy == ISA_TRACK_BLOCKS) {
+        for (int d = 1; d <= block; d++)
+            for (int f = 0; f + d < n; f++) add_row(f, f + d, f, f + d, 1);
+        for (int sh = 0; sh < block; sh++) {
+            int count = (n - 1) - sh;
+            for (int line = 0; line < count; line++) s.pairs.push_back({line, line + n - count});
+        }
+    } else {
+        return false;
+    }
+    return (int)s.a.size() == s.m && (int)s.pairs.size() == s.m;  // "Ooups" check (ShiftCollection.cs:522-525)
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct isa_ctx {
+    int max_w = 0, max_h = 0, max_n = 0;
+    isa_params p{};
+    int max_pairs = 0, max_rows = 0, max_tiles = 0, maxcx = 0, maxcy = 0;
+    int max_wo = 0, max_ho = 0;
+    // device memory (one arena, carved)
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    uint16_t* raw_stage = nullptr;
+    float *bw_track = nullptr, *bw_acc = nullptr, *tmp = nullptr;
+    float* pyr[ISA_MAX_LEVELS] = {};
+    float2* spec = nullptr;
+    float2 *grids = nullptr, *grids_tmp = nullptr, *x = nullptr, *tiles_opt = nullptr;
+    int* status = nullptr;
+    int *row_a = nullptr, *row_b = nullptr, *row_sign = nullptr, *row_grid = nullptr;
+    double* N0 = nullptr;
+    isa_pair_desc* pair_desc = nullptr;
+    const float** frame_tab = nullptr;
+    float2 *flows = nullptr, *flow_tmp = nullptr;
+    float *half_ref = nullptr, *half_mov = nullptr;
+    float4* masks = nullptr;
+    float *st3 = nullptr, *kparam = nullptr;
+    float *acc = nullptr, *wsum = nullptr, *out_stage = nullptr;
+    isa_frame_in* frame_in = nullptr;
+    // cuFFT plans for the current frame size
+    cufftHandle r2c = 0, c2r = 0;
+    int plan_w = 0, plan_h = 0;
+    void* fft_work = nullptr;
+    size_t fft_work_bytes = 0;
+    cudaEvent_t ev[8] = {};
+    int ev_count = 0;
+    // last call
+    int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0;
+};
+
+namespace {
+
+size_t bw_pitch(int W) { return (size_t)W * sizeof(float); }
+
+int level_tiles(const isa_level& l, int W, int H, int* tcx, int* tcy)
+{
+    int Wl = W / l.resize_level, Hl = H / l.resize_level;
+    *tcx = (Wl - 2 * l.max_shift) / l.tile_size;
+    *tcy = (Hl - 2 * l.max_shift) / l.tile_size;
+    return (*tcx > 0 && *tcy > 0) ? ISA_OK : ISA_EINVAL;
+}
+
+int check_params(const isa_params* p)
+{
+    if (!p) return fail(ISA_EINVAL, "params is NULL");
+    if (p->level_count < 1 || p->level_count > ISA_MAX_LEVELS) return fail(ISA_EINVAL, "level_count %d out of range", p->level_count);
+    for (int i = 0; i < p->level_count; i++) {
+        const isa_level& l = p->levels[i];
+        if (l.resize_level < 1 || l.tile_size < 2 || (l.tile_size & 1) || l.max_shift < 1)
+            return fail(ISA_EINVAL, "level %d: resize %d tile %d shift %d invalid", i, l.resize_level, l.tile_size, l.max_shift);
+    }
+    if (p->levels[0].resize_level != 1) return fail(ISA_EINVAL, "the finest level must have resize_level 1");
+    if (p->window_size_lk < 1 || p->window_size_lk / 2 > 15) return fail(ISA_EINVAL, "window_size_lk %d out of range", p->window_size_lk);
+    if (p->erode_size < 1 || p->erode_size / 2 > 4) return fail(ISA_EINVAL, "erode_size %d out of range", p->erode_size);
+    if (p->iterations_lk < 0) return fail(ISA_EINVAL, "iterations_lk < 0");
+    if (p->tracking_strategy < 0 || p->tracking_strategy > 3) return fail(ISA_EINVAL, "tracking_strategy %d", p->tracking_strategy);
+    if (p->merge_scale < 0 || p->merge_scale > 8) return fail(ISA_EINVAL, "merge_scale %g out of range", p->merge_scale);
+    return ISA_OK;
+}
+
+// Geometry of the accumulation for a W x H frame (see merge.cu).
+void accum_geom(const isa_params* p, int W, int H, isa_accum_geom& g, float& thr)
+{
+    g.W = W; g.H = H;
+    if (p->merge_scale > 0) {
+        g.s = p->merge_scale;
+        g.Wo = (int)std::lround(W * (double)p->merge_scale);
+        g.Ho = (int)std::lround(H * (double)p->merge_scale);
+        g.ox = g.oy = 0;
+        g.cx0 = 0; g.cy0 = 0; g.cx1 = W - 1; g.cy1 = H - 1;
+        thr = 0.f;
+    } else if (p->super_resolution) {
+        g.s = 2.f; g.Wo = W; g.Ho = H; g.ox = W / 2; g.oy = H / 2;
+        g.cx0 = W / 4; g.cy0 = H / 4; g.cx1 = W / 2 - 1 + W / 4; g.cy1 = H / 2 - 1 + H / 4;
+        thr = 0.f;
+    } else {
+        g.s = 1.f; g.Wo = W; g.Ho = H; g.ox = g.oy = 0;
+        g.cx0 = 0; g.cy0 = 0; g.cx1 = W - 1; g.cy1 = H - 1;
+        thr = 1.f;
+    }
+    float r = std::round(g.s);
+    g.s_int = (r == g.s && r >= 1.f) ? (int)r : 0;
+}
+
+int ensure_plans(isa_ctx* c, int W, int H)
+{
+    if (c->plan_w == W && c->plan_h == H) return ISA_OK;
+    if (c->r2c) { cufftDestroy(c->r2c); c->r2c = 0; }
+    if (c->c2r) { cufftDestroy(c->c2r); c->c2r = 0; }
+    size_t w1 = 0, w2 = 0;
+    ISA_FFT(cufftCreate(&c->r2c));
+    ISA_FFT(cufftCreate(&c->c2r));
+    ISA_FFT(cufftSetAutoAllocation(c->r2c, 0));
+    ISA_FFT(cufftSetAutoAllocation(c->c2r, 0));
+    ISA_FFT(cufftMakePlan2d(c->r2c, H, W, CUFFT_R2C, &w1));
+    ISA_FFT(cufftMakePlan2d(c->c2r, H, W, CUFFT_C2R, &w2));
+    size_t need = std::max(w1, w2);
+    if (need > c->fft_work_bytes) {
+        if (c->fft_work) cudaFree(c->fft_work);
+        c->fft_work = nullptr;
+        c->fft_work_bytes = 0;
+        if (cudaMalloc(&c->fft_work, need) != cudaSuccess) return fail(ISA_ENOMEM, "cuFFT work area of %zu bytes", need);
+        c->fft_work_bytes = need;
+    }
+    ISA_FFT(cufftSetWorkArea(c->r2c, c->fft_work));
+    ISA_FFT(cufftSetWorkArea(c->c2r, c->fft_work));
+    c->plan_w = W;
+    c->plan_h = H;
+    return ISA_OK;
+}
+
+void color_consts(const isa_raw_info* info, float black[3], float white[3], float scale[3], float divisor[3])
+{
+    for (int c = 0; c < 3; c++) {
+        black[c] = info->black[c];
+        white[c] = info->white[c];
+        float cw = info->camera_white[c] != 0.f ? info->camera_white[c] : 1.f;
+        scale[c] = 1.0f / cw;
+        divisor[c] = info->white[c] / cw;
+    }
+}
+
+// DeBayerBWGaussWB (controller :2384-2418) for one frame into `out`;
+// `gray_out`, when given, also receives the Gaussian of the un-filtered
+// gray image (the accumulation variant, skipFourierFilter = true).
+int bw_frame(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H, const isa_raw_info* info, bool high_pass, float* out,
+             const std::vector<float>& taps_hp, float* acc_out, const std::vector<float>& taps_acc, cudaStream_t st)
+{
+    float black[3], white[3], scale[3], divisor[3];
+    color_consts(info, black, white, scale, divisor);
+    const float gw_rgb[3] = {0.2989f, 0.5870f, 0.1141f}, gw_g[3] = {0.f, 1.f, 0.f};
+    const float* gw = c->p.green_channel_only ? gw_g : gw_rgb;
+    size_t pitch = bw_pitch(W);
+    ISA_CK(isa_launch_demosaic_gray(raw, raw_pitch, W, H, pack_cfa(info->cfa), black, scale, divisor, gw, 1, out, pitch, nullptr, 0, st));
+    if (acc_out)
+        ISA_CK(isa_launch_gauss(out, pitch, acc_out, pitch, c->tmp, pitch, W, H, 1, taps_acc.data(), (int)taps_acc.size(), 0, st));
+    if (high_pass) {
+        ISA_TRY(ensure_plans(c, W, H));
+        ISA_FFT(cufftSetStream(c->r2c, st));
+        ISA_FFT(cufftSetStream(c->c2r, st));
+        ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)out, (cufftComplex*)c->spec));
+        ISA_CK(isa_launch_fourier_filter(c->spec, (size_t)(W / 2 + 1) * sizeof(float2), W, H, 1, 0, 1.0f, c->p.high_pass, 1.0f,
+                                         c->p.high_pass_sigma, c->p.clear_axis, 1.0f / ((float)W * (float)H), st));
+        ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)out));
+    }
+    if (!taps_hp.empty())
+        ISA_CK(isa_launch_gauss(out, pitch, out, pitch, c->tmp, pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), high_pass ? 1 : 0, st));
+    return ISA_OK;
+}
+
+int check_info(const isa_raw_info* info)
+{
+    if (!info) return fail(ISA_EINVAL, "raw info is NULL");
+    if (info->width < 16 || info->height < 16 || (info->width & 1) || (info->height & 1))
+        return fail(ISA_EINVAL, "frame %dx%d: need even sizes of at least 16", info->width, info->height);
+    if (!cfa_ok(info->cfa)) return fail(ISA_EINVAL, "CFA codes must be 0 (R), 1 (G) or 2 (B)");
+    for (int c = 0; c < 3; c++)
+        if (!(info->white[c] > 0)) return fail(ISA_EINVAL, "white level must be positive");
+    return ISA_OK;
+}
+
+float prealign_rot(const isa_prealign* pre, int from, int to)
+{
+    if (!pre || !pre->rotations_deg) return 0.f;
+    float a = pre->rotations_deg[to] - pre->rotations_deg[from];
+    return a / 180.0f * (float)M_PI;
+}
+
+void prealign_shift(const isa_prealign* pre, int from, int to, float out[2])
+{
+    out[0] = out[1] = 0.f;
+    if (!pre || !pre->shifts) return;
+    out[0] = pre->shifts[2 * to] - pre->shifts[2 * from];
+    out[1] = pre->shifts[2 * to + 1] - pre->shifts[2 * from + 1];
+}
+
+int upload_strategy(isa_ctx* c, const Strategy& s, cudaStream_t st)
+{
+    std::vector<double> N0((size_t)s.n1 * s.n1, 0.0);
+    for (int k = 0; k < s.m; k++)
+        for (int i = s.a[k]; i < s.b[k]; i++)
+            for (int j = s.a[k]; j < s.b[k]; j++) N0[(size_t)i * s.n1 + j] += 1.0;
+    std::vector<int> rg(s.m);
+    for (int k = 0; k < s.m; k++) rg[k] = k;  // grid k holds measurement row k
+    ISA_CK(cudaMemcpyAsync(c->row_a, s.a.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(c->row_b, s.b.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(c->row_sign, s.sign.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(c->row_grid, rg.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(c->N0, N0.data(), N0.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    // pageable sources: the copies above complete before returning
+    return ISA_OK;
+}
+
+int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+              const isa_prealign* pre, float* out, size_t out_pitch, cudaStream_t st)
+{
+    const isa_params* p = &c->p;
+    ISA_TRY(check_info(info));
+    const int W = info->width, H = info->height;
+    if (W > c->max_w || H > c->max_h) return fail(ISA_EINVAL, "frame %dx%d exceeds the context's %dx%d", W, H, c->max_w, c->max_h);
+    if (n < 2 || n > c->max_n) return fail(ISA_EINVAL, "frame count %d outside [2, %d]", n, c->max_n);
+    if (!raw || !out) return fail(ISA_EINVAL, "NULL frame or output pointer");
+    const int ref = pre ? pre->reference : 0;
+    if (ref < 0 || ref >= n) return fail(ISA_EINVAL, "reference index %d outside [0, %d)", ref, n);
+    if (raw_pitch < (size_t)W * 2 || frame_stride < raw_pitch * H) return fail(ISA_EINVAL, "raw pitch/stride too small");
+    isa_accum_geom g;
+    float thr;
+    accum_geom(p, W, H, g, thr);
+    if (out_pitch < (size_t)g.Wo * 12) return fail(ISA_EINVAL, "output pitch %zu < %d", out_pitch, g.Wo * 12);
+    if (g.Wo > c->max_wo || g.Ho > c->max_ho) return fail(ISA_EINVAL, "output exceeds the context");
+    Strategy strat;
+    if (!build_strategy(n, ref, p->tracking_strategy, p->tracking_block_size, strat))
+        return fail(ISA_EINVAL, "tracking strategy %d with block %d and %d frames is inconsistent", p->tracking_strategy,
+                    p->tracking_block_size, n);
+    if (strat.m > c->max_rows || strat.n1 > 64) return fail(ISA_EINVAL, "too many frame pairs for the context");
+    const auto frame = [&](int i) { return (const uint16_t*)((const char*)raw + (size_t)i * frame_stride); };
+    const size_t pitch = bw_pitch(W);
+    const size_t fsz = (size_t)W * H;
+    const unsigned cfa = pack_cfa(info->cfa);
+    float black[3], white[3], scale[3], divisor[3];
+    color_consts(info, black, white, scale, divisor);
+    c->ev_count = 0;
+    auto mark = [&]() -> int {
+        ISA_CK(cudaEventRecord(c->ev[c->ev_count++], st));
+        return ISA_OK;
+    };
+    ISA_TRY(mark());
+    // 1. tracking (high-pass) and accumulation images of every frame
+    const std::vector<float> taps_trk = gauss_taps(p->sigma_debayer_tracking), taps_acc = gauss_taps(p->sigma_debayer_accumulation);
+    for (int i = 0; i < n; i++)
+        ISA_TRY(bw_frame(c, frame(i), raw_pitch, W, H, info, true, c->bw_track + i * fsz, taps_trk, c->bw_acc + i * fsz, taps_acc, st));
+    ISA_TRY(mark());
+    // 2. pyramid tile alignment, coarsest level first (TrackPatches :1640-1712)
+    ISA_TRY(upload_strategy(c, strat, st));
+    const int L = p->level_count;
+    const size_t gpitch = (size_t)c->maxcx * sizeof(float2), gstride = gpitch * c->maxcy;
+    int otcx = 0, otcy = 0, olevel = 0, oT = 0;
+    float2* grids = c->grids;
+    float2* grids_tmp = c->grids_tmp;
+    ISA_CK(cudaMemsetAsync(grids, 0, gstride * strat.m, st));
+    int tcx0 = 0, tcy0 = 0;
+    for (int li = L - 1; li >= 0; li--) {
+        const isa_level& lv = p->levels[li];
+        const int Wl = W / lv.resize_level, Hl = H / lv.resize_level;
+        int tcx, tcy;
+        if (level_tiles(lv, W, H, &tcx, &tcy) != ISA_OK) return fail(ISA_EINVAL, "level %d has no tiles for %dx%d", li, W, H);
+        if (li == 0) { tcx0 = tcx; tcy0 = tcy; }
+        if (li != L - 1) {
+            ISA_CK(isa_launch_upsample(grids, gpitch, gstride, grids_tmp, gpitch, gstride, strat.m, olevel, lv.resize_level, otcx, otcy, tcx,
+                                       tcy, oT, lv.tile_size, st));
+            std::swap(grids, grids_tmp);
+        }
+        std::vector<const float*> fptr(n);
+        size_t lpitch = bw_pitch(Wl);
+        if (lv.resize_level > 1) {
+            float* base = c->pyr[li];
+            for (int i = 0; i < n; i++) {
+                float* dst = base + (size_t)i * Wl * Hl;
+                ISA_CK(isa_launch_resize_box(c->bw_track + i * fsz, pitch, W, H, lv.resize_level, dst, lpitch, st));
+                fptr[i] = dst;
+            }
+        } else {
+            for (int i = 0; i < n; i++) fptr[i] = c->bw_track + i * fsz;
+        }
+        std::vector<isa_pair_desc> pd(strat.m);
+        for (size_t k = 0; k < strat.pairs.size(); k++) {
+            int r = strat.pairs[k].first, t = strat.pairs[k].second;
+            float br[2], bt[2];
+            prealign_shift(pre, ref, r, br);
+            prealign_shift(pre, ref, t, bt);
+            isa_pair_desc& d = pd[k];
+            d.ref = r; d.trk = t; d.grid = strat.idx[(size_t)r * n + t];
+            d.base_ref_x = br[0] / lv.resize_level; d.base_ref_y = br[1] / lv.resize_level; d.rot_ref = prealign_rot(pre, ref, r);
+            d.base_trk_x = bt[0] / lv.resize_level; d.base_trk_y = bt[1] / lv.resize_level; d.rot_trk = prealign_rot(pre, ref, t);
+        }
+        ISA_CK(cudaMemcpyAsync(c->pair_desc + (size_t)li * c->max_pairs, pd.data(), pd.size() * sizeof(isa_pair_desc),
+                               cudaMemcpyHostToDevice, st));
+        ISA_CK(cudaMemcpyAsync(c->frame_tab + (size_t)li * c->max_n, fptr.data(), n * sizeof(float*), cudaMemcpyHostToDevice, st));
+        ISA_CK(isa_launch_track(c->frame_tab + (size_t)li * c->max_n, lpitch, Wl, Hl, lv.tile_size, lv.max_shift, tcx, tcy,
+                                c->pair_desc + (size_t)li * c->max_pairs, strat.m, grids, gpitch, gstride, p->matching_threshold, nullptr,
+                                nullptr, st));
+        ISA_CK(isa_launch_solve(c->row_a, c->row_b, c->row_sign, c->N0, strat.m, strat.n1, grids, gpitch, gstride, c->row_grid, tcx, tcy,
+                                c->x, c->status, st));
+        otcx = tcx; otcy = tcy; olevel = lv.resize_level; oT = lv.tile_size;
+    }
+    ISA_TRY(mark());
+    // 3. kernel parameters from the reference frame (PrepareAccumulation :1851-1858)
+    const std::vector<float> taps_st = gauss_taps(p->sigma_structure_tensor);
+    const size_t p3 = (size_t)W * 12, p4 = (size_t)W * 16;
+    ISA_CK(isa_launch_structure_tensor(c->bw_acc + ref * fsz, pitch, W, H, c->st3, p3, st));
+    ISA_CK(isa_launch_gauss(c->st3, p3, c->st3, p3, c->tmp, p3, W, H, 3, taps_st.data(), (int)taps_st.size(), 0, st));
+    ISA_CK(isa_launch_kernel_param(c->st3, p3, W, H, c->kparam, p4, 4, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
+                                   st));
+    ISA_TRY(mark());
+    // 4. per frame: LK refinement and robustness mask (Accumulate :1961-1977)
+    const int Wh = W / 2, Hh = H / 2;
+    const size_t hp3 = (size_t)Wh * 12, hp4 = (size_t)Wh * 16, fp = (size_t)W * sizeof(float2);
+    float maxv = 0.f;
+    for (int ch = 0; ch < 3; ch++) maxv = std::max(maxv, white[ch] + black[ch]);
+    ISA_CK(isa_launch_subsample(frame(ref), raw_pitch, W, H, cfa, maxv, c->half_ref, hp3, st));
+    const int half = p->window_size_lk / 2;
+    std::vector<isa_frame_in> fin;
+    fin.push_back({frame(ref), nullptr, nullptr});
+    for (int i = 0; i < n; i++) {
+        if (i == ref) continue;
+        float2* flow = c->flows + (size_t)i * fsz;
+        ISA_CK(isa_launch_subsample(frame(i), raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
+        ISA_CK(isa_launch_optimal(c->x, strat.n1, tcx0, tcy0, ref, i, c->tiles_opt, (size_t)tcx0 * sizeof(float2), st));
+        float bs[2];
+        prealign_shift(pre, ref, i, bs);
+        // ping-pong so that the last iteration lands in `flow`
+        float2* a = (p->iterations_lk & 1) ? c->flow_tmp : flow;
+        float2* b = (p->iterations_lk & 1) ? flow : c->flow_tmp;
+        ISA_CK(isa_launch_flow_from_tiles(c->tiles_opt, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1], prealign_rot(pre, ref, i),
+                                          a, fp, st));
+        for (int it = 0; it < p->iterations_lk; it++) {
+            ISA_CK(isa_launch_lk_iteration(a, b, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, pitch, W, H, half, p->min_det_lk, st));
+            std::swap(a, b);
+        }
+        float4* mask = c->masks + (size_t)i * Wh * Hh;
+        ISA_CK(isa_launch_robustness_erode(c->half_ref, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha, info->noise_beta,
+                                           p->threshold_m, p->robust_s, p->robust_t, p->erode_size, mask, hp4, st));
+        fin.push_back({frame(i), flow, mask});
+    }
+    ISA_TRY(mark());
+    // 5. accumulation: reference frame first (PrepareAccumulation :1894-1902), then the others in order
+    const size_t op = (size_t)g.Wo * 12;
+    ISA_CK(cudaMemcpyAsync(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), cudaMemcpyHostToDevice, st));
+    if (p->fused_accumulate) {
+        ISA_CK(isa_launch_accumulate(g, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum,
+                                     op, 0, st));
+    } else {
+        ISA_CK(cudaMemsetAsync(c->acc, 0, op * g.Ho, st));
+        ISA_CK(cudaMemsetAsync(c->wsum, 0, op * g.Ho, st));
+        for (size_t f = 0; f < fin.size(); f++)
+            ISA_CK(isa_launch_accumulate(g, cfa, nullptr, 1, &fin[f], raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum, op, 1,
+                                         st));
+    }
+    ISA_TRY(mark());
+    // 6. ApplyWeighting (:1908-1917, :1994-2002)
+    if (thr > 0)
+        ISA_CK(isa_launch_demosaic_gray(frame(ref), raw_pitch, W, H, cfa, black, scale, divisor, nullptr, 0, nullptr, 0, out, out_pitch, st));
+    ISA_CK(isa_launch_apply_weighting(out, out_pitch, c->acc, c->wsum, op, g.Wo, g.Ho, thr, st));
+    ISA_TRY(mark());
+    c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1;
+    return ISA_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* isa_last_error(void) { return g_err.c_str(); }
+const char* isa_version(void) { return "isa-b200 0.1 (sm_100a)"; }
+
+void isa_params_default(isa_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->sigma_debayer_tracking = 0.5f;
+    p->sigma_debayer_accumulation = 0.5f;
+    p->high_pass = 0.01f;
+    p->high_pass_sigma = 0.0025f;
+    p->clear_axis = 0;
+    p->matching_threshold = 1.0f;
+    p->sigma_structure_tensor = 1.0f;
+    p->dth = 0.001f;
+    p->dtr = 0.006f;
+    p->k_detail = 0.25f;
+    p->k_denoise = 3.0f;
+    p->k_stretch = 4.0f;
+    p->k_shrink = 2.0f;
+    p->iterations_lk = 3;
+    p->window_size_lk = 11;
+    p->erode_size = 5;
+    p->min_det_lk = 0.01f;
+    p->threshold_m = 100000.0f;
+    p->tracking_strategy = ISA_TRACK_FULL;
+    p->tracking_block_size = 5;
+    p->green_channel_only = 0;
+    p->level_count = 4;
+    p->levels[0] = {1, 32, 2};
+    for (int i = 1; i < 4; i++) p->levels[i] = {p->levels[i - 1].resize_level * 2, 32, 4};
+    p->super_resolution = 0;
+    p->merge_scale = 0.f;
+    p->robust_s = 1.5f;
+    p->robust_t = 0.12f;
+    p->fused_accumulate = 1;
+}
+
+int isa_output_size(const isa_params* p, int width, int height, int* ow, int* oh)
+{
+    if (!p || !ow || !oh) return fail(ISA_EINVAL, "NULL argument");
+    isa_accum_geom g;
+    float thr;
+    accum_geom(p, width, height, g, thr);
+    *ow = g.Wo;
+    *oh = g.Ho;
+    return ISA_OK;
+}
+
+int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_params* p)
+{
+    if (!out) return fail(ISA_EINVAL, "ctx out pointer is NULL");
+    *out = nullptr;
+    ISA_TRY(check_params(p));
+    if (max_w < 16 || max_h < 16 || (max_w & 1) || (max_h & 1) || max_n < 2 || max_n > 65)
+        return fail(ISA_EINVAL, "context size %dx%d x %d frames invalid", max_w, max_h, max_n);
+    isa_ctx* c = new isa_ctx();
+    c->max_w = max_w; c->max_h = max_h; c->max_n = max_n; c->p = *p;
+    // worst case pairs over strategies for max_n frames
+    c->max_rows = 0;
+    for (int n = 2; n <= max_n; n++) {
+        int bn = p->tracking_block_size >= n ? n - 1 : p->tracking_block_size;
+        c->max_rows = std::max(c->max_rows, shift_count(n, p->tracking_strategy, bn));
+    }
+    c->max_pairs = c->max_rows;
+    for (int i = 0; i < p->level_count; i++) {
+        int tcx, tcy;
+        if (level_tiles(p->levels[i], max_w, max_h, &tcx, &tcy) != ISA_OK) { delete c; return fail(ISA_EINVAL, "level %d has no tiles", i); }
+        c->maxcx = std::max(c->maxcx, tcx);
+        c->maxcy = std::max(c->maxcy, tcy);
+    }
+    c->max_tiles = c->maxcx * c->maxcy;
+    isa_accum_geom g;
+    float thr;
+    accum_geom(p, max_w, max_h, g, thr);
+    c->max_wo = g.Wo; c->max_ho = g.Ho;
+    // carve one arena
+    const size_t A = 256, fsz = (size_t)max_w * max_h;
+    std::vector<std::pair<void**, size_t>> plan;
+    auto add = [&](void** ptr, size_t bytes) { plan.push_back({ptr, align_up(std::max<size_t>(bytes, 1), A)}); };
+    add((void**)&c->raw_stage, fsz * max_n * 2);
+    add((void**)&c->bw_track, fsz * max_n * 4);
+    add((void**)&c->bw_acc, fsz * max_n * 4);
+    add((void**)&c->tmp, fsz * 3 * 4);
+    for (int i = 0; i < p->level_count; i++) {
+        int L = p->levels[i].resize_level;
+        if (L > 1) add((void**)&c->pyr[i], (size_t)(max_w / L) * (max_h / L) * max_n * 4);
+    }
+    add((void**)&c->spec, (size_t)(max_w / 2 + 1) * max_h * 8);
+    size_t gbytes = (size_t)c->maxcx * c->maxcy * sizeof(float2) * c->max_rows;
+    add((void**)&c->grids, gbytes);
+    add((void**)&c->grids_tmp, gbytes);
+    add((void**)&c->x, (size_t)c->max_tiles * (max_n - 1) * sizeof(float2));
+    add((void**)&c->tiles_opt, (size_t)c->max_tiles * sizeof(float2));
+    add((void**)&c->status, (size_t)c->max_tiles * sizeof(int));
+    add((void**)&c->row_a, c->max_rows * sizeof(int));
+    add((void**)&c->row_b, c->max_rows * sizeof(int));
+    add((void**)&c->row_sign, c->max_rows * sizeof(int));
+    add((void**)&c->row_grid, c->max_rows * sizeof(int));
+    add((void**)&c->N0, (size_t)(max_n - 1) * (max_n - 1) * sizeof(double));
+    add((void**)&c->pair_desc, (size_t)c->max_pairs * ISA_MAX_LEVELS * sizeof(isa_pair_desc));
+    add((void**)&c->frame_tab, (size_t)max_n * ISA_MAX_LEVELS * sizeof(float*));
+    add((void**)&c->flows, fsz * max_n * sizeof(float2));
+    add((void**)&c->flow_tmp, fsz * sizeof(float2));
+    add((void**)&c->half_ref, fsz / 4 * 12);
+    add((void**)&c->half_mov, fsz / 4 * 12);
+    add((void**)&c->masks, fsz / 4 * 16 * max_n);
+    add((void**)&c->st3, fsz * 12);
+    add((void**)&c->kparam, fsz * 16);
+    add((void**)&c->acc, (size_t)c->max_wo * c->max_ho * 12);
+    add((void**)&c->wsum, (size_t)c->max_wo * c->max_ho * 12);
+    add((void**)&c->out_stage, (size_t)c->max_wo * c->max_ho * 12);
+    add((void**)&c->frame_in, (size_t)max_n * sizeof(isa_frame_in));
+    size_t total = 0;
+    for (auto& e : plan) total += e.second;
+    if (cudaMalloc(&c->arena, total) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return fail(ISA_ENOMEM, "device arena of %.2f GB", total / 1e9);
+    }
+    c->arena_bytes = total;
+    size_t off = 0;
+    for (auto& e : plan) { *e.first = (char*)c->arena + off; off += e.second; }
+    for (int i = 0; i < 8; i++)
+        if (cudaEventCreate(&c->ev[i]) != cudaSuccess) { isa_ctx_destroy(c); return fail(ISA_ECUDA, "cudaEventCreate failed"); }
+    int r = ensure_plans(c, max_w, max_h);
+    if (r != ISA_OK) { isa_ctx_destroy(c); return r; }
+    *out = c;
+    return ISA_OK;
+}
+
+int isa_ctx_destroy(isa_ctx* c)
+{
+    if (!c) return ISA_OK;
+    if (c->r2c) cufftDestroy(c->r2c);
+    if (c->c2r) cufftDestroy(c->c2r);
+    if (c->fft_work) cudaFree(c->fft_work);
+    for (int i = 0; i < 8; i++)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->arena) cudaFree(c->arena);
+    delete c;
+    return ISA_OK;
+}
+
+int isa_stage_times(isa_ctx* c, float* ms, int max_count)
+{
+    if (!c || !ms) return fail(ISA_EINVAL, "NULL argument");
+    if (c->ev_count < 2) return 0;
+    ISA_CK(cudaEventSynchronize(c->ev[c->ev_count - 1]));
+    int k = 0;
+    for (int i = 1; i < c->ev_count && k < max_count; i++, k++) ISA_CK(cudaEventElapsedTime(&ms[k], c->ev[i - 1], c->ev[i]));
+    return k;
+}
+
+int isa_merge_burst(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                    const isa_prealign* pre, float* out, size_t out_pitch, void* stream)
+{
+    if (!c) return fail(ISA_EINVAL, "ctx is NULL");
+    return run_merge(c, raw, raw_pitch, frame_stride, n, info, pre, out, out_pitch, S(stream));
+}
+
+int isa_merge_burst_host(isa_ctx* c, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre, float* host_out,
+                         void* stream)
+{
+    if (!c || !host_raw || !host_out) return fail(ISA_EINVAL, "NULL argument");
+    ISA_TRY(check_info(info));
+    const int W = info->width, H = info->height;
+    if (W > c->max_w || H > c->max_h || n < 2 || n > c->max_n) return fail(ISA_EINVAL, "burst exceeds the context");
+    isa_accum_geom g;
+    float thr;
+    accum_geom(&c->p, W, H, g, thr);
+    cudaStream_t st = S(stream);
+    const size_t fb = (size_t)W * H * 2;
+    ISA_CK(cudaMemcpyAsync(c->raw_stage, host_raw, fb * n, cudaMemcpyHostToDevice, st));
+    ISA_TRY(run_merge(c, c->raw_stage, (size_t)W * 2, fb, n, info, pre, c->out_stage, (size_t)g.Wo * 12, st));
+    ISA_CK(cudaMemcpyAsync(host_out, c->out_stage, (size_t)g.Wo * g.Ho * 12, cudaMemcpyDeviceToHost, st));
+    return ISA_OK;
+}
+
+int isa_debug_buffers(isa_ctx* c, int frame, const void** flow, size_t* flow_pitch, const void** mask, size_t* mask_pitch, const void** kparam,
+                      size_t* kparam_pitch, const void** bw_track, const void** bw_acc, size_t* bw_pitch_out, const void** acc,
+                      const void** wsum, size_t* acc_pitch)
+{
+    if (!c || c->last_n == 0) return fail(ISA_EINVAL, "no merge has run on this context");
+    if (frame < 0 || frame >= c->last_n) return fail(ISA_EINVAL, "frame %d out of range", frame);
+    const int W = c->last_w, H = c->last_h;
+    const size_t fsz = (size_t)W * H;
+    isa_accum_geom g;
+    float thr;
+    accum_geom(&c->p, W, H, g, thr);
+    if (flow) *flow = c->flows + frame * fsz;
+    if (flow_pitch) *flow_pitch = (size_t)W * 8;
+    if (mask) *mask = c->masks + (size_t)frame * (W / 2) * (H / 2);
+    if (mask_pitch) *mask_pitch = (size_t)(W / 2) * 16;
+    if (kparam) *kparam = c->kparam;
+    if (kparam_pitch) *kparam_pitch = (size_t)W * 16;
+    if (bw_track) *bw_track = c->bw_track + frame * fsz;
+    if (bw_acc) *bw_acc = c->bw_acc + frame * fsz;
+    if (bw_pitch_out) *bw_pitch_out = (size_t)W * 4;
+    if (acc) *acc = c->acc;
+    if (wsum) *wsum = c->wsum;
+    if (acc_pitch) *acc_pitch = (size_t)g.Wo * 12;
+    return ISA_OK;
+}
+
+int isa_debug_shifts(isa_ctx* c, const void** one_to_one, int* tx, int* ty)
+{
+    if (!c || c->last_n == 0) return fail(ISA_EINVAL, "no merge has run on this context");
+    if (one_to_one) *one_to_one = c->x;
+    if (tx) *tx = c->last_tcx0;
+    if (ty) *ty = c->last_tcy0;
+    return ISA_OK;
+}
+
+// ---- operator API -----------------------------------------------------------
+#define ISA_REQ(cond, msg)                          \
+    do {                                            \
+        if (!(cond)) return fail(ISA_EINVAL, "%s", msg); \
+    } while (0)
+
+int isa_debayer_full(const uint16_t* raw, size_t raw_pitch, int W, int H, const int cfa[4], const float black[3], const float scale[3],
+                     const float divisor[3], float* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(raw && out && cfa && black && scale && divisor, "NULL argument");
+    ISA_REQ(W > 0 && H > 0 && raw_pitch >= (size_t)W * 2 && out_pitch >= (size_t)W * 12, "bad size or pitch");
+    ISA_REQ(cfa_ok(cfa), "bad CFA code");
+    ISA_CK(isa_launch_demosaic_gray(raw, raw_pitch, W, H, pack_cfa(cfa), black, scale, divisor, nullptr, 0, nullptr, 0, out, out_pitch,
+                                    S(stream)));
+    return ISA_OK;
+}
+
+int isa_gamma_srgb(float* img, size_t pitch, int W, int H, void* stream)
+{
+    ISA_REQ(img && W > 0 && H > 0 && pitch >= (size_t)W * 12, "bad argument");
+    ISA_CK(isa_launch_gamma(img, pitch, W, H, S(stream)));
+    return ISA_OK;
+}
+
+int isa_bw_image(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H, const isa_raw_info* info, float sigma, int high_pass,
+                 float* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(c && raw && out && info, "NULL argument");
+    ISA_TRY(check_info(info));
+    ISA_REQ(info->width == W && info->height == H, "info size differs from width/height");
+    ISA_REQ(W <= c->max_w && H <= c->max_h, "frame exceeds the context");
+    ISA_REQ(out_pitch == (size_t)W * 4 && raw_pitch >= (size_t)W * 2, "out pitch must be width * 4");
+    std::vector<float> taps = gauss_taps(sigma), none;
+    return bw_frame(c, raw, raw_pitch, W, H, info, high_pass != 0, out, taps, nullptr, none, S(stream));
+}
+
+int isa_fourier_filter(void* spec, size_t pitch, int W, int H, float lp, float hp, float lps, float hps, int clear_axis, float post_scale,
+                       void* stream)
+{
+    ISA_REQ(spec && W > 1 && H > 0 && pitch >= (size_t)(W / 2 + 1) * 8, "bad argument");
+    ISA_CK(isa_launch_fourier_filter((float2*)spec, pitch, W, H, 1, 0, lp, hp, lps, hps, clear_axis, post_scale, S(stream)));
+    return ISA_OK;
+}
+
+int isa_gauss_filter(const float* in, size_t in_pitch, float* out, size_t out_pitch, float* tmp, size_t tmp_pitch, int W, int H, int C,
+                     float sigma, void* stream)
+{
+    ISA_REQ(in && out && tmp && W > 0 && H > 0 && (C == 1 || C == 3), "bad argument");
+    ISA_REQ(in_pitch >= (size_t)W * C * 4 && out_pitch >= (size_t)W * C * 4 && tmp_pitch >= (size_t)W * C * 4, "pitch too small");
+    std::vector<float> t = gauss_taps(sigma);
+    ISA_CK(isa_launch_gauss(in, in_pitch, out, out_pitch, tmp, tmp_pitch, W, H, C, t.data(), (int)t.size(), 0, S(stream)));
+    return ISA_OK;
+}
+
+int isa_resize_box(const float* in, size_t in_pitch, int W, int H, int level, float* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(in && out && level >= 1 && W >= level && H >= level, "bad argument");
+    ISA_REQ(in_pitch >= (size_t)W * 4 && out_pitch >= (size_t)(W / level) * 4, "pitch too small");
+    ISA_CK(isa_launch_resize_box(in, in_pitch, W, H, level, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_track_level(const float* const* frames, size_t frame_pitch, int W, int H, int T, int Smax, int tcx, int tcy, const isa_track_pair* pairs,
+                    int npairs, void* grids, size_t grid_pitch, size_t grid_stride, float threshold, float* scores, int* argmin, void* stream)
+{
+    ISA_REQ(frames && pairs && grids && npairs > 0, "NULL argument");
+    ISA_REQ(tcx > 0 && tcy > 0 && (W - 2 * Smax) / T >= tcx && (H - 2 * Smax) / T >= tcy, "tile counts exceed the frame");
+    ISA_REQ(grid_pitch >= (size_t)tcx * 8 && grid_stride >= grid_pitch * tcy, "grid pitch/stride too small");
+    static_assert(sizeof(isa_track_pair) == sizeof(isa_pair_desc), "pair layout");
+    cudaError_t e = isa_launch_track(frames, frame_pitch, W, H, T, Smax, tcx, tcy, (const isa_pair_desc*)pairs, npairs, (float2*)grids, grid_pitch,
+                                     grid_stride, threshold, scores, argmin, S(stream));
+    if (e == cudaErrorInvalidValue) return fail(ISA_EINVAL, "tile size %d / max shift %d not supported", T, Smax);
+    ISA_CK(e);
+    return ISA_OK;
+}
+
+int isa_upsample_shifts(const void* in, size_t in_pitch, size_t in_stride, void* out, size_t out_pitch, size_t out_stride, int ngrids, int oldLevel,
+                        int newLevel, int ocx, int ocy, int ncx, int ncy, int oT, int nT, void* stream)
+{
+    ISA_REQ(in && out && in != out && ngrids > 0 && ocx > 0 && ocy > 0 && ncx > 0 && ncy > 0 && newLevel > 0 && nT > 0, "bad argument");
+    ISA_CK(isa_launch_upsample((const float2*)in, in_pitch, in_stride, (float2*)out, out_pitch, out_stride, ngrids, oldLevel, newLevel, ocx, ocy, ncx,
+                               ncy, oT, nT, S(stream)));
+    return ISA_OK;
+}
+
+int isa_solve_shifts(isa_ctx* c, int n, int ref, int strategy, int block, void* grids, size_t grid_pitch, size_t grid_stride, int tcx, int tcy,
+                     void* x, int* status, void* stream)
+{
+    ISA_REQ(c && grids && x && status && tcx > 0 && tcy > 0, "bad argument");
+    ISA_REQ(n >= 2 && n <= c->max_n && ref >= 0 && ref < n, "frame count or reference out of range");
+    Strategy s;
+    ISA_REQ(build_strategy(n, ref, strategy, block, s), "inconsistent tracking strategy");
+    ISA_REQ(s.m <= c->max_rows, "too many pairs for the context");
+    ISA_TRY(upload_strategy(c, s, S(stream)));
+    cudaError_t e = isa_launch_solve(c->row_a, c->row_b, c->row_sign, c->N0, s.m, s.n1, (float2*)grids, grid_pitch, grid_stride, c->row_grid, tcx, tcy,
+                                     (float2*)x, status, S(stream));
+    if (e == cudaErrorInvalidValue) return fail(ISA_EINVAL, "solver shared memory exceeds the limit (m=%d, n-1=%d)", s.m, s.n1);
+    ISA_CK(e);
+    return ISA_OK;
+}
+
+int isa_optimal_shifts(const void* x, int n, int tcx, int tcy, int ref, int trk, void* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(x && out && n >= 2 && tcx > 0 && tcy > 0 && ref >= 0 && ref < n && trk >= 0 && trk < n, "bad argument");
+    ISA_CK(isa_launch_optimal((const float2*)x, n - 1, tcx, tcy, ref, trk, (float2*)out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_flow_from_tiles(const void* tiles, size_t tile_pitch, int tcx, int tcy, int W, int H, const float base[2], float rot, void* flow,
+                        size_t flow_pitch, void* stream)
+{
+    ISA_REQ(tiles && flow && base && tcx > 0 && tcy > 0 && W > 0 && H > 0, "bad argument");
+    ISA_CK(isa_launch_flow_from_tiles((const float2*)tiles, tile_pitch, tcx, tcy, W, H, base[0], base[1], rot, (float2*)flow, flow_pitch,
+                                      S(stream)));
+    return ISA_OK;
+}
+
+int isa_warp(const float* img, size_t img_pitch, int W, int H, const void* flow, size_t flow_pitch, float* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(img && flow && out && W > 0 && H > 0, "bad argument");
+    ISA_CK(isa_launch_warp(img, img_pitch, W, H, (const float2*)flow, flow_pitch, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_derivatives(const float* src, const float* tgt, size_t pitch, int W, int H, float* ix, float* iy, float* it, size_t out_pitch, void* stream)
+{
+    ISA_REQ(src && tgt && ix && iy && it && W > 0 && H > 0, "bad argument");
+    ISA_CK(isa_launch_derivatives(src, tgt, pitch, W, H, ix, iy, it, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_derivatives2(const float* img, size_t pitch, int W, int H, float* ix, float* iy, size_t out_pitch, void* stream)
+{
+    ISA_REQ(img && ix && iy && W > 0 && H > 0, "bad argument");
+    ISA_CK(isa_launch_derivatives2(img, pitch, W, H, ix, iy, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_lucas_kanade(void* flow, size_t flow_pitch, const float* ix, const float* iy, const float* it, size_t pitch, int W, int H, float min_det,
+                     int window, void* stream)
+{
+    ISA_REQ(flow && ix && iy && it && W > 0 && H > 0 && window >= 1, "bad argument");
+    ISA_CK(isa_launch_lk_sums((float2*)flow, flow_pitch, ix, iy, it, pitch, W, H, window / 2, min_det, S(stream)));
+    return ISA_OK;
+}
+
+int isa_lk_iteration(const void* flow_in, void* flow_out, size_t flow_pitch, const float* src, const float* ref, size_t img_pitch, int W, int H,
+                     float min_det, int window, void* stream)
+{
+    ISA_REQ(flow_in && flow_out && flow_in != flow_out && src && ref && W > 0 && H > 0, "bad argument");
+    ISA_REQ(window >= 1 && window / 2 <= 15, "window size out of range");
+    ISA_CK(isa_launch_lk_iteration((const float2*)flow_in, (float2*)flow_out, flow_pitch, src, ref, img_pitch, W, H, window / 2, min_det,
+                                   S(stream)));
+    return ISA_OK;
+}
+
+int isa_lk_refine(const float* src, const float* ref, size_t img_pitch, int W, int H, const void* tiles, size_t tile_pitch, int tcx, int tcy,
+                  const float base[2], float rot, int iterations, float min_det, int window, void* flow, void* flow_scratch, size_t flow_pitch,
+                  void* stream)
+{
+    ISA_REQ(src && ref && tiles && base && flow && flow_scratch && flow != flow_scratch && iterations >= 0, "bad argument");
+    ISA_REQ(window >= 1 && window / 2 <= 15, "window size out of range");
+    float2* a = (iterations & 1) ? (float2*)flow_scratch : (float2*)flow;
+    float2* b = (iterations & 1) ? (float2*)flow : (float2*)flow_scratch;
+    ISA_CK(isa_launch_flow_from_tiles((const float2*)tiles, tile_pitch, tcx, tcy, W, H, base[0], base[1], rot, a, flow_pitch, S(stream)));
+    for (int i = 0; i < iterations; i++) {
+        ISA_CK(isa_launch_lk_iteration(a, b, flow_pitch, src, ref, img_pitch, W, H, window / 2, min_det, S(stream)));
+        std::swap(a, b);
+    }
+    return ISA_OK;
+}
+
+int isa_debayer_subsample(const uint16_t* raw, size_t raw_pitch, int W, int H, const int cfa[4], float max_value, float* out, size_t out_pitch,
+                          void* stream)
+{
+    ISA_REQ(raw && out && cfa && W >= 2 && H >= 2 && cfa_ok(cfa) && max_value != 0.f, "bad argument");
+    ISA_CK(isa_launch_subsample(raw, raw_pitch, W, H, pack_cfa(cfa), max_value, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_robustness_mask(const float* ref3, const float* mov3, size_t img_pitch, void* mask, size_t mask_pitch, int Wh, int Hh, const void* flow,
+                        size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s, float t, void* stream)
+{
+    ISA_REQ(ref3 && mov3 && mask && flow && Wh >= 3 && Hh >= 3 && Wf > 0 && Hf > 0, "bad argument");
+    ISA_CK(isa_launch_robustness(ref3, mov3, img_pitch, (float4*)mask, mask_pitch, Wh, Hh, (const float2*)flow, flow_pitch, Wf, Hf, alpha, beta,
+                                 thr_m, s, t, S(stream)));
+    return ISA_OK;
+}
+
+int isa_erode(const void* in, size_t in_pitch, void* out, size_t out_pitch, int W, int H, int size, void* stream)
+{
+    ISA_REQ(in && out && in != out && W > 0 && H > 0 && size >= 1, "bad argument");
+    ISA_CK(isa_launch_erode((const float4*)in, in_pitch, (float4*)out, out_pitch, W, H, size, S(stream)));
+    return ISA_OK;
+}
+
+int isa_robustness_erode(const float* ref3, const float* mov3, size_t img_pitch, int Wh, int Hh, const void* flow, size_t flow_pitch, int Wf, int Hf,
+                         float alpha, float beta, float thr_m, float s, float t, int erode_size, void* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(ref3 && mov3 && flow && out && Wh >= 3 && Hh >= 3 && erode_size >= 1 && erode_size / 2 <= 4, "bad argument");
+    ISA_CK(isa_launch_robustness_erode(ref3, mov3, img_pitch, Wh, Hh, (const float2*)flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, erode_size,
+                                       (float4*)out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_structure_tensor(const float* img, size_t pitch, int W, int H, float* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(img && out && W > 0 && H > 0 && out_pitch >= (size_t)W * 12, "bad argument");
+    ISA_CK(isa_launch_structure_tensor(img, pitch, W, H, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_kernel_param(const float* st3, size_t st_pitch, int W, int H, float* out, size_t out_pitch, int oc, float dth, float dtr, float kd, float kn,
+                     float ks, float kh, void* stream)
+{
+    ISA_REQ(st3 && out && W > 0 && H > 0 && (oc == 3 || oc == 4), "bad argument");
+    ISA_REQ(oc == 3 || (const void*)st3 != (const void*)out, "4-channel output cannot alias the tensor");
+    ISA_CK(isa_launch_kernel_param(st3, st_pitch, W, H, out, out_pitch, oc, dth, dtr, kd, kn, ks, kh, S(stream)));
+    return ISA_OK;
+}
+
+int isa_accumulate(const uint16_t* raw, size_t raw_pitch, int W, int H, const int cfa[4], float* acc, float* wsum, size_t out_pitch, int Wo, int Ho,
+                   const void* mask, size_t mask_pitch, const float* kparam, size_t kparam_pitch, int kc, const void* flow, size_t flow_pitch,
+                   const float white[3], const float black[3], float scale, int ox, int oy, const int crop[4], void* stream)
+{
+    ISA_REQ(raw && acc && wsum && kparam && cfa && white && black && crop, "NULL argument");
+    ISA_REQ(W >= 2 && H >= 2 && !(W & 1) && !(H & 1) && Wo > 0 && Ho > 0 && (kc == 3 || kc == 4) && scale > 0, "bad size");
+    ISA_REQ(crop[0] >= 0 && crop[1] >= 0 && crop[2] < W && crop[3] < H && crop[0] <= crop[2] && crop[1] <= crop[3], "crop outside the frame");
+    ISA_REQ(cfa_ok(cfa), "bad CFA code");
+    isa_accum_geom g;
+    g.W = W; g.H = H; g.Wo = Wo; g.Ho = Ho; g.s = scale; g.ox = ox; g.oy = oy;
+    g.cx0 = crop[0]; g.cy0 = crop[1]; g.cx1 = crop[2]; g.cy1 = crop[3];
+    float r = std::round(scale);
+    g.s_int = (r == scale && r >= 1.f) ? (int)r : 0;
+    isa_frame_in f{raw, (const float2*)flow, (const float4*)mask};
+    ISA_CK(isa_launch_accumulate(g, pack_cfa(cfa), nullptr, 1, &f, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, kc, white, black, acc,
+                                 wsum, out_pitch, 1, S(stream)));
+    return ISA_OK;
+}
+
+int isa_apply_weighting(float* img, const float* acc, const float* wsum, size_t pitch, int W, int H, float thr, void* stream)
+{
+    ISA_REQ(img && acc && wsum && W > 0 && H > 0 && pitch >= (size_t)W * 12, "bad argument");
+    ISA_CK(isa_launch_apply_weighting(img, pitch, acc, wsum, pitch, W, H, thr, S(stream)));
+    return ISA_OK;
+}
+
+}  // extern "C"
+

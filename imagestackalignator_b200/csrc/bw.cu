@@ -1,0 +1,275 @@
+// Tracking-image preparation and demosaic kernels.
+//
+// k_demosaic_gray fuses, for one output tile, what the reference runs as
+// NPP Convert + Set(0) + deBayerGreenKernel + deBayerRedBlueKernel + NPP Div
+// (ImageStackAlignatorController.cs:1268-1311, DeBayerKernels.cu:55-231)
+// and, for tracking images, GammasRGB (kernel.cu:290-332) + NPP ColorToGray
+// (controller :2404-2408). The raw tile with a 3-pixel halo is staged in
+// shared memory as linear values, the green plane is built over a 1-pixel
+// halo, then red/blue by colour differences.
+#include "isa_internal.cuh"
+
+namespace {
+
+constexpr int DM_TX = 32, DM_TY = 16;       // output tile
+constexpr int DM_LW = DM_TX + 6, DM_LH = DM_TY + 6;  // linear tile (halo 3)
+constexpr int DM_GW = DM_TX + 2, DM_GH = DM_TY + 2;  // green tile (halo 1)
+
+struct Color3 { float v[3]; };
+
+__device__ __forceinline__ float srgb_gamma(float v) {
+    return v <= 0.0031308f ? 12.92f * v : (1.0f + 0.055f) * powf(v, 1.0f / 2.4f) - 0.055f;
+}
+
+__global__ void __launch_bounds__(256) k_demosaic_gray(const uint16_t* __restrict__ raw, size_t raw_pitch, int W, int H, unsigned cfa,
+                                                      Color3 black, Color3 scale, Color3 divisor, Color3 gw, int gamma_gray,
+                                                      float* __restrict__ gray, size_t gray_pitch, float* __restrict__ rgb,
+                                                      size_t rgb_pitch)
+{
+    __shared__ float lin[DM_LH][DM_LW];
+    __shared__ float grn[DM_GH][DM_GW];
+    const int x0 = blockIdx.x * DM_TX, y0 = blockIdx.y * DM_TY;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (int i = tid; i < DM_LW * DM_LH; i += nt) {
+        int ly = i / DM_LW, lx = i - ly * DM_LW;
+        int gx = x0 + lx - 3, gy = y0 + ly - 3;
+        float v = 0.f;
+        if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+            int c = isa::cfa_at(cfa, gx, gy);
+            float r = (float)isa::row_ptr(raw, raw_pitch, gy)[gx];
+            v = (r - black.v[c]) * scale.v[c];
+        }
+        lin[ly][lx] = v;
+    }
+    __syncthreads();
+    for (int i = tid; i < DM_GW * DM_GH; i += nt) {
+        int ly = i / DM_GW, lx = i - ly * DM_GW;
+        int gx = x0 + lx - 1, gy = y0 + ly - 1;
+        float g = 0.f;
+        if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2) {
+            int c = isa::cfa_at(cfa, gx, gy);
+            int cx = lx + 2, cy = ly + 2;  // position in lin
+            if (c == 1) {
+                g = lin[cy][cx];
+            } else if (c == 0 || c == 2) {
+                float p = lin[cy][cx];
+                float xm2 = lin[cy][cx - 2], xm1 = lin[cy][cx - 1], xp1 = lin[cy][cx + 1], xp2 = lin[cy][cx + 2];
+                float ym2 = lin[cy - 2][cx], ym1 = lin[cy - 1][cx], yp1 = lin[cy + 1][cx], yp2 = lin[cy + 2][cx];
+                float gradX = 0.5f * fabsf(xp1 - xm1), gradY = 0.5f * fabsf(yp1 - ym1);
+                float lapX = 0.25f * fabsf(2.0f * p - xm2 - xp2), lapY = 0.25f * fabsf(2.0f * p - ym2 - yp2);
+                float ipX = 0.125f * (-xm2 + 4.0f * xm1 + 2.0f * p + 4.0f * xp1 - xp2);
+                float ipY = 0.125f * (-ym2 + 4.0f * ym1 + 2.0f * p + 4.0f * yp1 - yp2);
+                float w = (gradY + lapY) / (gradX + gradY + lapX + lapY + 0.000000001f);
+                g = w * ipX + (1.0f - w) * ipY;
+            }
+        }
+        grn[ly][lx] = g;
+    }
+    __syncthreads();
+    for (int i = tid; i < DM_TX * DM_TY; i += nt) {
+        int ly = i / DM_TX, lx = i - ly * DM_TX;
+        int gx = x0 + lx, gy = y0 + ly;
+        if (gx >= W || gy >= H) continue;
+        float r = 0.f, g = 0.f, b = 0.f;
+        if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2) {
+            int c = isa::cfa_at(cfa, gx, gy);
+            int nx = isa::cfa_at(cfa, gx + 1, gy);
+            int cx = lx + 3, cy = ly + 3;      // lin
+            int kx = lx + 1, ky = ly + 1;      // grn
+            g = grn[ky][kx];
+            if (c == 1) {
+                float hsum = (lin[cy][cx - 1] - grn[ky][kx - 1]) + (lin[cy][cx + 1] - grn[ky][kx + 1]);
+                float vsum = (lin[cy - 1][cx] - grn[ky - 1][kx]) + (lin[cy + 1][cx] - grn[ky + 1][kx]);
+                float h = g + 0.5f * hsum, v = g + 0.5f * vsum;
+                if (nx == 0) { r = h; b = v; } else { b = h; r = v; }
+            } else if (c == 0 || c == 2) {
+                float own = lin[cy][cx];
+                float other = g + 0.25f * ((lin[cy - 1][cx - 1] - grn[ky - 1][kx - 1]) + (lin[cy - 1][cx + 1] - grn[ky - 1][kx + 1]) +
+                                           (lin[cy + 1][cx + 1] - grn[ky + 1][kx + 1]) + (lin[cy + 1][cx - 1] - grn[ky + 1][kx - 1]));
+                if (c == 0) { r = own; b = other; } else { b = own; r = other; }
+            }
+        }
+        r /= divisor.v[0]; g /= divisor.v[1]; b /= divisor.v[2];
+        if (rgb) {
+            float* o = isa::row_ptr(rgb, rgb_pitch, gy) + 3 * gx;
+            o[0] = r; o[1] = g; o[2] = b;
+        }
+        if (gray) {
+            if (gamma_gray) {
+                r = isnan(r) ? 0.f : r; g = isnan(g) ? 0.f : g; b = isnan(b) ? 0.f : b;
+                r = srgb_gamma(fmaxf(fminf(r, 1.0f), 0.0f));
+                g = srgb_gamma(fmaxf(fminf(g, 1.0f), 0.0f));
+                b = srgb_gamma(fmaxf(fminf(b, 1.0f), 0.0f));
+            }
+            isa::row_ptr(gray, gray_pitch, gy)[gx] = gw.v[0] * r + gw.v[1] * g + gw.v[2] * b;
+        }
+    }
+}
+
+// GammasRGB (kernel.cu:303-332) on an RGB image.
+__global__ void k_gamma(float* rgb, size_t pitch, int W, int H)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    float* p = isa::row_ptr(rgb, pitch, y) + 3 * x;
+    for (int c = 0; c < 3; c++) {
+        float v = p[c];
+        if (isnan(v)) v = 0.f;
+        p[c] = srgb_gamma(fmaxf(fminf(v, 1.0f), 0.0f));
+    }
+}
+
+// fourierFilter (kernel.cu:704-779) on a batch of half spectra; post_scale
+// folds in the 1/(W*H) of the inverse transform (PreAlignment.cs:277).
+__global__ void k_fourier_filter(float2* spec, size_t pitch, size_t batch_stride, int W, int H, float lp, float hp, float lps, float hps,
+                                 int clear_axis, float post_scale)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W / 2 + 1 || y >= H) return;
+    float mx = (float)x, my = (float)y;
+    if (my > H * 0.5f) my = (H - my) * -1.0f;
+    mx /= W;
+    my /= H;
+    float dist = sqrtf(mx * mx + my * my);
+    float fil = 0;
+    lp = lp - lps;
+    hp = hp + hps;
+    if (lp > 0) { if (dist <= lp) fil = 1; }
+    else { if (dist <= 1.0f) fil = 1; }
+    if (lps > 0) {
+        float f2 = (-fil + 1.0f) * expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
+        if (f2 > 0.001f) fil = f2;
+    }
+    if (lps > 0 && lp == 0 && hp == 0 && hps == 0) fil = expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
+    if (hp > 0) {
+        float f2 = dist >= hp ? 1.0f : 0.0f;
+        fil *= f2;
+        if (hps > 0) {
+            float f3 = (-f2 + 1.0f) * expf(-((dist - hp) * (dist - hp) / (2 * hps * hps)));
+            if (f3 > 0.001f) fil = f3;
+        }
+    }
+    if (x < clear_axis || fabsf(my) * H < clear_axis) fil = 0;
+    fil *= post_scale;
+    float2* p = (float2*)((char*)spec + blockIdx.z * batch_stride + (size_t)y * pitch) + x;
+    float2 v = *p;
+    v.x *= fil;
+    v.y *= fil;
+    *p = v;
+}
+
+struct Taps { float t[100]; int n; };
+
+// One pass of NPP FilterGaussBorder (separable, replicate border).
+template <bool VERT>
+__global__ void k_gauss_pass(const float* __restrict__ in, size_t in_pitch, float* __restrict__ out, size_t out_pitch, int W, int H, int C,
+                             Taps taps, int clamp_in)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W * C || y >= H) return;
+    int px = x / C, c = x - px * C;
+    int c0 = taps.n / 2;
+    float s = 0.f;
+    for (int k = 0; k < taps.n; k++) {
+        int sx = VERT ? px : isa::clampi(px + k - c0, 0, W - 1);
+        int sy = VERT ? isa::clampi(y + k - c0, 0, H - 1) : y;
+        float v = isa::row_ptr(in, in_pitch, sy)[sx * C + c];
+        if (clamp_in) v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+        s += taps.t[k] * v;
+    }
+    isa::row_ptr(out, out_pitch, y)[x] = s;
+}
+
+// NPP ResizeSqrPixel super-sampling by an integer factor: block mean.
+__global__ void k_resize_box(const float* __restrict__ in, size_t in_pitch, int L, float* __restrict__ out, size_t out_pitch, int Wo, int Ho)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wo || y >= Ho) return;
+    float s = 0.f;
+    for (int j = 0; j < L; j++) {
+        const float* r = isa::row_ptr(in, in_pitch, y * L + j) + x * L;
+        for (int i = 0; i < L; i++) s += r[i];
+    }
+    isa::row_ptr(out, out_pitch, y)[x] = s / (float)(L * L);
+}
+
+// deBayersSubSample3 (DeBayerKernels.cu:244-283).
+__global__ void k_subsample(const uint16_t* __restrict__ raw, size_t raw_pitch, int Wh, int Hh, unsigned cfa, float max_val,
+                            float* __restrict__ out, size_t out_pitch)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wh || y >= Hh) return;
+    float f = 1.0f / max_val;
+    float p[3] = {0.f, 0.f, 0.f};
+    for (int ix = 0; ix < 2; ix++)
+        for (int iy = 0; iy < 2; iy++) {
+            int c = isa::cfa_at(cfa, ix, iy);
+            float v = (float)isa::row_ptr(raw, raw_pitch, 2 * y + iy)[2 * x + ix];
+            if (c == 1) p[1] += v * f * 0.5f;
+            else if (c == 0) p[0] = v * f;
+            else if (c == 2) p[2] = v * f;
+        }
+    float* o = isa::row_ptr(out, out_pitch, y) + 3 * x;
+    o[0] = p[0]; o[1] = p[1]; o[2] = p[2];
+}
+
+inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+
+}  // namespace
+
+cudaError_t isa_launch_demosaic_gray(const uint16_t* raw, size_t raw_pitch, int W, int H, unsigned cfa, const float* black,
+                                     const float* scale, const float* divisor, const float* gray_w, int gamma_gray,
+                                     float* gray, size_t gray_pitch, float* rgb, size_t rgb_pitch, cudaStream_t st)
+{
+    Color3 b, s, d, g;
+    for (int c = 0; c < 3; c++) { b.v[c] = black[c]; s.v[c] = scale[c]; d.v[c] = divisor[c]; g.v[c] = gray_w ? gray_w[c] : 0.f; }
+    dim3 blk(32, 8), grd((W + DM_TX - 1) / DM_TX, (H + DM_TY - 1) / DM_TY);
+    k_demosaic_gray<<<grd, blk, 0, st>>>(raw, raw_pitch, W, H, cfa, b, s, d, g, gamma_gray, gray, gray_pitch, rgb, rgb_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_gamma(float* rgb, size_t pitch, int W, int H, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_gamma<<<grid2(W, H, b), b, 0, st>>>(rgb, pitch, W, H);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_fourier_filter(float2* spec, size_t pitch, int W, int H, int batch, size_t batch_stride, float lp, float hp,
+                                      float lps, float hps, int clear_axis, float post_scale, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    dim3 g = grid2(W / 2 + 1, H, b);
+    g.z = batch;
+    k_fourier_filter<<<g, b, 0, st>>>(spec, pitch, batch_stride, W, H, lp, hp, lps, hps, clear_axis, post_scale);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_gauss(const float* in, size_t in_pitch, float* out, size_t out_pitch, float* tmp, size_t tmp_pitch, int W, int H,
+                             int C, const float* taps, int ntaps, int clamp01_input, cudaStream_t st)
+{
+    if (ntaps < 1 || ntaps > 99) return cudaErrorInvalidValue;
+    Taps t;
+    t.n = ntaps;
+    for (int i = 0; i < ntaps; i++) t.t[i] = taps[i];
+    dim3 b(64, 4);
+    k_gauss_pass<false><<<grid2(W * C, H, b), b, 0, st>>>(in, in_pitch, tmp, tmp_pitch, W, H, C, t, clamp01_input);
+    k_gauss_pass<true><<<grid2(W * C, H, b), b, 0, st>>>(tmp, tmp_pitch, out, out_pitch, W, H, C, t, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_resize_box(const float* in, size_t in_pitch, int W, int H, int L, float* out, size_t out_pitch, cudaStream_t st)
+{
+    int Wo = W / L, Ho = H / L;
+    dim3 b(32, 8);
+    k_resize_box<<<grid2(Wo, Ho, b), b, 0, st>>>(in, in_pitch, L, out, out_pitch, Wo, Ho);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_subsample(const uint16_t* raw, size_t raw_pitch, int W, int H, unsigned cfa, float max_val, float* out,
+                                 size_t out_pitch, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_subsample<<<grid2(W / 2, H / 2, b), b, 0, st>>>(raw, raw_pitch, W / 2, H / 2, cfa, max_val, out, out_pitch);
+    return cudaGetLastError();
+}

@@ -1,0 +1,119 @@
+// Shared device helpers and launch declarations of the burst-merge library.
+// Layouts follow the reference's NPP images: row-major, pitch in bytes,
+// channels interleaved (float2 flow, float3 RGB, float4 masks/kernels).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#define ISA_DEV __device__ __forceinline__
+
+namespace isa {
+
+// ---- pitched access ------------------------------------------------------
+template <class T>
+ISA_DEV T* row_ptr(T* base, size_t pitch, int y) { return (T*)((char*)base + (size_t)y * pitch); }
+template <class T>
+ISA_DEV const T* row_ptr(const T* base, size_t pitch, int y) { return (const T*)((const char*)base + (size_t)y * pitch); }
+
+ISA_DEV int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Mirror addressing of a CUDA texture: reflect the texel index with the
+// edge texel repeated (period 2n).
+ISA_DEV int mirror(int i, int n) {
+    if (i >= 0 && i < n) return i;
+    int p = 2 * n;
+    int j = i % p;
+    if (j < 0) j += p;
+    return j >= n ? p - 1 - j : j;
+}
+
+// CFA code at (x, y): cfa packed as 4 x 2 bits, (y&1)*2 + (x&1) selects.
+ISA_DEV int cfa_at(unsigned cfa, int x, int y) { return (cfa >> ((((y & 1) << 1) | (x & 1)) * 2)) & 3; }
+
+}  // namespace isa
+
+// ---- launchers implemented in the .cu files (host side) -------------------
+struct isa_pair_desc {
+    int ref, trk;          // frame indices
+    int grid;              // index of this pair's shift grid
+    float base_ref_x, base_ref_y, rot_ref;
+    float base_trk_x, base_trk_y, rot_trk;
+};
+
+// bw.cu
+cudaError_t isa_launch_demosaic_gray(const uint16_t* raw, size_t raw_pitch, int W, int H, unsigned cfa, const float* black,
+                                     const float* scale, const float* divisor, const float* gray_w, int gamma_gray,
+                                     float* gray, size_t gray_pitch, float* rgb, size_t rgb_pitch, cudaStream_t st);
+cudaError_t isa_launch_gamma(float* rgb, size_t pitch, int W, int H, cudaStream_t st);
+cudaError_t isa_launch_fourier_filter(float2* spec, size_t pitch, int W, int H, int batch, size_t batch_stride, float lp, float hp,
+                                      float lps, float hps, int clear_axis, float post_scale, cudaStream_t st);
+cudaError_t isa_launch_gauss(const float* in, size_t in_pitch, float* out, size_t out_pitch, float* tmp, size_t tmp_pitch, int W,
+                             int H, int C, const float* taps, int ntaps, int clamp01_input, cudaStream_t st);
+cudaError_t isa_launch_resize_box(const float* in, size_t in_pitch, int W, int H, int L, float* out, size_t out_pitch,
+                                  cudaStream_t st);
+cudaError_t isa_launch_subsample(const uint16_t* raw, size_t raw_pitch, int W, int H, unsigned cfa, float max_val, float* out,
+                                 size_t out_pitch, cudaStream_t st);
+
+// track.cu
+cudaError_t isa_launch_track(const float* const* frames, size_t img_pitch, int Wl, int Hl, int T, int S, int tcx, int tcy,
+                             const isa_pair_desc* pairs, int npairs, float2* grids, size_t grid_pitch, size_t grid_stride,
+                             float threshold, float* scores, int* argmin, cudaStream_t st);
+cudaError_t isa_launch_upsample(const float2* in, size_t in_pitch, size_t in_stride, float2* out, size_t out_pitch,
+                                size_t out_stride, int ngrids, int oldLevel, int newLevel, int ocx, int ocy, int ncx, int ncy,
+                                int oldT, int newT, cudaStream_t st);
+size_t isa_solve_smem(int m, int n1);
+cudaError_t isa_launch_solve(const int* row_a, const int* row_b, const int* row_sign, const double* N0, int m, int n1,
+                             float2* grids, size_t grid_pitch, size_t grid_stride, const int* row_grid, int tcx, int tcy,
+                             float2* x_out, int* status, cudaStream_t st);
+cudaError_t isa_launch_optimal(const float2* x, int n1, int tcx, int tcy, int ref, int trk, float2* out, size_t out_pitch,
+                               cudaStream_t st);
+
+// flow.cu
+cudaError_t isa_launch_flow_from_tiles(const float2* tiles, size_t tile_pitch, int tcx, int tcy, int W, int H, float bx, float by,
+                                       float rot, float2* flow, size_t flow_pitch, cudaStream_t st);
+cudaError_t isa_launch_warp(const float* img, size_t img_pitch, int W, int H, const float2* flow, size_t flow_pitch, float* out,
+                            size_t out_pitch, cudaStream_t st);
+cudaError_t isa_launch_derivatives(const float* src, const float* tgt, size_t pitch, int W, int H, float* ix, float* iy, float* it,
+                                   size_t out_pitch, cudaStream_t st);
+cudaError_t isa_launch_derivatives2(const float* img, size_t pitch, int W, int H, float* ix, float* iy, size_t out_pitch,
+                                    cudaStream_t st);
+cudaError_t isa_launch_lk_sums(float2* flow, size_t flow_pitch, const float* ix, const float* iy, const float* it, size_t pitch, int W,
+                               int H, int half, float min_det, cudaStream_t st);
+cudaError_t isa_launch_lk_iteration(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref,
+                                    size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st);
+
+// robust.cu
+cudaError_t isa_launch_robustness(const float* ref3, const float* mov3, size_t img_pitch, float4* mask, size_t mask_pitch, int Wh,
+                                  int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
+                                  float thr_m, float s, float t, cudaStream_t st);
+cudaError_t isa_launch_erode(const float4* in, size_t in_pitch, float4* out, size_t out_pitch, int W, int H, int size,
+                             cudaStream_t st);
+cudaError_t isa_launch_robustness_erode(const float* ref3, const float* mov3, size_t img_pitch, int Wh, int Hh, const float2* flow,
+                                        size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s, float t, int size,
+                                        float4* out, size_t out_pitch, cudaStream_t st);
+
+// merge.cu
+struct isa_accum_geom {
+    int W, H;          // input frame
+    int Wo, Ho;        // output grid
+    float s;           // merge scale
+    int s_int;         // s when it is a positive integer, else 0
+    int ox, oy;        // output-grid origin
+    int cx0, cy0, cx1, cy1;  // inclusive source crop
+};
+struct isa_frame_in {
+    const uint16_t* raw;
+    const float2* flow;   // nullptr: zero flow
+    const float4* mask;   // nullptr: certainty 1
+};
+cudaError_t isa_launch_structure_tensor(const float* img, size_t pitch, int W, int H, float* st3, size_t st_pitch, cudaStream_t st);
+cudaError_t isa_launch_kernel_param(const float* st3, size_t st_pitch, int W, int H, float* out, size_t out_pitch, int out_channels,
+                                    float Dth, float Dtr, float kDetail, float kDenoise, float kStretch, float kShrink,
+                                    cudaStream_t st);
+cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const isa_frame_in* frames, int nframes,
+                                  const isa_frame_in* single, size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch,
+                                  int kparam_channels, const float* white, const float* black, float* acc, float* wsum,
+                                  size_t out_pitch, int accumulate_into, cudaStream_t st);
+cudaError_t isa_launch_apply_weighting(float* img, size_t img_pitch, const float* acc, const float* wsum, size_t pitch, int W, int H,
+                                       float thr, cudaStream_t st);

@@ -1,0 +1,257 @@
+// Kernel parameters (structure tensor -> anisotropic kernel, kernel.cu:601-700),
+// kernel-weighted Bayer accumulation (accumulateImages / accumulateImagesSuperRes,
+// DeBayerKernels.cu:290-468) generalised to a merge scale s, and the final
+// normalisation (ApplyWeighting, kernel.cu:336-391).
+//
+// Accumulation geometry: output pixel (x, y) samples the kernel parameters
+// (clamp) and the flow (mirror) bilinearly at input position
+// ((x + 0.5 + ox) / s, (y + 0.5 + oy) / s); the shift is round(s * flow);
+// tap (px, py) reads the raw sample floor((x + px + sx + ox) / s) clamped to
+// the crop, the certainty of the unshifted tap's half-resolution pixel and
+// adds to the channel of the sample's CFA colour. s = 1 / origin 0 / whole
+// frame is accumulateImages; s = 2 / origin (W/2, H/2) / central crop is
+// accumulateImagesSuperRes.
+//
+// k_accumulate takes a list of frames and keeps the running sums in
+// registers: with one frame and accumulate_into = 1 it is the reference's
+// per-frame read-modify-write pass; with all frames it reads each frame's
+// inputs once and writes the sums once. The 25 tap weights depend only on
+// the kernel parameters, so they are computed once per output pixel.
+#include "isa_internal.cuh"
+
+namespace {
+
+__global__ void k_structure_tensor(const float* __restrict__ img, size_t pitch, int W, int H, float* __restrict__ st3, size_t st_pitch)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    auto at = [&](int xx, int yy) { return __ldg(isa::row_ptr(img, pitch, isa::mirror(yy, H)) + isa::mirror(xx, W)); };
+    // ComputeDerivatives2Kernel (opticalFlow.cu:151-185) then ComputeStructureTensor (kernel.cu:601-625)
+    float dx = (at(x + 2, y) - at(x + 1, y) * 8.0f + at(x - 1, y) * 8.0f - at(x - 2, y)) / 12.0f;
+    float dy = (at(x, y + 2) - at(x, y + 1) * 8.0f + at(x, y - 1) * 8.0f - at(x, y - 2)) / 12.0f;
+    float* o = isa::row_ptr(st3, st_pitch, y) + 3 * x;
+    o[0] = dx * dx;
+    o[1] = dy * dy;
+    o[2] = dx * dy;
+}
+
+// ComputeKernelParam (kernel.cu:628-700) evaluated in FP64: the FP32 form
+// loses the determinant to cancellation where the kernel is strongly
+// anisotropic. Output channels 0..2 = (b22, b11, -b12) / det; a 4th channel,
+// when present, is 0 (the reference's float4 copy, controller :1865-1876).
+__global__ void k_kernel_param(const float* __restrict__ st3, size_t st_pitch, int W, int H, float* __restrict__ out, size_t out_pitch, int oc,
+                               float Dth, float Dtr, float kDetail, float kDenoise, float kStretch, float kShrink)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float* g = isa::row_ptr(st3, st_pitch, y) + 3 * x;
+    double a11 = g[0], a22 = g[1], a12 = g[2];
+    double hlp = sqrt((a22 - a11) * (a22 - a11) + 4.0 * a12 * a12);
+    double c = 2.0 * a12, s = a22 - a11 + hlp;
+    double nrm = sqrt(c * c + s * s);
+    if (nrm > 0) { c /= nrm; s /= nrm; } else { c = 1; s = 0; }
+    double l1 = (a11 + a22 + hlp) / 2.0, l2 = (a11 + a22 - hlp) / 2.0;
+    double A = 1 + sqrt((l1 - l2) * (l1 - l2) / ((l1 + l2) * (l1 + l2)));
+    double D = 1 - sqrt(l1) / (double)Dtr + (double)Dth;
+    D = fmax(fmin(1.0, D), 0.0);
+    double kd = kDetail;
+    double k1 = (1.0 - D) * (kd * (double)kStretch * A) + D * kd * (double)kDenoise;
+    double k2 = (1.0 - D) * (kd / (double)kShrink * A) + D * kd * (double)kDenoise;
+    k1 *= k1;
+    k2 *= k2;
+    double x2 = c, y2 = s, x1 = s, y1 = -c;
+    double b11 = k1 * x1 * x1 + x2 * x2 * k2;
+    double b12 = k1 * x1 * y1 + x2 * y2 * k2;
+    double b22 = k1 * y1 * y1 + y2 * y2 * k2;
+    double det = b11 * b22 - b12 * b12 + (double)0.0000000001f;
+    float* o = isa::row_ptr(out, out_pitch, y) + oc * x;
+    o[0] = (float)(b22 / det);
+    o[1] = (float)(b11 / det);
+    o[2] = (float)(-b12 / det);
+    if (oc == 4) o[3] = 0.f;
+}
+
+struct F3 { float v[3]; };
+
+__device__ __forceinline__ int floor_div_s(int v, const isa_accum_geom& g)
+{
+    if (g.s_int == 1) return v;
+    if (g.s_int == 2) return v >> 1;  // arithmetic shift: floor for negatives
+    if (g.s_int > 0) { int q = v / g.s_int; return (v % g.s_int != 0 && v < 0) ? q - 1 : q; }
+    return (int)floorf((float)v / g.s);
+}
+
+template <int KC>
+__device__ __forceinline__ void kparam_sample(const float* kp, size_t pitch, int W, int H, float xb, float yb, float k[3])
+{
+    float fx = floorf(xb), fy = floorf(yb);
+    int i = (int)fx, j = (int)fy;
+    float a = xb - fx, b = yb - fy;
+    if (a == 0.f && b == 0.f) {  // exact texel (s = 1)
+        const float* p = isa::row_ptr(kp, pitch, isa::clampi(j, 0, H - 1)) + KC * isa::clampi(i, 0, W - 1);
+        k[0] = __ldg(p); k[1] = __ldg(p + 1); k[2] = __ldg(p + 2);
+        return;
+    }
+    int i0 = isa::clampi(i, 0, W - 1), i1 = isa::clampi(i + 1, 0, W - 1), j0 = isa::clampi(j, 0, H - 1), j1 = isa::clampi(j + 1, 0, H - 1);
+    const float* r0 = isa::row_ptr(kp, pitch, j0);
+    const float* r1 = isa::row_ptr(kp, pitch, j1);
+    float w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        k[c] = w00 * __ldg(r0 + KC * i0 + c) + w10 * __ldg(r0 + KC * i1 + c) + w01 * __ldg(r1 + KC * i0 + c) + w11 * __ldg(r1 + KC * i1 + c);
+}
+
+__device__ __forceinline__ float2 flow_sample(const float2* fl, size_t pitch, int W, int H, float xb, float yb)
+{
+    float fx = floorf(xb), fy = floorf(yb);
+    int i = (int)fx, j = (int)fy;
+    float a = xb - fx, b = yb - fy;
+    if (a == 0.f && b == 0.f) return __ldg(isa::row_ptr(fl, pitch, isa::mirror(j, H)) + isa::mirror(i, W));
+    int i0 = isa::mirror(i, W), i1 = isa::mirror(i + 1, W), j0 = isa::mirror(j, H), j1 = isa::mirror(j + 1, H);
+    const float2* r0 = isa::row_ptr(fl, pitch, j0);
+    const float2* r1 = isa::row_ptr(fl, pitch, j1);
+    float2 p00 = __ldg(r0 + i0), p10 = __ldg(r0 + i1), p01 = __ldg(r1 + i0), p11 = __ldg(r1 + i1);
+    float w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+    return make_float2(w00 * p00.x + w10 * p10.x + w01 * p01.x + w11 * p11.x, w00 * p00.y + w10 * p10.y + w01 * p01.y + w11 * p11.y);
+}
+
+template <int KC>
+__global__ void __launch_bounds__(256) k_accumulate(isa_accum_geom g, unsigned cfa, const isa_frame_in* __restrict__ frames, int nframes,
+                                                   isa_frame_in single, size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* __restrict__ kparam,
+                                                   size_t kp_pitch, F3 white, F3 black, float* __restrict__ acc, float* __restrict__ wsum,
+                                                   size_t out_pitch, int accumulate_into)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= g.Wo || y >= g.Ho) return;
+    float* ap = isa::row_ptr(acc, out_pitch, y) + 3 * x;
+    float* wp = isa::row_ptr(wsum, out_pitch, y) + 3 * x;
+    if (x < 1 || y < 1 || x >= g.Wo - 1 || y >= g.Ho - 1) {
+        if (!accumulate_into) { ap[0] = ap[1] = ap[2] = 0.f; wp[0] = wp[1] = wp[2] = 0.f; }
+        return;
+    }
+    float a[3] = {0.f, 0.f, 0.f}, w[3] = {0.f, 0.f, 0.f};
+    if (accumulate_into) {
+        a[0] = ap[0]; a[1] = ap[1]; a[2] = ap[2];
+        w[0] = wp[0]; w[1] = wp[1]; w[2] = wp[2];
+    }
+    const float xb = ((float)x + 0.5f + (float)g.ox) / g.s - 0.5f;
+    const float yb = ((float)y + 0.5f + (float)g.oy) / g.s - 0.5f;
+    float k[3];
+    kparam_sample<KC>(kparam, kp_pitch, g.W, g.H, xb, yb, k);
+    float wt[25];
+#pragma unroll
+    for (int py = -2; py <= 2; py++)
+#pragma unroll
+        for (int px = -2; px <= 2; px++) {
+            float q = px * px * k[0] + 2 * px * py * k[2] + py * py * k[1];
+            float v = expf(-0.5f * q);
+            if (!isfinite(v)) v = px * py == 0 ? 1.f : 0.f;
+            wt[(py + 2) * 5 + px + 2] = v;
+        }
+    // unshifted taps (mask rows/columns) do not depend on the frame
+    int ux[5], uy[5];
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+        ux[d] = isa::clampi(floor_div_s(x + d - 2 + g.ox, g), g.cx0, g.cx1) >> 1;
+        uy[d] = isa::clampi(floor_div_s(y + d - 2 + g.oy, g), g.cy0, g.cy1) >> 1;
+    }
+    for (int f = 0; f < nframes; f++) {
+        const isa_frame_in fr = frames ? frames[f] : single;
+        int sx = 0, sy = 0;
+        if (fr.flow) {
+            float2 fl = flow_sample(fr.flow, flow_pitch, g.W, g.H, xb, yb);
+            sx = (int)roundf(fl.x * g.s);
+            sy = (int)roundf(fl.y * g.s);
+        }
+#pragma unroll
+        for (int py = 0; py < 5; py++) {
+            const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
+            const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
+            const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
+#pragma unroll
+            for (int px = 0; px < 5; px++) {
+                const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
+                const int c = isa::cfa_at(cfa, qx, qy);
+                if (c > 2) continue;
+                float raw = (float)__ldg(rr + qx);
+                raw = (raw - black.v[c]) / white.v[c];
+                float cert = 1.f;
+                if (mr) {
+                    float4 m = __ldg(mr + ux[px]);
+                    cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
+                    if (!isfinite(cert)) cert = 0.f;
+                }
+                const float ww = wt[py * 5 + px];
+                a[c] += raw * ww * cert;
+                w[c] += ww * cert;
+            }
+        }
+    }
+    ap[0] = a[0]; ap[1] = a[1]; ap[2] = a[2];
+    wp[0] = w[0]; wp[1] = w[1]; wp[2] = w[2];
+}
+
+__global__ void k_apply_weighting(float* img, size_t img_pitch, const float* __restrict__ acc, const float* __restrict__ wsum, size_t pitch,
+                                  int W, int H, float thr)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    float* o = isa::row_ptr(img, img_pitch, y) + 3 * x;
+    const float* a = isa::row_ptr(acc, pitch, y) + 3 * x;
+    const float* w = isa::row_ptr(wsum, pitch, y) + 3 * x;
+    for (int c = 0; c < 3; c++) {
+        float v = a[c], ww = w[c];
+        if (ww < thr) { v += o[c]; ww += 1; }
+        o[c] = ww != 0 ? v / ww : 0.f;
+    }
+}
+
+inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+
+}  // namespace
+
+cudaError_t isa_launch_structure_tensor(const float* img, size_t pitch, int W, int H, float* st3, size_t st_pitch, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_structure_tensor<<<grid2(W, H, b), b, 0, st>>>(img, pitch, W, H, st3, st_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_kernel_param(const float* st3, size_t st_pitch, int W, int H, float* out, size_t out_pitch, int out_channels, float Dth,
+                                    float Dtr, float kDetail, float kDenoise, float kStretch, float kShrink, cudaStream_t st)
+{
+    if (out_channels != 3 && out_channels != 4) return cudaErrorInvalidValue;
+    dim3 b(32, 8);
+    k_kernel_param<<<grid2(W, H, b), b, 0, st>>>(st3, st_pitch, W, H, out, out_pitch, out_channels, Dth, Dtr, kDetail, kDenoise, kStretch,
+                                                 kShrink);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const isa_frame_in* frames, int nframes, const isa_frame_in* single,
+                                  size_t raw_pitch,
+                                  size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch, int kparam_channels,
+                                  const float* white, const float* black, float* acc, float* wsum, size_t out_pitch, int accumulate_into,
+                                  cudaStream_t st)
+{
+    F3 wh, bl;
+    for (int c = 0; c < 3; c++) { wh.v[c] = white[c]; bl.v[c] = black[c]; }
+    isa_frame_in one = single ? *single : isa_frame_in{nullptr, nullptr, nullptr};
+    dim3 b(32, 8), grd = grid2(g.Wo, g.Ho, b);
+    if (kparam_channels == 4)
+        k_accumulate<4><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc, wsum,
+                                           out_pitch, accumulate_into);
+    else if (kparam_channels == 3)
+        k_accumulate<3><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc, wsum,
+                                           out_pitch, accumulate_into);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_apply_weighting(float* img, size_t img_pitch, const float* acc, const float* wsum, size_t pitch, int W, int H, float thr,
+                                       cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_apply_weighting<<<grid2(W, H, b), b, 0, st>>>(img, img_pitch, acc, wsum, pitch, W, H, thr);
+    return cudaGetLastError();
+}

@@ -1,0 +1,168 @@
+// Robustness mask (ComputeRobustnessMask, RobustnessModell.cu:29-157) and its
+// 5x5 erosion (NPP ErodeBorder, ImageStackAlignatorController.cs:1976).
+//
+// The flow is read as the reference's linear/mirror texture does at a
+// half-resolution pixel's normalized position: for a full-resolution flow
+// this is the mean of the 2x2 block under the half-res pixel. The running
+// max/min of the reference compares each of the 25 taps with the centre
+// only (RobustnessModell.cu:52-60), so M depends on the centre and the
+// (+2, +2) tap alone; that is what is evaluated here, with identical result.
+#include "isa_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ float2 flow_sample(const float2* flow, size_t pitch, int Wf, int Hf, int Wh, int Hh, int qx, int qy)
+{
+    float xb = ((float)qx + 0.5f) / (float)Wh * Wf - 0.5f, yb = ((float)qy + 0.5f) / (float)Hh * Hf - 0.5f;
+    float fx = floorf(xb), fy = floorf(yb);
+    int i = (int)fx, j = (int)fy;
+    float a = xb - fx, b = yb - fy;
+    int i0 = isa::mirror(i, Wf), i1 = isa::mirror(i + 1, Wf), j0 = isa::mirror(j, Hf), j1 = isa::mirror(j + 1, Hf);
+    const float2* r0 = isa::row_ptr(flow, pitch, j0);
+    const float2* r1 = isa::row_ptr(flow, pitch, j1);
+    float2 p00 = __ldg(r0 + i0), p10 = __ldg(r0 + i1), p01 = __ldg(r1 + i0), p11 = __ldg(r1 + i1);
+    float2 o;
+    o.x = (1.f - a) * (1.f - b) * p00.x + a * (1.f - b) * p10.x + (1.f - a) * b * p01.x + a * b * p11.x;
+    o.y = (1.f - a) * (1.f - b) * p00.y + a * (1.f - b) * p10.y + (1.f - a) * b * p01.y + a * b * p11.y;
+    return o;
+}
+
+// Mask value of interior half-res pixel (x, y); ref/mov are float3 images.
+__device__ float4 mask_at(const float* __restrict__ ref3, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                          const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m,
+                          float s_lit, float t_lit, int x, int y)
+{
+    float2 sf = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x, y);
+    float2 sl = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x + 2, y + 2);
+    float mxx = fmaxf(sl.x, sf.x), mxy = fmaxf(sl.y, sf.y);
+    float mnx = fminf(sl.x, sf.x), mny = fminf(sl.y, sf.y);
+    int shx = (int)roundf(sf.x * 0.5f), shy = (int)roundf(sf.y * 0.5f);
+    float mr[3] = {0.f, 0.f, 0.f}, mm[3] = {0.f, 0.f, 0.f}, pr[9][3];
+    for (int j = -1; j <= 1; j++)
+        for (int i = -1; i <= 1; i++) {
+            const float* p = isa::row_ptr(ref3, img_pitch, y + j) + 3 * (x + i);
+            int qy = isa::clampi(y + shy + j, 0, Hh - 1), qx = isa::clampi(x + shx + i, 0, Wh - 1);
+            const float* q = isa::row_ptr(mov3, img_pitch, qy) + 3 * qx;
+            int k = (j + 1) * 3 + i + 1;
+            for (int c = 0; c < 3; c++) {
+                pr[k][c] = __ldg(p + c);
+                mr[c] += pr[k][c];
+                mm[c] += __ldg(q + c);
+            }
+        }
+    for (int c = 0; c < 3; c++) { mr[c] /= 9.0f; mm[c] /= 9.0f; }
+    float md = fabsf(mr[0] - mm[0]) + fabsf(mr[1] - mm[1]) + fabsf(mr[2] - mm[2]);
+    md /= 3.0f;
+    mxx *= 0.5f * md; mxy *= 0.5f * md; mnx *= 0.5f * md; mny *= 0.5f * md;
+    float M = sqrtf((mxx - mnx) * (mxx - mnx) + (mxy - mny) * (mxy - mny));
+    float sd[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < 9; k++)
+        for (int c = 0; c < 3; c++) sd[c] += (pr[k][c] - mr[c]) * (pr[k][c] - mr[c]);
+    float sgain = M > thr_m ? 0.f : s_lit;
+    float out[3];
+    for (int c = 0; c < 3; c++) {
+        float sr = sqrtf(sd[c] / 9.0f);
+        float smd = sqrtf(alpha * mr[c] + beta);
+        if (c == 1) smd /= sqrtf(2.0f);
+        float dist = fabsf(mr[c] - mm[c]);
+        float sig = fmaxf(smd, sr);
+        dist = dist * (sr * sr / (sr * sr + smd * smd));
+        out[c] = fmaxf(fminf(sgain * expf(-dist * dist / (sig * sig)) - t_lit, 1.0f), 0.0f);
+    }
+    return make_float4(out[0], out[1], out[2], M);
+}
+
+__global__ void k_robustness(const float* __restrict__ ref3, const float* __restrict__ mov3, size_t img_pitch, float4* __restrict__ mask,
+                             size_t mask_pitch, int Wh, int Hh, const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf,
+                             float alpha, float beta, float thr_m, float s, float t)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wh - 1 || y >= Hh - 1 || x < 1 || y < 1) return;
+    isa::row_ptr(mask, mask_pitch, y)[x] =
+        mask_at(ref3, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, x, y);
+}
+
+__global__ void k_erode(const float4* __restrict__ in, size_t in_pitch, float4* __restrict__ out, size_t out_pitch, int W, int H, int size)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    int a = size / 2;
+    float4 m = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+    for (int j = 0; j < size; j++) {
+        const float4* r = isa::row_ptr(in, in_pitch, isa::clampi(y + j - a, 0, H - 1));
+        for (int i = 0; i < size; i++) {
+            float4 v = __ldg(r + isa::clampi(x + i - a, 0, W - 1));
+            m.x = fminf(m.x, v.x); m.y = fminf(m.y, v.y); m.z = fminf(m.z, v.z); m.w = fminf(m.w, v.w);
+        }
+    }
+    isa::row_ptr(out, out_pitch, y)[x] = m;
+}
+
+// Fused mask + erosion for one frame: the mask over the output tile plus an
+// (erode/2) halo is computed into shared memory (border pixels keep the
+// reference's initial value 1, controller :1891), then the min filter with
+// replicate border is taken. ref3 / mov3: half-res RGB of deBayersSubSample3.
+constexpr int RB_TX = 32, RB_TY = 8, RB_MAXA = 4;
+
+__global__ void __launch_bounds__(256) k_robustness_erode(const float* __restrict__ ref3, const float* __restrict__ mov3, size_t img_pitch,
+                                                         int Wh, int Hh, const float2* __restrict__ flow, size_t flow_pitch, int Wf,
+                                                         int Hf, float alpha, float beta, float thr_m, float s, float t, int size,
+                                                         float4* __restrict__ out, size_t out_pitch)
+{
+    __shared__ float4 sm[(RB_TY + 2 * RB_MAXA) * (RB_TX + 2 * RB_MAXA)];
+    const int a = size / 2;
+    const int SW = RB_TX + 2 * a, SH = RB_TY + 2 * a;
+    const int x0 = blockIdx.x * RB_TX, y0 = blockIdx.y * RB_TY;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (int i = tid; i < SW * SH; i += nt) {
+        int sy = i / SW, sx = i - sy * SW;
+        int qx = isa::clampi(x0 + sx - a, 0, Wh - 1), qy = isa::clampi(y0 + sy - a, 0, Hh - 1);
+        float4 v = make_float4(1.f, 1.f, 1.f, 1.f);
+        if (qx >= 1 && qx < Wh - 1 && qy >= 1 && qy < Hh - 1)
+            v = mask_at(ref3, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, qx, qy);
+        sm[i] = v;
+    }
+    __syncthreads();
+    int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= Wh || y >= Hh) return;
+    float4 m = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+    for (int j = 0; j < size; j++)
+        for (int i = 0; i < size; i++) {
+            float4 v = sm[(threadIdx.y + j) * SW + threadIdx.x + i];
+            m.x = fminf(m.x, v.x); m.y = fminf(m.y, v.y); m.z = fminf(m.z, v.z); m.w = fminf(m.w, v.w);
+        }
+    isa::row_ptr(out, out_pitch, y)[x] = m;
+}
+
+inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+
+}  // namespace
+
+cudaError_t isa_launch_robustness(const float* ref3, const float* mov3, size_t img_pitch, float4* mask, size_t mask_pitch, int Wh, int Hh,
+                                  const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s,
+                                  float t, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_robustness<<<grid2(Wh, Hh, b), b, 0, st>>>(ref3, mov3, img_pitch, mask, mask_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta,
+                                                 thr_m, s, t);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_erode(const float4* in, size_t in_pitch, float4* out, size_t out_pitch, int W, int H, int size, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_erode<<<grid2(W, H, b), b, 0, st>>>(in, in_pitch, out, out_pitch, W, H, size);
+    return cudaGetLastError();
+}
+
+// Fused mask + erosion from half-res RGB images.
+cudaError_t isa_launch_robustness_erode(const float* ref3, const float* mov3, size_t img_pitch, int Wh, int Hh, const float2* flow,
+                                        size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s, float t, int size,
+                                        float4* out, size_t out_pitch, cudaStream_t st)
+{
+    if (size < 1 || size / 2 > RB_MAXA) return cudaErrorInvalidValue;
+    dim3 b(RB_TX, RB_TY);
+    k_robustness_erode<<<grid2(Wh, Hh, b), b, 0, st>>>(ref3, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size,
+                                                       out, out_pitch);
+    return cudaGetLastError();
+}

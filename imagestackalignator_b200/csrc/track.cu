@@ -1,0 +1,391 @@
+// Pyramid tile alignment (PatchTracker.Track, PEFStudioDX/PatchTracker.cs:317-360)
+// and the multi-pair least-squares solve (ShiftCollection.MinimizeCUBLAS,
+// PEFStudioDX/ShiftCollection.cs:738-822).
+//
+// k_track: one CTA per (frame pair, tile). The reference template tile (T x T,
+// kernel.cu:175-228) and the search block (B x B, B = T + 2S, kernel.cu:234-288)
+// are staged in shared memory; the L2 map D(s) = sum (r - t(s))^2 for
+// s in [-S, S]^2 is computed directly (the reference's FFT cross-correlation,
+// squaredSum and box filters, kernel.cu:29-171, compute the same quantity as
+// sum r^2 + sum t^2 - 2 CC). Each thread owns one (template row, shift row)
+// item and keeps both rows in registers, producing 2S+1 partial sums; the
+// partials are reduced over rows in a fixed order (deterministic). Thread 0
+// then does findMinimum (kernel.cu:422-546) and preShift += result (:355-358).
+#include "isa_internal.cuh"
+#include <float.h>
+
+namespace {
+
+__constant__ float c_fit[5][9] = {
+    {0.25f, -0.5f, 0.25f, 0.5f, -1.0f, 0.5f, 0.25f, -0.5f, 0.25f},       // d2/dx2
+    {0.25f, 0.5f, 0.25f, -0.5f, -1.0f, -0.5f, 0.25f, 0.5f, 0.25f},       // d2/dy2
+    {0.25f, 0.f, -0.25f, 0.f, 0.f, 0.f, -0.25f, 0.f, 0.25f},             // d2/dxdy
+    {-0.125f, 0.f, 0.125f, -0.25f, 0.f, 0.25f, -0.125f, 0.f, 0.125f},   // d/dx
+    {-0.125f, -0.25f, -0.125f, 0.f, 0.f, 0.f, 0.125f, 0.25f, 0.125f}};  // d/dy
+
+__device__ __forceinline__ void tile_offset(int tx, int ty, int T, int Wl, int Hl, float bx, float by, float rot, float addx, float addy,
+                                            int& ox, int& oy)
+{
+    float sf = sinf(rot), cf = cosf(rot);
+    float sx = addx, sy = addy;
+    sx += cf * -bx - sf * -by;
+    sy += sf * -bx + cf * -by;
+    float pcx = (float)(tx * T + T / 2 - Wl / 2), pcy = (float)(ty * T + T / 2 - Hl / 2);
+    sx += cf * pcx - sf * pcy - pcx;
+    sy += sf * pcx + cf * pcy - pcy;
+    ox = (int)roundf(sx);
+    oy = (int)roundf(sy);
+}
+
+template <int T, int S>
+__global__ void __launch_bounds__(256) k_track(const float* const* __restrict__ frames, size_t pitch, int Wl, int Hl, int tcx, int tcy,
+                                             const isa_pair_desc* __restrict__ pairs, float2* __restrict__ grids, size_t grid_pitch,
+                                             size_t grid_stride, float threshold, float* __restrict__ scores, int* __restrict__ argmin_out)
+{
+    constexpr int B = T + 2 * S, D = 2 * S + 1;
+    constexpr int TP = T + 1, BP = B + 1;  // odd strides: conflict-free row reads across lanes
+    __shared__ float tpl[T * TP];
+    __shared__ float blk[B * BP];
+    __shared__ float part[D * T * D];
+    __shared__ float map[D * D];
+    const int p = blockIdx.x;
+    const int tile = blockIdx.y;
+    const int ty = tile / tcx, tx = tile - ty * tcx;
+    const isa_pair_desc pd = pairs[p];
+    float2* gline = (float2*)((char*)grids + (size_t)pd.grid * grid_stride + (size_t)ty * grid_pitch);
+    const float* imr = frames[pd.ref];
+    const float* imt = frames[pd.trk];
+    int oxr, oyr, oxt, oyt;
+    tile_offset(tx, ty, T, Wl, Hl, pd.base_ref_x, pd.base_ref_y, pd.rot_ref, 0.f, 0.f, oxr, oyr);
+    float2 pre = gline[tx];
+    tile_offset(tx, ty, T, Wl, Hl, pd.base_trk_x, pd.base_trk_y, pd.rot_trk, pre.x, pre.y, oxt, oyt);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < T * T; i += blockDim.x) {
+        int y = i / T, x = i - y * T;
+        int ix = isa::clampi(tx * T + S + x + oxr, 0, Wl - 1), iy = isa::clampi(ty * T + S + y + oyr, 0, Hl - 1);
+        tpl[y * TP + x] = isa::row_ptr(imr, pitch, iy)[ix];
+    }
+    for (int i = tid; i < B * B; i += blockDim.x) {
+        int y = i / B, x = i - y * B;
+        int ix = isa::clampi(tx * T + x + oxt, 0, Wl - 1), iy = isa::clampi(ty * T + y + oyt, 0, Hl - 1);
+        blk[y * BP + x] = isa::row_ptr(imt, pitch, iy)[ix];
+    }
+    __syncthreads();
+    for (int item = tid; item < T * D; item += blockDim.x) {
+        const int y = item % T, sy = item / T;
+        float r[T], t[B], acc[D];
+#pragma unroll
+        for (int x = 0; x < T; x++) r[x] = tpl[y * TP + x];
+#pragma unroll
+        for (int x = 0; x < B; x++) t[x] = blk[(y + sy) * BP + x];
+#pragma unroll
+        for (int k = 0; k < D; k++) acc[k] = 0.f;
+#pragma unroll
+        for (int x = 0; x < T; x++)
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                float d = r[x] - t[x + k];
+                acc[k] = fmaf(d, d, acc[k]);
+            }
+#pragma unroll
+        for (int k = 0; k < D; k++) part[(sy * T + y) * D + k] = acc[k];
+    }
+    __syncthreads();
+    for (int k = tid; k < D * D; k += blockDim.x) {
+        int sy = k / D, sx = k - sy * D;
+        float s = 0.f;
+        for (int y = 0; y < T; y++) s += part[(sy * T + y) * D + sx];
+        map[k] = s;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        float mn = FLT_MAX, mx = -FLT_MAX;
+        int mi = -1;
+        for (int i = 0; i < D * D; i++) {
+            float v = map[i];
+            mx = fmaxf(mx, v);
+            if (v < mn) { mn = v; mi = i; }
+        }
+        size_t tix = (size_t)p * tcx * tcy + tile;
+        if (scores)
+            for (int i = 0; i < D * D; i++) scores[tix * D * D + i] = map[i];
+        if (argmin_out) argmin_out[tix] = mi;
+        float cx = 0.f, cy = 0.f;
+        if (mi >= 0) {
+            int iy = mi / D, ix = mi - iy * D;
+            cy = (float)iy;
+            cx = (float)ix;
+            if (ix < 1 || iy < 1 || ix >= 2 * S || iy >= 2 * S) {
+                cx = 0.f; cy = 0.f;
+            } else {
+                float a11 = 0.f, a22 = 0.f, a12 = 0.f, b1 = 0.f, b2 = 0.f;
+                for (int k = 0; k < 9; k++) {
+                    float v = map[(iy + k / 3 - 1) * D + ix + k % 3 - 1];
+                    a11 += c_fit[0][k] * v; a22 += c_fit[1][k] * v; a12 += c_fit[2][k] * v;
+                    b1 += c_fit[3][k] * v; b2 += c_fit[4][k] * v;
+                }
+                a11 = fmaxf(a11, 0.0f);
+                a22 = fmaxf(a22, 0.0f);
+                float det = a11 * a22 - a12 * a12;
+                if (det < 0) { a12 = 0; det = a11 * a22; }
+                if (det != 0) {
+                    float mux = (a22 * b1 - a12 * b2) / det, muy = (a11 * b2 - a12 * b1) / det;
+                    if (fabsf(mux) > 1) mux = 0;
+                    if (fabsf(muy) > 1) muy = 0;
+                    cx -= mux; cy -= muy;
+                }
+                cx -= S; cy -= S;
+            }
+        }
+        if (threshold + mn > mx) { cx = 0.f; cy = 0.f; }
+        pre.x += cx;
+        pre.y += cy;
+        gline[tx] = pre;
+    }
+}
+
+template <int T, int S>
+cudaError_t launch_track_ts(const float* const* frames, size_t pitch, int Wl, int Hl, int tcx, int tcy, const isa_pair_desc* pairs,
+                            int npairs, float2* grids, size_t grid_pitch, size_t grid_stride, float thr, float* scores, int* argmin,
+                            cudaStream_t st)
+{
+    dim3 g(npairs, tcx * tcy);
+    k_track<T, S><<<g, 256, 0, st>>>(frames, pitch, Wl, Hl, tcx, tcy, pairs, grids, grid_pitch, grid_stride, thr, scores, argmin);
+    return cudaGetLastError();
+}
+
+// UpSampleShifts (kernel.cu:552-598) for a batch of pair grids.
+__global__ void k_upsample(const float2* __restrict__ in, size_t in_pitch, size_t in_stride, float2* __restrict__ out, size_t out_pitch,
+                           size_t out_stride, int oldLevel, int newLevel, int ocx, int ocy, int ncx, int ncy, int oldT, int newT)
+{
+    int nx = blockIdx.x * blockDim.x + threadIdx.x, ny = blockIdx.y * blockDim.y + threadIdx.y;
+    if (nx >= ncx || ny >= ncy) return;
+    const char* ib = (const char*)in + blockIdx.z * in_stride;
+    float factor = (float)oldLevel * oldT / (float)(newLevel * newT);
+    float ox = nx / factor, oy = ny / factor;
+    int x0 = (int)floorf(ox), x1 = (int)ceilf(ox), y0 = (int)floorf(oy), y1 = (int)ceilf(oy);
+    x0 = min(x0, ocx - 1); x1 = min(x1, ocx - 1); y0 = min(y0, ocy - 1); y1 = min(y1, ocy - 1);
+    const float2* r0 = (const float2*)(ib + (size_t)y0 * in_pitch);
+    const float2* r1 = (const float2*)(ib + (size_t)y1 * in_pitch);
+    float2 v00 = r0[x0], v10 = r0[x1], v01 = r1[x0], v11 = r1[x1];
+    float wx = 1.0f - (x1 - ox), wy = 1.0f - (y1 - oy);
+    float t0 = v00.x + (v10.x - v00.x) * wx, t1 = v01.x + (v11.x - v01.x) * wx;
+    float2 o;
+    o.x = t0 + (t1 - t0) * wy;
+    t0 = v00.y + (v10.y - v00.y) * wx;
+    t1 = v01.y + (v11.y - v01.y) * wx;
+    o.y = t0 + (t1 - t0) * wy;
+    o.x *= oldLevel / (float)newLevel;
+    o.y *= oldLevel / (float)newLevel;
+    ((float2*)((char*)out + blockIdx.z * out_stride + (size_t)ny * out_pitch))[nx] = o;
+}
+
+// Per-tile least squares with outlier removal. Rows of the incidence matrix
+// are intervals [a, b) of the one-to-one shifts with a common sign (true for
+// every tracking strategy of ShiftCollection.CreateShiftMatrix), so
+// N = A^T A is updated incrementally when a row is removed, and A x is a
+// difference of prefix sums. Solved in FP64 by Gauss-Jordan on [N | A^T b].
+constexpr int SOLVE_THREADS = 128;
+
+__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const int* __restrict__ row_a, const int* __restrict__ row_b,
+                                                         const int* __restrict__ row_sign, const double* __restrict__ N0, int m, int n1,
+                                                         float2* __restrict__ grids, size_t grid_pitch, size_t grid_stride,
+                                                         const int* __restrict__ row_grid, int tcx, int tcy, float2* __restrict__ x_out,
+                                                         int* __restrict__ status)
+{
+    extern __shared__ double sm[];
+    const int tile = blockIdx.x;
+    const int ty = tile / tcx, tx = tile - ty * tcx;
+    const int na = n1 + 2;
+    double* N = sm;                       // n1 x n1
+    double* aug = N + n1 * n1;            // n1 x (n1 + 2)
+    double* fac = aug + n1 * na;          // n1
+    double* P = fac + n1;                 // (n1 + 1) x 2 prefix sums of x
+    double* xs = P + 2 * (n1 + 1);        // n1 x 2 last solution
+    float* b = (float*)(xs + 2 * n1);     // m x 2 measurements
+    unsigned char* active = (unsigned char*)(b + 2 * m);
+    __shared__ double red_v[SOLVE_THREADS / 32];
+    __shared__ int red_i[SOLVE_THREADS / 32];
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n1 * n1; i += blockDim.x) N[i] = N0[i];
+    for (int k = tid; k < m; k += blockDim.x) {
+        float2 v = ((const float2*)((const char*)grids + (size_t)row_grid[k] * grid_stride + (size_t)ty * grid_pitch))[tx];
+        b[2 * k] = v.x; b[2 * k + 1] = v.y;
+        active[k] = 1;
+    }
+    for (int i = tid; i < 2 * n1; i += blockDim.x) xs[i] = 0.0;
+    __syncthreads();
+    // rhs = A^T b
+    for (int i = tid; i < n1; i += blockDim.x) {
+        double sx = 0, sy = 0;
+        for (int k = 0; k < m; k++)
+            if (row_a[k] <= i && i < row_b[k]) { sx += row_sign[k] * (double)b[2 * k]; sy += row_sign[k] * (double)b[2 * k + 1]; }
+        aug[i * na + n1] = sx; aug[i * na + n1 + 1] = sy;
+    }
+    int st = -1;
+    double scale = 0;
+    for (int i = 0; i < n1; i++) scale = fmax(scale, fabs(N0[i * n1 + i]));
+    const double tol = 1e-12 * (scale > 0 ? scale : 1.0);
+    for (int round_ = 0; round_ < 10; round_++) {
+        __syncthreads();
+        // augmented copy; the rhs columns persist in aug[.][n1..n1+1] across rounds via P? keep separately:
+        for (int i = tid; i < n1 * n1; i += blockDim.x) { int r = i / n1, c = i - r * n1; aug[r * na + c] = N[i]; }
+        __syncthreads();
+        // stash rhs (aug columns are destroyed by elimination)
+        for (int i = tid; i < n1; i += blockDim.x) { P[2 * i] = aug[i * na + n1]; P[2 * i + 1] = aug[i * na + n1 + 1]; }
+        if (tid == 0) s_flag = 0;
+        __syncthreads();
+        for (int c = 0; c < n1; c++) {
+            double piv = aug[c * na + c];
+            if (!(fabs(piv) > tol)) { if (tid == 0) s_flag = 1; break; }
+            __syncthreads();
+            for (int j = tid; j < na; j += blockDim.x) if (j != c) aug[c * na + j] /= piv;
+            __syncthreads();
+            if (tid == 0) aug[c * na + c] = 1.0;
+            for (int r = tid; r < n1; r += blockDim.x) fac[r] = aug[r * na + c];
+            __syncthreads();
+            for (int i = tid; i < n1 * na; i += blockDim.x) {
+                int r = i / na, j = i - r * na;
+                if (r != c) aug[i] -= fac[r] * aug[c * na + j];
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        if (s_flag) {
+            // singular: keep the previous solution, restore rhs and stop
+            for (int i = tid; i < n1; i += blockDim.x) { aug[i * na + n1] = P[2 * i]; aug[i * na + n1 + 1] = P[2 * i + 1]; }
+            st = -3;
+            break;
+        }
+        for (int i = tid; i < n1; i += blockDim.x) { xs[2 * i] = aug[i * na + n1]; xs[2 * i + 1] = aug[i * na + n1 + 1]; }
+        __syncthreads();
+        // restore rhs into aug, build prefix sums of x into fac-adjacent storage (reuse P after copying rhs back)
+        for (int i = tid; i < n1; i += blockDim.x) { aug[i * na + n1] = P[2 * i]; aug[i * na + n1 + 1] = P[2 * i + 1]; }
+        __syncthreads();
+        if (tid == 0) {
+            P[0] = 0; P[1] = 0;
+            for (int i = 0; i < n1; i++) { P[2 * (i + 1)] = P[2 * i] + xs[2 * i]; P[2 * (i + 1) + 1] = P[2 * i + 1] + xs[2 * i + 1]; }
+        }
+        __syncthreads();
+        double best = 1.0;
+        int bi = -1;
+        for (int k = tid; k < m; k += blockDim.x) {
+            if (!active[k]) continue;
+            double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
+            double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
+            double dx = b[2 * k] - px, dy = b[2 * k + 1] - py;
+            double d = dx * dx + dy * dy;
+            if (d > best) { best = d; bi = k; }
+        }
+        // block arg-max, lowest index on ties (the reference scans rows in order)
+        for (int off = 16; off > 0; off >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, best, off);
+            int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) { best = ov; bi = oi; }
+        }
+        if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = red_v[0];
+            int bj = red_i[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+                if (red_i[w] >= 0 && (bj < 0 || red_v[w] > bv || (red_v[w] == bv && red_i[w] < bj))) { bv = red_v[w]; bj = red_i[w]; }
+            red_i[0] = bj;
+        }
+        __syncthreads();
+        const int k = red_i[0];
+        st = k;
+        if (k < 0) break;
+        const int a = row_a[k], e = row_b[k];
+        const double sg = row_sign[k];
+        const double bx = b[2 * k], by = b[2 * k + 1];
+        __syncthreads();
+        for (int i = tid; i < n1 * n1; i += blockDim.x) {
+            int r = i / n1, c = i - r * n1;
+            if (r >= a && r < e && c >= a && c < e) N[i] -= 1.0;
+        }
+        for (int i = tid; i < n1; i += blockDim.x)
+            if (i >= a && i < e) { aug[i * na + n1] -= sg * bx; aug[i * na + n1 + 1] -= sg * by; }
+        if (tid == 0) { b[2 * k] = 0.f; b[2 * k + 1] = 0.f; active[k] = 0; }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        status[tile] = st;
+        P[0] = 0; P[1] = 0;
+        for (int i = 0; i < n1; i++) { P[2 * (i + 1)] = P[2 * i] + xs[2 * i]; P[2 * (i + 1) + 1] = P[2 * i + 1] + xs[2 * i + 1]; }
+    }
+    for (int i = tid; i < n1; i += blockDim.x) x_out[(size_t)tile * n1 + i] = make_float2((float)xs[2 * i], (float)xs[2 * i + 1]);
+    __syncthreads();
+    for (int k = tid; k < m; k += blockDim.x) {
+        double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
+        double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
+        ((float2*)((char*)grids + (size_t)row_grid[k] * grid_stride + (size_t)ty * grid_pitch))[tx] = make_float2((float)px, (float)py);
+    }
+}
+
+// getOptimalShifts (ShiftMinimizerKernels.cu:179-218).
+__global__ void k_optimal(const float2* __restrict__ x, int n1, int tcx, int tcy, int ref, int trk, float2* __restrict__ out, size_t out_pitch)
+{
+    int tx = blockIdx.x * blockDim.x + threadIdx.x, ty = blockIdx.y * blockDim.y + threadIdx.y;
+    if (tx >= tcx || ty >= tcy) return;
+    const float2* r = x + (size_t)(tx + ty * tcx) * n1;
+    float2 s = make_float2(0.f, 0.f);
+    if (ref < trk) for (int i = ref; i < trk; i++) { s.x += r[i].x; s.y += r[i].y; }
+    else if (trk < ref) for (int i = trk; i < ref; i++) { s.x -= r[i].x; s.y -= r[i].y; }
+    ((float2*)((char*)out + (size_t)ty * out_pitch))[tx] = s;
+}
+
+}  // namespace
+
+#define ISA_TRACK_CASE(TT, SS) \
+    if (T == TT && S == SS) return launch_track_ts<TT, SS>(frames, img_pitch, Wl, Hl, tcx, tcy, pairs, npairs, grids, grid_pitch, grid_stride, threshold, scores, argmin, st);
+
+cudaError_t isa_launch_track(const float* const* frames, size_t img_pitch, int Wl, int Hl, int T, int S, int tcx, int tcy,
+                             const isa_pair_desc* pairs, int npairs, float2* grids, size_t grid_pitch, size_t grid_stride, float threshold,
+                             float* scores, int* argmin, cudaStream_t st)
+{
+    if (npairs <= 0 || tcx <= 0 || tcy <= 0) return cudaSuccess;
+    ISA_TRACK_CASE(32, 1) ISA_TRACK_CASE(32, 2) ISA_TRACK_CASE(32, 3) ISA_TRACK_CASE(32, 4)
+    ISA_TRACK_CASE(32, 5) ISA_TRACK_CASE(32, 6)
+    ISA_TRACK_CASE(16, 1) ISA_TRACK_CASE(16, 2) ISA_TRACK_CASE(16, 4) ISA_TRACK_CASE(16, 8)
+    ISA_TRACK_CASE(64, 2)
+    ISA_TRACK_CASE(8, 2) ISA_TRACK_CASE(8, 4)
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t isa_launch_upsample(const float2* in, size_t in_pitch, size_t in_stride, float2* out, size_t out_pitch, size_t out_stride,
+                                int ngrids, int oldLevel, int newLevel, int ocx, int ocy, int ncx, int ncy, int oldT, int newT,
+                                cudaStream_t st)
+{
+    if (ngrids <= 0) return cudaSuccess;
+    dim3 b(16, 16), g((ncx + 15) / 16, (ncy + 15) / 16, ngrids);
+    k_upsample<<<g, b, 0, st>>>(in, in_pitch, in_stride, out, out_pitch, out_stride, oldLevel, newLevel, ocx, ocy, ncx, ncy, oldT, newT);
+    return cudaGetLastError();
+}
+
+size_t isa_solve_smem(int m, int n1)
+{
+    size_t d = (size_t)n1 * n1 + (size_t)n1 * (n1 + 2) + n1 + 2 * (n1 + 1) + 2 * n1;
+    return d * sizeof(double) + (size_t)2 * m * sizeof(float) + m + 16;
+}
+
+cudaError_t isa_launch_solve(const int* row_a, const int* row_b, const int* row_sign, const double* N0, int m, int n1, float2* grids,
+                             size_t grid_pitch, size_t grid_stride, const int* row_grid, int tcx, int tcy, float2* x_out, int* status,
+                             cudaStream_t st)
+{
+    size_t smem = isa_solve_smem(m, n1);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_solve<<<tcx * tcy, SOLVE_THREADS, smem, st>>>(row_a, row_b, row_sign, N0, m, n1, grids, grid_pitch, grid_stride, row_grid, tcx, tcy,
+                                                    x_out, status);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_optimal(const float2* x, int n1, int tcx, int tcy, int ref, int trk, float2* out, size_t out_pitch, cudaStream_t st)
+{
+    dim3 b(32, 8), g((tcx + 31) / 32, (tcy + 7) / 8);
+    k_optimal<<<g, b, 0, st>>>(x, n1, tcx, tcy, ref, trk, out, out_pitch);
+    return cudaGetLastError();
+}

@@ -1,0 +1,278 @@
+"""ctypes binding of libisa.so (include/isa.h) -- the same surface a C# host
+would bind with [DllImport]. Device buffers are passed as raw pointers;
+torch tensors are accepted for convenience (torch is plumbing here: device
+memory and streams).
+
+There is no CPU fallback: every compute entry point runs the CUDA kernels of
+libisa.so and raises if the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import params as P
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libisa.so")
+
+ISA_OK, ISA_EINVAL, ISA_ECUDA, ISA_ESINGULAR, ISA_ETIMEDOUT, ISA_ENOMEM = 0, -1, -2, -3, -4, -5
+MAX_LEVELS = 8
+
+
+class IsaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"isa error {code}: {msg}")
+        self.code = code
+
+
+class IsaLevel(ctypes.Structure):
+    _fields_ = [("resize_level", ctypes.c_int), ("tile_size", ctypes.c_int), ("max_shift", ctypes.c_int)]
+
+
+class IsaParams(ctypes.Structure):
+    _fields_ = [
+        ("sigma_debayer_tracking", ctypes.c_float), ("sigma_debayer_accumulation", ctypes.c_float),
+        ("high_pass", ctypes.c_float), ("high_pass_sigma", ctypes.c_float), ("clear_axis", ctypes.c_int),
+        ("matching_threshold", ctypes.c_float), ("sigma_structure_tensor", ctypes.c_float),
+        ("dth", ctypes.c_float), ("dtr", ctypes.c_float), ("k_detail", ctypes.c_float), ("k_denoise", ctypes.c_float),
+        ("k_stretch", ctypes.c_float), ("k_shrink", ctypes.c_float), ("iterations_lk", ctypes.c_int),
+        ("window_size_lk", ctypes.c_int), ("erode_size", ctypes.c_int), ("min_det_lk", ctypes.c_float),
+        ("threshold_m", ctypes.c_float), ("tracking_strategy", ctypes.c_int), ("tracking_block_size", ctypes.c_int),
+        ("green_channel_only", ctypes.c_int), ("level_count", ctypes.c_int), ("levels", IsaLevel * MAX_LEVELS),
+        ("super_resolution", ctypes.c_int), ("merge_scale", ctypes.c_float), ("robust_s", ctypes.c_float),
+        ("robust_t", ctypes.c_float), ("fused_accumulate", ctypes.c_int),
+    ]
+
+
+class IsaRawInfo(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("cfa", ctypes.c_int * 4), ("black", ctypes.c_float * 3),
+                ("white", ctypes.c_float * 3), ("camera_white", ctypes.c_float * 3), ("noise_alpha", ctypes.c_float),
+                ("noise_beta", ctypes.c_float)]
+
+
+class IsaPrealign(ctypes.Structure):
+    _fields_ = [("shifts", ctypes.POINTER(ctypes.c_float)), ("rotations_deg", ctypes.POINTER(ctypes.c_float)),
+                ("reference", ctypes.c_int)]
+
+
+class IsaTrackPair(ctypes.Structure):
+    _fields_ = [("reference", ctypes.c_int), ("to_track", ctypes.c_int), ("grid", ctypes.c_int),
+                ("base_shift_ref", ctypes.c_float * 2), ("rotation_ref", ctypes.c_float),
+                ("base_shift_trk", ctypes.c_float * 2), ("rotation_trk", ctypes.c_float)]
+
+
+# every symbol include/isa.h declares (checked by the CPU tests)
+EXPORTS = [
+    "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
+    "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_bw_image", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
+    "isa_solve_shifts", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
+    "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
+    "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
+]
+
+_lib = None
+
+
+def lib():
+    """Load libisa.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build
+            build.build()
+        if not os.path.exists(LIB_PATH):
+            raise IsaError(ISA_EINVAL, f"{LIB_PATH} is missing; build it with python -m imagestackalignator_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        L.isa_last_error.restype = ctypes.c_char_p
+        L.isa_version.restype = ctypes.c_char_p
+        for name in EXPORTS:
+            f = getattr(L, name)
+            if name not in ("isa_last_error", "isa_version", "isa_params_default"):
+                f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(code):
+    if code != ISA_OK:
+        raise IsaError(code, lib().isa_last_error().decode())
+    return code
+
+
+def vp(x):
+    """Device pointer of a torch tensor (or an int / None)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    return ctypes.c_void_p(x.data_ptr())
+
+
+def stream_ptr(stream=None):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def make_params(p: Optional[P.MergeParams] = None, fused_accumulate=True) -> IsaParams:
+    p = p or P.MergeParams()
+    c = IsaParams()
+    lib().isa_params_default(ctypes.byref(c))
+    for name in ("sigma_debayer_tracking", "sigma_debayer_accumulation", "high_pass", "high_pass_sigma", "matching_threshold",
+                 "sigma_structure_tensor", "dth", "dtr", "k_detail", "k_denoise", "k_stretch", "k_shrink", "min_det_lk", "threshold_m",
+                 "merge_scale", "robust_s", "robust_t"):
+        setattr(c, name, float(getattr(p, name)))
+    for name in ("clear_axis", "iterations_lk", "window_size_lk", "erode_size", "tracking_strategy", "tracking_block_size"):
+        setattr(c, name, int(getattr(p, name)))
+    c.green_channel_only = int(bool(p.green_channel_only))
+    c.super_resolution = int(bool(p.super_resolution))
+    c.level_count = len(p.levels)
+    for i, lv in enumerate(p.levels):
+        c.levels[i] = IsaLevel(lv.resize_level, lv.tile_size, lv.max_shift)
+    c.fused_accumulate = int(bool(fused_accumulate))
+    return c
+
+
+def make_info(burst) -> IsaRawInfo:
+    i = IsaRawInfo()
+    i.width, i.height = burst.width, burst.height
+    for k in range(4):
+        i.cfa[k] = int(burst.cfa[k])
+    for k in range(3):
+        i.black[k] = float(burst.black[k])
+        i.white[k] = float(burst.white[k])
+        i.camera_white[k] = float(burst.camera_white[k])
+    i.noise_alpha = float(burst.noise_a)
+    i.noise_beta = float(burst.noise_b)
+    return i
+
+
+def output_size(p: IsaParams, width, height):
+    w, h = ctypes.c_int(), ctypes.c_int()
+    check(lib().isa_output_size(ctypes.byref(p), width, height, ctypes.byref(w), ctypes.byref(h)))
+    return w.value, h.value
+
+
+class Merger:
+    """Owns an isa_ctx: the B200 counterpart of the controller's
+    TrackPatches + PrepareAccumulation + Accumulate for one burst size."""
+
+    def __init__(self, max_width, max_height, max_frames, params: Optional[P.MergeParams] = None, fused_accumulate=True):
+        self.params = make_params(params, fused_accumulate)
+        self.ctx = ctypes.c_void_p()
+        check(lib().isa_ctx_create(ctypes.byref(self.ctx), max_width, max_height, max_frames, ctypes.byref(self.params)))
+
+    def close(self):
+        if self.ctx:
+            lib().isa_ctx_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def output_size(self, width, height):
+        return output_size(self.params, width, height)
+
+    @staticmethod
+    def _pre(n, shifts=None, rotations=None, reference=0):
+        pre = IsaPrealign()
+        keep = []
+        if shifts is not None:
+            a = np.ascontiguousarray(shifts, dtype=np.float32).reshape(n, 2)
+            keep.append(a)
+            pre.shifts = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        if rotations is not None:
+            r = np.ascontiguousarray(rotations, dtype=np.float32).reshape(n)
+            keep.append(r)
+            pre.rotations_deg = r.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        pre.reference = int(reference)
+        return pre, keep
+
+    def merge(self, raw, info: IsaRawInfo, out=None, shifts=None, rotations=None, reference=0, stream=None):
+        """raw: cuda uint16-compatible tensor n x H x W (torch.int16/uint16 storage); returns out (Ho x Wo x 3 float32)."""
+        import torch
+        n, H, W = raw.shape
+        Wo, Ho = self.output_size(W, H)
+        if out is None:
+            out = torch.empty((Ho, Wo, 3), dtype=torch.float32, device=raw.device)
+        pre, keep = self._pre(n, shifts, rotations, reference)
+        check(lib().isa_merge_burst(self.ctx, vp(raw), ctypes.c_size_t(W * 2), ctypes.c_size_t(W * H * 2), n, ctypes.byref(info),
+                                    ctypes.byref(pre), vp(out), ctypes.c_size_t(Wo * 12), stream_ptr(stream)))
+        return out
+
+    def merge_host(self, raw_host, info: IsaRawInfo, out_host=None, shifts=None, rotations=None, reference=0, stream=None):
+        """raw_host: host uint16 array/tensor (pinned for full speed); returns host float32 Ho x Wo x 3."""
+        n, H, W = raw_host.shape
+        Wo, Ho = self.output_size(W, H)
+        if out_host is None:
+            out_host = np.empty((Ho, Wo, 3), np.float32)
+        pre, keep = self._pre(n, shifts, rotations, reference)
+        rp = ctypes.c_void_p(raw_host.data_ptr()) if hasattr(raw_host, "data_ptr") else raw_host.ctypes.data_as(ctypes.c_void_p)
+        op = ctypes.c_void_p(out_host.data_ptr()) if hasattr(out_host, "data_ptr") else out_host.ctypes.data_as(ctypes.c_void_p)
+        check(lib().isa_merge_burst_host(self.ctx, rp, n, ctypes.byref(info), ctypes.byref(pre), op, stream_ptr(stream)))
+        return out_host
+
+    def stage_times(self):
+        ms = (ctypes.c_float * 8)()
+        k = lib().isa_stage_times(self.ctx, ms, 8)
+        if k < 0:
+            check(k)
+        return [ms[i] for i in range(k)]
+
+    def debug(self, frame):
+        ptrs = [ctypes.c_void_p() for _ in range(7)]
+        pitches = [ctypes.c_size_t() for _ in range(4)]
+        check(lib().isa_debug_buffers(self.ctx, frame, ctypes.byref(ptrs[0]), ctypes.byref(pitches[0]), ctypes.byref(ptrs[1]),
+                                      ctypes.byref(pitches[1]), ctypes.byref(ptrs[2]), ctypes.byref(pitches[2]), ctypes.byref(ptrs[3]),
+                                      ctypes.byref(ptrs[4]), ctypes.byref(pitches[3]), ctypes.byref(ptrs[5]), ctypes.byref(ptrs[6]),
+                                      ctypes.byref(ctypes.c_size_t())))
+        return {"flow": ptrs[0].value, "mask": ptrs[1].value, "kparam": ptrs[2].value, "bw_track": ptrs[3].value,
+                "bw_acc": ptrs[4].value, "acc": ptrs[5].value, "wsum": ptrs[6].value}
+
+    def debug_shifts(self):
+        p = ctypes.c_void_p()
+        tx, ty = ctypes.c_int(), ctypes.c_int()
+        check(lib().isa_debug_shifts(self.ctx, ctypes.byref(p), ctypes.byref(tx), ctypes.byref(ty)))
+        return p.value, tx.value, ty.value
+
+
+def device_copy(ptr, shape, dtype, device="cuda"):
+    """Copy `shape` elements of `dtype` from a device pointer into a new torch tensor."""
+    import torch
+    t = torch.empty(shape, dtype=dtype, device=device)
+    s = torch.cuda.current_stream()
+    rc = _cudart().cudaMemcpyAsync(ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(ptr), ctypes.c_size_t(t.numel() * t.element_size()), 3,
+                                   ctypes.c_void_p(s.cuda_stream))
+    if rc != 0:
+        raise IsaError(ISA_ECUDA, f"cudaMemcpyAsync failed ({rc})")
+    return t
+
+
+_CUDART = None
+
+
+def _cudart():
+    global _CUDART
+    if _CUDART is None:
+        import glob
+        import torch
+        cands = glob.glob(os.path.join(os.path.dirname(torch.__file__), "..", "nvidia", "cuda_runtime", "lib", "libcudart.so*"))
+        cands += ["/usr/local/cuda/lib64/libcudart.so"]
+        for c in cands:
+            try:
+                _CUDART = ctypes.CDLL(c)
+                break
+            except OSError:
+                continue
+        if _CUDART is None:
+            raise IsaError(ISA_ECUDA, "libcudart not found")
+    return _CUDART

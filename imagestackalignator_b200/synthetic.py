@@ -1,0 +1,151 @@
+"""Seeded synthetic Bayer bursts (the stand-in for real PEF/DNG bursts).
+
+A linear-RGB scene is drawn from Gaussian blobs, straight and curved step
+edges, sinusoidal gratings (period 2-16 px) and a checker patch. Each frame
+is the scene under a global rotation about the frame centre and a translation
+(frame 0 is the reference, unmoved), resampled with bicubic interpolation,
+mosaicked with the CFA, given Poisson-Gaussian noise of variance a*x + b
+(full scale) and quantised to unsigned 16-bit values with a black level.
+
+The metadata follows the reference RawFile fields (PefFile/RawFile.cs:94-119):
+WhiteLevel excludes the black level (PEFFile.cs:271-274, DNGFile.cs:832-834),
+so values map to [0, 1] by (raw - black) / white.
+
+Rendering uses torch (CPU or CUDA) only as a resampler for test data.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+CFA_CODES = {"RGGB": (0, 1, 1, 2), "BGGR": (2, 1, 1, 0), "GRBG": (1, 0, 2, 1), "GBRG": (1, 2, 0, 1)}
+
+
+@dataclass
+class Burst:
+    raw: np.ndarray                  # n x H x W uint16
+    cfa: tuple                       # codes at (0,0), (0,1), (1,0), (1,1)
+    black: tuple                     # per R, G, B
+    white: tuple                     # per R, G, B, black excluded
+    noise_a: float
+    noise_b: float
+    shifts: np.ndarray               # n x 2 true translation (px) of each frame
+    rotations: np.ndarray            # n true rotation (degrees)
+    truth: Optional[np.ndarray] = None  # H x W x 3 clean linear scene of frame 0 (float64)
+    camera_white: tuple = (1.0, 1.0, 1.0)
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return self.raw.shape[0]
+
+    @property
+    def height(self):
+        return self.raw.shape[1]
+
+    @property
+    def width(self):
+        return self.raw.shape[2]
+
+
+def _render_scene(Wp, Hp, rng, torch, device, dtype):
+    """Procedural linear-RGB scene on a Wp x Hp grid, values in about [0.03, 0.9]."""
+    yy, xx = torch.meshgrid(torch.arange(Hp, device=device, dtype=dtype),
+                            torch.arange(Wp, device=device, dtype=dtype), indexing="ij")
+    base = torch.tensor(rng.uniform(0.15, 0.45, 3), device=device, dtype=dtype)
+    grad = torch.tensor(rng.uniform(-0.1, 0.1, (2, 3)), device=device, dtype=dtype)
+    img = base.view(3, 1, 1) + grad[0].view(3, 1, 1) * (xx / Wp - 0.5) + grad[1].view(3, 1, 1) * (yy / Hp - 0.5)
+    area = Wp * Hp
+    unit = max(1, int(area / (512 * 384)))
+    scale = float(np.sqrt(area / (2048 * 1536)))
+
+    def color(lo=-0.25, hi=0.25):
+        return torch.tensor(rng.uniform(lo, hi, 3), device=device, dtype=dtype).view(3, 1, 1)
+
+    def window(cx, cy, hw, hh):
+        return ((xx - cx).abs() <= hw) & ((yy - cy).abs() <= hh)
+
+    # Gaussian blobs
+    for _ in range(6 * unit):
+        cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
+        s = rng.uniform(4, 60) * max(scale, 0.25)
+        img = img + color() * torch.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2 * s * s))
+    # straight step edges inside a window
+    for _ in range(3 * unit):
+        cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
+        th = rng.uniform(0, np.pi)
+        hw = rng.uniform(20, 160) * max(scale, 0.25)
+        side = ((xx - cx) * np.cos(th) + (yy - cy) * np.sin(th)) > 0
+        img = img + color() * (side & window(cx, cy, hw, hw)).to(dtype)
+    # curved edges: discs and rings
+    for _ in range(3 * unit):
+        cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
+        r = rng.uniform(10, 120) * max(scale, 0.25)
+        d = torch.sqrt((xx - cx) ** 2 + (yy - cy) ** 2)
+        img = img + color() * (d < r).to(dtype)
+    # sinusoidal gratings, period 2..16 px
+    for _ in range(3 * unit):
+        cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
+        period = rng.uniform(2, 16)
+        th = rng.uniform(0, np.pi)
+        hw, hh = rng.uniform(20, 120) * max(scale, 0.25), rng.uniform(20, 120) * max(scale, 0.25)
+        ph = 2 * np.pi / period * ((xx - cx) * np.cos(th) + (yy - cy) * np.sin(th))
+        img = img + color(0.05, 0.2) * torch.sin(ph) * window(cx, cy, hw, hh).to(dtype)
+    # one checker patch
+    cx, cy = rng.uniform(0.2, 0.8) * Wp, rng.uniform(0.2, 0.8) * Hp
+    sq = int(rng.integers(4, 17))
+    hw = 80 * max(scale, 0.25)
+    chk = (((torch.floor(xx / sq) + torch.floor(yy / sq)) % 2) * 2 - 1)
+    img = img + color(0.1, 0.2) * chk * window(cx, cy, hw, hw).to(dtype)
+    return img.clamp(0.03, 0.9)
+
+
+def make_burst(width=2048, height=1536, frames=8, seed=0, max_shift=6.0, max_rot_deg=0.2,
+               noise_a=4e-4, noise_b=2e-6, black=512, white_max=16383, cfa="RGGB", device="cpu",
+               keep_truth=False, dtype=None) -> Burst:
+    """Seeded burst; frame 0 is the reference with zero motion."""
+    import torch
+    import torch.nn.functional as F
+
+    if dtype is None:
+        dtype = torch.float64 if device == "cpu" else torch.float32
+    rng = np.random.default_rng(seed)
+    margin = int(np.ceil(max_shift + np.deg2rad(max_rot_deg) * 0.5 * np.hypot(width, height))) + 4
+    Wp, Hp = width + 2 * margin, height + 2 * margin
+    scene = _render_scene(Wp, Hp, rng, torch, device, dtype)
+    shifts = np.zeros((frames, 2))
+    rots = np.zeros(frames)
+    shifts[1:] = rng.uniform(-max_shift, max_shift, (frames - 1, 2))
+    rots[1:] = rng.uniform(-max_rot_deg, max_rot_deg, frames - 1)
+    codes = CFA_CODES[cfa]
+    ys, xs = torch.meshgrid(torch.arange(height, device=device, dtype=dtype),
+                            torch.arange(width, device=device, dtype=dtype), indexing="ij")
+    cfa_idx = ((ys.long() & 1) * 2 + (xs.long() & 1))
+    chan = torch.tensor(codes, device=device)[cfa_idx]
+    raw = np.empty((frames, height, width), dtype=np.uint16)
+    gen = torch.Generator(device=device).manual_seed(int(seed) * 7919 + 17)
+    truth = None
+    for f in range(frames):
+        th = np.deg2rad(rots[f])
+        c, s = np.cos(th), np.sin(th)
+        cxf, cyf = (width - 1) / 2.0, (height - 1) / 2.0
+        # frame pixel p sees scene point R(th) (p - c) + c + t
+        dx, dy = xs - cxf, ys - cyf
+        sx = c * dx - s * dy + cxf + shifts[f, 0] + margin
+        sy = s * dx + c * dy + cyf + shifts[f, 1] + margin
+        grid = torch.stack([(sx + 0.5) / Wp * 2 - 1, (sy + 0.5) / Hp * 2 - 1], dim=-1)[None]
+        frame = F.grid_sample(scene[None], grid, mode="bicubic", padding_mode="border", align_corners=False)[0]
+        frame = frame.clamp(0, 1)
+        if f == 0 and keep_truth:
+            truth = frame.permute(1, 2, 0).double().cpu().numpy()
+        mosaic = torch.gather(frame, 0, chan[None]).squeeze(0)
+        noise = torch.randn(mosaic.shape, generator=gen, device=device, dtype=dtype)
+        noisy = mosaic + torch.sqrt(noise_a * mosaic + noise_b) * noise
+        q = torch.round(black + noisy * (white_max - black)).clamp(0, white_max)
+        raw[f] = q.to(torch.int32).cpu().numpy().astype(np.uint16)
+        del frame, mosaic, noise, noisy, q, grid
+    w = float(white_max - black)
+    return Burst(raw=raw, cfa=codes, black=(float(black),) * 3, white=(w, w, w), noise_a=noise_a, noise_b=noise_b,
+                 shifts=shifts, rotations=rots, truth=truth)

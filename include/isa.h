@@ -1,0 +1,274 @@
+/*
+ * isa.h -- C ABI of the B200 burst-merge library (libisa.so).
+ *
+ * Drop-in for the GPU hot path of ImageStackAlignator (PEFStudioDX): the
+ * per-kernel operator wrappers (PEFStudioDX/*Kernels.cs, one CudaKernel
+ * subclass per __global__) and the controller steps that chain them
+ * (ImageStackAlignatorController.cs TrackPatches :1601, PrepareAccumulation
+ * :1795, Accumulate :1928). Every declaration names the reference interface
+ * it replaces.
+ *
+ * Conventions
+ *  - Images are device pointers with a row pitch in bytes, channels
+ *    interleaved, as the reference's NPPImage_* buffers: float (32fC1),
+ *    float2 flow (32fC2), float3 RGB (32fC3), float4 masks / kernels (32fC4),
+ *    uint16 Bayer frames (16uC1).
+ *  - CFA: int cfa[4] = colour codes at (row 0, col 0), (0, 1), (1, 0), (1, 1);
+ *    R = 0, G = 1, B = 2 (RawFile.BayerColor, PefFile/RawFile.cs:30-39,
+ *    set through c_cfaPattern in DeBayerKernels.cs:53-63).
+ *  - Every call returns an int status (ISA_OK or a negative ISA_E* code) and
+ *    never throws; isa_last_error() gives the message of the calling
+ *    thread's last failure. Work is ordered on the caller's stream (a
+ *    cudaStream_t passed as void*, NULL = legacy default stream). Per-op
+ *    entry points allocate nothing; isa_ctx owns all scratch of the fused
+ *    pipeline and is created once (isa_ctx_create) per maximum size.
+ *  - An isa_ctx must not be used by two host threads at once.
+ */
+#ifndef ISA_H
+#define ISA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define ISA_API __declspec(dllexport)
+#elif defined(__GNUC__)
+#define ISA_API __attribute__((visibility("default")))
+#else
+#define ISA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ISA_OK 0
+#define ISA_EINVAL (-1)      /* bad size, pointer or parameter */
+#define ISA_ECUDA (-2)       /* a CUDA runtime or cuFFT call failed */
+#define ISA_ESINGULAR (-3)   /* reported per tile in the solver status array, never returned */
+#define ISA_ETIMEDOUT (-4)   /* reserved for bounded waits */
+#define ISA_ENOMEM (-5)      /* device allocation failed (isa_ctx_create only) */
+
+#define ISA_MAX_LEVELS 8
+
+/* Tracking strategies of ShiftCollection.TrackingStrategy (ShiftCollection.cs:36-47). */
+#define ISA_TRACK_FULL 0
+#define ISA_TRACK_ONLY_ON_REFERENCE 1
+#define ISA_TRACK_ON_REFERENCE_BLOCK 2
+#define ISA_TRACK_BLOCKS 3
+
+/* PatchTrackingLevel (PatchTrackingLevel.cs:27-63). */
+typedef struct isa_level {
+    int resize_level;
+    int tile_size;
+    int max_shift;
+} isa_level;
+
+/* Controller parameters with the reference names and defaults
+ * (ImageStackAlignatorController.cs:443-675), plus extensions that default
+ * to the reference behaviour. */
+typedef struct isa_params {
+    float sigma_debayer_tracking;     /* 0.5    :450 */
+    float sigma_debayer_accumulation; /* 0.5    :459 */
+    float high_pass;                  /* 0.01   :468 */
+    float high_pass_sigma;            /* 0.0025 :477 */
+    int clear_axis;                   /* 0      :486 */
+    float matching_threshold;         /* 1.0    :495 */
+    float sigma_structure_tensor;     /* 1.0    :522 */
+    float dth;                        /* 0.001  :531 */
+    float dtr;                        /* 0.006  :540 */
+    float k_detail;                   /* 0.25   :549 */
+    float k_denoise;                  /* 3.0    :558 */
+    float k_stretch;                  /* 4.0    :567 */
+    float k_shrink;                   /* 2.0    :576 */
+    int iterations_lk;                /* 3      :585 */
+    int window_size_lk;               /* 11     :594 */
+    int erode_size;                   /* 5      :603 */
+    float min_det_lk;                 /* 0.01   :612 */
+    float threshold_m;                /* 1e5    :621 */
+    int tracking_strategy;            /* FULL   :657 */
+    int tracking_block_size;          /* 5      :666 */
+    int green_channel_only;           /* 0      :675 */
+    int level_count;                  /* 4: (1,32,2) then (2*prev,32,4) (:1572-1586) */
+    isa_level levels[ISA_MAX_LEVELS];
+    /* extensions */
+    int super_resolution;             /* SuperResolution (:648): 2x over the central crop */
+    float merge_scale;                /* 0 = reference modes; > 0: the whole frame at this scale */
+    float robust_s;                   /* 1.5, literal at RobustnessModell.cu:472 */
+    float robust_t;                   /* 0.12, literal at RobustnessModell.cu:476 */
+    int fused_accumulate;             /* 1: all frames in one accumulation pass (same sums, same order) */
+} isa_params;
+
+/* RawFile metadata the merge uses (PefFile/RawFile.cs:94-119). white excludes black. */
+typedef struct isa_raw_info {
+    int width, height;
+    int cfa[4];
+    float black[3];
+    float white[3];
+    float camera_white[3];            /* AsShot white balance (DNGColorSpec CameraWhite), 1 = none */
+    float noise_alpha, noise_beta;    /* NoiseModelA / NoiseModelB */
+} isa_raw_info;
+
+/* PreAlignmentStore state (PreAlignmentStore.cs:27-150); NULL arrays = all zero. */
+typedef struct isa_prealign {
+    const float* shifts;              /* n x 2, host memory */
+    const float* rotations_deg;       /* n, host memory */
+    int reference;                    /* ReferenceIndex */
+} isa_prealign;
+
+typedef struct isa_ctx isa_ctx;
+
+/* ---- context, parameters, errors --------------------------------------- */
+ISA_API void isa_params_default(isa_params* p);
+ISA_API const char* isa_last_error(void);
+ISA_API const char* isa_version(void);
+/* Allocates every buffer of the fused pipeline for frames up to
+ * max_width x max_height and max_frames (replaces the allocations of
+ * PatchTracker.AllocateDeviceMemory PatchTracker.cs:96-117, OpticalFlow
+ * OpticalFlow.cs:115-138, ShiftCollection ShiftCollection.cs:490-560 and
+ * the controller buffers :1832-1849). */
+ISA_API int isa_ctx_create(isa_ctx** ctx, int max_width, int max_height, int max_frames, const isa_params* p);
+ISA_API int isa_ctx_destroy(isa_ctx* ctx);
+/* Output size of the merge for a frame size under p. */
+ISA_API int isa_output_size(const isa_params* p, int width, int height, int* out_width, int* out_height);
+/* Stage times (ms) of the last isa_merge_burst call, in order: tracking
+ * images, tile alignment, kernel parameters, LK + robustness, accumulation,
+ * finalize. Synchronises the context's events. Returns the count written. */
+ISA_API int isa_stage_times(isa_ctx* ctx, float* ms, int max_count);
+
+/* ---- fused pipeline ------------------------------------------------------ */
+/* Whole forward merge of one burst (TrackPatches :1601 + PrepareAccumulation
+ * :1795 + Accumulate :1928 + ApplyWeighting :1994-2002). raw: n frames of
+ * width x height uint16, frame i at raw + i * frame_stride bytes, rows at
+ * raw_pitch. out: float3 image of isa_output_size() with out_pitch. */
+ISA_API int isa_merge_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                    const isa_prealign* pre, float* out, size_t out_pitch, void* stream);
+/* The same with host buffers: frames are copied in and the image copied out
+ * on `stream` (pinned host memory gives full PCIe speed). */
+ISA_API int isa_merge_burst_host(isa_ctx* ctx, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre,
+                         float* host_out, void* stream);
+/* Intermediates of the last isa_merge_burst (device pointers owned by ctx,
+ * valid until the next call): per-frame dense flow (float2, W x H), eroded
+ * robustness mask (float4, W/2 x H/2), kernel parameters (float4, W x H),
+ * tracking images (float), accumulation sums (float3, output size). */
+ISA_API int isa_debug_buffers(isa_ctx* ctx, int frame, const void** flow, size_t* flow_pitch, const void** mask, size_t* mask_pitch,
+                      const void** kparam, size_t* kparam_pitch, const void** bw_track, const void** bw_acc, size_t* bw_pitch,
+                      const void** acc, const void** wsum, size_t* acc_pitch);
+/* Tile-alignment intermediates of the last isa_merge_burst: one-to-one shifts
+ * of the finest level (tiles x (n-1) float2, device) and its tile counts. */
+ISA_API int isa_debug_shifts(isa_ctx* ctx, const void** one_to_one, int* tiles_x, int* tiles_y);
+
+/* ---- operator API: one entry point per reference kernel wrapper ----------- */
+/* DeBayerFullRes (controller :1268-1311): NPP Convert + Set(0) +
+ * deBayerGreenKernel (DeBayerKernels.cs:36-44) + deBayerRedBlueKernel
+ * (DeBayerKernels.cs:72-80) + NPP Div by divisor. out: float3. */
+ISA_API int isa_debayer_full(const uint16_t* raw, size_t raw_pitch, int width, int height, const int cfa[4], const float black[3],
+                     const float scale[3], const float divisor[3], float* out, size_t out_pitch, void* stream);
+/* GammasRGBKernel (BasicKernels.cs:243-257), in place on float3. */
+ISA_API int isa_gamma_srgb(float* img, size_t pitch, int width, int height, void* stream);
+/* DeBayerBWGaussWB (controller :2384-2418) for one frame: demosaic, gamma,
+ * gray, optional Fourier high-pass + clamp (PreAlignment.FourierFilter
+ * PreAlignment.cs:268-281), Gaussian. Needs ctx for the FFT plan/scratch. */
+ISA_API int isa_bw_image(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, int width, int height, const isa_raw_info* info,
+                 float sigma, int high_pass, float* out, size_t out_pitch, void* stream);
+/* fourierFilterKernel (BasicKernels.cs:81-100) on a (width/2+1) x height
+ * half spectrum (float2), times post_scale. */
+ISA_API int isa_fourier_filter(void* spectrum, size_t pitch, int width, int height, float lp, float hp, float lps, float hps, int clear_axis,
+                       float post_scale, void* stream);
+/* NPP FilterGaussBorder with gaussian_filter_1D(sigma) taps (controller
+ * :2351-2382) and replicate border; channels 1 or 3; tmp: same size as in. */
+ISA_API int isa_gauss_filter(const float* in, size_t in_pitch, float* out, size_t out_pitch, float* tmp, size_t tmp_pitch, int width, int height,
+                     int channels, float sigma, void* stream);
+/* NPP ResizeSqrPixel SuperSampling by 1/level (controller :1688-1703). */
+ISA_API int isa_resize_box(const float* in, size_t in_pitch, int width, int height, int level, float* out, size_t out_pitch, void* stream);
+/* PatchTracker.Track (PatchTracker.cs:317-360) for a batch of pairs at one
+ * level: frames = device array of level-image pointers; pairs = device
+ * array of isa_track_pair; grids = per-pair preShift grids (float2), grid k
+ * at grids + k * grid_stride bytes, rows at grid_pitch; updated in place
+ * (preShift += found shift). scores / argmin (optional, device): per pair
+ * and tile the (2S+1)^2 L2 map and the index of its first minimum. */
+typedef struct isa_track_pair {
+    int reference, to_track, grid;
+    float base_shift_ref[2], rotation_ref;   /* PreAlignmentStore GetShift/level, GetRotation (radians) */
+    float base_shift_trk[2], rotation_trk;
+} isa_track_pair;
+ISA_API int isa_track_level(const float* const* frames, size_t frame_pitch, int width, int height, int tile_size, int max_shift, int tiles_x,
+                    int tiles_y, const isa_track_pair* pairs, int npairs, void* grids, size_t grid_pitch, size_t grid_stride,
+                    float threshold, float* scores, int* argmin, void* stream);
+/* upsampleShiftsKernel (BasicKernels.cs:219-233) over ngrids grids. */
+ISA_API int isa_upsample_shifts(const void* in, size_t in_pitch, size_t in_stride, void* out, size_t out_pitch, size_t out_stride, int ngrids,
+                        int old_level, int new_level, int old_count_x, int old_count_y, int new_count_x, int new_count_y,
+                        int old_tile_size, int new_tile_size, void* stream);
+/* ShiftCollection.MinimizeCUBLAS (ShiftCollection.cs:738-822) for one level:
+ * strategy/reference/n define the incidence matrix; grids as in
+ * isa_track_level, grid k holding measurement row k (FillIndexTable order);
+ * rewritten with the consistent pair shifts. one_to_one (device, tiles x
+ * (n-1) float2) and status (device, tiles: -1 converged, -3 singular,
+ * >= 0 row removed in the tenth round) are outputs. Needs ctx scratch. */
+ISA_API int isa_solve_shifts(isa_ctx* ctx, int n, int reference, int strategy, int block_size, void* grids, size_t grid_pitch,
+                     size_t grid_stride, int tiles_x, int tiles_y, void* one_to_one, int* status, void* stream);
+/* getOptimalShiftsKernel (ShiftMinimizerKernels.cs): shift of frame
+ * to_track relative to reference from the one-to-one shifts. */
+ISA_API int isa_optimal_shifts(const void* one_to_one, int n, int tiles_x, int tiles_y, int reference, int to_track, void* out,
+                       size_t out_pitch, void* stream);
+/* CreateFlowFieldFromTiles (OpticalFlowKernels.cs:59-83). base_shift: 2 floats (host). */
+ISA_API int isa_flow_from_tiles(const void* tiles, size_t tile_pitch, int tiles_x, int tiles_y, int width, int height, const float base_shift[2],
+                        float base_rotation, void* flow, size_t flow_pitch, void* stream);
+/* WarpingKernel (OpticalFlowKernels.cs:31-56). */
+ISA_API int isa_warp(const float* img, size_t img_pitch, int width, int height, const void* flow, size_t flow_pitch, float* out, size_t out_pitch,
+             void* stream);
+/* ComputeDerivativesKernel (OpticalFlowKernels.cs:86-114). */
+ISA_API int isa_derivatives(const float* src, const float* tgt, size_t pitch, int width, int height, float* ix, float* iy, float* it,
+                    size_t out_pitch, void* stream);
+/* ComputeDerivatives2Kernel (OpticalFlowKernels.cs:117-140). */
+ISA_API int isa_derivatives2(const float* img, size_t pitch, int width, int height, float* ix, float* iy, size_t out_pitch, void* stream);
+/* LukasKanadeKernel (OpticalFlowKernels.cs:143-173) on derivative images. */
+ISA_API int isa_lucas_kanade(void* flow, size_t flow_pitch, const float* ix, const float* iy, const float* it, size_t pitch, int width, int height,
+                     float min_det, int window_size, void* stream);
+/* One fused LK iteration: warp + derivatives + LK (OpticalFlow.cs:151-158);
+ * flow_in and flow_out must differ. */
+ISA_API int isa_lk_iteration(const void* flow_in, void* flow_out, size_t flow_pitch, const float* src, const float* ref, size_t img_pitch, int width,
+                     int height, float min_det, int window_size, void* stream);
+/* OpticalFlow.LucasKanade (OpticalFlow.cs:147-164): flow from tiles then
+ * `iterations` fused iterations; scratch: a second flow buffer. */
+ISA_API int isa_lk_refine(const float* src, const float* ref, size_t img_pitch, int width, int height, const void* tiles, size_t tile_pitch,
+                  int tiles_x, int tiles_y, const float base_shift[2], float base_rotation, int iterations, float min_det,
+                  int window_size, void* flow, void* flow_scratch, size_t flow_pitch, void* stream);
+/* DeBayersSubSampleKernel (DeBayerKernels.cs:84-118): 2x2 quad -> float3. */
+ISA_API int isa_debayer_subsample(const uint16_t* raw, size_t raw_pitch, int width, int height, const int cfa[4], float max_value, float* out,
+                          size_t out_pitch, void* stream);
+/* RobustnessModellKernel (RobustnessModellKernel.cs:30-66); s and t are the
+ * reference literals 1.5 / 0.12 unless changed. mask border untouched. */
+ISA_API int isa_robustness_mask(const float* ref3, const float* moved3, size_t img_pitch, void* mask, size_t mask_pitch, int half_width,
+                        int half_height, const void* flow, size_t flow_pitch, int flow_width, int flow_height, float alpha, float beta,
+                        float threshold_m, float s, float t, void* stream);
+/* NPP ErodeBorder (controller :1976) on float4, square all-ones mask. */
+ISA_API int isa_erode(const void* in, size_t in_pitch, void* out, size_t out_pitch, int width, int height, int size, void* stream);
+/* Mask + erosion fused (border pixels 1, as after controller :1891). */
+ISA_API int isa_robustness_erode(const float* ref3, const float* moved3, size_t img_pitch, int half_width, int half_height, const void* flow,
+                         size_t flow_pitch, int flow_width, int flow_height, float alpha, float beta, float threshold_m, float s, float t,
+                         int erode_size, void* out, size_t out_pitch, void* stream);
+/* computeStructureTensorKernel + ComputeDerivatives2Kernel (BasicKernels.cs:285-301). out: float3. */
+ISA_API int isa_structure_tensor(const float* img, size_t pitch, int width, int height, float* out, size_t out_pitch, void* stream);
+/* computeKernelParamKernel (BasicKernels.cs:303-318): float3 tensor ->
+ * out (3 or 4 channels; may alias st when channels == 3). */
+ISA_API int isa_kernel_param(const float* st, size_t st_pitch, int width, int height, float* out, size_t out_pitch, int out_channels, float dth,
+                     float dtr, float k_detail, float k_denoise, float k_stretch, float k_shrink, void* stream);
+/* AccumulateImagesKernel / AccumulateImagesSuperResKernel
+ * (DeBayerKernels.cs:121-211), generalised: output out_width x out_height at
+ * scale s with output-grid origin (ox, oy) and inclusive source crop
+ * crop[4] = x0, y0, x1, y1. Reference plain: s = 1, origin 0, crop = frame;
+ * super-resolution: s = 2, origin (W/2, H/2), crop = central W/2 x H/2.
+ * acc / wsum: float3 read-modify-write. flow NULL = zero, mask NULL = 1. */
+ISA_API int isa_accumulate(const uint16_t* raw, size_t raw_pitch, int width, int height, const int cfa[4], float* acc, float* wsum,
+                   size_t out_pitch, int out_width, int out_height, const void* mask, size_t mask_pitch, const float* kparam,
+                   size_t kparam_pitch, int kparam_channels, const void* flow, size_t flow_pitch, const float white[3],
+                   const float black[3], float scale, int ox, int oy, const int crop[4], void* stream);
+/* ApplyWeightingKernel (BasicKernels.cs:259-284): img (fallback in, result out). */
+ISA_API int isa_apply_weighting(float* img, const float* acc, const float* wsum, size_t pitch, int width, int height, float threshold,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
