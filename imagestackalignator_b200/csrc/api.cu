@@ -40,6 +40,11 @@ int fail(int code, const char* fmt, ...)
         cufftResult r_ = (call);                                                   \
         if (r_ != CUFFT_SUCCESS) return fail(ISA_ECUDA, "%s: cufft error %d", #call, (int)r_); \
     } while (0)
+#define ISA_LAUNCH(ctx, call) \
+    do {                      \
+        ISA_CK(call);         \
+        ++(ctx)->launches;    \
+    } while (0)
 #define ISA_TRY(call)            \
     do {                         \
         int s_ = (call);         \
@@ -195,6 +200,7 @@ struct isa_ctx {
     size_t fft_work_bytes = 0;
     cudaEvent_t ev[8] = {};
     int ev_count = 0;
+    long launches = 0;  // kernels of this library launched by the last merge
     // last call
     int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0;
 };
@@ -302,20 +308,20 @@ int bw_frame(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H, co
     const float gw_rgb[3] = {0.2989f, 0.5870f, 0.1141f}, gw_g[3] = {0.f, 1.f, 0.f};
     const float* gw = c->p.green_channel_only ? gw_g : gw_rgb;
     size_t pitch = bw_pitch(W);
-    ISA_CK(isa_launch_demosaic_gray(raw, raw_pitch, W, H, pack_cfa(info->cfa), black, scale, divisor, gw, 1, out, pitch, nullptr, 0, st));
+    ISA_LAUNCH(c, isa_launch_demosaic_gray(raw, raw_pitch, W, H, pack_cfa(info->cfa), black, scale, divisor, gw, 1, out, pitch, nullptr, 0, st));
     if (acc_out)
-        ISA_CK(isa_launch_gauss(out, pitch, acc_out, pitch, c->tmp, pitch, W, H, 1, taps_acc.data(), (int)taps_acc.size(), 0, st));
+        ISA_LAUNCH(c, isa_launch_gauss(out, pitch, acc_out, pitch, c->tmp, pitch, W, H, 1, taps_acc.data(), (int)taps_acc.size(), 0, st));
     if (high_pass) {
         ISA_TRY(ensure_plans(c, W, H));
         ISA_FFT(cufftSetStream(c->r2c, st));
         ISA_FFT(cufftSetStream(c->c2r, st));
         ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)out, (cufftComplex*)c->spec));
-        ISA_CK(isa_launch_fourier_filter(c->spec, (size_t)(W / 2 + 1) * sizeof(float2), W, H, 1, 0, 1.0f, c->p.high_pass, 1.0f,
+        ISA_LAUNCH(c, isa_launch_fourier_filter(c->spec, (size_t)(W / 2 + 1) * sizeof(float2), W, H, 1, 0, 1.0f, c->p.high_pass, 1.0f,
                                          c->p.high_pass_sigma, c->p.clear_axis, 1.0f / ((float)W * (float)H), st));
         ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)out));
     }
     if (!taps_hp.empty())
-        ISA_CK(isa_launch_gauss(out, pitch, out, pitch, c->tmp, pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), high_pass ? 1 : 0, st));
+        ISA_LAUNCH(c, isa_launch_gauss(out, pitch, out, pitch, c->tmp, pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), high_pass ? 1 : 0, st));
     return ISA_OK;
 }
 
@@ -391,6 +397,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     float black[3], white[3], scale[3], divisor[3];
     color_consts(info, black, white, scale, divisor);
     c->ev_count = 0;
+    c->launches = 0;
     auto mark = [&]() -> int {
         ISA_CK(cudaEventRecord(c->ev[c->ev_count++], st));
         return ISA_OK;
@@ -417,7 +424,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         if (level_tiles(lv, W, H, &tcx, &tcy) != ISA_OK) return fail(ISA_EINVAL, "level %d has no tiles for %dx%d", li, W, H);
         if (li == 0) { tcx0 = tcx; tcy0 = tcy; }
         if (li != L - 1) {
-            ISA_CK(isa_launch_upsample(grids, gpitch, gstride, grids_tmp, gpitch, gstride, strat.m, olevel, lv.resize_level, otcx, otcy, tcx,
+            ISA_LAUNCH(c, isa_launch_upsample(grids, gpitch, gstride, grids_tmp, gpitch, gstride, strat.m, olevel, lv.resize_level, otcx, otcy, tcx,
                                        tcy, oT, lv.tile_size, st));
             std::swap(grids, grids_tmp);
         }
@@ -427,7 +434,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
             float* base = c->pyr[li];
             for (int i = 0; i < n; i++) {
                 float* dst = base + (size_t)i * Wl * Hl;
-                ISA_CK(isa_launch_resize_box(c->bw_track + i * fsz, pitch, W, H, lv.resize_level, dst, lpitch, st));
+                ISA_LAUNCH(c, isa_launch_resize_box(c->bw_track + i * fsz, pitch, W, H, lv.resize_level, dst, lpitch, st));
                 fptr[i] = dst;
             }
         } else {
@@ -447,10 +454,10 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         ISA_CK(cudaMemcpyAsync(c->pair_desc + (size_t)li * c->max_pairs, pd.data(), pd.size() * sizeof(isa_pair_desc),
                                cudaMemcpyHostToDevice, st));
         ISA_CK(cudaMemcpyAsync(c->frame_tab + (size_t)li * c->max_n, fptr.data(), n * sizeof(float*), cudaMemcpyHostToDevice, st));
-        ISA_CK(isa_launch_track(c->frame_tab + (size_t)li * c->max_n, lpitch, Wl, Hl, lv.tile_size, lv.max_shift, tcx, tcy,
+        ISA_LAUNCH(c, isa_launch_track(c->frame_tab + (size_t)li * c->max_n, lpitch, Wl, Hl, lv.tile_size, lv.max_shift, tcx, tcy,
                                 c->pair_desc + (size_t)li * c->max_pairs, strat.m, grids, gpitch, gstride, p->matching_threshold, nullptr,
                                 nullptr, st));
-        ISA_CK(isa_launch_solve(c->row_a, c->row_b, c->row_sign, c->N0, strat.m, strat.n1, grids, gpitch, gstride, c->row_grid, tcx, tcy,
+        ISA_LAUNCH(c, isa_launch_solve(c->row_a, c->row_b, c->row_sign, c->N0, strat.m, strat.n1, grids, gpitch, gstride, c->row_grid, tcx, tcy,
                                 c->x, c->status, st));
         otcx = tcx; otcy = tcy; olevel = lv.resize_level; oT = lv.tile_size;
     }
@@ -458,9 +465,9 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     // 3. kernel parameters from the reference frame (PrepareAccumulation :1851-1858)
     const std::vector<float> taps_st = gauss_taps(p->sigma_structure_tensor);
     const size_t p3 = (size_t)W * 12, p4 = (size_t)W * 16;
-    ISA_CK(isa_launch_structure_tensor(c->bw_acc + ref * fsz, pitch, W, H, c->st3, p3, st));
-    ISA_CK(isa_launch_gauss(c->st3, p3, c->st3, p3, c->tmp, p3, W, H, 3, taps_st.data(), (int)taps_st.size(), 0, st));
-    ISA_CK(isa_launch_kernel_param(c->st3, p3, W, H, c->kparam, p4, 4, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
+    ISA_LAUNCH(c, isa_launch_structure_tensor(c->bw_acc + ref * fsz, pitch, W, H, c->st3, p3, st));
+    ISA_LAUNCH(c, isa_launch_gauss(c->st3, p3, c->st3, p3, c->tmp, p3, W, H, 3, taps_st.data(), (int)taps_st.size(), 0, st));
+    ISA_LAUNCH(c, isa_launch_kernel_param(c->st3, p3, W, H, c->kparam, p4, 4, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
                                    st));
     ISA_TRY(mark());
     // 4. per frame: LK refinement and robustness mask (Accumulate :1961-1977)
@@ -468,28 +475,28 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     const size_t hp3 = (size_t)Wh * 12, hp4 = (size_t)Wh * 16, fp = (size_t)W * sizeof(float2);
     float maxv = 0.f;
     for (int ch = 0; ch < 3; ch++) maxv = std::max(maxv, white[ch] + black[ch]);
-    ISA_CK(isa_launch_subsample(frame(ref), raw_pitch, W, H, cfa, maxv, c->half_ref, hp3, st));
+    ISA_LAUNCH(c, isa_launch_subsample(frame(ref), raw_pitch, W, H, cfa, maxv, c->half_ref, hp3, st));
     const int half = p->window_size_lk / 2;
     std::vector<isa_frame_in> fin;
     fin.push_back({frame(ref), nullptr, nullptr});
     for (int i = 0; i < n; i++) {
         if (i == ref) continue;
         float2* flow = c->flows + (size_t)i * fsz;
-        ISA_CK(isa_launch_subsample(frame(i), raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
-        ISA_CK(isa_launch_optimal(c->x, strat.n1, tcx0, tcy0, ref, i, c->tiles_opt, (size_t)tcx0 * sizeof(float2), st));
+        ISA_LAUNCH(c, isa_launch_subsample(frame(i), raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
+        ISA_LAUNCH(c, isa_launch_optimal(c->x, strat.n1, tcx0, tcy0, ref, i, c->tiles_opt, (size_t)tcx0 * sizeof(float2), st));
         float bs[2];
         prealign_shift(pre, ref, i, bs);
         // ping-pong so that the last iteration lands in `flow`
         float2* a = (p->iterations_lk & 1) ? c->flow_tmp : flow;
         float2* b = (p->iterations_lk & 1) ? flow : c->flow_tmp;
-        ISA_CK(isa_launch_flow_from_tiles(c->tiles_opt, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1], prealign_rot(pre, ref, i),
+        ISA_LAUNCH(c, isa_launch_flow_from_tiles(c->tiles_opt, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1], prealign_rot(pre, ref, i),
                                           a, fp, st));
         for (int it = 0; it < p->iterations_lk; it++) {
-            ISA_CK(isa_launch_lk_iteration(a, b, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, pitch, W, H, half, p->min_det_lk, st));
+            ISA_LAUNCH(c, isa_launch_lk_iteration(a, b, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, pitch, W, H, half, p->min_det_lk, st));
             std::swap(a, b);
         }
         float4* mask = c->masks + (size_t)i * Wh * Hh;
-        ISA_CK(isa_launch_robustness_erode(c->half_ref, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha, info->noise_beta,
+        ISA_LAUNCH(c, isa_launch_robustness_erode(c->half_ref, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha, info->noise_beta,
                                            p->threshold_m, p->robust_s, p->robust_t, p->erode_size, mask, hp4, st));
         fin.push_back({frame(i), flow, mask});
     }
@@ -498,20 +505,20 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     const size_t op = (size_t)g.Wo * 12;
     ISA_CK(cudaMemcpyAsync(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), cudaMemcpyHostToDevice, st));
     if (p->fused_accumulate) {
-        ISA_CK(isa_launch_accumulate(g, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum,
+        ISA_LAUNCH(c, isa_launch_accumulate(g, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum,
                                      op, 0, st));
     } else {
         ISA_CK(cudaMemsetAsync(c->acc, 0, op * g.Ho, st));
         ISA_CK(cudaMemsetAsync(c->wsum, 0, op * g.Ho, st));
         for (size_t f = 0; f < fin.size(); f++)
-            ISA_CK(isa_launch_accumulate(g, cfa, nullptr, 1, &fin[f], raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum, op, 1,
+            ISA_LAUNCH(c, isa_launch_accumulate(g, cfa, nullptr, 1, &fin[f], raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum, op, 1,
                                          st));
     }
     ISA_TRY(mark());
     // 6. ApplyWeighting (:1908-1917, :1994-2002)
     if (thr > 0)
-        ISA_CK(isa_launch_demosaic_gray(frame(ref), raw_pitch, W, H, cfa, black, scale, divisor, nullptr, 0, nullptr, 0, out, out_pitch, st));
-    ISA_CK(isa_launch_apply_weighting(out, out_pitch, c->acc, c->wsum, op, g.Wo, g.Ho, thr, st));
+        ISA_LAUNCH(c, isa_launch_demosaic_gray(frame(ref), raw_pitch, W, H, cfa, black, scale, divisor, nullptr, 0, nullptr, 0, out, out_pitch, st));
+    ISA_LAUNCH(c, isa_launch_apply_weighting(out, out_pitch, c->acc, c->wsum, op, g.Wo, g.Ho, thr, st));
     ISA_TRY(mark());
     c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1;
     return ISA_OK;
@@ -675,6 +682,8 @@ int isa_stage_times(isa_ctx* c, float* ms, int max_count)
     for (int i = 1; i < c->ev_count && k < max_count; i++, k++) ISA_CK(cudaEventElapsedTime(&ms[k], c->ev[i - 1], c->ev[i]));
     return k;
 }
+
+long isa_launch_count(isa_ctx* c) { return c ? c->launches : -1; }
 
 int isa_merge_burst(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
                     const isa_prealign* pre, float* out, size_t out_pitch, void* stream)

@@ -68,6 +68,7 @@ class IsaTrackPair(ctypes.Structure):
 # every symbol include/isa.h declares (checked by the CPU tests)
 EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
+    "isa_launch_count",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
@@ -94,6 +95,7 @@ def lib():
             f = getattr(L, name)
             if name not in ("isa_last_error", "isa_version", "isa_params_default"):
                 f.restype = ctypes.c_int
+        L.isa_launch_count.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -227,6 +229,9 @@ class Merger:
         if k < 0:
             check(k)
         return [ms[i] for i in range(k)]
+
+    def launch_count(self):
+        return int(lib().isa_launch_count(self.ctx))
 
     def debug(self, frame):
         ptrs = [ctypes.c_void_p() for _ in range(7)]

@@ -51,54 +51,61 @@ class Burst:
 
 
 def _render_scene(Wp, Hp, rng, torch, device, dtype):
-    """Procedural linear-RGB scene on a Wp x Hp grid, values in about [0.03, 0.9]."""
-    yy, xx = torch.meshgrid(torch.arange(Hp, device=device, dtype=dtype),
-                            torch.arange(Wp, device=device, dtype=dtype), indexing="ij")
+    """Procedural linear-RGB scene on a Wp x Hp grid, values in about [0.03, 0.9].
+    Each element is drawn inside its bounding box only."""
+    yy = torch.arange(Hp, device=device, dtype=dtype).view(Hp, 1)
+    xx = torch.arange(Wp, device=device, dtype=dtype).view(1, Wp)
     base = torch.tensor(rng.uniform(0.15, 0.45, 3), device=device, dtype=dtype)
     grad = torch.tensor(rng.uniform(-0.1, 0.1, (2, 3)), device=device, dtype=dtype)
     img = base.view(3, 1, 1) + grad[0].view(3, 1, 1) * (xx / Wp - 0.5) + grad[1].view(3, 1, 1) * (yy / Hp - 0.5)
+    img = img.contiguous()
     area = Wp * Hp
     unit = max(1, int(area / (512 * 384)))
-    scale = float(np.sqrt(area / (2048 * 1536)))
+    scale = max(float(np.sqrt(area / (2048 * 1536))), 0.25)
 
     def color(lo=-0.25, hi=0.25):
         return torch.tensor(rng.uniform(lo, hi, 3), device=device, dtype=dtype).view(3, 1, 1)
 
-    def window(cx, cy, hw, hh):
-        return ((xx - cx).abs() <= hw) & ((yy - cy).abs() <= hh)
+    def box(cx, cy, r):
+        x0, x1 = max(int(cx - r), 0), min(int(cx + r) + 1, Wp)
+        y0, y1 = max(int(cy - r), 0), min(int(cy + r) + 1, Hp)
+        return x0, x1, y0, y1
 
-    # Gaussian blobs
-    for _ in range(6 * unit):
+    def add(cx, cy, r, fn):
+        x0, x1, y0, y1 = box(cx, cy, r)
+        if x1 <= x0 or y1 <= y0:
+            return
+        X, Y = xx[:, x0:x1], yy[y0:y1, :]
+        img[:, y0:y1, x0:x1] += fn(X, Y)
+
+    for _ in range(6 * unit):  # Gaussian blobs
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
-        s = rng.uniform(4, 60) * max(scale, 0.25)
-        img = img + color() * torch.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2 * s * s))
-    # straight step edges inside a window
-    for _ in range(3 * unit):
+        s = rng.uniform(4, 60) * min(scale, 1.0)
+        c = color()
+        add(cx, cy, 4 * s, lambda X, Y: c * torch.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s)))
+    for _ in range(3 * unit):  # straight step edges inside a window
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
         th = rng.uniform(0, np.pi)
-        hw = rng.uniform(20, 160) * max(scale, 0.25)
-        side = ((xx - cx) * np.cos(th) + (yy - cy) * np.sin(th)) > 0
-        img = img + color() * (side & window(cx, cy, hw, hw)).to(dtype)
-    # curved edges: discs and rings
-    for _ in range(3 * unit):
+        hw = rng.uniform(20, 160) * min(scale, 1.0)
+        c = color()
+        add(cx, cy, hw, lambda X, Y: c * (((X - cx) * np.cos(th) + (Y - cy) * np.sin(th)) > 0).to(dtype))
+    for _ in range(3 * unit):  # curved edges: discs
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
-        r = rng.uniform(10, 120) * max(scale, 0.25)
-        d = torch.sqrt((xx - cx) ** 2 + (yy - cy) ** 2)
-        img = img + color() * (d < r).to(dtype)
-    # sinusoidal gratings, period 2..16 px
-    for _ in range(3 * unit):
+        r = rng.uniform(10, 120) * min(scale, 1.0)
+        c = color()
+        add(cx, cy, r + 1, lambda X, Y: c * (((X - cx) ** 2 + (Y - cy) ** 2) < r * r).to(dtype))
+    for _ in range(3 * unit):  # sinusoidal gratings, period 2..16 px
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
         period = rng.uniform(2, 16)
         th = rng.uniform(0, np.pi)
-        hw, hh = rng.uniform(20, 120) * max(scale, 0.25), rng.uniform(20, 120) * max(scale, 0.25)
-        ph = 2 * np.pi / period * ((xx - cx) * np.cos(th) + (yy - cy) * np.sin(th))
-        img = img + color(0.05, 0.2) * torch.sin(ph) * window(cx, cy, hw, hh).to(dtype)
-    # one checker patch
-    cx, cy = rng.uniform(0.2, 0.8) * Wp, rng.uniform(0.2, 0.8) * Hp
-    sq = int(rng.integers(4, 17))
-    hw = 80 * max(scale, 0.25)
-    chk = (((torch.floor(xx / sq) + torch.floor(yy / sq)) % 2) * 2 - 1)
-    img = img + color(0.1, 0.2) * chk * window(cx, cy, hw, hw).to(dtype)
+        hw = rng.uniform(20, 120) * min(scale, 1.0)
+        c = color(0.05, 0.2)
+        add(cx, cy, hw, lambda X, Y: c * torch.sin(2 * np.pi / period * ((X - cx) * np.cos(th) + (Y - cy) * np.sin(th))))
+    for _ in range(max(1, unit // 16)):  # checker patches
+        cx, cy = rng.uniform(0.1, 0.9) * Wp, rng.uniform(0.1, 0.9) * Hp
+        sq = int(rng.integers(4, 17))
+        c = color(0.1, 0.2)
+        add(cx, cy, 80, lambda X, Y: c * (((torch.floor(X / sq) + torch.floor(Y / sq)) % 2) * 2 - 1))
     return img.clamp(0.03, 0.9)
 
 

@@ -135,6 +135,9 @@ ISA_API int isa_output_size(const isa_params* p, int width, int height, int* out
  * images, tile alignment, kernel parameters, LK + robustness, accumulation,
  * finalize. Synchronises the context's events. Returns the count written. */
 ISA_API int isa_stage_times(isa_ctx* ctx, float* ms, int max_count);
+/* Number of this library's kernels the last isa_merge_burst launched
+ * (cuFFT's own kernels are not counted). */
+ISA_API long isa_launch_count(isa_ctx* ctx);
 
 /* ---- fused pipeline ------------------------------------------------------ */
 /* Whole forward merge of one burst (TrackPatches :1601 + PrepareAccumulation
