@@ -751,6 +751,23 @@ int isa_debug_shifts(isa_ctx* c, const void** one_to_one, int* tx, int* ty)
         if (!(cond)) return fail(ISA_EINVAL, "%s", msg); \
     } while (0)
 
+int isa_tracking_pairs(int n, int ref, int strategy, int block, int* pairs, int* rows, int max_pairs)
+{
+    if (n < 2 || ref < 0 || ref >= n) return fail(ISA_EINVAL, "frame count or reference out of range");
+    Strategy s;
+    if (!build_strategy(n, ref, strategy, block, s)) return fail(ISA_EINVAL, "inconsistent tracking strategy");
+    if (pairs || rows) {
+        if (max_pairs < s.m) return fail(ISA_EINVAL, "%d pairs do not fit in %d", s.m, max_pairs);
+        for (int k = 0; k < s.m; k++) {
+            if (pairs) { pairs[2 * k] = s.pairs[k].first; pairs[2 * k + 1] = s.pairs[k].second; }
+            if (rows) {
+                rows[3 * k] = s.a[k]; rows[3 * k + 1] = s.b[k]; rows[3 * k + 2] = s.sign[k];
+            }
+        }
+    }
+    return s.m;
+}
+
 int isa_debayer_full(const uint16_t* raw, size_t raw_pitch, int W, int H, const int cfa[4], const float black[3], const float scale[3],
                      const float divisor[3], float* out, size_t out_pitch, void* stream)
 {

@@ -26,7 +26,7 @@ __device__ __forceinline__ float bilinear_mirror(const float* img, size_t pitch,
     const float* r0 = isa::row_ptr(img, pitch, y0);
     const float* r1 = isa::row_ptr(img, pitch, y1);
     float p00 = __ldg(r0 + x0), p10 = __ldg(r0 + x1), p01 = __ldg(r1 + x0), p11 = __ldg(r1 + x1);
-    return (1.f - a) * (1.f - b) * p00 + a * (1.f - b) * p10 + (1.f - a) * b * p01 + a * b * p11;
+    return isa::lerp2(p00, p10, p01, p11, a, b);
 }
 
 // lucasKanadeOptim's pseudo-inverse (opticalFlow.cu:229-290) in FP64. For a
@@ -100,8 +100,8 @@ __global__ void k_flow_from_tiles(const float2* __restrict__ tiles, size_t tile_
     const float2* r0 = isa::row_ptr(tiles, tile_pitch, j0);
     const float2* r1 = isa::row_ptr(tiles, tile_pitch, j1);
     float2 p00 = r0[i0], p10 = r0[i1], p01 = r1[i0], p11 = r1[i1];
-    fx += (1.f - a) * (1.f - b) * p00.x + a * (1.f - b) * p10.x + (1.f - a) * b * p01.x + a * b * p11.x;
-    fy += (1.f - a) * (1.f - b) * p00.y + a * (1.f - b) * p10.y + (1.f - a) * b * p01.y + a * b * p11.y;
+    fx += isa::lerp2(p00.x, p10.x, p01.x, p11.x, a, b);
+    fy += isa::lerp2(p00.y, p10.y, p01.y, p11.y, a, b);
     isa::row_ptr(flow, flow_pitch, y)[x] = make_float2(fx, fy);
 }
 

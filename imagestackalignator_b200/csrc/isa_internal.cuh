@@ -28,6 +28,17 @@ ISA_DEV int mirror(int i, int n) {
     return j >= n ? p - 1 - j : j;
 }
 
+// Bilinear blend with the weights (1-a)(1-b), a(1-b), (1-a)b, ab, a and b in
+// [0, 1). Texels whose weight is zero do not contribute, so a non-finite
+// neighbour does not leak into an exact-texel sample.
+ISA_DEV float lerp2(float p00, float p10, float p01, float p11, float a, float b) {
+    float v = (1.f - a) * (1.f - b) * p00;
+    if (a != 0.f) v += a * (1.f - b) * p10;
+    if (b != 0.f) v += (1.f - a) * b * p01;
+    if (a != 0.f && b != 0.f) v += a * b * p11;
+    return v;
+}
+
 // CFA code at (x, y): cfa packed as 4 x 2 bits, (y&1)*2 + (x&1) selects.
 ISA_DEV int cfa_at(unsigned cfa, int x, int y) { return (cfa >> ((((y & 1) << 1) | (x & 1)) * 2)) & 3; }
 

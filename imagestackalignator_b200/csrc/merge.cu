@@ -95,10 +95,9 @@ __device__ __forceinline__ void kparam_sample(const float* kp, size_t pitch, int
     int i0 = isa::clampi(i, 0, W - 1), i1 = isa::clampi(i + 1, 0, W - 1), j0 = isa::clampi(j, 0, H - 1), j1 = isa::clampi(j + 1, 0, H - 1);
     const float* r0 = isa::row_ptr(kp, pitch, j0);
     const float* r1 = isa::row_ptr(kp, pitch, j1);
-    float w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
 #pragma unroll
     for (int c = 0; c < 3; c++)
-        k[c] = w00 * __ldg(r0 + KC * i0 + c) + w10 * __ldg(r0 + KC * i1 + c) + w01 * __ldg(r1 + KC * i0 + c) + w11 * __ldg(r1 + KC * i1 + c);
+        k[c] = isa::lerp2(__ldg(r0 + KC * i0 + c), __ldg(r0 + KC * i1 + c), __ldg(r1 + KC * i0 + c), __ldg(r1 + KC * i1 + c), a, b);
 }
 
 __device__ __forceinline__ float2 flow_sample(const float2* fl, size_t pitch, int W, int H, float xb, float yb)
@@ -111,8 +110,7 @@ __device__ __forceinline__ float2 flow_sample(const float2* fl, size_t pitch, in
     const float2* r0 = isa::row_ptr(fl, pitch, j0);
     const float2* r1 = isa::row_ptr(fl, pitch, j1);
     float2 p00 = __ldg(r0 + i0), p10 = __ldg(r0 + i1), p01 = __ldg(r1 + i0), p11 = __ldg(r1 + i1);
-    float w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
-    return make_float2(w00 * p00.x + w10 * p10.x + w01 * p01.x + w11 * p11.x, w00 * p00.y + w10 * p10.y + w01 * p01.y + w11 * p11.y);
+    return make_float2(isa::lerp2(p00.x, p10.x, p01.x, p11.x, a, b), isa::lerp2(p00.y, p10.y, p01.y, p11.y, a, b));
 }
 
 template <int KC>

@@ -21,10 +21,7 @@ __device__ __forceinline__ float2 flow_sample(const float2* flow, size_t pitch, 
     const float2* r0 = isa::row_ptr(flow, pitch, j0);
     const float2* r1 = isa::row_ptr(flow, pitch, j1);
     float2 p00 = __ldg(r0 + i0), p10 = __ldg(r0 + i1), p01 = __ldg(r1 + i0), p11 = __ldg(r1 + i1);
-    float2 o;
-    o.x = (1.f - a) * (1.f - b) * p00.x + a * (1.f - b) * p10.x + (1.f - a) * b * p01.x + a * b * p11.x;
-    o.y = (1.f - a) * (1.f - b) * p00.y + a * (1.f - b) * p10.y + (1.f - a) * b * p01.y + a * b * p11.y;
-    return o;
+    return make_float2(isa::lerp2(p00.x, p10.x, p01.x, p11.x, a, b), isa::lerp2(p00.y, p10.y, p01.y, p11.y, a, b));
 }
 
 // Mask value of interior half-res pixel (x, y); ref/mov are float3 images.

@@ -224,21 +224,36 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const int* __restrict__
         aug[i * na + n1] = sx; aug[i * na + n1 + 1] = sy;
     }
     int st = -1;
-    double scale = 0;
-    for (int i = 0; i < n1; i++) scale = fmax(scale, fabs(N0[i * n1 + i]));
-    const double tol = 1e-12 * (scale > 0 ? scale : 1.0);
+    __shared__ int s_piv;
+    __shared__ double s_tol, s_pval;
     for (int round_ = 0; round_ < 10; round_++) {
         __syncthreads();
-        // augmented copy; the rhs columns persist in aug[.][n1..n1+1] across rounds via P? keep separately:
         for (int i = tid; i < n1 * n1; i += blockDim.x) { int r = i / n1, c = i - r * n1; aug[r * na + c] = N[i]; }
         __syncthreads();
         // stash rhs (aug columns are destroyed by elimination)
         for (int i = tid; i < n1; i += blockDim.x) { P[2 * i] = aug[i * na + n1]; P[2 * i + 1] = aug[i * na + n1 + 1]; }
-        if (tid == 0) s_flag = 0;
+        if (tid == 0) {
+            s_flag = 0;
+            double sc = 0;
+            for (int i = 0; i < n1; i++) sc = fmax(sc, fabs(N[i * n1 + i]));
+            s_tol = 1e-12 * (sc > 0 ? sc : 1.0);
+        }
         __syncthreads();
+        // Gauss-Jordan with partial pivoting (first largest |pivot|), as the oracle
         for (int c = 0; c < n1; c++) {
-            double piv = aug[c * na + c];
-            if (!(fabs(piv) > tol)) { if (tid == 0) s_flag = 1; break; }
+            if (tid == 0) {
+                int pr = c;
+                for (int r = c + 1; r < n1; r++)
+                    if (fabs(aug[r * na + c]) > fabs(aug[pr * na + c])) pr = r;
+                s_piv = pr;
+                s_pval = aug[pr * na + c];
+            }
+            __syncthreads();
+            const int pr = s_piv;
+            const double piv = s_pval;
+            if (!(fabs(piv) > s_tol)) { if (tid == 0) s_flag = 1; break; }
+            if (pr != c)
+                for (int j = tid; j < na; j += blockDim.x) { double t = aug[c * na + j]; aug[c * na + j] = aug[pr * na + j]; aug[pr * na + j] = t; }
             __syncthreads();
             for (int j = tid; j < na; j += blockDim.x) if (j != c) aug[c * na + j] /= piv;
             __syncthreads();
@@ -268,30 +283,46 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const int* __restrict__
             for (int i = 0; i < n1; i++) { P[2 * (i + 1)] = P[2 * i] + xs[2 * i]; P[2 * (i + 1) + 1] = P[2 * i + 1] + xs[2 * i + 1]; }
         }
         __syncthreads();
+        // largest squared residual above 1; residuals within a relative 1e-9
+        // of it count as ties and the lowest row wins (order independent)
         double best = 1.0;
-        int bi = -1;
         for (int k = tid; k < m; k += blockDim.x) {
             if (!active[k]) continue;
             double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
             double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
             double dx = b[2 * k] - px, dy = b[2 * k + 1] - py;
-            double d = dx * dx + dy * dy;
-            if (d > best) { best = d; bi = k; }
+            best = fmax(best, dx * dx + dy * dy);
         }
-        // block arg-max, lowest index on ties (the reference scans rows in order)
-        for (int off = 16; off > 0; off >>= 1) {
-            double ov = __shfl_down_sync(0xffffffffu, best, off);
-            int oi = __shfl_down_sync(0xffffffffu, bi, off);
-            if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) { best = ov; bi = oi; }
-        }
-        if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
+        for (int off = 16; off > 0; off >>= 1) best = fmax(best, __shfl_down_sync(0xffffffffu, best, off));
+        if ((tid & 31) == 0) red_v[tid >> 5] = best;
         __syncthreads();
         if (tid == 0) {
             double bv = red_v[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); w++) bv = fmax(bv, red_v[w]);
+            red_v[0] = bv;
+        }
+        __syncthreads();
+        const double top = red_v[0];
+        int bi = 0x7fffffff;
+        if (top > 1.0) {
+            const double thr = top * (1 - 1e-9);
+            for (int k = tid; k < m; k += blockDim.x) {
+                if (!active[k]) continue;
+                double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
+                double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
+                double dx = b[2 * k] - px, dy = b[2 * k + 1] - py;
+                double d = dx * dx + dy * dy;
+                if (d >= thr && d > 1.0) { bi = k; break; }
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) bi = min(bi, __shfl_down_sync(0xffffffffu, bi, off));
+        __syncthreads();
+        if ((tid & 31) == 0) red_i[tid >> 5] = bi;
+        __syncthreads();
+        if (tid == 0) {
             int bj = red_i[0];
-            for (int w = 1; w < (int)(blockDim.x >> 5); w++)
-                if (red_i[w] >= 0 && (bj < 0 || red_v[w] > bv || (red_v[w] == bv && red_i[w] < bj))) { bv = red_v[w]; bj = red_i[w]; }
-            red_i[0] = bj;
+            for (int w = 1; w < (int)(blockDim.x >> 5); w++) bj = min(bj, red_i[w]);
+            red_i[0] = bj == 0x7fffffff ? -1 : bj;
         }
         __syncthreads();
         const int k = red_i[0];

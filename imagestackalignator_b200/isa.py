@@ -68,7 +68,7 @@ class IsaTrackPair(ctypes.Structure):
 # every symbol include/isa.h declares (checked by the CPU tests)
 EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
-    "isa_launch_count",
+    "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
@@ -153,6 +153,18 @@ def make_info(burst) -> IsaRawInfo:
     i.noise_alpha = float(burst.noise_a)
     i.noise_beta = float(burst.noise_b)
     return i
+
+
+def tracking_pairs(n, reference, strategy, block):
+    """(pairs m x 2 in tracking order, rows m x 3 = (a, b, sign) per measurement row)."""
+    m = lib().isa_tracking_pairs(n, reference, strategy, block, None, None, 0)
+    check(m if m < 0 else 0)
+    pairs = np.zeros((m, 2), np.int32)
+    rows = np.zeros((m, 3), np.int32)
+    got = lib().isa_tracking_pairs(n, reference, strategy, block, pairs.ctypes.data_as(ctypes.c_void_p),
+                                   rows.ctypes.data_as(ctypes.c_void_p), m)
+    check(got if got < 0 else 0)
+    return pairs, rows
 
 
 def output_size(p: IsaParams, width, height):

@@ -78,30 +78,30 @@ def _render_scene(Wp, Hp, rng, torch, device, dtype):
         X, Y = xx[:, x0:x1], yy[y0:y1, :]
         img[:, y0:y1, x0:x1] += fn(X, Y)
 
-    for _ in range(6 * unit):  # Gaussian blobs
+    for _ in range(24 * unit):  # Gaussian blobs
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
         s = rng.uniform(4, 60) * min(scale, 1.0)
         c = color()
         add(cx, cy, 4 * s, lambda X, Y: c * torch.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s)))
-    for _ in range(3 * unit):  # straight step edges inside a window
+    for _ in range(8 * unit):  # straight step edges inside a window
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
         th = rng.uniform(0, np.pi)
         hw = rng.uniform(20, 160) * min(scale, 1.0)
         c = color()
         add(cx, cy, hw, lambda X, Y: c * (((X - cx) * np.cos(th) + (Y - cy) * np.sin(th)) > 0).to(dtype))
-    for _ in range(3 * unit):  # curved edges: discs
+    for _ in range(8 * unit):  # curved edges: discs
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
         r = rng.uniform(10, 120) * min(scale, 1.0)
         c = color()
         add(cx, cy, r + 1, lambda X, Y: c * (((X - cx) ** 2 + (Y - cy) ** 2) < r * r).to(dtype))
-    for _ in range(3 * unit):  # sinusoidal gratings, period 2..16 px
+    for _ in range(6 * unit):  # sinusoidal gratings, period 2..16 px
         cx, cy = rng.uniform(0, Wp), rng.uniform(0, Hp)
         period = rng.uniform(2, 16)
         th = rng.uniform(0, np.pi)
         hw = rng.uniform(20, 120) * min(scale, 1.0)
         c = color(0.05, 0.2)
         add(cx, cy, hw, lambda X, Y: c * torch.sin(2 * np.pi / period * ((X - cx) * np.cos(th) + (Y - cy) * np.sin(th))))
-    for _ in range(max(1, unit // 16)):  # checker patches
+    for _ in range(max(1, unit // 8)):  # checker patches
         cx, cy = rng.uniform(0.1, 0.9) * Wp, rng.uniform(0.1, 0.9) * Hp
         sq = int(rng.integers(4, 17))
         c = color(0.1, 0.2)

@@ -161,6 +161,13 @@ ISA_API int isa_debug_buffers(isa_ctx* ctx, int frame, const void** flow, size_t
  * of the finest level (tiles x (n-1) float2, device) and its tile counts. */
 ISA_API int isa_debug_shifts(isa_ctx* ctx, const void** one_to_one, int* tiles_x, int* tiles_y);
 
+/* ShiftCollection pair bookkeeping (ShiftCollection.cs:100-512), host only:
+ * returns the pair count m; pairs (m x 2, optional) = (reference, toTrack)
+ * in tracking order (FillShiftPairs / GetShiftPairs); rows (m x 3, optional)
+ * = incidence interval [a, b) and sign of measurement row k (FillIndexTable
+ * order, CreateShiftMatrix). */
+ISA_API int isa_tracking_pairs(int n, int reference, int strategy, int block_size, int* pairs, int* rows, int max_pairs);
+
 /* ---- operator API: one entry point per reference kernel wrapper ----------- */
 /* DeBayerFullRes (controller :1268-1311): NPP Convert + Set(0) +
  * deBayerGreenKernel (DeBayerKernels.cs:36-44) + deBayerRedBlueKernel

@@ -48,7 +48,8 @@ static inline int mirror_index(int i, int n) {
 }
 
 /* Exact bilinear sample of channel c of a (h x w x ch) image at texel-space
- * position (xb, yb) = (u*w - 0.5, v*h - 0.5); mode 0 clamps, 1 mirrors. */
+ * position (xb, yb) = (u*w - 0.5, v*h - 0.5); mode 0 clamps, 1 mirrors.
+ * (The hardware keeps 8 fractional bits of the weights; exact weights here.) */
 static real bilinear(const real* img, int w, int h, int ch, int c, real xb, real yb, int mirror) {
     real fx = floor(xb), fy = floor(yb);
     int i = (int)fx, j = (int)fy;
@@ -56,9 +57,14 @@ static real bilinear(const real* img, int w, int h, int ch, int c, real xb, real
     int i0, i1, j0, j1;
     if (mirror) { i0 = mirror_index(i, w); i1 = mirror_index(i + 1, w); j0 = mirror_index(j, h); j1 = mirror_index(j + 1, h); }
     else { i0 = clampi(i, 0, w - 1); i1 = clampi(i + 1, 0, w - 1); j0 = clampi(j, 0, h - 1); j1 = clampi(j + 1, 0, h - 1); }
-    real p00 = img[((size_t)j0 * w + i0) * ch + c], p10 = img[((size_t)j0 * w + i1) * ch + c];
-    real p01 = img[((size_t)j1 * w + i0) * ch + c], p11 = img[((size_t)j1 * w + i1) * ch + c];
-    return (1 - a) * (1 - b) * p00 + a * (1 - b) * p10 + (1 - a) * b * p01 + a * b * p11;
+    /* texels with zero weight are not read, so a non-finite neighbour only
+     * affects samples that actually weight it */
+    real v = 0;
+    if (a != 1 && b != 1) v += (1 - a) * (1 - b) * img[((size_t)j0 * w + i0) * ch + c];
+    if (a != 0 && b != 1) v += a * (1 - b) * img[((size_t)j0 * w + i1) * ch + c];
+    if (a != 1 && b != 0) v += (1 - a) * b * img[((size_t)j1 * w + i0) * ch + c];
+    if (a != 0 && b != 0) v += a * b * img[((size_t)j1 * w + i1) * ch + c];
+    return v;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -126,15 +132,19 @@ EXPORT void orc_debayer_full(const uint16_t* raw, int W, int H, const int* cfa,
     free(g);
 }
 
-/* A2: sRGB gamma with NaN -> 0 and clamp to [0,1] (kernel.cu:290-332). */
+/* A2: sRGB gamma with NaN -> 0 and clamp to [0,1] (kernel.cu:290-332). The
+ * constants are the reference's float literals (e.g. 1.0f / 2.4f is a float
+ * quotient), carried into double exactly. */
 EXPORT void orc_gamma_srgb(real* rgb, int W, int H)
 {
+    const real knee = (real)0.0031308f, slope = (real)12.92f, gain = (real)(1.0f + 0.055f);
+    const real expo = (real)(1.0f / 2.4f), off = (real)0.055f;
     size_t n = (size_t)W * H * 3;
     for (size_t i = 0; i < n; i++) {
         real v = rgb[i];
         if (isnan(v)) v = 0;
         v = v < 0 ? 0 : (v > 1 ? 1 : v);
-        rgb[i] = v <= 0.0031308 ? 12.92 * v : (1.0 + 0.055) * pow(v, 1.0 / 2.4) - 0.055;
+        rgb[i] = v <= knee ? slope * v : gain * pow(v, expo) - off;
     }
 }
 
@@ -442,14 +452,24 @@ EXPORT void orc_solve_shifts(const real* Aorig, int m, int n1, int tiles, real* 
                     for (int j = 0; j < n1; j++) s += Ni[i * n1 + j] * rhs[j * 2 + c];
                     sol[i * 2 + c] = s;
                 }
+            /* largest squared residual above 1 (checkForOutliers,
+             * ShiftMinimizerKernels.cu:104-117); residuals within a relative
+             * 1e-9 of the largest count as ties and the lowest row wins, so the
+             * choice does not depend on rounding when two rows are equal in
+             * exact arithmetic */
             double worst = 1;
             int wi = -1;
-            for (int k = 0; k < m; k++) {
-                double px = 0, py = 0;
-                for (int j = 0; j < n1; j++) { px += A[k * n1 + j] * sol[j * 2]; py += A[k * n1 + j] * sol[j * 2 + 1]; }
-                double dx = b[k * 2] - px, dy = b[k * 2 + 1] - py;
-                double d = dx * dx + dy * dy;
-                if (d > worst) { worst = d; wi = k; }
+            for (int pass = 0; pass < 2; pass++) {
+                double thr = worst * (1 - 1e-9);
+                for (int k = 0; k < m; k++) {
+                    double px = 0, py = 0;
+                    for (int j = 0; j < n1; j++) { px += A[k * n1 + j] * sol[j * 2]; py += A[k * n1 + j] * sol[j * 2 + 1]; }
+                    double dx = b[k * 2] - px, dy = b[k * 2 + 1] - py;
+                    double d = dx * dx + dy * dy;
+                    if (pass == 0) { if (d > worst) { worst = d; wi = k; } }
+                    else if (wi >= 0 && d >= thr && d > 1) { wi = k; break; }
+                }
+                if (wi < 0) break;
             }
             st = wi;
             if (wi < 0) break;
@@ -674,7 +694,7 @@ EXPORT void orc_robustness_mask(const real* ref, const real* mov, int Wh, int Hh
             for (int c = 0; c < 3; c++) {
                 real sr = sqrt(sd[c] / 9);
                 real smd = sqrt(alpha * mr[c] + beta);
-                if (c == 1) smd /= sqrt(2.0);
+                if (c == 1) smd /= (real)sqrtf(2.0f); /* the float constant of the reference */
                 real dist = fabs(mr[c] - mm[c]) * (sr * sr / (sr * sr + smd * smd));
                 real sig = fmax(smd, sr);
                 real v = sgain * exp(-dist * dist / (sig * sig)) - t_lit;

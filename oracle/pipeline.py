@@ -101,7 +101,7 @@ class StageLib:
 
     def track_pair(self, img_trk, img_ref, T, S, tcx, tcy, pre, base_ref, rot_ref, base_trk, rot_trk, thr, want_scores=False):
         Hl, Wl = img_trk.shape
-        pre = self.arr(pre)
+        pre = self.arr(pre).copy()
         D = 2 * S + 1
         scores = np.empty((tcy * tcx, D * D), self.dtype) if want_scores else None
         R = self.R
@@ -177,7 +177,7 @@ class StageLib:
         self.kf("debayer_subsample")(_p(np.ascontiguousarray(raw)), W, H, _p(c), self.R(max_val), _p(out))
         return out
 
-    def robustness_mask(self, ref, mov, flow, alpha, beta, thr_m, mask, s=1.5, t=0.12):
+    def robustness_mask(self, ref, mov, flow, alpha, beta, thr_m, mask, s=1.5, t=float(np.float32(0.12))):
         Hh, Wh, _ = ref.shape
         Hf, Wf, _ = flow.shape
         mask = self.arr(mask).copy()
@@ -200,7 +200,8 @@ class StageLib:
         st = self.arr(st).copy()
         H, W, _ = st.shape
         R = self.R
-        self.kf("kernel_param")(_p(st), W, H, R(p.dth), R(p.dtr), R(p.k_detail), R(p.k_denoise), R(p.k_stretch), R(p.k_shrink))
+        self.kf("kernel_param")(_p(st), W, H, R(p.f32("dth")), R(p.f32("dtr")), R(p.f32("k_detail")), R(p.f32("k_denoise")),
+                                R(p.f32("k_stretch")), R(p.f32("k_shrink")))
         return st
 
     def apply_weighting(self, img, acc, wsum, thr):
@@ -459,7 +460,7 @@ def merge_burst(burst, p: P.MergeParams = None, kind="oracle64", pre: Optional[P
             ix, iy, it = lib.derivatives(warped, bw_acc[ref])
             flow = lib.lucas_kanade(flow, ix, iy, it, p.window_size_lk // 2, p.f32("min_det_lk"))
         mask = lib.robustness_mask(ref_half, mov_half, flow, float(np.float32(burst.noise_a)), float(np.float32(burst.noise_b)),
-                                   p.f32("threshold_m"), mask, p.robust_s, p.robust_t)
+                                   p.f32("threshold_m"), mask, p.f32("robust_s"), p.f32("robust_t"))
         eroded = lib.erode(mask, p.erode_size)
         if keep is not None:
             keep.setdefault("flow", {})[i] = flow

@@ -105,8 +105,15 @@ static inline void isa_ref_fetch(const isa_ref_tex* t, float u, float v, float* 
     const float* p10 = isa_ref_texel(t, i + 1, j);
     const float* p01 = isa_ref_texel(t, i, j + 1);
     const float* p11 = isa_ref_texel(t, i + 1, j + 1);
-    for (int c = 0; c < t->channels; c++)
-        out[c] = (1 - a) * (1 - b) * p00[c] + a * (1 - b) * p10[c] + (1 - a) * b * p01[c] + a * b * p11[c];
+    // texels with zero weight are skipped (a non-finite neighbour does not leak)
+    for (int c = 0; c < t->channels; c++) {
+        float v = 0;
+        if (a != 1 && b != 1) v += (1 - a) * (1 - b) * p00[c];
+        if (a != 0 && b != 1) v += a * (1 - b) * p10[c];
+        if (a != 1 && b != 0) v += (1 - a) * b * p01[c];
+        if (a != 0 && b != 0) v += a * b * p11[c];
+        out[c] = v;
+    }
 }
 
 template <class T> static inline T tex2D(cudaTextureObject_t obj, float u, float v);
