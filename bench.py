@@ -299,7 +299,14 @@ def main():
     ap.add_argument("--per-frame", action="store_true", help="accumulate frame by frame (reference layout) instead of fused")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", default=None, help="WxH override for profiling runs on a smaller burst (not a bench line)")
+    ap.add_argument("--frames", type=int, default=None, help="frame-count override for profiling runs (not a bench line)")
     args = ap.parse_args()
+    if args.size:
+        w, h = args.size.lower().split("x")
+        WORKLOAD["width"], WORKLOAD["height"] = int(w), int(h)
+    if args.frames:
+        WORKLOAD["frames"] = args.frames
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

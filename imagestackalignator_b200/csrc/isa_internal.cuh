@@ -126,5 +126,9 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
                                   const isa_frame_in* single, size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch,
                                   int kparam_channels, const float* white, const float* black, float* acc, float* wsum,
                                   size_t out_pitch, int accumulate_into, cudaStream_t st);
+cudaError_t isa_launch_accumulate_x2(const isa_accum_geom& g, unsigned cfa, const isa_frame_in* frames, int nframes, const isa_frame_in* single,
+                                     size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch,
+                                     const float* white, const float* black, float* acc, float* wsum, size_t out_pitch, int accumulate_into,
+                                     cudaStream_t st);
 cudaError_t isa_launch_apply_weighting(float* img, size_t img_pitch, const float* acc, const float* wsum, size_t pitch, int W, int H,
                                        float thr, cudaStream_t st);

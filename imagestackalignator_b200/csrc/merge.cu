@@ -231,6 +231,9 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
                                   const float* white, const float* black, float* acc, float* wsum, size_t out_pitch, int accumulate_into,
                                   cudaStream_t st)
 {
+    if (g.s_int == 2 && kparam_channels == 4)
+        return isa_launch_accumulate_x2(g, cfa, frames, nframes, single, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, white, black, acc,
+                                        wsum, out_pitch, accumulate_into, st);
     F3 wh, bl;
     for (int c = 0; c < 3; c++) { wh.v[c] = white[c]; bl.v[c] = black[c]; }
     isa_frame_in one = single ? *single : isa_frame_in{nullptr, nullptr, nullptr};
