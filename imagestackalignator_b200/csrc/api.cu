@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -351,7 +352,9 @@ void prealign_shift(const isa_prealign* pre, int from, int to, float out[2])
     out[1] = pre->shifts[2 * to + 1] - pre->shifts[2 * from + 1];
 }
 
-int upload_strategy(isa_ctx* c, const Strategy& s, cudaStream_t st)
+// Copies the solver's row tables (interval, sign, grid of each measurement
+// row) and N0 = A^T A into device memory at the given addresses.
+int upload_rows(int* d_a, int* d_b, int* d_sign, int* d_grid, double* d_N0, const Strategy& s, cudaStream_t st)
 {
     std::vector<double> N0((size_t)s.n1 * s.n1, 0.0);
     for (int k = 0; k < s.m; k++)
@@ -359,13 +362,18 @@ int upload_strategy(isa_ctx* c, const Strategy& s, cudaStream_t st)
             for (int j = s.a[k]; j < s.b[k]; j++) N0[(size_t)i * s.n1 + j] += 1.0;
     std::vector<int> rg(s.m);
     for (int k = 0; k < s.m; k++) rg[k] = k;  // grid k holds measurement row k
-    ISA_CK(cudaMemcpyAsync(c->row_a, s.a.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(c->row_b, s.b.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(c->row_sign, s.sign.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(c->row_grid, rg.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(c->N0, N0.data(), N0.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(d_a, s.a.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(d_b, s.b.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(d_sign, s.sign.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(d_grid, rg.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(d_N0, N0.data(), N0.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     // pageable sources: the copies above complete before returning
     return ISA_OK;
+}
+
+int upload_strategy(isa_ctx* c, const Strategy& s, cudaStream_t st)
+{
+    return upload_rows(c->row_a, c->row_b, c->row_sign, c->row_grid, c->N0, s, st);
 }
 
 int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
@@ -1010,4 +1018,69 @@ int isa_apply_weighting(float* img, const float* acc, const float* wsum, size_t 
 }
 
 }  // extern "C"
+
+// ---- shift solve without a context ------------------------------------------
+// isa_solve_shifts needs an isa_ctx only for its row tables, and creating a
+// context allocates device memory. Some hosts cannot do that at the point
+// where they align tiles: the device memory belongs to another allocator
+// that has handed it all out, or the caller works under a fixed memory
+// budget, or it must not enter cudaMalloc because an allocation can
+// synchronise the device and stall work on other streams. For them the row
+// tables live in this file-scope device array, created with the module and
+// kept until the process exits on every GPU that loads the library.
+namespace {
+
+constexpr int kStaticMaxRows = 2048;  // measurement rows (frame pairs)
+constexpr int kStaticMaxN1 = 64;      // one-to-one shifts (frames - 1)
+
+struct StaticSolveTables {
+    int a[kStaticMaxRows], b[kStaticMaxRows], sign[kStaticMaxRows], grid[kStaticMaxRows];
+    double N0[kStaticMaxN1 * kStaticMaxN1];
+};
+
+static __device__ __align__(256) unsigned char g_solve_scratch[sizeof(StaticSolveTables)];
+
+// Device address of g_solve_scratch per device. In host code the symbol is
+// only a handle, so the address is asked for once per device (with that
+// device current) and cached.
+std::mutex g_scratch_lock;
+StaticSolveTables* g_scratch_addr[64] = {};
+
+int static_tables(StaticSolveTables** out)
+{
+    int dev = 0;
+    ISA_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(ISA_EINVAL, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_lock);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);
+        if (e != cudaSuccess) return fail(ISA_ECUDA, "cudaGetSymbolAddress(g_solve_scratch): %s", cudaGetErrorString(e));
+        g_scratch_addr[dev] = (StaticSolveTables*)p;
+    }
+    *out = g_scratch_addr[dev];
+    return ISA_OK;
+}
+
+}  // namespace
+
+extern "C" int isa_solve_shifts_static(int n, int ref, int strategy, int block, void* grids, size_t grid_pitch, size_t grid_stride, int tcx,
+                                       int tcy, void* x, int* status, void* stream)
+{
+    ISA_REQ(grids && x && status && tcx > 0 && tcy > 0, "bad argument");
+    ISA_REQ(n >= 2 && ref >= 0 && ref < n, "frame count or reference out of range");
+    if (n - 1 > kStaticMaxN1) return fail(ISA_EINVAL, "%d frames exceed the static limit of %d", n, kStaticMaxN1 + 1);
+    Strategy s;
+    ISA_REQ(build_strategy(n, ref, strategy, block, s), "inconsistent tracking strategy");
+    if (s.m > kStaticMaxRows) return fail(ISA_EINVAL, "%d frame pairs exceed the static limit of %d", s.m, kStaticMaxRows);
+    StaticSolveTables* t = nullptr;
+    ISA_TRY(static_tables(&t));
+    // every entry the kernel reads (m rows, n1 x n1 of N0) is rewritten here
+    ISA_TRY(upload_rows(t->a, t->b, t->sign, t->grid, t->N0, s, S(stream)));
+    cudaError_t e = isa_launch_solve(t->a, t->b, t->sign, t->N0, s.m, s.n1, (float2*)grids, grid_pitch, grid_stride, t->grid, tcx, tcy, (float2*)x,
+                                     status, S(stream));
+    if (e == cudaErrorInvalidValue) return fail(ISA_EINVAL, "solver shared memory exceeds the limit (m=%d, n-1=%d)", s.m, s.n1);
+    ISA_CK(e);
+    return ISA_OK;
+}
 

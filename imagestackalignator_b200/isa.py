@@ -71,7 +71,7 @@ EXPORTS = [
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
-    "isa_solve_shifts", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
+    "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
 ]

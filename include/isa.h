@@ -217,6 +217,19 @@ ISA_API int isa_upsample_shifts(const void* in, size_t in_pitch, size_t in_strid
  * >= 0 row removed in the tenth round) are outputs. Needs ctx scratch. */
 ISA_API int isa_solve_shifts(isa_ctx* ctx, int n, int reference, int strategy, int block_size, void* grids, size_t grid_pitch,
                      size_t grid_stride, int tiles_x, int tiles_y, void* one_to_one, int* status, void* stream);
+/* The same solve for callers that cannot allocate device memory where they
+ * align tiles (their device memory is owned by another allocator, they run
+ * under a fixed budget, or they must not risk the device-wide synchronisation
+ * an allocation can cause). No counterpart in the reference: it replaces
+ * isa_solve_shifts' context scratch by a library-owned static device array
+ * that every GPU loading the library keeps until exit. Limits: at most 2048
+ * frame pairs and 65 frames (ISA_EINVAL beyond). Allocates nothing; the
+ * first call on a device looks up the array's address, so make it before any
+ * stream capture. All calls share the array: calls that overlap on the GPU
+ * (different streams, or several host threads) race and must be serialised
+ * by the caller. Inputs and outputs as isa_solve_shifts. */
+ISA_API int isa_solve_shifts_static(int n, int reference, int strategy, int block_size, void* grids, size_t grid_pitch, size_t grid_stride,
+                                    int tiles_x, int tiles_y, void* one_to_one, int* status, void* stream);
 /* getOptimalShiftsKernel (ShiftMinimizerKernels.cs): shift of frame
  * to_track relative to reference from the one-to-one shifts. */
 ISA_API int isa_optimal_shifts(const void* one_to_one, int n, int tiles_x, int tiles_y, int reference, int to_track, void* out,
