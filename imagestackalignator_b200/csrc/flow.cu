@@ -35,11 +35,13 @@ __device__ __forceinline__ float bilinear_mirror(const float* img, size_t pitch,
 // relative; below that the reference's own construction is evaluated.
 // Returns false where the reference leaves the pixel unchanged
 // (sigma1 < minDet; the reference tests min(sigma1, sigma1)).
-__device__ bool lk_pinv(double a, double b, double d, double min_det, double M[4])
+__device__ __forceinline__ bool lk_pinv(double a, double b, double d, double min_det, double (&M)[4])
 {
+    // the largest eigenvalue only steers two threshold tests, so a float
+    // square root is enough (the reference compares sigma1 with minDet and
+    // the branch point is a conditioning bound)
     double hd = 0.5 * (a - d);
-    double disc = sqrt(hd * hd + b * b);
-    double l1 = 0.5 * (a + d) + disc;
+    double l1 = 0.5 * (a + d) + (double)sqrtf((float)(hd * hd + b * b));
     double det = a * d - b * b;
     if (det > 1e-3 * l1 * l1) {
         if (l1 < min_det) return false;
@@ -170,113 +172,125 @@ __global__ void k_lk_sums(float2* flow, size_t flow_pitch, const float* __restri
 
 constexpr int LK_TW = 32, LK_TH = 16;
 
-struct LkSmem {
-    int h, R, EW, EH, GW, GH;
-    size_t off_w, off_r, off_p, off_hs, off_vs, total;
+// Tile geometry for half window H: warped/reference images over the tile
+// plus an (H + 2) halo (E), gradient products over the tile plus an H halo
+// (G), per-column vertical window sums of the products for the tile rows,
+// stored with one leading slot per row for the in-place prefix sum (V).
+template <int H>
+struct LkDims {
+    static constexpr int R = H + 2, EW = LK_TW + 2 * R, EH = LK_TH + 2 * R;
+    static constexpr int GW = LK_TW + 2 * H, GH = LK_TH + 2 * H, GN = GW * GH, WIN = 2 * H + 1;
+    static constexpr int VS = GW + 1;
+    static constexpr size_t E_BYTES = (size_t)EW * EH * 4;
+    static constexpr size_t P_BYTES = (size_t)5 * GN * 4;
+    static constexpr size_t OFF_R = E_BYTES, OFF_P = 2 * E_BYTES, OFF_V = (OFF_P + P_BYTES + 15) / 16 * 16;
+    static constexpr size_t TOTAL = OFF_V + (size_t)5 * LK_TH * VS * 8;
 };
 
-__host__ __device__ inline LkSmem lk_smem_layout(int h)
-{
-    LkSmem L;
-    L.h = h; L.R = h + 2;
-    L.EW = LK_TW + 2 * L.R; L.EH = LK_TH + 2 * L.R;
-    L.GW = LK_TW + 2 * h; L.GH = LK_TH + 2 * h;
-    size_t e = (size_t)L.EW * L.EH * sizeof(float);
-    size_t p = (size_t)5 * L.GW * L.GH * sizeof(float);
-    size_t hs = (size_t)5 * LK_TW * L.GH * sizeof(double);
-    size_t vs = (size_t)5 * LK_TW * LK_TH * sizeof(double);
-    L.off_w = 0;
-    L.off_r = e;
-    L.off_p = 2 * e;
-    L.off_hs = (L.off_p + p + 15) & ~(size_t)15;
-    L.off_vs = L.off_p;  // products are dead once the horizontal sums exist
-    if (vs > p) L.off_vs = (L.off_hs + hs + 15) & ~(size_t)15;
-    L.total = (L.off_vs == L.off_p) ? L.off_hs + hs : L.off_vs + vs;
-    return L;
-}
-
+// One reference iteration (warp, Set(0) x3, derivatives, lucasKanadeOptim)
+// for a 32 x 16 tile, blockDim (32, 8). Window sums: FP32 products summed in
+// FP64, first down each column with a sliding window (exact: FP64 holds the
+// sum of a few FP32 values), then along each row through a prefix sum.
+template <int H>
 __global__ void __launch_bounds__(256) k_lk_iteration(const float2* __restrict__ flow_in, float2* __restrict__ flow_out, size_t flow_pitch,
                                                      const float* __restrict__ src, const float* __restrict__ ref, size_t img_pitch, int W,
-                                                     int H, int h, float min_det)
+                                                     int Himg, float min_det)
 {
+    using D = LkDims<H>;
     extern __shared__ __align__(16) unsigned char smem[];
-    const LkSmem L = lk_smem_layout(h);
-    float* Ew = (float*)(smem + L.off_w);
-    float* Er = (float*)(smem + L.off_r);
-    float* Pr = (float*)(smem + L.off_p);
-    double* Hs = (double*)(smem + L.off_hs);
-    double* Vs = (double*)(smem + L.off_vs);
+    float* Ew = (float*)smem;
+    float* Er = (float*)(smem + D::OFF_R);
+    float* P = (float*)(smem + D::OFF_P);
+    double* V = (double*)(smem + D::OFF_V);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const int x0 = blockIdx.x * LK_TW, y0 = blockIdx.y * LK_TH;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int R = L.R, EW = L.EW, EH = L.EH, GW = L.GW, GH = L.GH;
-    // 1. warped source and reference over the tile + (h + 2) halo, mirrored at the image border
-    for (int i = tid; i < EW * EH; i += nt) {
-        int ey = i / EW, ex = i - ey * EW;
-        int mx = isa::mirror(x0 - R + ex, W), my = isa::mirror(y0 - R + ey, H);
-        float2 f = __ldg(isa::row_ptr(flow_in, flow_pitch, my) + mx);
-        Ew[i] = bilinear_mirror(src, img_pitch, W, H, mx, my, f.x, f.y);
-        Er[i] = __ldg(isa::row_ptr(ref, img_pitch, my) + mx);
-    }
-    __syncthreads();
-    // 2. derivatives and their products over the tile + h halo
-    const int GN = GW * GH;
-    for (int i = tid; i < GN; i += nt) {
-        int gy = i / GW, gx = i - gy * GW;
-        int e = (gy + 2) * EW + gx + 2;
-        float t0 = (Ew[e + 2] - Ew[e + 1] * 8.0f + Ew[e - 1] * 8.0f - Ew[e - 2]) / 12.0f;
-        float t1 = (Er[e + 2] - Er[e + 1] * 8.0f + Er[e - 1] * 8.0f - Er[e - 2]) / 12.0f;
-        float dx = (t0 + t1) * 0.5f;
-        t0 = (Ew[e + 2 * EW] - Ew[e + EW] * 8.0f + Ew[e - EW] * 8.0f - Ew[e - 2 * EW]) / 12.0f;
-        t1 = (Er[e + 2 * EW] - Er[e + EW] * 8.0f + Er[e - EW] * 8.0f - Er[e - 2 * EW]) / 12.0f;
-        float dy = (t0 + t1) * 0.5f;
-        float dt = Ew[e] - Er[e];
-        Pr[i] = dx * dx;
-        Pr[GN + i] = dx * dy;
-        Pr[2 * GN + i] = dy * dy;
-        Pr[3 * GN + i] = dx * dt;
-        Pr[4 * GN + i] = dy * dt;
-    }
-    __syncthreads();
-    // 3. horizontal sliding sums (exact in FP64 for FP32 inputs of moderate range)
-    const int win = 2 * h + 1;
-    for (int job = tid; job < 5 * GH; job += nt) {
-        int ch = job / GH, gy = job - ch * GH;
-        const float* row = Pr + ch * GN + gy * GW;
-        double* out = Hs + (size_t)(ch * GH + gy) * LK_TW;
-        double s = 0;
-        for (int k = 0; k < win; k++) s += (double)row[k];
-        out[0] = s;
-        for (int x = 1; x < LK_TW; x++) {
-            s += (double)row[x + win - 1] - (double)row[x - 1];
-            out[x] = s;
+    // 1. warped source and reference, mirrored at the image border
+    for (int ey = ty; ey < D::EH; ey += 8) {
+        const int my = isa::mirror(y0 - D::R + ey, Himg);
+        const float2* frow = isa::row_ptr(flow_in, flow_pitch, my);
+        const float* rrow = isa::row_ptr(ref, img_pitch, my);
+        for (int ex = tx; ex < D::EW; ex += 32) {
+            const int mx = isa::mirror(x0 - D::R + ex, W);
+            const float2 f = __ldg(frow + mx);
+            Ew[ey * D::EW + ex] = bilinear_mirror(src, img_pitch, W, Himg, mx, my, f.x, f.y);
+            Er[ey * D::EW + ex] = __ldg(rrow + mx);
         }
     }
     __syncthreads();
-    // 4. vertical sliding sums
-    for (int job = tid; job < 5 * LK_TW; job += nt) {
-        int ch = job / LK_TW, x = job - ch * LK_TW;
-        const double* col = Hs + (size_t)ch * GH * LK_TW + x;
-        double* out = Vs + (size_t)ch * LK_TH * LK_TW + x;
-        double s = 0;
-        for (int k = 0; k < win; k++) s += col[k * LK_TW];
-        out[0] = s;
+    // 2. derivatives (five-tap, averaged over both images) and products
+    for (int gy = ty; gy < D::GH; gy += 8)
+        for (int gx = tx; gx < D::GW; gx += 32) {
+            const int e = (gy + 2) * D::EW + gx + 2;
+            float t0 = (Ew[e + 2] - Ew[e + 1] * 8.0f + Ew[e - 1] * 8.0f - Ew[e - 2]) / 12.0f;
+            float t1 = (Er[e + 2] - Er[e + 1] * 8.0f + Er[e - 1] * 8.0f - Er[e - 2]) / 12.0f;
+            const float dx = (t0 + t1) * 0.5f;
+            t0 = (Ew[e + 2 * D::EW] - Ew[e + D::EW] * 8.0f + Ew[e - D::EW] * 8.0f - Ew[e - 2 * D::EW]) / 12.0f;
+            t1 = (Er[e + 2 * D::EW] - Er[e + D::EW] * 8.0f + Er[e - D::EW] * 8.0f - Er[e - 2 * D::EW]) / 12.0f;
+            const float dy = (t0 + t1) * 0.5f;
+            const float dt = Ew[e] - Er[e];
+            const int g = gy * D::GW + gx;
+            P[g] = dx * dx;
+            P[D::GN + g] = dx * dy;
+            P[2 * D::GN + g] = dy * dy;
+            P[3 * D::GN + g] = dx * dt;
+            P[4 * D::GN + g] = dy * dt;
+        }
+    __syncthreads();
+    // 3. vertical sliding sums per (channel, column)
+    for (int job = tid; job < 5 * D::GW; job += 256) {
+        const int ch = job / D::GW, gx = job - ch * D::GW;
+        const float* col = P + ch * D::GN + gx;
+        double* out = V + (size_t)ch * LK_TH * D::VS + 1 + gx;
+        double sum = 0;
+#pragma unroll
+        for (int k = 0; k < D::WIN; k++) sum += (double)col[k * D::GW];
+        out[0] = sum;
+#pragma unroll 4
         for (int y = 1; y < LK_TH; y++) {
-            s += col[(y + win - 1) * LK_TW] - col[(y - 1) * LK_TW];
-            out[y * LK_TW] = s;
+            sum += (double)col[(y + D::WIN - 1) * D::GW] - (double)col[(y - 1) * D::GW];
+            out[y * D::VS] = sum;
         }
     }
     __syncthreads();
-    // 5. solve and update
-    const int PN = LK_TW * LK_TH;
-    for (int i = tid; i < PN; i += nt) {
-        int ly = i / LK_TW, lx = i - ly * LK_TW;
-        int x = x0 + lx, y = y0 + ly;
-        if (x >= W || y >= H) continue;
+    // 4. prefix sums along each row (slot 0 holds 0)
+    if (tid < 5 * LK_TH) {
+        double* row = V + (size_t)tid * D::VS;
+        double acc = 0;
+        row[0] = 0;
+        for (int k = 1; k < D::VS; k++) {
+            acc += row[k];
+            row[k] = acc;
+        }
+    }
+    __syncthreads();
+    // 5. window sums = prefix differences; 2x2 solve; update
+    for (int ly = ty; ly < LK_TH; ly += 8) {
+        const int x = x0 + tx, y = y0 + ly;
+        if (x >= W || y >= Himg) continue;
         float2 f = __ldg(isa::row_ptr(flow_in, flow_pitch, y) + x);
-        if (x >= h && x < W - h && y >= h && y < H - h)
-            f = lk_update(f, Vs[i], Vs[PN + i], Vs[2 * PN + i], Vs[3 * PN + i], Vs[4 * PN + i], min_det);
+        if (x >= H && x < W - H && y >= H && y < Himg - H) {
+            double v[5];
+#pragma unroll
+            for (int ch = 0; ch < 5; ch++) {
+                const double* row = V + (size_t)(ch * LK_TH + ly) * D::VS;
+                v[ch] = row[tx + D::WIN] - row[tx];
+            }
+            f = lk_update(f, v[0], v[1], v[2], v[3], v[4], min_det);
+        }
         isa::row_ptr(flow_out, flow_pitch, y)[x] = f;
     }
+}
+
+template <int H>
+cudaError_t launch_lk(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref, size_t img_pitch, int W, int Himg,
+                      float min_det, cudaStream_t st)
+{
+    using D = LkDims<H>;
+    cudaError_t e = cudaFuncSetAttribute(k_lk_iteration<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::TOTAL);
+    if (e != cudaSuccess) return e;
+    dim3 g((W + LK_TW - 1) / LK_TW, (Himg + LK_TH - 1) / LK_TH);
+    k_lk_iteration<H><<<g, dim3(32, 8), D::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, min_det);
+    return cudaGetLastError();
 }
 
 inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
@@ -325,11 +339,11 @@ cudaError_t isa_launch_lk_sums(float2* flow, size_t flow_pitch, const float* ix,
 cudaError_t isa_launch_lk_iteration(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref,
                                     size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st)
 {
-    if (half < 0 || half > 15) return cudaErrorInvalidValue;
-    LkSmem L = lk_smem_layout(half);
-    cudaError_t e = cudaFuncSetAttribute(k_lk_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-    if (e != cudaSuccess) return e;
-    dim3 g((W + LK_TW - 1) / LK_TW, (H + LK_TH - 1) / LK_TH);
-    k_lk_iteration<<<g, 256, L.total, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, H, half, min_det);
-    return cudaGetLastError();
+    switch (half) {
+#define ISA_LK_CASE(h) case h: return launch_lk<h>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, H, min_det, st);
+    ISA_LK_CASE(0) ISA_LK_CASE(1) ISA_LK_CASE(2) ISA_LK_CASE(3) ISA_LK_CASE(4) ISA_LK_CASE(5) ISA_LK_CASE(6) ISA_LK_CASE(7) ISA_LK_CASE(8)
+    ISA_LK_CASE(9) ISA_LK_CASE(10) ISA_LK_CASE(11) ISA_LK_CASE(12) ISA_LK_CASE(13) ISA_LK_CASE(14) ISA_LK_CASE(15)
+#undef ISA_LK_CASE
+    }
+    return cudaErrorInvalidValue;
 }
