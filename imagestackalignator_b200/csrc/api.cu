@@ -240,6 +240,7 @@ int check_params(const isa_params* p)
 void accum_geom(const isa_params* p, int W, int H, isa_accum_geom& g, float& thr)
 {
     g.W = W; g.H = H;
+    g.masks_finite = 0;
     if (p->merge_scale > 0) {
         g.s = p->merge_scale;
         g.Wo = (int)std::lround(W * (double)p->merge_scale);
@@ -511,6 +512,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     ISA_TRY(mark());
     // 5. accumulation: reference frame first (PrepareAccumulation :1894-1902), then the others in order
     const size_t op = (size_t)g.Wo * 12;
+    g.masks_finite = 1;  // the masks come from isa_launch_robustness_erode, whose values are clamped to [0, 1]
     ISA_CK(cudaMemcpyAsync(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), cudaMemcpyHostToDevice, st));
     if (p->fused_accumulate) {
         ISA_LAUNCH(c, isa_launch_accumulate(g, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum,
@@ -1002,6 +1004,7 @@ int isa_accumulate(const uint16_t* raw, size_t raw_pitch, int W, int H, const in
     isa_accum_geom g;
     g.W = W; g.H = H; g.Wo = Wo; g.Ho = Ho; g.s = scale; g.ox = ox; g.oy = oy;
     g.cx0 = crop[0]; g.cy0 = crop[1]; g.cx1 = crop[2]; g.cy1 = crop[3];
+    g.masks_finite = 0;
     float r = std::round(scale);
     g.s_int = (r == scale && r >= 1.f) ? (int)r : 0;
     isa_frame_in f{raw, (const float2*)flow, (const float4*)mask};

@@ -112,6 +112,7 @@ struct isa_accum_geom {
     int s_int;         // s when it is a positive integer, else 0
     int ox, oy;        // output-grid origin
     int cx0, cy0, cx1, cy1;  // inclusive source crop
+    int masks_finite;  // 1: every mask value is finite (masks made by this library)
 };
 struct isa_frame_in {
     const uint16_t* raw;
@@ -126,6 +127,7 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
                                   const isa_frame_in* single, size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch,
                                   int kparam_channels, const float* white, const float* black, float* acc, float* wsum,
                                   size_t out_pitch, int accumulate_into, cudaStream_t st);
+bool isa_accumulate_x2_supported(unsigned cfa);
 cudaError_t isa_launch_accumulate_x2(const isa_accum_geom& g, unsigned cfa, const isa_frame_in* frames, int nframes, const isa_frame_in* single,
                                      size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch,
                                      const float* white, const float* black, float* acc, float* wsum, size_t out_pitch, int accumulate_into,

@@ -231,7 +231,7 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
                                   const float* white, const float* black, float* acc, float* wsum, size_t out_pitch, int accumulate_into,
                                   cudaStream_t st)
 {
-    if (g.s_int == 2 && kparam_channels == 4)
+    if (g.s_int == 2 && kparam_channels == 4 && isa_accumulate_x2_supported(cfa))
         return isa_launch_accumulate_x2(g, cfa, frames, nframes, single, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, white, black, acc,
                                         wsum, out_pitch, accumulate_into, st);
     F3 wh, bl;
