@@ -7,10 +7,9 @@
 // are staged in shared memory; the L2 map D(s) = sum (r - t(s))^2 for
 // s in [-S, S]^2 is computed directly (the reference's FFT cross-correlation,
 // squaredSum and box filters, kernel.cu:29-171, compute the same quantity as
-// sum r^2 + sum t^2 - 2 CC). Each thread owns one (template row, shift row)
-// item and keeps both rows in registers, producing 2S+1 partial sums; the
-// partials are reduced over rows in a fixed order (deterministic). Thread 0
-// then does findMinimum (kernel.cu:422-546) and preShift += result (:355-358).
+// sum r^2 + sum t^2 - 2 CC). One thread per (template row, shift row), rows
+// reduced with warp shuffles; warp 0 then does findMinimum (kernel.cu:422-546)
+// and preShift += result (:355-358).
 #include "isa_internal.cuh"
 #include <float.h>
 
@@ -37,17 +36,38 @@ __device__ __forceinline__ void tile_offset(int tx, int ty, int T, int Wl, int H
     oy = (int)roundf(sy);
 }
 
+// Shared-memory layout of k_track, in floats.
 template <int T, int S>
-__global__ void __launch_bounds__(256) k_track(const float* const* __restrict__ frames, size_t pitch, int Wl, int Hl, int tcx, int tcy,
-                                             const isa_pair_desc* __restrict__ pairs, float2* __restrict__ grids, size_t grid_pitch,
-                                             size_t grid_stride, float threshold, float* __restrict__ scores, int* __restrict__ argmin_out)
+struct TrackDims {
+    static constexpr int B = T + 2 * S, D = 2 * S + 1;
+    static constexpr int TP = T + 1, BP = B + 1;  // odd strides: conflict-free column reads across lanes
+    static constexpr int NI = T * D;              // (template row, shift row) items
+    static constexpr int NT = (NI + 31) / 32 * 32;
+    static constexpr int RW = T < 32 ? T : 32;    // template rows summed by one warp
+    static constexpr int NCC = T / RW;            // partial sums per map entry (2 when T = 64)
+    static constexpr int OFF_TPL = 0, OFF_BLK = OFF_TPL + T * TP, OFF_PART = OFF_BLK + B * BP;
+    static constexpr int OFF_MAP = OFF_PART + D * D * NCC;
+    static constexpr int TOTAL = OFF_MAP + D * D;
+    static constexpr size_t BYTES = (size_t)TOTAL * sizeof(float);
+};
+
+// Thread (y, sy) streams template row y against block row y + sy with a
+// D-wide register window, accumulating (r - t)^2 for the D column shifts;
+// the template rows are then summed across lanes with shuffles in a fixed
+// order (deterministic), and warp 0 finds the first minimum.
+template <int T, int S>
+__global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* const* __restrict__ frames, size_t pitch, int Wl, int Hl, int tcx,
+                                                               int tcy, const isa_pair_desc* __restrict__ pairs, float2* __restrict__ grids,
+                                                               size_t grid_pitch, size_t grid_stride, float threshold, float* __restrict__ scores,
+                                                               int* __restrict__ argmin_out)
 {
-    constexpr int B = T + 2 * S, D = 2 * S + 1;
-    constexpr int TP = T + 1, BP = B + 1;  // odd strides: conflict-free row reads across lanes
-    __shared__ float tpl[T * TP];
-    __shared__ float blk[B * BP];
-    __shared__ float part[D * T * D];
-    __shared__ float map[D * D];
+    using L = TrackDims<T, S>;
+    constexpr int B = L::B, D = L::D, TP = L::TP, BP = L::BP, RW = L::RW;
+    extern __shared__ float smf[];
+    float* tpl = smf + L::OFF_TPL;
+    float* blk = smf + L::OFF_BLK;
+    float* part = smf + L::OFF_PART;
+    float* map = smf + L::OFF_MAP;
     const int p = blockIdx.x;
     const int tile = blockIdx.y;
     const int ty = tile / tcx, tx = tile - ty * tcx;
@@ -59,88 +79,112 @@ __global__ void __launch_bounds__(256) k_track(const float* const* __restrict__ 
     tile_offset(tx, ty, T, Wl, Hl, pd.base_ref_x, pd.base_ref_y, pd.rot_ref, 0.f, 0.f, oxr, oyr);
     float2 pre = gline[tx];
     tile_offset(tx, ty, T, Wl, Hl, pd.base_trk_x, pd.base_trk_y, pd.rot_trk, pre.x, pre.y, oxt, oyt);
-    const int tid = threadIdx.x;
-    for (int i = tid; i < T * T; i += blockDim.x) {
-        int y = i / T, x = i - y * T;
-        int ix = isa::clampi(tx * T + S + x + oxr, 0, Wl - 1), iy = isa::clampi(ty * T + S + y + oyr, 0, Hl - 1);
-        tpl[y * TP + x] = isa::row_ptr(imr, pitch, iy)[ix];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = L::NT / 32;
+    // stage the template and the search block, one row per warp iteration
+    for (int y = warp; y < T; y += NW) {
+        const float* row = isa::row_ptr(imr, pitch, isa::clampi(ty * T + S + y + oyr, 0, Hl - 1));
+        for (int x = lane; x < T; x += 32) tpl[y * TP + x] = __ldg(row + isa::clampi(tx * T + S + x + oxr, 0, Wl - 1));
     }
-    for (int i = tid; i < B * B; i += blockDim.x) {
-        int y = i / B, x = i - y * B;
-        int ix = isa::clampi(tx * T + x + oxt, 0, Wl - 1), iy = isa::clampi(ty * T + y + oyt, 0, Hl - 1);
-        blk[y * BP + x] = isa::row_ptr(imt, pitch, iy)[ix];
+    for (int y = warp; y < B; y += NW) {
+        const float* row = isa::row_ptr(imt, pitch, isa::clampi(ty * T + y + oyt, 0, Hl - 1));
+        for (int x = lane; x < B; x += 32) blk[y * BP + x] = __ldg(row + isa::clampi(tx * T + x + oxt, 0, Wl - 1));
     }
     __syncthreads();
-    for (int item = tid; item < T * D; item += blockDim.x) {
-        const int y = item % T, sy = item / T;
-        float r[T], t[B], acc[D];
+    const int y = tid % T, sy = tid / T;
+    float acc[D];
 #pragma unroll
-        for (int x = 0; x < T; x++) r[x] = tpl[y * TP + x];
+    for (int k = 0; k < D; k++) acc[k] = 0.f;
+    if (tid < L::NI) {
+        const float* tr = tpl + y * TP;
+        const float* br = blk + (y + sy) * BP;
+        float win[D];
 #pragma unroll
-        for (int x = 0; x < B; x++) t[x] = blk[(y + sy) * BP + x];
+        for (int k = 0; k < D - 1; k++) win[k] = br[k];
 #pragma unroll
-        for (int k = 0; k < D; k++) acc[k] = 0.f;
-#pragma unroll
-        for (int x = 0; x < T; x++)
+        for (int x = 0; x < T; x++) {
+            win[D - 1] = br[x + D - 1];
+            const float r = tr[x];
 #pragma unroll
             for (int k = 0; k < D; k++) {
-                float d = r[x] - t[x + k];
+                const float d = r - win[k];
                 acc[k] = fmaf(d, d, acc[k]);
             }
 #pragma unroll
-        for (int k = 0; k < D; k++) part[(sy * T + y) * D + k] = acc[k];
+            for (int k = 0; k < D - 1; k++) win[k] = win[k + 1];
+        }
+    }
+#pragma unroll
+    for (int o = RW / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < D; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (tid < L::NI && (y % RW) == 0) {
+#pragma unroll
+        for (int k = 0; k < D; k++) part[(sy * D + k) * L::NCC + y / RW] = acc[k];
     }
     __syncthreads();
-    for (int k = tid; k < D * D; k += blockDim.x) {
-        int sy = k / D, sx = k - sy * D;
-        float s = 0.f;
-        for (int y = 0; y < T; y++) s += part[(sy * T + y) * D + sx];
-        map[k] = s;
-    }
-    __syncthreads();
-    if (tid == 0) {
+    if (warp == 0) {
+        // map = sum of the partials; first strict minimum and maximum over the map
         float mn = FLT_MAX, mx = -FLT_MAX;
-        int mi = -1;
-        for (int i = 0; i < D * D; i++) {
-            float v = map[i];
+        int mi = 0x7fffffff;
+        for (int i = lane; i < D * D; i += 32) {
+            float v = part[i * L::NCC];
+#pragma unroll
+            for (int q = 1; q < L::NCC; q++) v += part[i * L::NCC + q];
+            map[i] = v;
             mx = fmaxf(mx, v);
             if (v < mn) { mn = v; mi = i; }
         }
-        size_t tix = (size_t)p * tcx * tcy + tile;
-        if (scores)
-            for (int i = 0; i < D * D; i++) scores[tix * D * D + i] = map[i];
-        if (argmin_out) argmin_out[tix] = mi;
-        float cx = 0.f, cy = 0.f;
-        if (mi >= 0) {
-            int iy = mi / D, ix = mi - iy * D;
-            cy = (float)iy;
-            cx = (float)ix;
-            if (ix < 1 || iy < 1 || ix >= 2 * S || iy >= 2 * S) {
-                cx = 0.f; cy = 0.f;
-            } else {
-                float a11 = 0.f, a22 = 0.f, a12 = 0.f, b1 = 0.f, b2 = 0.f;
-                for (int k = 0; k < 9; k++) {
-                    float v = map[(iy + k / 3 - 1) * D + ix + k % 3 - 1];
-                    a11 += c_fit[0][k] * v; a22 += c_fit[1][k] * v; a12 += c_fit[2][k] * v;
-                    b1 += c_fit[3][k] * v; b2 += c_fit[4][k] * v;
-                }
-                a11 = fmaxf(a11, 0.0f);
-                a22 = fmaxf(a22, 0.0f);
-                float det = a11 * a22 - a12 * a12;
-                if (det < 0) { a12 = 0; det = a11 * a22; }
-                if (det != 0) {
-                    float mux = (a22 * b1 - a12 * b2) / det, muy = (a11 * b2 - a12 * b1) / det;
-                    if (fabsf(mux) > 1) mux = 0;
-                    if (fabsf(muy) > 1) muy = 0;
-                    cx -= mux; cy -= muy;
-                }
-                cx -= S; cy -= S;
-            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float omn = __shfl_xor_sync(0xffffffffu, mn, o), omx = __shfl_xor_sync(0xffffffffu, mx, o);
+            const int omi = __shfl_xor_sync(0xffffffffu, mi, o);
+            if (omn < mn || (omn == mn && omi < mi)) { mn = omn; mi = omi; }
+            mx = fmaxf(mx, omx);
         }
-        if (threshold + mn > mx) { cx = 0.f; cy = 0.f; }
-        pre.x += cx;
-        pre.y += cy;
-        gline[tx] = pre;
+        __syncwarp();
+        if (lane == 0) {
+            if (mi == 0x7fffffff) mi = -1;
+            size_t tix = (size_t)p * tcx * tcy + tile;
+            if (argmin_out) argmin_out[tix] = mi;
+            float cx = 0.f, cy = 0.f;
+            if (mi >= 0) {
+                int iy = mi / D, ix = mi - iy * D;
+                cy = (float)iy;
+                cx = (float)ix;
+                if (ix < 1 || iy < 1 || ix >= 2 * S || iy >= 2 * S) {
+                    cx = 0.f; cy = 0.f;
+                } else {
+                    float a11 = 0.f, a22 = 0.f, a12 = 0.f, b1 = 0.f, b2 = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 9; k++) {
+                        float v = map[(iy + k / 3 - 1) * D + ix + k % 3 - 1];
+                        a11 += c_fit[0][k] * v; a22 += c_fit[1][k] * v; a12 += c_fit[2][k] * v;
+                        b1 += c_fit[3][k] * v; b2 += c_fit[4][k] * v;
+                    }
+                    a11 = fmaxf(a11, 0.0f);
+                    a22 = fmaxf(a22, 0.0f);
+                    float det = a11 * a22 - a12 * a12;
+                    if (det < 0) { a12 = 0; det = a11 * a22; }
+                    if (det != 0) {
+                        float mux = (a22 * b1 - a12 * b2) / det, muy = (a11 * b2 - a12 * b1) / det;
+                        if (fabsf(mux) > 1) mux = 0;
+                        if (fabsf(muy) > 1) muy = 0;
+                        cx -= mux; cy -= muy;
+                    }
+                    cx -= S; cy -= S;
+                }
+            }
+            if (threshold + mn > mx) { cx = 0.f; cy = 0.f; }
+            pre.x += cx;
+            pre.y += cy;
+            gline[tx] = pre;
+        }
+        if (scores) {
+            __syncwarp();
+            const size_t tix = (size_t)p * tcx * tcy + tile;
+            for (int i = lane; i < D * D; i += 32) scores[tix * D * D + i] = map[i];
+        }
     }
 }
 
@@ -149,8 +193,14 @@ cudaError_t launch_track_ts(const float* const* frames, size_t pitch, int Wl, in
                             int npairs, float2* grids, size_t grid_pitch, size_t grid_stride, float thr, float* scores, int* argmin,
                             cudaStream_t st)
 {
+    using L = TrackDims<T, S>;
+    static_assert(T <= 32 ? (32 % T == 0) : (T % 32 == 0), "tile rows must tile a warp");
+    if (L::BYTES > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_track<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+        if (e != cudaSuccess) return e;
+    }
     dim3 g(npairs, tcx * tcy);
-    k_track<T, S><<<g, 256, 0, st>>>(frames, pitch, Wl, Hl, tcx, tcy, pairs, grids, grid_pitch, grid_stride, thr, scores, argmin);
+    k_track<T, S><<<g, L::NT, L::BYTES, st>>>(frames, pitch, Wl, Hl, tcx, tcy, pairs, grids, grid_pitch, grid_stride, thr, scores, argmin);
     return cudaGetLastError();
 }
 
