@@ -9,10 +9,10 @@
 // the integer pixel and the sub-pixel flow part so that FP32 keeps full
 // sub-pixel precision far from the origin.
 //
-// k_lk_iteration fuses one reference iteration (warp, Set(0) x3, derivatives,
-// lucasKanadeOptim) for a 32 x 16 tile: warped and reference images over the
-// tile plus a (h + 2) halo in shared memory, FP32 gradient products over the
-// h halo, exact FP64 sliding window sums, and the 2x2 pseudo-inverse in FP64.
+// k_lk_stream fuses one reference iteration (warp, Set(0) x3, derivatives,
+// lucasKanadeOptim) for a vertical strip of the image, walking down it row by
+// row: FP32 gradient products, FP64 sliding window sums, and the 2x2
+// pseudo-inverse in FP64.
 #include "isa_internal.cuh"
 
 namespace {
@@ -170,114 +170,142 @@ __global__ void k_lk_sums(float2* flow, size_t flow_pitch, const float* __restri
     *fp = lk_update(*fp, sxx, sxy, syy, sxt, syt, min_det);
 }
 
-constexpr int LK_TW = 32, LK_TH = 16;
+// Streaming form of one reference iteration (warp, Set(0) x3, derivatives,
+// lucasKanadeOptim). A CTA of LKS_NT threads owns a vertical strip: thread t
+// owns image column x0 - R + t (R = h + 2, mirrored at the border) and walks
+// down the strip one row at a time:
+//   1. the warped source and the reference at (column, row) go into a
+//      five-row ring in shared memory; the global loads for the next rows
+//      are issued one and two rows ahead (flow, then the bilinear samples);
+//   2. five-tap derivatives at the ring's centre row (neighbouring columns
+//      from shared memory), FP32 products, and per-column vertical window
+//      sums in FP64 registers (the product leaving the window comes from a
+//      per-thread ring of the last 2h + 1 rows);
+//   3. every two output rows, the row window sums (sliding FP64 sums over
+//      2h + 1 columns, two pixels per thread) and the 2x2 solve.
+// The FP64 sums hold the FP32 products exactly enough that the order of
+// summation does not matter at FP32 output precision.
+constexpr int LKS_NT = 128, LKS_SH = 64;
 
-// Tile geometry for half window H: warped/reference images over the tile
-// plus an (H + 2) halo (E), gradient products over the tile plus an H halo
-// (G), per-column vertical window sums of the products for the tile rows,
-// stored with one leading slot per row for the in-place prefix sum (V).
 template <int H>
-struct LkDims {
-    static constexpr int R = H + 2, EW = LK_TW + 2 * R, EH = LK_TH + 2 * R;
-    static constexpr int GW = LK_TW + 2 * H, GH = LK_TH + 2 * H, GN = GW * GH, WIN = 2 * H + 1;
-    static constexpr int VS = GW + 1;
-    static constexpr size_t E_BYTES = (size_t)EW * EH * 4;
-    static constexpr size_t P_BYTES = (size_t)5 * GN * 4;
-    static constexpr size_t OFF_R = E_BYTES, OFF_P = 2 * E_BYTES, OFF_V = (OFF_P + P_BYTES + 15) / 16 * 16;
-    static constexpr size_t TOTAL = OFF_V + (size_t)5 * LK_TH * VS * 8;
+struct LkStream {
+    static constexpr int R = H + 2, SW = LKS_NT - 2 * R, WIN = 2 * H + 1;
+    static constexpr int NSEG = (SW + 1) / 2;
+    static constexpr size_t E_BYTES = (size_t)2 * 5 * LKS_NT * 4;
+    static constexpr size_t P_BYTES = (size_t)WIN * 5 * LKS_NT * 4;
+    static constexpr size_t OFF_P = E_BYTES, OFF_C = (OFF_P + P_BYTES + 15) / 16 * 16;
+    static constexpr size_t TOTAL = OFF_C + (size_t)2 * 5 * LKS_NT * 8;
 };
 
-// One reference iteration (warp, Set(0) x3, derivatives, lucasKanadeOptim)
-// for a 32 x 16 tile, blockDim (32, 8). Window sums: FP32 products summed in
-// FP64, first down each column with a sliding window (exact: FP64 holds the
-// sum of a few FP32 values), then along each row through a prefix sum.
 template <int H>
-__global__ void __launch_bounds__(256) k_lk_iteration(const float2* __restrict__ flow_in, float2* __restrict__ flow_out, size_t flow_pitch,
-                                                     const float* __restrict__ src, const float* __restrict__ ref, size_t img_pitch, int W,
-                                                     int Himg, float min_det)
+__global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__ flow_in, float2* __restrict__ flow_out, size_t flow_pitch,
+                                                      const float* __restrict__ src, const float* __restrict__ ref, size_t img_pitch, int W,
+                                                      int Himg, float min_det)
 {
-    using D = LkDims<H>;
+    using L = LkStream<H>;
+    constexpr int R = L::R, SW = L::SW, WIN = L::WIN, NT = LKS_NT;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* Ew = (float*)smem;
-    float* Er = (float*)(smem + D::OFF_R);
-    float* P = (float*)(smem + D::OFF_P);
-    double* V = (double*)(smem + D::OFF_V);
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-    const int x0 = blockIdx.x * LK_TW, y0 = blockIdx.y * LK_TH;
-    // 1. warped source and reference, mirrored at the image border
-    for (int ey = ty; ey < D::EH; ey += 8) {
-        const int my = isa::mirror(y0 - D::R + ey, Himg);
-        const float2* frow = isa::row_ptr(flow_in, flow_pitch, my);
-        const float* rrow = isa::row_ptr(ref, img_pitch, my);
-        for (int ex = tx; ex < D::EW; ex += 32) {
-            const int mx = isa::mirror(x0 - D::R + ex, W);
-            const float2 f = __ldg(frow + mx);
-            Ew[ey * D::EW + ex] = bilinear_mirror(src, img_pitch, W, Himg, mx, my, f.x, f.y);
-            Er[ey * D::EW + ex] = __ldg(rrow + mx);
+    float* Ew = (float*)smem;            // [5][NT]
+    float* Er = Ew + 5 * NT;              // [5][NT]
+    float* Pr = (float*)(smem + L::OFF_P);    // [WIN][5][NT]
+    double* Cs = (double*)(smem + L::OFF_C);  // [2][5][NT]
+    const int t = threadIdx.x;
+    const int x0 = blockIdx.x * SW, y0 = blockIdx.y * LKS_SH;
+    const int nout = min(LKS_SH, Himg - y0);
+    const int nE = nout + 2 * R;
+    const int col = isa::mirror(x0 - R + t, W);
+    // pipeline: flow two rows ahead, bilinear samples one row ahead
+    float2 fnext;
+    float s00, s10, s01, s11, sa, sb, sref;
+    const auto erow = [&](int e) { return isa::mirror(y0 - R + e, Himg); };
+    const auto issue_samples = [&](int row, float2 f) {
+        const float flx = floorf(f.x), fly = floorf(f.y);
+        const int ix = col + (int)flx, iy = row + (int)fly;
+        sa = f.x - flx;
+        sb = f.y - fly;
+        const int xa = isa::mirror(ix, W), xb = isa::mirror(ix + 1, W);
+        const float* r0 = isa::row_ptr(src, img_pitch, isa::mirror(iy, Himg));
+        const float* r1 = isa::row_ptr(src, img_pitch, isa::mirror(iy + 1, Himg));
+        s00 = __ldg(r0 + xa); s10 = __ldg(r0 + xb); s01 = __ldg(r1 + xa); s11 = __ldg(r1 + xb);
+        sref = __ldg(isa::row_ptr(ref, img_pitch, row) + col);
+    };
+    issue_samples(erow(0), __ldg(isa::row_ptr(flow_in, flow_pitch, erow(0)) + col));
+    if (nE > 1) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(1)) + col);
+    double cs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int e = 0; e < nE; e++) {
+        const int slot = e % 5;
+        Ew[slot * NT + t] = isa::lerp2(s00, s10, s01, s11, sa, sb);
+        Er[slot * NT + t] = sref;
+        if (e + 1 < nE) {
+            issue_samples(erow(e + 1), fnext);
+            if (e + 2 < nE) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(e + 2)) + col);
         }
-    }
-    __syncthreads();
-    // 2. derivatives (five-tap, averaged over both images) and products
-    for (int gy = ty; gy < D::GH; gy += 8)
-        for (int gx = tx; gx < D::GW; gx += 32) {
-            const int e = (gy + 2) * D::EW + gx + 2;
-            float t0 = (Ew[e + 2] - Ew[e + 1] * 8.0f + Ew[e - 1] * 8.0f - Ew[e - 2]) / 12.0f;
-            float t1 = (Er[e + 2] - Er[e + 1] * 8.0f + Er[e - 1] * 8.0f - Er[e - 2]) / 12.0f;
-            const float dx = (t0 + t1) * 0.5f;
-            t0 = (Ew[e + 2 * D::EW] - Ew[e + D::EW] * 8.0f + Ew[e - D::EW] * 8.0f - Ew[e - 2 * D::EW]) / 12.0f;
-            t1 = (Er[e + 2 * D::EW] - Er[e + D::EW] * 8.0f + Er[e - D::EW] * 8.0f - Er[e - 2 * D::EW]) / 12.0f;
-            const float dy = (t0 + t1) * 0.5f;
-            const float dt = Ew[e] - Er[e];
-            const int g = gy * D::GW + gx;
-            P[g] = dx * dx;
-            P[D::GN + g] = dx * dy;
-            P[2 * D::GN + g] = dy * dy;
-            P[3 * D::GN + g] = dx * dt;
-            P[4 * D::GN + g] = dy * dt;
-        }
-    __syncthreads();
-    // 3. vertical sliding sums per (channel, column)
-    for (int job = tid; job < 5 * D::GW; job += 256) {
-        const int ch = job / D::GW, gx = job - ch * D::GW;
-        const float* col = P + ch * D::GN + gx;
-        double* out = V + (size_t)ch * LK_TH * D::VS + 1 + gx;
-        double sum = 0;
+        __syncthreads();
+        if (e >= 4) {
+            const int gi = e - 4;  // product row: image row y0 - h + gi
+            if (t >= 2 && t < NT - 2) {
+                const float* ew = Ew + ((e - 2) % 5) * NT + t;
+                const float* er = Er + ((e - 2) % 5) * NT + t;
+                float t0 = (ew[2] - ew[1] * 8.0f + ew[-1] * 8.0f - ew[-2]) / 12.0f;
+                float t1 = (er[2] - er[1] * 8.0f + er[-1] * 8.0f - er[-2]) / 12.0f;
+                const float dx = (t0 + t1) * 0.5f;
+                const int sp2 = (e % 5) * NT + t, sp1 = ((e - 1) % 5) * NT + t, sm1 = ((e - 3) % 5) * NT + t, sm2 = ((e - 4) % 5) * NT + t;
+                t0 = (Ew[sp2] - Ew[sp1] * 8.0f + Ew[sm1] * 8.0f - Ew[sm2]) / 12.0f;
+                t1 = (Er[sp2] - Er[sp1] * 8.0f + Er[sm1] * 8.0f - Er[sm2]) / 12.0f;
+                const float dy = (t0 + t1) * 0.5f;
+                const float dt = ew[0] - er[0];
+                const float p[5] = {dx * dx, dx * dy, dy * dy, dx * dt, dy * dt};
+                float* pr = Pr + (gi % WIN) * 5 * NT + t;
 #pragma unroll
-        for (int k = 0; k < D::WIN; k++) sum += (double)col[k * D::GW];
-        out[0] = sum;
-#pragma unroll 4
-        for (int y = 1; y < LK_TH; y++) {
-            sum += (double)col[(y + D::WIN - 1) * D::GW] - (double)col[(y - 1) * D::GW];
-            out[y * D::VS] = sum;
-        }
-    }
-    __syncthreads();
-    // 4. prefix sums along each row (slot 0 holds 0)
-    if (tid < 5 * LK_TH) {
-        double* row = V + (size_t)tid * D::VS;
-        double acc = 0;
-        row[0] = 0;
-        for (int k = 1; k < D::VS; k++) {
-            acc += row[k];
-            row[k] = acc;
-        }
-    }
-    __syncthreads();
-    // 5. window sums = prefix differences; 2x2 solve; update
-    for (int ly = ty; ly < LK_TH; ly += 8) {
-        const int x = x0 + tx, y = y0 + ly;
-        if (x >= W || y >= Himg) continue;
-        float2 f = __ldg(isa::row_ptr(flow_in, flow_pitch, y) + x);
-        if (x >= H && x < W - H && y >= H && y < Himg - H) {
-            double v[5];
-#pragma unroll
-            for (int ch = 0; ch < 5; ch++) {
-                const double* row = V + (size_t)(ch * LK_TH + ly) * D::VS;
-                v[ch] = row[tx + D::WIN] - row[tx];
+                for (int ch = 0; ch < 5; ch++) {
+                    const float old = gi >= WIN ? pr[ch * NT] : 0.f;
+                    cs[ch] += (double)p[ch] - (double)old;
+                    pr[ch * NT] = p[ch];
+                }
             }
-            f = lk_update(f, v[0], v[1], v[2], v[3], v[4], min_det);
+            if (gi >= 2 * H) {
+                const int o = gi - 2 * H;  // output row y0 + o
+                if (t >= 2 && t < NT - 2) {
+#pragma unroll
+                    for (int ch = 0; ch < 5; ch++) Cs[((o & 1) * 5 + ch) * NT + t] = cs[ch];
+                }
+                if ((o & 1) || o == nout - 1) {
+                    __syncthreads();
+                    const int rlo = o & ~1, nr = o - rlo + 1;
+                    if (t < nr * L::NSEG) {
+                        const int r = rlo + t / L::NSEG, j0 = 2 * (t % L::NSEG);
+                        const double* cr = Cs + (r & 1) * 5 * NT + j0 + 2;
+                        double v0[5], v1[5];
+#pragma unroll
+                        for (int ch = 0; ch < 5; ch++) {
+                            const double* c = cr + ch * NT;
+                            double s = 0.0;
+#pragma unroll
+                            for (int d = 0; d < WIN; d++) s += c[d];
+                            v0[ch] = s;
+                            v1[ch] = s + (c[WIN] - c[0]);
+                        }
+                        const int y = y0 + r;
+                        const bool yin = y >= H && y < Himg - H;
+                        float2* orow = isa::row_ptr(flow_out, flow_pitch, y);
+                        const float2* irow = isa::row_ptr(flow_in, flow_pitch, y);
+                        int x = x0 + j0;
+                        if (j0 < SW && x < W) {
+                            float2 f = __ldg(irow + x);
+                            if (yin && x >= H && x < W - H) f = lk_update(f, v0[0], v0[1], v0[2], v0[3], v0[4], min_det);
+                            orow[x] = f;
+                        }
+                        x++;
+                        if (j0 + 1 < SW && x < W) {
+                            float2 f = __ldg(irow + x);
+                            if (yin && x >= H && x < W - H) f = lk_update(f, v1[0], v1[1], v1[2], v1[3], v1[4], min_det);
+                            orow[x] = f;
+                        }
+                    }
+                }
+            }
         }
-        isa::row_ptr(flow_out, flow_pitch, y)[x] = f;
+        __syncthreads();
     }
 }
 
@@ -285,11 +313,11 @@ template <int H>
 cudaError_t launch_lk(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref, size_t img_pitch, int W, int Himg,
                       float min_det, cudaStream_t st)
 {
-    using D = LkDims<H>;
-    cudaError_t e = cudaFuncSetAttribute(k_lk_iteration<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::TOTAL);
+    using L = LkStream<H>;
+    cudaError_t e = cudaFuncSetAttribute(k_lk_stream<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL);
     if (e != cudaSuccess) return e;
-    dim3 g((W + LK_TW - 1) / LK_TW, (Himg + LK_TH - 1) / LK_TH);
-    k_lk_iteration<H><<<g, dim3(32, 8), D::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, min_det);
+    dim3 g((W + L::SW - 1) / L::SW, (Himg + LKS_SH - 1) / LKS_SH);
+    k_lk_stream<H><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, min_det);
     return cudaGetLastError();
 }
 
