@@ -12,6 +12,7 @@
 // and preShift += result (:355-358).
 #include "isa_internal.cuh"
 #include <float.h>
+#include <algorithm>
 
 namespace {
 
@@ -25,7 +26,8 @@ __constant__ float c_fit[5][9] = {
 __device__ __forceinline__ void tile_offset(int tx, int ty, int T, int Wl, int Hl, float bx, float by, float rot, float addx, float addy,
                                             int& ox, int& oy)
 {
-    float sf = sinf(rot), cf = cosf(rot);
+    float sf = 0.f, cf = 1.f;  // sinf(0) and cosf(0) are exact
+    if (rot != 0.f) { sf = sinf(rot); cf = cosf(rot); }
     float sx = addx, sy = addy;
     sx += cf * -bx - sf * -by;
     sy += sf * -bx + cf * -by;
@@ -81,14 +83,24 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
     tile_offset(tx, ty, T, Wl, Hl, pd.base_trk_x, pd.base_trk_y, pd.rot_trk, pre.x, pre.y, oxt, oyt);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = L::NT / 32;
-    // stage the template and the search block, one row per warp iteration
+    // stage the template and the search block: clamped columns once per lane, one row per warp iteration
+    constexpr int TX = (T + 31) / 32, BX = (B + 31) / 32;
+    int cr[TX], ct[BX];
+#pragma unroll
+    for (int k = 0; k < TX; k++) cr[k] = isa::clampi(tx * T + S + lane + 32 * k + oxr, 0, Wl - 1);
+#pragma unroll
+    for (int k = 0; k < BX; k++) ct[k] = isa::clampi(tx * T + lane + 32 * k + oxt, 0, Wl - 1);
     for (int y = warp; y < T; y += NW) {
         const float* row = isa::row_ptr(imr, pitch, isa::clampi(ty * T + S + y + oyr, 0, Hl - 1));
-        for (int x = lane; x < T; x += 32) tpl[y * TP + x] = __ldg(row + isa::clampi(tx * T + S + x + oxr, 0, Wl - 1));
+#pragma unroll
+        for (int k = 0; k < TX; k++)
+            if (lane + 32 * k < T) tpl[y * TP + lane + 32 * k] = __ldg(row + cr[k]);
     }
     for (int y = warp; y < B; y += NW) {
         const float* row = isa::row_ptr(imt, pitch, isa::clampi(ty * T + y + oyt, 0, Hl - 1));
-        for (int x = lane; x < B; x += 32) blk[y * BP + x] = __ldg(row + isa::clampi(tx * T + x + oxt, 0, Wl - 1));
+#pragma unroll
+        for (int k = 0; k < BX; k++)
+            if (lane + 32 * k < B) blk[y * BP + lane + 32 * k] = __ldg(row + ct[k]);
     }
     __syncthreads();
     const int y = tid % T, sy = tid / T;
@@ -230,177 +242,184 @@ __global__ void k_upsample(const float2* __restrict__ in, size_t in_pitch, size_
     ((float2*)((char*)out + blockIdx.z * out_stride + (size_t)ny * out_pitch))[nx] = o;
 }
 
-// Per-tile least squares with outlier removal. Rows of the incidence matrix
-// are intervals [a, b) of the one-to-one shifts with a common sign (true for
-// every tracking strategy of ShiftCollection.CreateShiftMatrix), so
-// N = A^T A is updated incrementally when a row is removed, and A x is a
-// difference of prefix sums. Solved in FP64 by Gauss-Jordan on [N | A^T b].
-constexpr int SOLVE_THREADS = 128;
+// Per-tile least squares with outlier removal, one warp per tile (no block
+// barriers). Rows of the incidence matrix are intervals [a, b) of the
+// one-to-one shifts with a common sign (true for every tracking strategy of
+// ShiftCollection.CreateShiftMatrix), so N = A^T A is updated in place when a
+// row is removed, and A x is a difference of prefix sums. Each round solves
+// [N | A^T b] in FP64 by Gauss-Jordan with partial pivoting: lane r owns row
+// r of the augmented matrix (odd row stride: conflict-free 64-bit access).
+struct SolveLayout {
+    int n1, m, as;          // unknowns, rows, augmented row stride (odd)
+    int off_aug, off_rhs, off_xs, off_p;  // in doubles, after N
+    int nd;                 // doubles per warp
+    size_t bytes;           // per warp (doubles + b floats + active bytes, 16-aligned)
+};
 
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const int* __restrict__ row_a, const int* __restrict__ row_b,
-                                                         const int* __restrict__ row_sign, const double* __restrict__ N0, int m, int n1,
-                                                         float2* __restrict__ grids, size_t grid_pitch, size_t grid_stride,
-                                                         const int* __restrict__ row_grid, int tcx, int tcy, float2* __restrict__ x_out,
-                                                         int* __restrict__ status)
+__host__ __device__ inline SolveLayout solve_layout(int m, int n1)
 {
-    extern __shared__ double sm[];
-    const int tile = blockIdx.x;
-    const int ty = tile / tcx, tx = tile - ty * tcx;
-    const int na = n1 + 2;
-    double* N = sm;                       // n1 x n1
-    double* aug = N + n1 * n1;            // n1 x (n1 + 2)
-    double* fac = aug + n1 * na;          // n1
-    double* P = fac + n1;                 // (n1 + 1) x 2 prefix sums of x
-    double* xs = P + 2 * (n1 + 1);        // n1 x 2 last solution
-    float* b = (float*)(xs + 2 * n1);     // m x 2 measurements
+    SolveLayout L;
+    L.n1 = n1; L.m = m; L.as = (n1 + 2) | 1;
+    L.off_aug = n1 * n1;
+    L.off_rhs = L.off_aug + n1 * L.as;
+    L.off_xs = L.off_rhs + 2 * n1;
+    L.off_p = L.off_xs + 2 * n1;
+    L.nd = L.off_p + 2 * (n1 + 1);
+    L.bytes = ((size_t)L.nd * 8 + (size_t)2 * m * 4 + (size_t)m + 15) / 16 * 16;
+    return L;
+}
+
+__global__ void k_solve(const int* __restrict__ row_a, const int* __restrict__ row_b, const int* __restrict__ row_sign,
+                        const double* __restrict__ N0, int m, int n1, float2* __restrict__ grids, size_t grid_pitch, size_t grid_stride,
+                        const int* __restrict__ row_grid, int tcx, int tcy, float2* __restrict__ x_out, int* __restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char smem_s[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (tile >= tcx * tcy) return;  // the whole warp leaves; only warp-level synchronisation below
+    const SolveLayout L = solve_layout(m, n1);
+    double* N = (double*)(smem_s + (size_t)warp * L.bytes);
+    double* aug = N + L.off_aug;
+    double* rhs = N + L.off_rhs;
+    double* xs = N + L.off_xs;
+    double* P = N + L.off_p;
+    float* b = (float*)(N + L.nd);
     unsigned char* active = (unsigned char*)(b + 2 * m);
-    __shared__ double red_v[SOLVE_THREADS / 32];
-    __shared__ int red_i[SOLVE_THREADS / 32];
-    __shared__ int s_flag;
-    const int tid = threadIdx.x;
-    for (int i = tid; i < n1 * n1; i += blockDim.x) N[i] = N0[i];
-    for (int k = tid; k < m; k += blockDim.x) {
-        float2 v = ((const float2*)((const char*)grids + (size_t)row_grid[k] * grid_stride + (size_t)ty * grid_pitch))[tx];
+    const int AS = L.as, na = n1 + 2;
+    const int ty = tile / tcx, tx = tile - ty * tcx;
+    for (int i = lane; i < n1 * n1; i += 32) N[i] = N0[i];
+    for (int k = lane; k < m; k += 32) {
+        const float2 v = ((const float2*)((const char*)grids + (size_t)row_grid[k] * grid_stride + (size_t)ty * grid_pitch))[tx];
         b[2 * k] = v.x; b[2 * k + 1] = v.y;
         active[k] = 1;
     }
-    for (int i = tid; i < 2 * n1; i += blockDim.x) xs[i] = 0.0;
-    __syncthreads();
+    for (int i = lane; i < 2 * n1; i += 32) xs[i] = 0.0;
+    __syncwarp();
     // rhs = A^T b
-    for (int i = tid; i < n1; i += blockDim.x) {
+    for (int i = lane; i < n1; i += 32) {
         double sx = 0, sy = 0;
         for (int k = 0; k < m; k++)
-            if (row_a[k] <= i && i < row_b[k]) { sx += row_sign[k] * (double)b[2 * k]; sy += row_sign[k] * (double)b[2 * k + 1]; }
-        aug[i * na + n1] = sx; aug[i * na + n1 + 1] = sy;
+            if (__ldg(row_a + k) <= i && i < __ldg(row_b + k)) {
+                const double sg = __ldg(row_sign + k);
+                sx += sg * (double)b[2 * k]; sy += sg * (double)b[2 * k + 1];
+            }
+        rhs[2 * i] = sx; rhs[2 * i + 1] = sy;
     }
     int st = -1;
-    __shared__ int s_piv;
-    __shared__ double s_tol, s_pval;
     for (int round_ = 0; round_ < 10; round_++) {
-        __syncthreads();
-        for (int i = tid; i < n1 * n1; i += blockDim.x) { int r = i / n1, c = i - r * n1; aug[r * na + c] = N[i]; }
-        __syncthreads();
-        // stash rhs (aug columns are destroyed by elimination)
-        for (int i = tid; i < n1; i += blockDim.x) { P[2 * i] = aug[i * na + n1]; P[2 * i + 1] = aug[i * na + n1 + 1]; }
-        if (tid == 0) {
-            s_flag = 0;
-            double sc = 0;
-            for (int i = 0; i < n1; i++) sc = fmax(sc, fabs(N[i * n1 + i]));
-            s_tol = 1e-12 * (sc > 0 ? sc : 1.0);
+        __syncwarp();
+        for (int i = lane; i < n1 * n1; i += 32) { const int r = i / n1, c = i - r * n1; aug[r * AS + c] = N[i]; }
+        double sc = 0;
+        for (int i = lane; i < n1; i += 32) {
+            aug[i * AS + n1] = rhs[2 * i]; aug[i * AS + n1 + 1] = rhs[2 * i + 1];
+            sc = fmax(sc, fabs(N[i * n1 + i]));
         }
-        __syncthreads();
-        // Gauss-Jordan with partial pivoting (first largest |pivot|), as the oracle
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sc = fmax(sc, __shfl_xor_sync(0xffffffffu, sc, o));
+        const double tol = 1e-12 * (sc > 0 ? sc : 1.0);
+        __syncwarp();
+        // Gauss-Jordan with partial pivoting (first largest |pivot|)
+        bool singular = false;
         for (int c = 0; c < n1; c++) {
-            if (tid == 0) {
-                int pr = c;
-                for (int r = c + 1; r < n1; r++)
-                    if (fabs(aug[r * na + c]) > fabs(aug[pr * na + c])) pr = r;
-                s_piv = pr;
-                s_pval = aug[pr * na + c];
+            double bv = -2.0;
+            int br = 0x7fffffff;
+            for (int r = c + lane; r < n1; r += 32) {
+                // the first largest |pivot| scanning down from row c; a NaN
+                // is never chosen, except a NaN in row c, which nothing beats
+                double v = fabs(aug[r * AS + c]);
+                if (!(v >= 0)) v = r == c ? INFINITY : -1.0;
+                if (v > bv) { bv = v; br = r; }
             }
-            __syncthreads();
-            const int pr = s_piv;
-            const double piv = s_pval;
-            if (!(fabs(piv) > s_tol)) { if (tid == 0) s_flag = 1; break; }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+                if (ov > bv || (ov == bv && orr < br)) { bv = ov; br = orr; }
+            }
+            const int pr = br;
+            const double piv = aug[pr * AS + c];
+            if (!(fabs(piv) > tol)) { singular = true; break; }
+            __syncwarp();
             if (pr != c)
-                for (int j = tid; j < na; j += blockDim.x) { double t = aug[c * na + j]; aug[c * na + j] = aug[pr * na + j]; aug[pr * na + j] = t; }
-            __syncthreads();
-            for (int j = tid; j < na; j += blockDim.x) if (j != c) aug[c * na + j] /= piv;
-            __syncthreads();
-            if (tid == 0) aug[c * na + c] = 1.0;
-            for (int r = tid; r < n1; r += blockDim.x) fac[r] = aug[r * na + c];
-            __syncthreads();
-            for (int i = tid; i < n1 * na; i += blockDim.x) {
-                int r = i / na, j = i - r * na;
-                if (r != c) aug[i] -= fac[r] * aug[c * na + j];
+                for (int j = lane; j < na; j += 32) {
+                    const double t = aug[c * AS + j];
+                    aug[c * AS + j] = aug[pr * AS + j];
+                    aug[pr * AS + j] = t;
+                }
+            __syncwarp();
+            for (int j = c + 1 + lane; j < na; j += 32) aug[c * AS + j] /= piv;
+            if (lane == 0) aug[c * AS + c] = 1.0;
+            __syncwarp();
+            for (int r = lane; r < n1; r += 32) {
+                if (r == c) continue;
+                double* row = aug + r * AS;
+                const double f = row[c];
+                const double* prow = aug + c * AS;
+                for (int j = c; j < na; j++) row[j] -= f * prow[j];
             }
-            __syncthreads();
+            __syncwarp();
         }
-        __syncthreads();
-        if (s_flag) {
-            // singular: keep the previous solution, restore rhs and stop
-            for (int i = tid; i < n1; i += blockDim.x) { aug[i * na + n1] = P[2 * i]; aug[i * na + n1 + 1] = P[2 * i + 1]; }
-            st = -3;
-            break;
-        }
-        for (int i = tid; i < n1; i += blockDim.x) { xs[2 * i] = aug[i * na + n1]; xs[2 * i + 1] = aug[i * na + n1 + 1]; }
-        __syncthreads();
-        // restore rhs into aug, build prefix sums of x into fac-adjacent storage (reuse P after copying rhs back)
-        for (int i = tid; i < n1; i += blockDim.x) { aug[i * na + n1] = P[2 * i]; aug[i * na + n1 + 1] = P[2 * i + 1]; }
-        __syncthreads();
-        if (tid == 0) {
+        if (singular) { st = -3; break; }  // keep the previous solution
+        for (int i = lane; i < n1; i += 32) { xs[2 * i] = aug[i * AS + n1]; xs[2 * i + 1] = aug[i * AS + n1 + 1]; }
+        __syncwarp();
+        if (lane == 0) {
             P[0] = 0; P[1] = 0;
             for (int i = 0; i < n1; i++) { P[2 * (i + 1)] = P[2 * i] + xs[2 * i]; P[2 * (i + 1) + 1] = P[2 * i + 1] + xs[2 * i + 1]; }
         }
-        __syncthreads();
+        __syncwarp();
         // largest squared residual above 1; residuals within a relative 1e-9
         // of it count as ties and the lowest row wins (order independent)
         double best = 1.0;
-        for (int k = tid; k < m; k += blockDim.x) {
+        for (int k = lane; k < m; k += 32) {
             if (!active[k]) continue;
-            double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
-            double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
-            double dx = b[2 * k] - px, dy = b[2 * k + 1] - py;
+            const int ra = __ldg(row_a + k), rb = __ldg(row_b + k);
+            const double sg = __ldg(row_sign + k);
+            const double dx = b[2 * k] - sg * (P[2 * rb] - P[2 * ra]), dy = b[2 * k + 1] - sg * (P[2 * rb + 1] - P[2 * ra + 1]);
             best = fmax(best, dx * dx + dy * dy);
         }
-        for (int off = 16; off > 0; off >>= 1) best = fmax(best, __shfl_down_sync(0xffffffffu, best, off));
-        if ((tid & 31) == 0) red_v[tid >> 5] = best;
-        __syncthreads();
-        if (tid == 0) {
-            double bv = red_v[0];
-            for (int w = 1; w < (int)(blockDim.x >> 5); w++) bv = fmax(bv, red_v[w]);
-            red_v[0] = bv;
-        }
-        __syncthreads();
-        const double top = red_v[0];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
         int bi = 0x7fffffff;
-        if (top > 1.0) {
-            const double thr = top * (1 - 1e-9);
-            for (int k = tid; k < m; k += blockDim.x) {
+        if (best > 1.0) {
+            const double thr = best * (1 - 1e-9);
+            for (int k = lane; k < m; k += 32) {
                 if (!active[k]) continue;
-                double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
-                double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
-                double dx = b[2 * k] - px, dy = b[2 * k + 1] - py;
-                double d = dx * dx + dy * dy;
+                const int ra = __ldg(row_a + k), rb = __ldg(row_b + k);
+                const double sg = __ldg(row_sign + k);
+                const double dx = b[2 * k] - sg * (P[2 * rb] - P[2 * ra]), dy = b[2 * k + 1] - sg * (P[2 * rb + 1] - P[2 * ra + 1]);
+                const double d = dx * dx + dy * dy;
                 if (d >= thr && d > 1.0) { bi = k; break; }
             }
         }
-        for (int off = 16; off > 0; off >>= 1) bi = min(bi, __shfl_down_sync(0xffffffffu, bi, off));
-        __syncthreads();
-        if ((tid & 31) == 0) red_i[tid >> 5] = bi;
-        __syncthreads();
-        if (tid == 0) {
-            int bj = red_i[0];
-            for (int w = 1; w < (int)(blockDim.x >> 5); w++) bj = min(bj, red_i[w]);
-            red_i[0] = bj == 0x7fffffff ? -1 : bj;
-        }
-        __syncthreads();
-        const int k = red_i[0];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bi = min(bi, __shfl_xor_sync(0xffffffffu, bi, o));
+        const int k = bi == 0x7fffffff ? -1 : bi;
         st = k;
         if (k < 0) break;
-        const int a = row_a[k], e = row_b[k];
-        const double sg = row_sign[k];
+        const int a = __ldg(row_a + k), e = __ldg(row_b + k);
+        const double sg = __ldg(row_sign + k);
         const double bx = b[2 * k], by = b[2 * k + 1];
-        __syncthreads();
-        for (int i = tid; i < n1 * n1; i += blockDim.x) {
-            int r = i / n1, c = i - r * n1;
-            if (r >= a && r < e && c >= a && c < e) N[i] -= 1.0;
+        __syncwarp();
+        const int w = e - a;
+        for (int i = lane; i < w * w; i += 32) {
+            const int r = a + i / w, c = a + i % w;
+            N[r * n1 + c] -= 1.0;
         }
-        for (int i = tid; i < n1; i += blockDim.x)
-            if (i >= a && i < e) { aug[i * na + n1] -= sg * bx; aug[i * na + n1 + 1] -= sg * by; }
-        if (tid == 0) { b[2 * k] = 0.f; b[2 * k + 1] = 0.f; active[k] = 0; }
+        for (int i = a + lane; i < e; i += 32) { rhs[2 * i] -= sg * bx; rhs[2 * i + 1] -= sg * by; }
+        if (lane == 0) { b[2 * k] = 0.f; b[2 * k + 1] = 0.f; active[k] = 0; }
     }
-    __syncthreads();
-    if (tid == 0) {
+    __syncwarp();
+    if (lane == 0) {
         status[tile] = st;
         P[0] = 0; P[1] = 0;
         for (int i = 0; i < n1; i++) { P[2 * (i + 1)] = P[2 * i] + xs[2 * i]; P[2 * (i + 1) + 1] = P[2 * i + 1] + xs[2 * i + 1]; }
     }
-    for (int i = tid; i < n1; i += blockDim.x) x_out[(size_t)tile * n1 + i] = make_float2((float)xs[2 * i], (float)xs[2 * i + 1]);
-    __syncthreads();
-    for (int k = tid; k < m; k += blockDim.x) {
-        double px = row_sign[k] * (P[2 * row_b[k]] - P[2 * row_a[k]]);
-        double py = row_sign[k] * (P[2 * row_b[k] + 1] - P[2 * row_a[k] + 1]);
+    for (int i = lane; i < n1; i += 32) x_out[(size_t)tile * n1 + i] = make_float2((float)xs[2 * i], (float)xs[2 * i + 1]);
+    __syncwarp();
+    for (int k = lane; k < m; k += 32) {
+        const int ra = __ldg(row_a + k), rb = __ldg(row_b + k);
+        const double sg = __ldg(row_sign + k);
+        const double px = sg * (P[2 * rb] - P[2 * ra]), py = sg * (P[2 * rb + 1] - P[2 * ra + 1]);
         ((float2*)((char*)grids + (size_t)row_grid[k] * grid_stride + (size_t)ty * grid_pitch))[tx] = make_float2((float)px, (float)py);
     }
 }
@@ -445,22 +464,21 @@ cudaError_t isa_launch_upsample(const float2* in, size_t in_pitch, size_t in_str
     return cudaGetLastError();
 }
 
-size_t isa_solve_smem(int m, int n1)
-{
-    size_t d = (size_t)n1 * n1 + (size_t)n1 * (n1 + 2) + n1 + 2 * (n1 + 1) + 2 * n1;
-    return d * sizeof(double) + (size_t)2 * m * sizeof(float) + m + 16;
-}
+size_t isa_solve_smem(int m, int n1) { return solve_layout(m, n1).bytes; }
 
 cudaError_t isa_launch_solve(const int* row_a, const int* row_b, const int* row_sign, const double* N0, int m, int n1, float2* grids,
                              size_t grid_pitch, size_t grid_stride, const int* row_grid, int tcx, int tcy, float2* x_out, int* status,
                              cudaStream_t st)
 {
-    size_t smem = isa_solve_smem(m, n1);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    const size_t per_warp = isa_solve_smem(m, n1);
+    if (per_warp > 227 * 1024) return cudaErrorInvalidValue;
+    const int wpc = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / per_warp));
+    const size_t smem = per_warp * wpc;
     cudaError_t e = cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_solve<<<tcx * tcy, SOLVE_THREADS, smem, st>>>(row_a, row_b, row_sign, N0, m, n1, grids, grid_pitch, grid_stride, row_grid, tcx, tcy,
-                                                    x_out, status);
+    const int ntiles = tcx * tcy;
+    k_solve<<<(ntiles + wpc - 1) / wpc, 32 * wpc, smem, st>>>(row_a, row_b, row_sign, N0, m, n1, grids, grid_pitch, grid_stride, row_grid, tcx, tcy,
+                                                          x_out, status);
     return cudaGetLastError();
 }
 
