@@ -302,6 +302,8 @@ void color_consts(const isa_raw_info* info, float black[3], float white[3], floa
 // DeBayerBWGaussWB (controller :2384-2418) for one frame into `out`;
 // `gray_out`, when given, also receives the Gaussian of the un-filtered
 // gray image (the accumulation variant, skipFourierFilter = true).
+inline size_t fsz_of(int W, int H) { return (size_t)W * H; }
+
 int bw_frame(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H, const isa_raw_info* info, bool high_pass, float* out,
              const std::vector<float>& taps_hp, float* acc_out, const std::vector<float>& taps_acc, cudaStream_t st)
 {
@@ -320,10 +322,18 @@ int bw_frame(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H, co
         ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)out, (cufftComplex*)c->spec));
         ISA_LAUNCH(c, isa_launch_fourier_filter(c->spec, (size_t)(W / 2 + 1) * sizeof(float2), W, H, 1, 0, 1.0f, c->p.high_pass, 1.0f,
                                          c->p.high_pass_sigma, c->p.clear_axis, 1.0f / ((float)W * (float)H), st));
-        ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)out));
+        if (taps_hp.empty()) {
+            ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)out));
+        } else {
+            // inverse transform into scratch, then clamp + Gauss back into `out` in one pass
+            ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)c->tmp));
+            ISA_LAUNCH(c, isa_launch_gauss(c->tmp, pitch, out, pitch, c->tmp + fsz_of(W, H), pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), 1,
+                                           st));
+        }
+        return ISA_OK;
     }
     if (!taps_hp.empty())
-        ISA_LAUNCH(c, isa_launch_gauss(out, pitch, out, pitch, c->tmp, pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), high_pass ? 1 : 0, st));
+        ISA_LAUNCH(c, isa_launch_gauss(out, pitch, out, pitch, c->tmp, pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), 0, st));
     return ISA_OK;
 }
 

@@ -175,9 +175,60 @@ __global__ void k_gauss_pass(const float* __restrict__ in, size_t in_pitch, floa
         int sy = VERT ? isa::clampi(y + k - c0, 0, H - 1) : y;
         float v = isa::row_ptr(in, in_pitch, sy)[sx * C + c];
         if (clamp_in) v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
-        s += taps.t[k] * v;
+        s = fmaf(taps.t[k], v, s);
     }
     isa::row_ptr(out, out_pitch, y)[x] = s;
+}
+
+// Both passes of the separable Gauss in one launch for one channel and
+// radius R <= 4: the input tile with an R halo (replicate border, optional
+// clamp to [0, 1]) and the horizontally filtered rows live in shared memory.
+// The arithmetic and its order are those of the two k_gauss_pass launches,
+// so the result is the same; HBM traffic is one read and one write.
+constexpr int G2_TX = 128, G2_TY = 32;
+
+template <int R>
+__global__ void __launch_bounds__(256) k_gauss2d(const float* __restrict__ in, size_t in_pitch, float* __restrict__ out, size_t out_pitch, int W,
+                                                 int H, Taps taps, int clamp_in)
+{
+    constexpr int SW = G2_TX + 2 * R, SH = G2_TY + 2 * R, NT = 2 * R + 1;
+    __shared__ float s_in[SH][SW];
+    __shared__ float s_h[SH][G2_TX];
+    const int x0 = blockIdx.x * G2_TX, y0 = blockIdx.y * G2_TY;
+    const int tid = threadIdx.x;
+    float t[NT];
+#pragma unroll
+    for (int k = 0; k < NT; k++) t[k] = taps.t[k];
+    for (int yy = tid >> 5; yy < SH; yy += 8) {
+        const float* row = isa::row_ptr(in, in_pitch, isa::clampi(y0 - R + yy, 0, H - 1));
+        for (int xx = tid & 31; xx < SW; xx += 32) {
+            float v = __ldg(row + isa::clampi(x0 - R + xx, 0, W - 1));
+            if (clamp_in) v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+            s_in[yy][xx] = v;
+        }
+    }
+    __syncthreads();
+    for (int yy = tid >> 5; yy < SH; yy += 8)
+        for (int xx = tid & 31; xx < G2_TX; xx += 32) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < NT; k++) s = fmaf(t[k], s_in[yy][xx + k], s);
+            s_h[yy][xx] = s;
+        }
+    __syncthreads();
+    for (int yy = tid >> 5; yy < G2_TY; yy += 8) {
+        const int y = y0 + yy;
+        if (y >= H) break;
+        float* orow = isa::row_ptr(out, out_pitch, y);
+        for (int xx = tid & 31; xx < G2_TX; xx += 32) {
+            const int x = x0 + xx;
+            if (x >= W) break;
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < NT; k++) s = fmaf(t[k], s_h[yy + k][xx], s);
+            orow[x] = s;
+        }
+    }
 }
 
 // NPP ResizeSqrPixel super-sampling by an integer factor: block mean.
@@ -252,6 +303,17 @@ cudaError_t isa_launch_gauss(const float* in, size_t in_pitch, float* out, size_
     Taps t;
     t.n = ntaps;
     for (int i = 0; i < ntaps; i++) t.t[i] = taps[i];
+    if (C == 1 && in != out && (ntaps & 1) && ntaps <= 9) {
+        dim3 g((W + G2_TX - 1) / G2_TX, (H + G2_TY - 1) / G2_TY);
+        switch (ntaps / 2) {
+        case 0: k_gauss2d<0><<<g, 256, 0, st>>>(in, in_pitch, out, out_pitch, W, H, t, clamp01_input); break;
+        case 1: k_gauss2d<1><<<g, 256, 0, st>>>(in, in_pitch, out, out_pitch, W, H, t, clamp01_input); break;
+        case 2: k_gauss2d<2><<<g, 256, 0, st>>>(in, in_pitch, out, out_pitch, W, H, t, clamp01_input); break;
+        case 3: k_gauss2d<3><<<g, 256, 0, st>>>(in, in_pitch, out, out_pitch, W, H, t, clamp01_input); break;
+        default: k_gauss2d<4><<<g, 256, 0, st>>>(in, in_pitch, out, out_pitch, W, H, t, clamp01_input); break;
+        }
+        return cudaGetLastError();
+    }
     dim3 b(64, 4);
     k_gauss_pass<false><<<grid2(W * C, H, b), b, 0, st>>>(in, in_pitch, tmp, tmp_pitch, W, H, C, t, clamp01_input);
     k_gauss_pass<true><<<grid2(W * C, H, b), b, 0, st>>>(tmp, tmp_pitch, out, out_pitch, W, H, C, t, 0);

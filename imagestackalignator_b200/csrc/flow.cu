@@ -232,10 +232,11 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
     issue_samples(erow(0), __ldg(isa::row_ptr(flow_in, flow_pitch, erow(0)) + col));
     if (nE > 1) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(1)) + col);
     double cs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // ring slots of rows e, e-1, e-2, e-3, e-4 (mod 5) and of the product row (mod WIN), advanced incrementally
+    int r0 = 0, r1 = 4, r2 = 3, r3 = 2, r4 = 1, pw = 0;
     for (int e = 0; e < nE; e++) {
-        const int slot = e % 5;
-        Ew[slot * NT + t] = isa::lerp2(s00, s10, s01, s11, sa, sb);
-        Er[slot * NT + t] = sref;
+        Ew[r0 * NT + t] = isa::lerp2(s00, s10, s01, s11, sa, sb);
+        Er[r0 * NT + t] = sref;
         if (e + 1 < nE) {
             issue_samples(erow(e + 1), fnext);
             if (e + 2 < nE) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(e + 2)) + col);
@@ -244,18 +245,16 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
         if (e >= 4) {
             const int gi = e - 4;  // product row: image row y0 - h + gi
             if (t >= 2 && t < NT - 2) {
-                const float* ew = Ew + ((e - 2) % 5) * NT + t;
-                const float* er = Er + ((e - 2) % 5) * NT + t;
-                float t0 = (ew[2] - ew[1] * 8.0f + ew[-1] * 8.0f - ew[-2]) / 12.0f;
-                float t1 = (er[2] - er[1] * 8.0f + er[-1] * 8.0f - er[-2]) / 12.0f;
-                const float dx = (t0 + t1) * 0.5f;
-                const int sp2 = (e % 5) * NT + t, sp1 = ((e - 1) % 5) * NT + t, sm1 = ((e - 3) % 5) * NT + t, sm2 = ((e - 4) % 5) * NT + t;
-                t0 = (Ew[sp2] - Ew[sp1] * 8.0f + Ew[sm1] * 8.0f - Ew[sm2]) / 12.0f;
-                t1 = (Er[sp2] - Er[sp1] * 8.0f + Er[sm1] * 8.0f - Er[sm2]) / 12.0f;
-                const float dy = (t0 + t1) * 0.5f;
+                // five-tap derivatives averaged over both images: ((8 (c[-1] - c[1]) + c[2] - c[-2]) / 12 of each) / 2
+                const float* ew = Ew + r2 * NT + t;
+                const float* er = Er + r2 * NT + t;
+                const float gx = (ew[2] - ew[-2]) + (er[2] - er[-2]) + 8.0f * ((ew[-1] - ew[1]) + (er[-1] - er[1]));
+                const float gy = (Ew[r0 * NT + t] - Ew[r4 * NT + t]) + (Er[r0 * NT + t] - Er[r4 * NT + t]) +
+                                 8.0f * ((Ew[r3 * NT + t] - Ew[r1 * NT + t]) + (Er[r3 * NT + t] - Er[r1 * NT + t]));
+                const float dx = gx * (1.0f / 24.0f), dy = gy * (1.0f / 24.0f);
                 const float dt = ew[0] - er[0];
                 const float p[5] = {dx * dx, dx * dy, dy * dy, dx * dt, dy * dt};
-                float* pr = Pr + (gi % WIN) * 5 * NT + t;
+                float* pr = Pr + pw * 5 * NT + t;
 #pragma unroll
                 for (int ch = 0; ch < 5; ch++) {
                     const float old = gi >= WIN ? pr[ch * NT] : 0.f;
@@ -263,6 +262,7 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
                     pr[ch * NT] = p[ch];
                 }
             }
+            pw = pw + 1 == WIN ? 0 : pw + 1;
             if (gi >= 2 * H) {
                 const int o = gi - 2 * H;  // output row y0 + o
                 if (t >= 2 && t < NT - 2) {
@@ -306,6 +306,7 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
             }
         }
         __syncthreads();
+        r4 = r3; r3 = r2; r2 = r1; r1 = r0; r0 = r0 + 1 == 5 ? 0 : r0 + 1;
     }
 }
 
