@@ -83,12 +83,12 @@ __device__ __forceinline__ float2 lk_update(float2 f, double sxx, double sxy, do
     return make_float2((float)((double)f.x + u), (float)((double)f.y + v));
 }
 
+// c, s: cosine and sine of the pre-alignment rotation (uniform, computed once on the host).
 __global__ void k_flow_from_tiles(const float2* __restrict__ tiles, size_t tile_pitch, int tcx, int tcy, int W, int H, float bx, float by,
-                                  float rot, float2* __restrict__ flow, size_t flow_pitch)
+                                  float c, float s, float2* __restrict__ flow, size_t flow_pitch)
 {
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
-    float c = cosf(rot), s = sinf(rot);
     float fx = c * -bx - s * -by;
     float fy = s * -bx + c * -by;
     float pcx = (float)(x - W / 2), pcy = (float)(y - H / 2);
@@ -330,7 +330,8 @@ cudaError_t isa_launch_flow_from_tiles(const float2* tiles, size_t tile_pitch, i
                                        float2* flow, size_t flow_pitch, cudaStream_t st)
 {
     dim3 b(32, 8);
-    k_flow_from_tiles<<<grid2(W, H, b), b, 0, st>>>(tiles, tile_pitch, tcx, tcy, W, H, bx, by, rot, flow, flow_pitch);
+    const float c = rot == 0.f ? 1.f : (float)cos((double)rot), s = rot == 0.f ? 0.f : (float)sin((double)rot);
+    k_flow_from_tiles<<<grid2(W, H, b), b, 0, st>>>(tiles, tile_pitch, tcx, tcy, W, H, bx, by, c, s, flow, flow_pitch);
     return cudaGetLastError();
 }
 

@@ -152,9 +152,14 @@ __device__ __forceinline__ void pixel_x2(const X2Args& A, int x, int y)
     // flow: bilinear, mirror addressing (same position for every frame)
     const int fi0 = isa::mirror(ib, g.W), fi1 = isa::mirror(ib + 1, g.W);
     const size_t fr0 = (size_t)isa::mirror(jb, g.H) * A.flow_pitch, fr1 = (size_t)isa::mirror(jb + 1, g.H) * A.flow_pitch;
-    // interior: the unshifted taps' mask cells are (X - 2) >> 2 + {0, 1}, rows alike
+    // interior: the unshifted taps' mask cells are (X - 2) >> 2 + {0, 1}, rows alike,
+    // and the shifted 3 x 3 block [k0, k0 + 2] x [j0, j0 + 2] lies inside the crop:
+    // k0 = (X + sx - 2) >> 1 in [cx0, cx1 - 2]  <=>  sx in [2 cx0 + 2 - X, 2 cx1 - 1 - X]
     const bool mask_interior = ((X - 2) >> 1) >= g.cx0 && ((X + 2) >> 1) <= g.cx1 && ((Y - 2) >> 1) >= g.cy0 && ((Y + 2) >> 1) <= g.cy1;
+    const int sxlo = mask_interior ? 2 * g.cx0 + 2 - X : (1 << 29), sylo = 2 * g.cy0 + 2 - Y;
+    const unsigned sxspan = mask_interior ? (unsigned)(2 * g.cx1 - 1 - X - sxlo) : 0u, syspan = (unsigned)(2 * g.cy1 - 1 - Y - sylo);
     const int ux0 = (X - 2) >> 2, uy0 = (Y - 2) >> 2;
+    const size_t moff = (size_t)uy0 * A.mask_pitch + (size_t)ux0 * sizeof(float4);
     for (int f = 0; f < A.nframes; f++) {
         const isa_frame_in fr = A.frames ? A.frames[f] : A.single;
         int sx = 0, sy = 0;
@@ -168,7 +173,7 @@ __device__ __forceinline__ void pixel_x2(const X2Args& A, int x, int y)
         const int Xs = X + sx, Ys = Y + sy;
         const int k0 = (Xs - 2) >> 1, j0 = (Ys - 2) >> 1;
         float Ac[3] = {0.f, 0.f, 0.f}, Wc[3] = {0.f, 0.f, 0.f};
-        if (mask_interior && k0 >= g.cx0 && k0 + 2 <= g.cx1 && j0 >= g.cy0 && j0 + 2 <= g.cy1) {
+        if ((unsigned)(sx - sxlo) <= sxspan && (unsigned)(sy - sylo) <= syspan) {
             float v[3][3];
 #pragma unroll
             for (int j = 0; j < 3; j++) {
@@ -181,8 +186,8 @@ __device__ __forceinline__ void pixel_x2(const X2Args& A, int x, int y)
             const bool hG = (int)(fx ^ fy) == A.bayer.g0, frr = (int)fy == A.bayer.ry;
             float cq[2][2][4];
             if (fr.mask) {
-                const float4* m0 = isa::row_ptr(fr.mask, A.mask_pitch, uy0) + ux0;
-                const float4* m1 = isa::row_ptr(fr.mask, A.mask_pitch, uy0 + 1) + ux0;
+                const float4* m0 = (const float4*)((const char*)fr.mask + moff);
+                const float4* m1 = (const float4*)((const char*)fr.mask + moff + A.mask_pitch);
                 float4 M00 = __ldg(m0), M01 = __ldg(m0 + 1), M10 = __ldg(m1), M11 = __ldg(m1 + 1);
                 if (!SANE) { M00 = sanitize(M00); M01 = sanitize(M01); M10 = sanitize(M10); M11 = sanitize(M11); }
                 class_certs(M00, hG, frr, cq[0][0]);
@@ -274,7 +279,7 @@ __device__ __forceinline__ void pixel_x2(const X2Args& A, int x, int y)
 }
 
 template <bool SANE>
-__global__ void __launch_bounds__(256, 2) k_accumulate_x2(const X2Args A)
+__global__ void __launch_bounds__(256, SANE ? 3 : 2) k_accumulate_x2(const X2Args A)
 {
     const int ph = blockIdx.x & 3, rph = blockIdx.y & 3;
     const int x = (blockIdx.x >> 2) * 128 + 4 * threadIdx.x + ph;
