@@ -38,25 +38,29 @@ __device__ __forceinline__ void tile_offset(int tx, int ty, int T, int Wl, int H
     oy = (int)roundf(sy);
 }
 
-// Shared-memory layout of k_track, in floats.
+// Shared-memory layout of k_track, in floats. The template is stored as
+// interleaved row pairs (rows 2i and 2i + 1 side by side), so one 64-bit
+// load gives a thread both of its template rows.
 template <int T, int S>
 struct TrackDims {
+    static_assert(T % 2 == 0 && T <= 64 && 32 % (T / 2 > 32 ? 32 : T / 2) == 0, "tile size");
     static constexpr int B = T + 2 * S, D = 2 * S + 1;
-    static constexpr int TP = T + 1, BP = B + 1;  // odd strides: conflict-free column reads across lanes
-    static constexpr int NI = T * D;              // (template row, shift row) items
+    static constexpr int HP = T / 2;        // template row pairs = lanes summed per shift row
+    static constexpr int TP2 = T + 1;       // row-pair stride in float2: odd, so 64-bit column reads are conflict-free
+    static constexpr int BP = B + 1;        // odd stride: conflict-free column reads
+    static constexpr int NI = HP * D;       // (row pair, shift row) items
     static constexpr int NT = (NI + 31) / 32 * 32;
-    static constexpr int RW = T < 32 ? T : 32;    // template rows summed by one warp
-    static constexpr int NCC = T / RW;            // partial sums per map entry (2 when T = 64)
-    static constexpr int OFF_TPL = 0, OFF_BLK = OFF_TPL + T * TP, OFF_PART = OFF_BLK + B * BP;
-    static constexpr int OFF_MAP = OFF_PART + D * D * NCC;
+    static constexpr int OFF_TPL = 0, OFF_BLK = OFF_TPL + HP * TP2 * 2, OFF_MAP = OFF_BLK + B * BP;
     static constexpr int TOTAL = OFF_MAP + D * D;
     static constexpr size_t BYTES = (size_t)TOTAL * sizeof(float);
 };
 
-// Thread (y, sy) streams template row y against block row y + sy with a
-// D-wide register window, accumulating (r - t)^2 for the D column shifts;
-// the template rows are then summed across lanes with shuffles in a fixed
-// order (deterministic), and warp 0 finds the first minimum.
+// Thread (row pair, sy) streams template rows 2i, 2i + 1 against block rows
+// 2i + sy, 2i + 1 + sy with a D-wide register window of float2 pairs,
+// accumulating (r - t)^2 for both rows and the D column shifts with packed
+// FP32x2 arithmetic (each lane of a pair rounds exactly as the scalar
+// operation would); the rows are then summed across lanes with shuffles in
+// a fixed order (deterministic), and warp 0 finds the first minimum.
 template <int T, int S>
 __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* const* __restrict__ frames, size_t pitch, int Wl, int Hl, int tcx,
                                                                int tcy, const isa_pair_desc* __restrict__ pairs, float2* __restrict__ grids,
@@ -64,11 +68,10 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
                                                                int* __restrict__ argmin_out)
 {
     using L = TrackDims<T, S>;
-    constexpr int B = L::B, D = L::D, TP = L::TP, BP = L::BP, RW = L::RW;
-    extern __shared__ float smf[];
+    constexpr int B = L::B, D = L::D, TP2 = L::TP2, BP = L::BP, HP = L::HP;
+    extern __shared__ __align__(16) float smf[];
     float* tpl = smf + L::OFF_TPL;
     float* blk = smf + L::OFF_BLK;
-    float* part = smf + L::OFF_PART;
     float* map = smf + L::OFF_MAP;
     const int p = blockIdx.x;
     const int tile = blockIdx.y;
@@ -92,9 +95,10 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
     for (int k = 0; k < BX; k++) ct[k] = isa::clampi(tx * T + lane + 32 * k + oxt, 0, Wl - 1);
     for (int y = warp; y < T; y += NW) {
         const float* row = isa::row_ptr(imr, pitch, isa::clampi(ty * T + S + y + oyr, 0, Hl - 1));
+        float* dst = tpl + (y >> 1) * TP2 * 2 + (y & 1);
 #pragma unroll
         for (int k = 0; k < TX; k++)
-            if (lane + 32 * k < T) tpl[y * TP + lane + 32 * k] = __ldg(row + cr[k]);
+            if (lane + 32 * k < T) dst[2 * (lane + 32 * k)] = __ldg(row + cr[k]);
     }
     for (int y = warp; y < B; y += NW) {
         const float* row = isa::row_ptr(imt, pitch, isa::clampi(ty * T + y + oyt, 0, Hl - 1));
@@ -103,36 +107,41 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
             if (lane + 32 * k < B) blk[y * BP + lane + 32 * k] = __ldg(row + ct[k]);
     }
     __syncthreads();
-    const int y = tid % T, sy = tid / T;
-    float acc[D];
+    const int yp = tid % HP, sy = tid / HP;
+    float2 acc[D];
 #pragma unroll
-    for (int k = 0; k < D; k++) acc[k] = 0.f;
+    for (int k = 0; k < D; k++) acc[k] = make_float2(0.f, 0.f);
     if (tid < L::NI) {
-        const float* tr = tpl + y * TP;
-        const float* br = blk + (y + sy) * BP;
-        float win[D];
+        const float2* tr = (const float2*)tpl + yp * TP2;
+        const float* b0 = blk + (2 * yp + sy) * BP;
+        const float* b1 = b0 + BP;
+        const float2 m1 = make_float2(-1.f, -1.f);
+        float2 win[D];
 #pragma unroll
-        for (int k = 0; k < D - 1; k++) win[k] = br[k];
+        for (int k = 0; k < D - 1; k++) win[k] = make_float2(b0[k], b1[k]);
 #pragma unroll
         for (int x = 0; x < T; x++) {
-            win[D - 1] = br[x + D - 1];
-            const float r = tr[x];
+            win[D - 1] = make_float2(b0[x + D - 1], b1[x + D - 1]);
+            const float2 r = tr[x];
 #pragma unroll
             for (int k = 0; k < D; k++) {
-                const float d = r - win[k];
-                acc[k] = fmaf(d, d, acc[k]);
+                const float2 d = __ffma2_rn(win[k], m1, r);  // r - t, exactly rounded
+                acc[k] = __ffma2_rn(d, d, acc[k]);
             }
 #pragma unroll
             for (int k = 0; k < D - 1; k++) win[k] = win[k + 1];
         }
     }
+    float sum[D];
 #pragma unroll
-    for (int o = RW / 2; o > 0; o >>= 1)
+    for (int k = 0; k < D; k++) sum[k] = acc[k].x + acc[k].y;
 #pragma unroll
-        for (int k = 0; k < D; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-    if (tid < L::NI && (y % RW) == 0) {
+    for (int o = HP / 2; o > 0; o >>= 1)
 #pragma unroll
-        for (int k = 0; k < D; k++) part[(sy * D + k) * L::NCC + y / RW] = acc[k];
+        for (int k = 0; k < D; k++) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
+    if (tid < L::NI && yp == 0) {
+#pragma unroll
+        for (int k = 0; k < D; k++) map[sy * D + k] = sum[k];
     }
     __syncthreads();
     if (warp == 0) {
@@ -140,10 +149,7 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
         float mn = FLT_MAX, mx = -FLT_MAX;
         int mi = 0x7fffffff;
         for (int i = lane; i < D * D; i += 32) {
-            float v = part[i * L::NCC];
-#pragma unroll
-            for (int q = 1; q < L::NCC; q++) v += part[i * L::NCC + q];
-            map[i] = v;
+            const float v = map[i];
             mx = fmaxf(mx, v);
             if (v < mn) { mn = v; mi = i; }
         }
@@ -206,7 +212,6 @@ cudaError_t launch_track_ts(const float* const* frames, size_t pitch, int Wl, in
                             cudaStream_t st)
 {
     using L = TrackDims<T, S>;
-    static_assert(T <= 32 ? (32 % T == 0) : (T % 32 == 0), "tile rows must tile a warp");
     if (L::BYTES > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_track<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
         if (e != cudaSuccess) return e;
