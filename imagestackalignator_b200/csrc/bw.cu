@@ -11,7 +11,7 @@
 
 namespace {
 
-constexpr int DM_TX = 32, DM_TY = 16;       // output tile
+constexpr int DM_TX = 64, DM_TY = 16;                // output tile
 constexpr int DM_LW = DM_TX + 6, DM_LH = DM_TY + 6;  // linear tile (halo 3)
 constexpr int DM_GW = DM_TX + 2, DM_GH = DM_TY + 2;  // green tile (halo 1)
 
@@ -21,87 +21,134 @@ __device__ __forceinline__ float srgb_gamma(float v) {
     return v <= 0.0031308f ? 12.92f * v : (1.0f + 0.055f) * powf(v, 1.0f / 2.4f) - 0.055f;
 }
 
+// The same curve with the power evaluated as exp2(log2(v) / 2.4) (hardware
+// log2 approximation; relative error about 3e-7 on [0.0031308, 1]).
+__device__ __forceinline__ float srgb_gamma_fast(float v) {
+    return v <= 0.0031308f ? 12.92f * v : (1.0f + 0.055f) * exp2f(__log2f(v) * (1.0f / 2.4f)) - 0.055f;
+}
+
+// Thread (tx, ty) of a (32, 8) block works on pixel pairs (2 tx, 2 tx + 1)
+// of a row: the column parity of each pixel of the pair is a compile-time
+// constant and the row parity is the same for the whole warp, so the CFA
+// colour, and with it every branch below, is uniform across the warp.
 __global__ void __launch_bounds__(256) k_demosaic_gray(const uint16_t* __restrict__ raw, size_t raw_pitch, int W, int H, unsigned cfa,
-                                                      Color3 black, Color3 scale, Color3 divisor, Color3 gw, int gamma_gray,
+                                                      Color3 black, Color3 scale, Color3 rdivisor, Color3 gw, int gamma_gray,
                                                       float* __restrict__ gray, size_t gray_pitch, float* __restrict__ rgb,
-                                                      size_t rgb_pitch)
+                                                      size_t rgb_pitch, bool vec_gray, bool vec_rgb)
 {
     __shared__ float lin[DM_LH][DM_LW];
     __shared__ float grn[DM_GH][DM_GW];
-    const int x0 = blockIdx.x * DM_TX, y0 = blockIdx.y * DM_TY;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
-    for (int i = tid; i < DM_LW * DM_LH; i += nt) {
-        int ly = i / DM_LW, lx = i - ly * DM_LW;
-        int gx = x0 + lx - 3, gy = y0 + ly - 3;
-        float v = 0.f;
-        if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-            int c = isa::cfa_at(cfa, gx, gy);
-            float r = (float)isa::row_ptr(raw, raw_pitch, gy)[gx];
-            v = (r - black.v[c]) * scale.v[c];
-        }
-        lin[ly][lx] = v;
-    }
-    __syncthreads();
-    for (int i = tid; i < DM_GW * DM_GH; i += nt) {
-        int ly = i / DM_GW, lx = i - ly * DM_GW;
-        int gx = x0 + lx - 1, gy = y0 + ly - 1;
-        float g = 0.f;
-        if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2) {
-            int c = isa::cfa_at(cfa, gx, gy);
-            int cx = lx + 2, cy = ly + 2;  // position in lin
-            if (c == 1) {
-                g = lin[cy][cx];
-            } else if (c == 0 || c == 2) {
-                float p = lin[cy][cx];
-                float xm2 = lin[cy][cx - 2], xm1 = lin[cy][cx - 1], xp1 = lin[cy][cx + 1], xp2 = lin[cy][cx + 2];
-                float ym2 = lin[cy - 2][cx], ym1 = lin[cy - 1][cx], yp1 = lin[cy + 1][cx], yp2 = lin[cy + 2][cx];
-                float gradX = 0.5f * fabsf(xp1 - xm1), gradY = 0.5f * fabsf(yp1 - ym1);
-                float lapX = 0.25f * fabsf(2.0f * p - xm2 - xp2), lapY = 0.25f * fabsf(2.0f * p - ym2 - yp2);
-                float ipX = 0.125f * (-xm2 + 4.0f * xm1 + 2.0f * p + 4.0f * xp1 - xp2);
-                float ipY = 0.125f * (-ym2 + 4.0f * ym1 + 2.0f * p + 4.0f * yp1 - yp2);
-                float w = (gradY + lapY) / (gradX + gradY + lapX + lapY + 0.000000001f);
-                g = w * ipX + (1.0f - w) * ipY;
+    const int x0 = blockIdx.x * DM_TX, y0 = blockIdx.y * DM_TY;  // x0, y0 even
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    // 1. black-subtracted, white-balanced linear values with a 3-pixel halo
+    for (int ly = ty; ly < DM_LH; ly += 8) {
+        const int gy = y0 + ly - 3;
+        const bool yin = gy >= 0 && gy < H;
+        const uint16_t* rr = isa::row_ptr(raw, raw_pitch, yin ? gy : 0);
+        for (int pi = tx; pi < DM_LW / 2; pi += 32) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int lx = 2 * pi + k, gx = x0 + lx - 3;
+                float v = 0.f;
+                if (yin && gx >= 0 && gx < W) {
+                    const int c = isa::cfa_at(cfa, gx, gy);
+                    v = ((float)__ldg(rr + gx) - black.v[c]) * scale.v[c];
+                }
+                lin[ly][lx] = v;
             }
         }
-        grn[ly][lx] = g;
     }
     __syncthreads();
-    for (int i = tid; i < DM_TX * DM_TY; i += nt) {
-        int ly = i / DM_TX, lx = i - ly * DM_TX;
-        int gx = x0 + lx, gy = y0 + ly;
-        if (gx >= W || gy >= H) continue;
-        float r = 0.f, g = 0.f, b = 0.f;
-        if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2) {
-            int c = isa::cfa_at(cfa, gx, gy);
-            int nx = isa::cfa_at(cfa, gx + 1, gy);
-            int cx = lx + 3, cy = ly + 3;      // lin
-            int kx = lx + 1, ky = ly + 1;      // grn
-            g = grn[ky][kx];
-            if (c == 1) {
-                float hsum = (lin[cy][cx - 1] - grn[ky][kx - 1]) + (lin[cy][cx + 1] - grn[ky][kx + 1]);
-                float vsum = (lin[cy - 1][cx] - grn[ky - 1][kx]) + (lin[cy + 1][cx] - grn[ky + 1][kx]);
-                float h = g + 0.5f * hsum, v = g + 0.5f * vsum;
-                if (nx == 0) { r = h; b = v; } else { b = h; r = v; }
-            } else if (c == 0 || c == 2) {
-                float own = lin[cy][cx];
-                float other = g + 0.25f * ((lin[cy - 1][cx - 1] - grn[ky - 1][kx - 1]) + (lin[cy - 1][cx + 1] - grn[ky - 1][kx + 1]) +
-                                           (lin[cy + 1][cx + 1] - grn[ky + 1][kx + 1]) + (lin[cy + 1][cx - 1] - grn[ky + 1][kx - 1]));
-                if (c == 0) { r = own; b = other; } else { b = own; r = other; }
+    // 2. green plane (Wu-Zhang gradient-weighted interpolation) with a 1-pixel halo
+    for (int ly = ty; ly < DM_GH; ly += 8) {
+        const int gy = y0 + ly - 1;
+        for (int pi = tx; pi < DM_GW / 2; pi += 32) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int lx = 2 * pi + k, gx = x0 + lx - 1;
+                float g = 0.f;
+                if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2) {
+                    const int c = isa::cfa_at(cfa, gx, gy);
+                    const int cx = lx + 2, cy = ly + 2;  // position in lin
+                    if (c == 1) {
+                        g = lin[cy][cx];
+                    } else if (c == 0 || c == 2) {
+                        const float p = lin[cy][cx];
+                        const float xm2 = lin[cy][cx - 2], xm1 = lin[cy][cx - 1], xp1 = lin[cy][cx + 1], xp2 = lin[cy][cx + 2];
+                        const float ym2 = lin[cy - 2][cx], ym1 = lin[cy - 1][cx], yp1 = lin[cy + 1][cx], yp2 = lin[cy + 2][cx];
+                        const float gradX = 0.5f * fabsf(xp1 - xm1), gradY = 0.5f * fabsf(yp1 - ym1);
+                        const float lapX = 0.25f * fabsf(2.0f * p - xm2 - xp2), lapY = 0.25f * fabsf(2.0f * p - ym2 - yp2);
+                        const float ipX = 0.125f * (-xm2 + 4.0f * xm1 + 2.0f * p + 4.0f * xp1 - xp2);
+                        const float ipY = 0.125f * (-ym2 + 4.0f * ym1 + 2.0f * p + 4.0f * yp1 - yp2);
+                        const float w = __fdividef(gradY + lapY, gradX + gradY + lapX + lapY + 0.000000001f);
+                        g = w * ipX + (1.0f - w) * ipY;
+                    }
+                }
+                grn[ly][lx] = g;
             }
         }
-        r /= divisor.v[0]; g /= divisor.v[1]; b /= divisor.v[2];
+    }
+    __syncthreads();
+    // 3. red and blue by colour differences, removal of the white balance, output
+    for (int ly = ty; ly < DM_TY; ly += 8) {
+        const int gy = y0 + ly;
+        if (gy >= H) break;
+        float o[2][3];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int lx = 2 * tx + k, gx = x0 + lx;
+            float r = 0.f, g = 0.f, b = 0.f;
+            if (gx >= 2 && gx < W - 2 && gy >= 2 && gy < H - 2) {
+                const int c = isa::cfa_at(cfa, gx, gy);
+                const int nx = isa::cfa_at(cfa, gx + 1, gy);
+                const int cx = lx + 3, cy = ly + 3;  // lin
+                const int kx = lx + 1, ky = ly + 1;  // grn
+                g = grn[ky][kx];
+                if (c == 1) {
+                    const float hsum = (lin[cy][cx - 1] - grn[ky][kx - 1]) + (lin[cy][cx + 1] - grn[ky][kx + 1]);
+                    const float vsum = (lin[cy - 1][cx] - grn[ky - 1][kx]) + (lin[cy + 1][cx] - grn[ky + 1][kx]);
+                    const float h = g + 0.5f * hsum, v = g + 0.5f * vsum;
+                    if (nx == 0) { r = h; b = v; } else { b = h; r = v; }
+                } else if (c == 0 || c == 2) {
+                    const float own = lin[cy][cx];
+                    const float other = g + 0.25f * ((lin[cy - 1][cx - 1] - grn[ky - 1][kx - 1]) + (lin[cy - 1][cx + 1] - grn[ky - 1][kx + 1]) +
+                                                     (lin[cy + 1][cx + 1] - grn[ky + 1][kx + 1]) + (lin[cy + 1][cx - 1] - grn[ky + 1][kx - 1]));
+                    if (c == 0) { r = own; b = other; } else { b = own; r = other; }
+                }
+            }
+            o[k][0] = r * rdivisor.v[0];
+            o[k][1] = g * rdivisor.v[1];
+            o[k][2] = b * rdivisor.v[2];
+        }
+        const int gx0 = x0 + 2 * tx;
+        if (gx0 >= W) continue;  // W is even: both pixels of the pair are inside or outside together
         if (rgb) {
-            float* o = isa::row_ptr(rgb, rgb_pitch, gy) + 3 * gx;
-            o[0] = r; o[1] = g; o[2] = b;
+            float* op = isa::row_ptr(rgb, rgb_pitch, gy) + 3 * gx0;
+            if (vec_rgb) {
+                ((float2*)op)[0] = make_float2(o[0][0], o[0][1]);
+                ((float2*)op)[1] = make_float2(o[0][2], o[1][0]);
+                ((float2*)op)[2] = make_float2(o[1][1], o[1][2]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 6; k++) op[k] = o[k / 3][k % 3];
+            }
         }
         if (gray) {
-            if (gamma_gray) {
-                r = isnan(r) ? 0.f : r; g = isnan(g) ? 0.f : g; b = isnan(b) ? 0.f : b;
-                r = srgb_gamma(fmaxf(fminf(r, 1.0f), 0.0f));
-                g = srgb_gamma(fmaxf(fminf(g, 1.0f), 0.0f));
-                b = srgb_gamma(fmaxf(fminf(b, 1.0f), 0.0f));
+            float q[2];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                float r = o[k][0], g = o[k][1], b = o[k][2];
+                if (gamma_gray) {
+                    r = isnan(r) ? 0.f : r; g = isnan(g) ? 0.f : g; b = isnan(b) ? 0.f : b;
+                    r = srgb_gamma_fast(fmaxf(fminf(r, 1.0f), 0.0f));
+                    g = srgb_gamma_fast(fmaxf(fminf(g, 1.0f), 0.0f));
+                    b = srgb_gamma_fast(fmaxf(fminf(b, 1.0f), 0.0f));
+                }
+                q[k] = gw.v[0] * r + gw.v[1] * g + gw.v[2] * b;
             }
-            isa::row_ptr(gray, gray_pitch, gy)[gx] = gw.v[0] * r + gw.v[1] * g + gw.v[2] * b;
+            float* gp = isa::row_ptr(gray, gray_pitch, gy) + gx0;
+            if (vec_gray) *(float2*)gp = make_float2(q[0], q[1]);
+            else { gp[0] = q[0]; gp[1] = q[1]; }
         }
     }
 }
@@ -273,9 +320,12 @@ cudaError_t isa_launch_demosaic_gray(const uint16_t* raw, size_t raw_pitch, int 
                                      float* gray, size_t gray_pitch, float* rgb, size_t rgb_pitch, cudaStream_t st)
 {
     Color3 b, s, d, g;
-    for (int c = 0; c < 3; c++) { b.v[c] = black[c]; s.v[c] = scale[c]; d.v[c] = divisor[c]; g.v[c] = gray_w ? gray_w[c] : 0.f; }
+    for (int c = 0; c < 3; c++) { b.v[c] = black[c]; s.v[c] = scale[c]; d.v[c] = (float)(1.0 / (double)divisor[c]); g.v[c] = gray_w ? gray_w[c] : 0.f; }
+    if (W & 1) return cudaErrorInvalidValue;
+    // pixel pairs are stored as float2 where rows are 8-byte aligned
+    const bool vg = !((gray_pitch & 7) || ((uintptr_t)gray & 7)), vr = !((rgb_pitch & 7) || ((uintptr_t)rgb & 7));
     dim3 blk(32, 8), grd((W + DM_TX - 1) / DM_TX, (H + DM_TY - 1) / DM_TY);
-    k_demosaic_gray<<<grd, blk, 0, st>>>(raw, raw_pitch, W, H, cfa, b, s, d, g, gamma_gray, gray, gray_pitch, rgb, rgb_pitch);
+    k_demosaic_gray<<<grd, blk, 0, st>>>(raw, raw_pitch, W, H, cfa, b, s, d, g, gamma_gray, gray, gray_pitch, rgb, rgb_pitch, vg, vr);
     return cudaGetLastError();
 }
 
