@@ -11,7 +11,7 @@
 
 namespace {
 
-constexpr int DM_TX = 64, DM_TY = 16;                // output tile
+constexpr int DM_TX = 58, DM_TY = 16;                // output tile (58 + 6 = 32 pixel pairs of halo'd tile)
 constexpr int DM_LW = DM_TX + 6, DM_LH = DM_TY + 6;  // linear tile (halo 3)
 constexpr int DM_GW = DM_TX + 2, DM_GH = DM_TY + 2;  // green tile (halo 1)
 
@@ -45,15 +45,20 @@ __global__ void __launch_bounds__(256) k_demosaic_gray(const uint16_t* __restric
         const int gy = y0 + ly - 3;
         const bool yin = gy >= 0 && gy < H;
         const uint16_t* rr = isa::row_ptr(raw, raw_pitch, yin ? gy : 0);
+        // colours of the two columns of a pair on this row (odd, then even image column)
+        float bl[2], sc[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int c = isa::cfa_at(cfa, k + 1, gy);
+            bl[k] = c == 0 ? black.v[0] : (c == 1 ? black.v[1] : black.v[2]);
+            sc[k] = c == 0 ? scale.v[0] : (c == 1 ? scale.v[1] : scale.v[2]);
+        }
         for (int pi = tx; pi < DM_LW / 2; pi += 32) {
 #pragma unroll
             for (int k = 0; k < 2; k++) {
                 const int lx = 2 * pi + k, gx = x0 + lx - 3;
                 float v = 0.f;
-                if (yin && gx >= 0 && gx < W) {
-                    const int c = isa::cfa_at(cfa, gx, gy);
-                    v = ((float)__ldg(rr + gx) - black.v[c]) * scale.v[c];
-                }
+                if (yin && gx >= 0 && gx < W) v = ((float)__ldg(rr + gx) - bl[k]) * sc[k];
                 lin[ly][lx] = v;
             }
         }
@@ -90,6 +95,7 @@ __global__ void __launch_bounds__(256) k_demosaic_gray(const uint16_t* __restric
     }
     __syncthreads();
     // 3. red and blue by colour differences, removal of the white balance, output
+    if (tx >= DM_TX / 2) return;
     for (int ly = ty; ly < DM_TY; ly += 8) {
         const int gy = y0 + ly;
         if (gy >= H) break;

@@ -93,18 +93,47 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
     for (int k = 0; k < TX; k++) cr[k] = isa::clampi(tx * T + S + lane + 32 * k + oxr, 0, Wl - 1);
 #pragma unroll
     for (int k = 0; k < BX; k++) ct[k] = isa::clampi(tx * T + lane + 32 * k + oxt, 0, Wl - 1);
-    for (int y = warp; y < T; y += NW) {
-        const float* row = isa::row_ptr(imr, pitch, isa::clampi(ty * T + S + y + oyr, 0, Hl - 1));
-        float* dst = tpl + (y >> 1) * TP2 * 2 + (y & 1);
+    // all loads of a warp are issued before any store, so their latencies overlap
+    constexpr int TR = (T + NW - 1) / NW, BR = (B + NW - 1) / NW;
+    float vt[TR][TX], vb[BR][BX];
 #pragma unroll
-        for (int k = 0; k < TX; k++)
-            if (lane + 32 * k < T) dst[2 * (lane + 32 * k)] = __ldg(row + cr[k]);
+    for (int i = 0; i < TR; i++) {
+        const int y = warp + i * NW;
+        if (y < T) {
+            const float* row = isa::row_ptr(imr, pitch, isa::clampi(ty * T + S + y + oyr, 0, Hl - 1));
+#pragma unroll
+            for (int k = 0; k < TX; k++)
+                if (lane + 32 * k < T) vt[i][k] = __ldg(row + cr[k]);
+        }
     }
-    for (int y = warp; y < B; y += NW) {
-        const float* row = isa::row_ptr(imt, pitch, isa::clampi(ty * T + y + oyt, 0, Hl - 1));
 #pragma unroll
-        for (int k = 0; k < BX; k++)
-            if (lane + 32 * k < B) blk[y * BP + lane + 32 * k] = __ldg(row + ct[k]);
+    for (int i = 0; i < BR; i++) {
+        const int y = warp + i * NW;
+        if (y < B) {
+            const float* row = isa::row_ptr(imt, pitch, isa::clampi(ty * T + y + oyt, 0, Hl - 1));
+#pragma unroll
+            for (int k = 0; k < BX; k++)
+                if (lane + 32 * k < B) vb[i][k] = __ldg(row + ct[k]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < TR; i++) {
+        const int y = warp + i * NW;
+        if (y < T) {
+            float* dst = tpl + (y >> 1) * TP2 * 2 + (y & 1);
+#pragma unroll
+            for (int k = 0; k < TX; k++)
+                if (lane + 32 * k < T) dst[2 * (lane + 32 * k)] = vt[i][k];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < BR; i++) {
+        const int y = warp + i * NW;
+        if (y < B) {
+#pragma unroll
+            for (int k = 0; k < BX; k++)
+                if (lane + 32 * k < B) blk[y * BP + lane + 32 * k] = vb[i][k];
+        }
     }
     __syncthreads();
     const int yp = tid % HP, sy = tid / HP;
