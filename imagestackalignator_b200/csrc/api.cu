@@ -190,6 +190,7 @@ struct isa_ctx {
     const float** frame_tab = nullptr;
     float2 *flows = nullptr, *flow_tmp = nullptr;
     float *half_ref = nullptr, *half_mov = nullptr;
+    float4 *ref_mr = nullptr, *ref_sr = nullptr, *mov_box = nullptr;  // robustness statistics (half resolution)
     float4* masks = nullptr;
     float *st3 = nullptr, *kparam = nullptr;
     float *acc = nullptr, *wsum = nullptr, *out_stage = nullptr;
@@ -495,6 +496,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     float maxv = 0.f;
     for (int ch = 0; ch < 3; ch++) maxv = std::max(maxv, white[ch] + black[ch]);
     ISA_LAUNCH(c, isa_launch_subsample(frame(ref), raw_pitch, W, H, cfa, maxv, c->half_ref, hp3, st));
+    ISA_LAUNCH(c, isa_launch_ref_stats(c->half_ref, hp3, Wh, Hh, c->ref_mr, c->ref_sr, hp4, st));
     const int half = p->window_size_lk / 2;
     std::vector<isa_frame_in> fin;
     fin.push_back({frame(ref), nullptr, nullptr});
@@ -515,14 +517,16 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
             std::swap(a, b);
         }
         float4* mask = c->masks + (size_t)i * Wh * Hh;
-        ISA_LAUNCH(c, isa_launch_robustness_erode(c->half_ref, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha, info->noise_beta,
-                                           p->threshold_m, p->robust_s, p->robust_t, p->erode_size, mask, hp4, st));
+        ISA_LAUNCH(c, isa_launch_box3(c->half_mov, hp3, Wh, Hh, c->mov_box, hp4, st));
+        ISA_LAUNCH(c, isa_launch_robustness_erode_tabs(c->ref_mr, c->ref_sr, c->mov_box, hp4, c->half_mov, hp3, Wh, Hh, flow, fp, W, H,
+                                                       info->noise_alpha, info->noise_beta, p->threshold_m, p->robust_s, p->robust_t,
+                                                       p->erode_size, mask, hp4, st));
         fin.push_back({frame(i), flow, mask});
     }
     ISA_TRY(mark());
     // 5. accumulation: reference frame first (PrepareAccumulation :1894-1902), then the others in order
     const size_t op = (size_t)g.Wo * 12;
-    g.masks_finite = 1;  // the masks come from isa_launch_robustness_erode, whose values are clamped to [0, 1]
+    g.masks_finite = 1;  // the masks come from isa_launch_robustness_erode_tabs, whose values are clamped to [0, 1]
     ISA_CK(cudaMemcpyAsync(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), cudaMemcpyHostToDevice, st));
     if (p->fused_accumulate) {
         ISA_LAUNCH(c, isa_launch_accumulate(g, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum,
@@ -655,6 +659,9 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     add((void**)&c->flow_tmp, fsz * sizeof(float2));
     add((void**)&c->half_ref, fsz / 4 * 12);
     add((void**)&c->half_mov, fsz / 4 * 12);
+    add((void**)&c->ref_mr, fsz / 4 * 16);
+    add((void**)&c->ref_sr, fsz / 4 * 16);
+    add((void**)&c->mov_box, fsz / 4 * 16);
     add((void**)&c->masks, fsz / 4 * 16 * max_n);
     add((void**)&c->st3, fsz * 12);
     add((void**)&c->kparam, fsz * 16);

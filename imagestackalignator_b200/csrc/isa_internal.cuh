@@ -104,6 +104,13 @@ cudaError_t isa_launch_robustness_erode(const float* ref3, const float* mov3, si
                                         size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s, float t, int size,
                                         float4* out, size_t out_pitch, cudaStream_t st);
 
+// pipeline form of the mask: reference statistics once per burst, moved 3x3 means per frame
+cudaError_t isa_launch_ref_stats(const float* ref3, size_t img_pitch, int Wh, int Hh, float4* mr, float4* sr, size_t sp, cudaStream_t st);
+cudaError_t isa_launch_box3(const float* mov3, size_t img_pitch, int Wh, int Hh, float4* box, size_t sp, cudaStream_t st);
+cudaError_t isa_launch_robustness_erode_tabs(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch,
+                                             int Wh, int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
+                                             float thr_m, float s, float t, int size, float4* out, size_t out_pitch, cudaStream_t st);
+
 // merge.cu
 struct isa_accum_geom {
     int W, H;          // input frame

@@ -131,6 +131,152 @@ __global__ void __launch_bounds__(256) k_robustness_erode(const float* __restric
     isa::row_ptr(out, out_pitch, y)[x] = m;
 }
 
+// ---- pipeline form: statistics that do not depend on the moved frame are
+// computed once per burst, the moved image's 3x3 means once per frame, and
+// the mask itself reads them; every value is produced by the same arithmetic
+// in the same order as mask_at, so the masks are identical.
+
+// 3x3 means and standard deviations of the reference (interior pixels).
+__global__ void k_ref_stats(const float* __restrict__ ref3, size_t img_pitch, int Wh, int Hh, float4* __restrict__ mr_out,
+                            float4* __restrict__ sr_out, size_t sp)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wh - 1 || y >= Hh - 1 || x < 1 || y < 1) return;
+    float mr[3] = {0.f, 0.f, 0.f}, pr[9][3];
+    for (int j = -1; j <= 1; j++)
+        for (int i = -1; i <= 1; i++) {
+            const float* p = isa::row_ptr(ref3, img_pitch, y + j) + 3 * (x + i);
+            const int k = (j + 1) * 3 + i + 1;
+            for (int c = 0; c < 3; c++) {
+                pr[k][c] = __ldg(p + c);
+                mr[c] += pr[k][c];
+            }
+        }
+    for (int c = 0; c < 3; c++) mr[c] /= 9.0f;
+    float sd[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < 9; k++)
+        for (int c = 0; c < 3; c++) sd[c] += (pr[k][c] - mr[c]) * (pr[k][c] - mr[c]);
+    isa::row_ptr(mr_out, sp, y)[x] = make_float4(mr[0], mr[1], mr[2], 0.f);
+    isa::row_ptr(sr_out, sp, y)[x] = make_float4(sqrtf(sd[0] / 9.0f), sqrtf(sd[1] / 9.0f), sqrtf(sd[2] / 9.0f), 0.f);
+}
+
+// 3x3 means of the moved image with the reference's per-tap clamping, at
+// every centre inside the image.
+__global__ void k_box3(const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh, float4* __restrict__ box, size_t sp)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wh || y >= Hh) return;
+    float mm[3] = {0.f, 0.f, 0.f};
+    for (int j = -1; j <= 1; j++)
+        for (int i = -1; i <= 1; i++) {
+            const float* q = isa::row_ptr(mov3, img_pitch, isa::clampi(y + j, 0, Hh - 1)) + 3 * isa::clampi(x + i, 0, Wh - 1);
+            for (int c = 0; c < 3; c++) mm[c] += __ldg(q + c);
+        }
+    isa::row_ptr(box, sp, y)[x] = make_float4(mm[0] / 9.0f, mm[1] / 9.0f, mm[2] / 9.0f, 0.f);
+}
+
+struct RobustTabs {
+    const float4* mr;
+    const float4* sr;
+    const float4* box;
+    size_t sp;
+};
+
+// mask_at with the reference statistics and the moved 3x3 means looked up;
+// a shifted centre outside the image (whose clamped taps differ from the
+// clamped centre's) is summed directly.
+__device__ float4 mask_fast(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                            const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m,
+                            float s_lit, float t_lit, int x, int y)
+{
+    float2 sf = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x, y);
+    float2 sl = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x + 2, y + 2);
+    float mxx = fmaxf(sl.x, sf.x), mxy = fmaxf(sl.y, sf.y);
+    float mnx = fminf(sl.x, sf.x), mny = fminf(sl.y, sf.y);
+    int shx = (int)roundf(sf.x * 0.5f), shy = (int)roundf(sf.y * 0.5f);
+    const float4 r4 = __ldg(isa::row_ptr(tb.mr, tb.sp, y) + x), s4 = __ldg(isa::row_ptr(tb.sr, tb.sp, y) + x);
+    const float mr[3] = {r4.x, r4.y, r4.z}, sr3[3] = {s4.x, s4.y, s4.z};
+    float mm[3];
+    const int cx = x + shx, cy = y + shy;
+    if ((unsigned)cx < (unsigned)Wh && (unsigned)cy < (unsigned)Hh) {
+        const float4 b4 = __ldg(isa::row_ptr(tb.box, tb.sp, cy) + cx);
+        mm[0] = b4.x; mm[1] = b4.y; mm[2] = b4.z;
+    } else {
+        mm[0] = mm[1] = mm[2] = 0.f;
+        for (int j = -1; j <= 1; j++)
+            for (int i = -1; i <= 1; i++) {
+                const float* q = isa::row_ptr(mov3, img_pitch, isa::clampi(cy + j, 0, Hh - 1)) + 3 * isa::clampi(cx + i, 0, Wh - 1);
+                for (int c = 0; c < 3; c++) mm[c] += __ldg(q + c);
+            }
+        for (int c = 0; c < 3; c++) mm[c] /= 9.0f;
+    }
+    float md = fabsf(mr[0] - mm[0]) + fabsf(mr[1] - mm[1]) + fabsf(mr[2] - mm[2]);
+    md /= 3.0f;
+    mxx *= 0.5f * md; mxy *= 0.5f * md; mnx *= 0.5f * md; mny *= 0.5f * md;
+    float M = sqrtf((mxx - mnx) * (mxx - mnx) + (mxy - mny) * (mxy - mny));
+    float sgain = M > thr_m ? 0.f : s_lit;
+    float out[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        float sr = sr3[c];
+        float smd = sqrtf(alpha * mr[c] + beta);
+        if (c == 1) smd /= sqrtf(2.0f);
+        float dist = fabsf(mr[c] - mm[c]);
+        float sig = fmaxf(smd, sr);
+        dist = dist * (sr * sr / (sr * sr + smd * smd));
+        out[c] = fmaxf(fminf(sgain * expf(-dist * dist / (sig * sig)) - t_lit, 1.0f), 0.0f);
+    }
+    return make_float4(out[0], out[1], out[2], M);
+}
+
+// Mask over a 32 x 32 output tile plus the erosion halo in shared memory
+// (border pixels 1, replicate addressing as k_robustness_erode), then the
+// separable min filter: rows, then columns.
+constexpr int RF_T = 32;
+
+__global__ void __launch_bounds__(256) k_robustness_erode_fast(RobustTabs tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                                                              const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha,
+                                                              float beta, float thr_m, float s, float t, int size, float4* __restrict__ out,
+                                                              size_t out_pitch)
+{
+    __shared__ float4 sm[(RF_T + 2 * RB_MAXA) * (RF_T + 2 * RB_MAXA)];
+    __shared__ float4 hm[(RF_T + 2 * RB_MAXA) * RF_T];
+    const int a = size / 2;
+    const int SW = RF_T + 2 * a, SH = RF_T + 2 * a;
+    const int x0 = blockIdx.x * RF_T, y0 = blockIdx.y * RF_T;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < SW * SH; i += 256) {
+        const int sy = i / SW, sx = i - sy * SW;
+        const int qx = isa::clampi(x0 + sx - a, 0, Wh - 1), qy = isa::clampi(y0 + sy - a, 0, Hh - 1);
+        float4 v = make_float4(1.f, 1.f, 1.f, 1.f);
+        if (qx >= 1 && qx < Wh - 1 && qy >= 1 && qy < Hh - 1)
+            v = mask_fast(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, qx, qy);
+        sm[i] = v;
+    }
+    __syncthreads();
+    for (int i = tid; i < SH * RF_T; i += 256) {
+        const int sy = i / RF_T, x = i - sy * RF_T;
+        float4 m = sm[sy * SW + x];
+        for (int k = 1; k < size; k++) {
+            const float4 v = sm[sy * SW + x + k];
+            m.x = fminf(m.x, v.x); m.y = fminf(m.y, v.y); m.z = fminf(m.z, v.z); m.w = fminf(m.w, v.w);
+        }
+        hm[sy * RF_T + x] = m;
+    }
+    __syncthreads();
+    for (int i = tid; i < RF_T * RF_T; i += 256) {
+        const int ly = i / RF_T, lx = i - ly * RF_T;
+        const int x = x0 + lx, y = y0 + ly;
+        if (x >= Wh || y >= Hh) continue;
+        float4 m = hm[ly * RF_T + lx];
+        for (int k = 1; k < size; k++) {
+            const float4 v = hm[(ly + k) * RF_T + lx];
+            m.x = fminf(m.x, v.x); m.y = fminf(m.y, v.y); m.z = fminf(m.z, v.z); m.w = fminf(m.w, v.w);
+        }
+        isa::row_ptr(out, out_pitch, y)[x] = m;
+    }
+}
+
 inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
 
 }  // namespace
@@ -161,5 +307,31 @@ cudaError_t isa_launch_robustness_erode(const float* ref3, const float* mov3, si
     dim3 b(RB_TX, RB_TY);
     k_robustness_erode<<<grid2(Wh, Hh, b), b, 0, st>>>(ref3, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size,
                                                        out, out_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_ref_stats(const float* ref3, size_t img_pitch, int Wh, int Hh, float4* mr, float4* sr, size_t sp, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_ref_stats<<<grid2(Wh, Hh, b), b, 0, st>>>(ref3, img_pitch, Wh, Hh, mr, sr, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_box3(const float* mov3, size_t img_pitch, int Wh, int Hh, float4* box, size_t sp, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_box3<<<grid2(Wh, Hh, b), b, 0, st>>>(mov3, img_pitch, Wh, Hh, box, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_robustness_erode_tabs(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch,
+                                             int Wh, int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
+                                             float thr_m, float s, float t, int size, float4* out, size_t out_pitch, cudaStream_t st)
+{
+    if (size < 1 || size / 2 > RB_MAXA) return cudaErrorInvalidValue;
+    RobustTabs tb{mr, sr, box, sp};
+    dim3 g((Wh + RF_T - 1) / RF_T, (Hh + RF_T - 1) / RF_T);
+    k_robustness_erode_fast<<<g, 256, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size, out,
+                                               out_pitch);
     return cudaGetLastError();
 }

@@ -213,3 +213,41 @@ def test_full_size_known_shift(cuda):
         assert float(exact) > 0.98, (i, float(exact))
         assert float((fl - want).abs().median()) < 1e-2
     m.close()
+
+
+def test_pipeline_masks_equal_operator_masks(cuda, burst):
+    """The merge computes the robustness mask from reference statistics made
+    once per burst and the moved image's 3x3 means made once per frame; the
+    operator entry point isa_robustness_erode evaluates every tap directly.
+    Both must give the same masks bit for bit, on the pipeline's own flows."""
+    import torch
+    p = P.MergeParams()
+    p.merge_scale = 2.0
+    m = isa.Merger(burst.width, burst.height, burst.n, p)
+    info = isa.make_info(burst)
+    raw = to_dev(burst.raw)
+    m.merge(raw, info)
+    torch.cuda.synchronize()
+    H, W, n = burst.height, burst.width, burst.n
+    Wh, Hh = W // 2, H // 2
+    maxv = max(w + b for w, b in zip(burst.white, burst.black))
+    cfa = (ctypes.c_int * 4)(*burst.cfa)
+    sz = ctypes.c_size_t
+    frames = raw.view(n, H, W)
+    half = []
+    for i in range(n):
+        h = torch.zeros((Hh, Wh, 3), dtype=torch.float32, device="cuda")
+        isa.check(isa.lib().isa_debayer_subsample(isa.vp(frames[i]), sz(W * 2), W, H, cfa, ctypes.c_float(maxv), isa.vp(h), sz(Wh * 12), None))
+        half.append(h)
+    for i in range(1, n):
+        d = m.debug(i)
+        flow = isa.device_copy(d["flow"], (H, W, 2), torch.float32)
+        want = isa.device_copy(d["mask"], (Hh, Wh, 4), torch.float32)
+        got = torch.zeros_like(want)
+        isa.check(isa.lib().isa_robustness_erode(isa.vp(half[0]), isa.vp(half[i]), sz(Wh * 12), Wh, Hh, isa.vp(flow), sz(W * 8), W, H,
+                                                 ctypes.c_float(burst.noise_a), ctypes.c_float(burst.noise_b), ctypes.c_float(p.threshold_m),
+                                                 ctypes.c_float(p.robust_s), ctypes.c_float(p.robust_t), p.erode_size, isa.vp(got), sz(Wh * 16),
+                                                 None))
+        torch.cuda.synchronize()
+        assert torch.equal(got, want), f"frame {i}: {(got != want).sum().item()} values differ"
+    m.close()
