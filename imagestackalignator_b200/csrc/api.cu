@@ -201,6 +201,12 @@ struct isa_ctx {
     void* fft_work = nullptr;
     size_t fft_work_bytes = 0;
     cudaEvent_t ev[8] = {};
+    // host entry point: frames copied in and the image copied out on a second stream, overlapped with the work
+    static constexpr int kBands = 8;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> ev_frame;         // frame i resident
+    cudaEvent_t ev_band[kBands] = {};          // output rows of band b final
+    cudaEvent_t ev_free = nullptr, ev_copied = nullptr;
     int ev_count = 0;
     long launches = 0;  // kernels of this library launched by the last merge
     // last call
@@ -260,6 +266,8 @@ void accum_geom(const isa_params* p, int W, int H, isa_accum_geom& g, float& thr
     }
     float r = std::round(g.s);
     g.s_int = (r == g.s && r >= 1.f) ? (int)r : 0;
+    g.yb0 = 0;
+    g.yb1 = g.Ho;
 }
 
 int ensure_plans(isa_ctx* c, int W, int H)
@@ -388,8 +396,15 @@ int upload_strategy(isa_ctx* c, const Strategy& s, cudaStream_t st)
     return upload_rows(c->row_a, c->row_b, c->row_sign, c->row_grid, c->N0, s, st);
 }
 
+// Host buffers of isa_merge_burst_host: frames arrive on the copy stream
+// (event per frame) and the image leaves on it band by band.
+struct HostIo {
+    bool frames_async;  // wait for ev_frame[i] before the first use of frame i
+    float* host_out;    // when set: the output is copied out band by band (rows of 12 * Wo bytes)
+};
+
 int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
-              const isa_prealign* pre, float* out, size_t out_pitch, cudaStream_t st)
+              const isa_prealign* pre, float* out, size_t out_pitch, cudaStream_t st, const HostIo* hio = nullptr)
 {
     const isa_params* p = &c->p;
     ISA_TRY(check_info(info));
@@ -425,8 +440,10 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     ISA_TRY(mark());
     // 1. tracking (high-pass) and accumulation images of every frame
     const std::vector<float> taps_trk = gauss_taps(p->sigma_debayer_tracking), taps_acc = gauss_taps(p->sigma_debayer_accumulation);
-    for (int i = 0; i < n; i++)
+    for (int i = 0; i < n; i++) {
+        if (hio && hio->frames_async) ISA_CK(cudaStreamWaitEvent(st, c->ev_frame[i], 0));
         ISA_TRY(bw_frame(c, frame(i), raw_pitch, W, H, info, true, c->bw_track + i * fsz, taps_trk, c->bw_acc + i * fsz, taps_acc, st));
+    }
     ISA_TRY(mark());
     // 2. pyramid tile alignment, coarsest level first (TrackPatches :1640-1712)
     ISA_TRY(upload_strategy(c, strat, st));
@@ -528,6 +545,43 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     const size_t op = (size_t)g.Wo * 12;
     g.masks_finite = 1;  // the masks come from isa_launch_robustness_erode_tabs, whose values are clamped to [0, 1]
     ISA_CK(cudaMemcpyAsync(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), cudaMemcpyHostToDevice, st));
+    if (hio && hio->host_out) {
+        // bands of output rows: accumulate, normalise, then copy out on the copy stream while the next band runs
+        if (thr > 0)
+            ISA_LAUNCH(c, isa_launch_demosaic_gray(frame(ref), raw_pitch, W, H, cfa, black, scale, divisor, nullptr, 0, nullptr, 0, out, out_pitch, st));
+        const int rows = std::max(32, (g.Ho / isa_ctx::kBands + 31) / 32 * 32);
+        int b = 0;
+        for (int y0 = 0; y0 < g.Ho; y0 += rows, b++) {
+            isa_accum_geom gb = g;
+            gb.yb0 = y0;
+            gb.yb1 = std::min(g.Ho, y0 + rows);
+            const int nr = gb.yb1 - gb.yb0;
+            if (p->fused_accumulate) {
+                ISA_LAUNCH(c, isa_launch_accumulate(gb, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black,
+                                                    c->acc, c->wsum, op, 0, st));
+            } else {
+                ISA_CK(cudaMemsetAsync((char*)c->acc + (size_t)y0 * op, 0, op * nr, st));
+                ISA_CK(cudaMemsetAsync((char*)c->wsum + (size_t)y0 * op, 0, op * nr, st));
+                for (size_t f = 0; f < fin.size(); f++)
+                    ISA_LAUNCH(c, isa_launch_accumulate(gb, cfa, nullptr, 1, &fin[f], raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc,
+                                                        c->wsum, op, 1, st));
+            }
+            float* ob = (float*)((char*)out + (size_t)y0 * out_pitch);
+            ISA_LAUNCH(c, isa_launch_apply_weighting(ob, out_pitch, (const float*)((const char*)c->acc + (size_t)y0 * op),
+                                                     (const float*)((const char*)c->wsum + (size_t)y0 * op), op, g.Wo, nr, thr, st));
+            ISA_CK(cudaEventRecord(c->ev_band[b % isa_ctx::kBands], st));
+            ISA_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_band[b % isa_ctx::kBands], 0));
+            ISA_CK(cudaMemcpy2DAsync((char*)hio->host_out + (size_t)y0 * g.Wo * 12, (size_t)g.Wo * 12, ob, out_pitch, (size_t)g.Wo * 12, nr,
+                                     cudaMemcpyDeviceToHost, c->copy_stream));
+        }
+        ISA_TRY(mark());
+        ISA_TRY(mark());
+        // the caller's stream completes only when the image has left the device
+        ISA_CK(cudaEventRecord(c->ev_copied, c->copy_stream));
+        ISA_CK(cudaStreamWaitEvent(st, c->ev_copied, 0));
+        c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1;
+        return ISA_OK;
+    }
     if (p->fused_accumulate) {
         ISA_LAUNCH(c, isa_launch_accumulate(g, cfa, c->frame_in, (int)fin.size(), nullptr, raw_pitch, fp, hp4, c->kparam, p4, 4, white, black, c->acc, c->wsum,
                                      op, 0, st));
@@ -681,6 +735,13 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     for (auto& e : plan) { *e.first = (char*)c->arena + off; off += e.second; }
     for (int i = 0; i < 8; i++)
         if (cudaEventCreate(&c->ev[i]) != cudaSuccess) { isa_ctx_destroy(c); return fail(ISA_ECUDA, "cudaEventCreate failed"); }
+    bool ok = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) == cudaSuccess;
+    c->ev_frame.assign(max_n, nullptr);
+    for (int i = 0; i < max_n && ok; i++) ok = cudaEventCreateWithFlags(&c->ev_frame[i], cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < isa_ctx::kBands && ok; i++) ok = cudaEventCreateWithFlags(&c->ev_band[i], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->ev_free, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) { isa_ctx_destroy(c); return fail(ISA_ECUDA, "stream/event creation failed"); }
     int r = ensure_plans(c, max_w, max_h);
     if (r != ISA_OK) { isa_ctx_destroy(c); return r; }
     *out = c;
@@ -695,6 +756,13 @@ int isa_ctx_destroy(isa_ctx* c)
     if (c->fft_work) cudaFree(c->fft_work);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (cudaEvent_t e : c->ev_frame)
+        if (e) cudaEventDestroy(e);
+    for (int i = 0; i < isa_ctx::kBands; i++)
+        if (c->ev_band[i]) cudaEventDestroy(c->ev_band[i]);
+    if (c->ev_free) cudaEventDestroy(c->ev_free);
+    if (c->ev_copied) cudaEventDestroy(c->ev_copied);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->arena) cudaFree(c->arena);
     delete c;
     return ISA_OK;
@@ -731,10 +799,22 @@ int isa_merge_burst_host(isa_ctx* c, const uint16_t* host_raw, int n, const isa_
     accum_geom(&c->p, W, H, g, thr);
     cudaStream_t st = S(stream);
     const size_t fb = (size_t)W * H * 2;
-    ISA_CK(cudaMemcpyAsync(c->raw_stage, host_raw, fb * n, cudaMemcpyHostToDevice, st));
-    ISA_TRY(run_merge(c, c->raw_stage, (size_t)W * 2, fb, n, info, pre, c->out_stage, (size_t)g.Wo * 12, st));
-    ISA_CK(cudaMemcpyAsync(host_out, c->out_stage, (size_t)g.Wo * g.Ho * 12, cudaMemcpyDeviceToHost, st));
-    return ISA_OK;
+    // frames go in on the copy stream, one event each, once earlier work on `st` no longer reads the staging buffers
+    ISA_CK(cudaEventRecord(c->ev_free, st));
+    ISA_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free, 0));
+    for (int i = 0; i < n; i++) {
+        ISA_CK(cudaMemcpyAsync((char*)c->raw_stage + (size_t)i * fb, (const char*)host_raw + (size_t)i * fb, fb, cudaMemcpyHostToDevice,
+                               c->copy_stream));
+        ISA_CK(cudaEventRecord(c->ev_frame[i], c->copy_stream));
+    }
+    HostIo hio{true, host_out};
+    const int rc = run_merge(c, c->raw_stage, (size_t)W * 2, fb, n, info, pre, c->out_stage, (size_t)g.Wo * 12, st, &hio);
+    if (rc != ISA_OK) {
+        // leave nothing of this call running on the copy stream past the caller's stream
+        cudaEventRecord(c->ev_copied, c->copy_stream);
+        cudaStreamWaitEvent(st, c->ev_copied, 0);
+    }
+    return rc;
 }
 
 int isa_debug_buffers(isa_ctx* c, int frame, const void** flow, size_t* flow_pitch, const void** mask, size_t* mask_pitch, const void** kparam,
@@ -1022,6 +1102,8 @@ int isa_accumulate(const uint16_t* raw, size_t raw_pitch, int W, int H, const in
     g.W = W; g.H = H; g.Wo = Wo; g.Ho = Ho; g.s = scale; g.ox = ox; g.oy = oy;
     g.cx0 = crop[0]; g.cy0 = crop[1]; g.cx1 = crop[2]; g.cy1 = crop[3];
     g.masks_finite = 0;
+    g.yb0 = 0;
+    g.yb1 = Ho;
     float r = std::round(scale);
     g.s_int = (r == scale && r >= 1.f) ? (int)r : 0;
     isa_frame_in f{raw, (const float2*)flow, (const float4*)mask};

@@ -120,6 +120,7 @@ struct isa_accum_geom {
     int ox, oy;        // output-grid origin
     int cx0, cy0, cx1, cy1;  // inclusive source crop
     int masks_finite;  // 1: every mask value is finite (masks made by this library)
+    int yb0, yb1;      // output rows [yb0, yb1) computed by this launch (yb0 a multiple of 32)
 };
 struct isa_frame_in {
     const uint16_t* raw;

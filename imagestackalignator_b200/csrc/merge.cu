@@ -119,8 +119,8 @@ __global__ void __launch_bounds__(256) k_accumulate(isa_accum_geom g, unsigned c
                                                    size_t kp_pitch, F3 white, F3 black, float* __restrict__ acc, float* __restrict__ wsum,
                                                    size_t out_pitch, int accumulate_into)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= g.Wo || y >= g.Ho) return;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = g.yb0 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= g.Wo || y >= g.yb1) return;
     float* ap = isa::row_ptr(acc, out_pitch, y) + 3 * x;
     float* wp = isa::row_ptr(wsum, out_pitch, y) + 3 * x;
     if (x < 1 || y < 1 || x >= g.Wo - 1 || y >= g.Ho - 1) {
@@ -237,7 +237,8 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
     F3 wh, bl;
     for (int c = 0; c < 3; c++) { wh.v[c] = white[c]; bl.v[c] = black[c]; }
     isa_frame_in one = single ? *single : isa_frame_in{nullptr, nullptr, nullptr};
-    dim3 b(32, 8), grd = grid2(g.Wo, g.Ho, b);
+    if (g.yb0 < 0 || g.yb1 > g.Ho || g.yb1 <= g.yb0) return cudaErrorInvalidValue;
+    dim3 b(32, 8), grd = grid2(g.Wo, g.yb1 - g.yb0, b);
     if (kparam_channels == 4)
         k_accumulate<4><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc, wsum,
                                            out_pitch, accumulate_into);

@@ -283,8 +283,8 @@ __global__ void __launch_bounds__(256, SANE ? 3 : 2) k_accumulate_x2(const X2Arg
 {
     const int ph = blockIdx.x & 3, rph = blockIdx.y & 3;
     const int x = (blockIdx.x >> 2) * 128 + 4 * threadIdx.x + ph;
-    const int y = (blockIdx.y >> 2) * 32 + 4 * threadIdx.y + rph;
-    if (x >= A.g.Wo || y >= A.g.Ho) return;
+    const int y = A.g.yb0 + (blockIdx.y >> 2) * 32 + 4 * threadIdx.y + rph;
+    if (x >= A.g.Wo || y >= A.g.yb1) return;
     // X mod 4 and Y mod 4 are the same for the whole CTA
     switch (((ph + A.g.ox) & 3) | (((rph + A.g.oy) & 3) << 2)) {
 #define ISA_X2_CASE(k) \
@@ -338,7 +338,8 @@ cudaError_t isa_launch_accumulate_x2(const isa_accum_geom& g, unsigned cfa, cons
     A.kparam = (const float4*)kparam; A.kp_pitch = kparam_pitch;
     for (int c = 0; c < 3; c++) { A.rwhite.v[c] = (float)(1.0 / (double)white[c]); A.black.v[c] = black[c]; }
     A.acc = acc; A.wsum = wsum; A.out_pitch = out_pitch; A.accumulate_into = accumulate_into;
-    dim3 b(32, 8), grd(((g.Wo + 127) / 128) * 4, ((g.Ho + 31) / 32) * 4);
+    if (g.yb0 % 32 || g.yb0 < 0 || g.yb1 > g.Ho || g.yb1 <= g.yb0) return cudaErrorInvalidValue;
+    dim3 b(32, 8), grd(((g.Wo + 127) / 128) * 4, ((g.yb1 - g.yb0 + 31) / 32) * 4);
     if (g.masks_finite)
         k_accumulate_x2<true><<<grd, b, 0, st>>>(A);
     else
