@@ -35,7 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(width=6016, height=4000, frames=20, max_shift=24.0, max_rot_deg=0.5, noise_a=1e-3, noise_b=8e-6, scale=2.0)
-SAMPLE = dict(width=768, height=512)          # CPU baseline sample (same statistics, 20 frames)
+SAMPLE = dict(width=1280, height=960)         # CPU baseline sample (same statistics, 20 frames; about 10 s on 16 cores)
 REF_STEP = dict(width=512, height=384)        # one `--impl reference` step
 METRIC = "merged MP/s"
 UNIT = "MP/s"
