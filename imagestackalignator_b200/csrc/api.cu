@@ -8,6 +8,7 @@
 
 #include <cufft.h>
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -602,6 +603,94 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     return ISA_OK;
 }
 
+// ---- global pre-alignment ---------------------------------------------------
+struct ScanResult { double x, y, ang, val; };
+struct ArgMax { float v; int i; };
+
+// PreAlignment.ScanAngles (PreAlignment.cs:176-261) of tracking image `img`
+// against the reference spectrum in c->spec. Scratch in c->tmp: the rotated
+// image (and its inverse transform), its spectrum, the arg-max partials and
+// one (value, index) per angle.
+int scan_angles(isa_ctx* c, const float* img, int W, int H, double incr, double range, double zero, cudaStream_t st, ScanResult& out)
+{
+    const size_t fsz = (size_t)W * H, hw = (size_t)(W / 2 + 1);
+    float* rot = c->tmp;
+    float2* spec = (float2*)(c->tmp + fsz);
+    char* scratch = (char*)(c->tmp + fsz + (W + 2) * (size_t)H);
+    scratch = (char*)(((uintptr_t)scratch + 255) & ~(uintptr_t)255);
+    ArgMax* res = (ArgMax*)(scratch + isa_argmax_scratch_bytes());
+    constexpr int kMaxAngles = 256;
+    const float N = (float)W * (float)H;
+    double maxVal = -DBL_MAX, maxAng = 0, maxX = 0, maxY = 0;
+    ISA_FFT(cufftSetStream(c->r2c, st));
+    ISA_FFT(cufftSetStream(c->c2r, st));
+    for (int phase = 0; phase < 2; phase++) {
+        // the reference's loops, in the same double arithmetic
+        std::vector<double> angles;
+        const double step = phase == 0 ? 5 * incr : incr;
+        for (double ang = zero - range; ang <= zero + range; ang += step) {
+            angles.push_back(ang);
+            if ((int)angles.size() > kMaxAngles) return fail(ISA_EINVAL, "more than %d rotation angles per scan", kMaxAngles);
+        }
+        for (size_t k = 0; k < angles.size(); k++) {
+            ISA_LAUNCH(c, isa_launch_rotate_cubic(img, (size_t)W * 4, W, H, angles[k], rot, (size_t)W * 4, st));
+            ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)rot, (cufftComplex*)spec));
+            ISA_LAUNCH(c, isa_launch_conj_mul(c->spec, spec, hw * H, st));
+            ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)spec, (cufftReal*)rot));
+            ISA_LAUNCH(c, isa_launch_argmax(rot, (int)fsz, scratch, res + k, st));
+        }
+        std::vector<ArgMax> h(angles.size());
+        ISA_CK(cudaMemcpyAsync(h.data(), res, h.size() * sizeof(ArgMax), cudaMemcpyDeviceToHost, st));
+        ISA_CK(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < angles.size(); k++) {
+            const float v = h[k].v / N;  // the reference divides the correlation by W * H before MaxIndex
+            if (v > maxVal) {
+                maxVal = v;
+                maxAng = angles[k];
+                maxX = h[k].i % W;
+                maxY = h[k].i / W;
+            }
+        }
+        zero = maxAng;
+        range = 10 * incr;
+    }
+    if (maxX > W / 2) maxX -= W;
+    if (maxY > H / 2) maxY -= H;
+    out = ScanResult{-maxX, -maxY, maxAng, maxVal};
+    return ISA_OK;
+}
+
+// PreAlignmentStore (PreAlignmentStore.cs:36-110): consecutive differences of
+// the per-frame results, the reference index that minimises the remaining
+// total shift, and every frame's shift and rotation relative to it.
+int prealign_store(const std::vector<ScanResult>& init, float* shifts, float* rots, int* reference)
+{
+    const int n = (int)init.size();
+    std::vector<ScanResult> basic(n, ScanResult{0, 0, 0, 0});
+    for (int i = 1; i < n; i++)
+        basic[i - 1] = ScanResult{init[i].x - init[i - 1].x, init[i].y - init[i - 1].y, init[i].ang - init[i - 1].ang, 0};
+    int minIndex = -1;
+    double minShift = DBL_MAX;
+    for (int i = 0; i < n - 1; i++) {
+        double ax = 0, ay = 0, bx = 0, by = 0;
+        for (int j = 0; j < i; j++) { ax -= basic[j].x; ay -= basic[j].y; }
+        for (int j = i; j < n - 1; j++) { bx += basic[j].x; by += basic[j].y; }
+        const double sx = ax + bx, sy = ay + by;
+        const double d = std::sqrt(sx * sx + sy * sy);
+        if (d < minShift) { minShift = d; minIndex = i; }
+    }
+    for (int i = 0; i < n; i++) {
+        double ax = 0, ay = 0, az = 0;
+        for (int j = i; j < minIndex; j++) { ax -= basic[j].x; ay -= basic[j].y; az -= basic[j].ang; }
+        for (int j = minIndex; j < i; j++) { ax += basic[j].x; ay += basic[j].y; az += basic[j].ang; }
+        shifts[2 * i] = (float)ax;
+        shifts[2 * i + 1] = (float)ay;
+        rots[i] = (float)az;
+    }
+    *reference = minIndex;
+    return ISA_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -903,6 +992,40 @@ int isa_bw_image(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H
     ISA_REQ(out_pitch == (size_t)W * 4 && raw_pitch >= (size_t)W * 2, "out pitch must be width * 4");
     std::vector<float> taps = gauss_taps(sigma), none;
     return bw_frame(c, raw, raw_pitch, W, H, info, high_pass != 0, out, taps, nullptr, none, S(stream));
+}
+
+int isa_prealign_burst(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info, float increment_deg,
+                       float range_deg, const float* roll_deg, float* shifts, float* rotations_deg, int* reference, double* scan, void* stream)
+{
+    ISA_REQ(c && raw && info && shifts && rotations_deg && reference, "NULL argument");
+    ISA_TRY(check_info(info));
+    const int W = info->width, H = info->height;
+    ISA_REQ(W <= c->max_w && H <= c->max_h && n >= 2 && n <= c->max_n, "burst exceeds the context");
+    ISA_REQ(raw_pitch >= (size_t)W * 2 && frame_stride >= raw_pitch * H, "bad frame layout");
+    ISA_REQ(increment_deg > 0.f && range_deg >= 0.f, "increment must be positive and range non-negative");
+    ISA_REQ((size_t)W * H >= 4096, "frames too small for the pre-alignment scratch");
+    cudaStream_t st = S(stream);
+    const size_t fsz = (size_t)W * H;
+    // tracking images of every frame (DeBayerBWGaussWB with the high-pass, controller :1474-1478)
+    const std::vector<float> taps = gauss_taps(c->p.sigma_debayer_tracking), none;
+    for (int i = 0; i < n; i++)
+        ISA_TRY(bw_frame(c, (const uint16_t*)((const char*)raw + (size_t)i * frame_stride), raw_pitch, W, H, info, true, c->bw_track + i * fsz, taps,
+                         nullptr, none, st));
+    // reference spectrum (SetReferenceImage, PreAlignment.cs:164-175): frame 0
+    ISA_TRY(ensure_plans(c, W, H));
+    ISA_FFT(cufftSetStream(c->r2c, st));
+    ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)c->bw_track, (cufftComplex*)c->spec));
+    std::vector<ScanResult> init(n, ScanResult{0, 0, 0, 0});
+    const float roll0 = roll_deg ? -roll_deg[0] : 0.f;
+    for (int i = 1; i < n; i++) {
+        const float rollt = roll_deg ? -roll_deg[i] : 0.f;
+        ISA_TRY(scan_angles(c, c->bw_track + i * fsz, W, H, (double)increment_deg, (double)range_deg, (double)(rollt - roll0), st, init[i]));
+    }
+    if (scan)
+        for (int i = 0; i < n; i++) {
+            scan[4 * i] = init[i].x; scan[4 * i + 1] = init[i].y; scan[4 * i + 2] = init[i].ang; scan[4 * i + 3] = init[i].val;
+        }
+    return prealign_store(init, shifts, rotations_deg, reference);
 }
 
 int isa_fourier_filter(void* spec, size_t pitch, int W, int H, float lp, float hp, float lps, float hps, int clear_axis, float post_scale,

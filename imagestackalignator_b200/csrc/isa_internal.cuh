@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
+#include <algorithm>
 
 #define ISA_DEV __device__ __forceinline__
 
@@ -110,6 +111,12 @@ cudaError_t isa_launch_box3(const float* mov3, size_t img_pitch, int Wh, int Hh,
 cudaError_t isa_launch_robustness_erode_tabs(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch,
                                              int Wh, int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
                                              float thr_m, float s, float t, int size, float4* out, size_t out_pitch, cudaStream_t st);
+
+// prealign.cu
+cudaError_t isa_launch_rotate_cubic(const float* src, size_t pitch, int W, int H, double angle_deg, float* dst, size_t dst_pitch, cudaStream_t st);
+cudaError_t isa_launch_conj_mul(const float2* a, float2* b, size_t n, cudaStream_t st);
+size_t isa_argmax_scratch_bytes();
+cudaError_t isa_launch_argmax(const float* img, int n, void* scratch, void* out, cudaStream_t st);
 
 // merge.cu
 struct isa_accum_geom {

@@ -70,7 +70,7 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
-    "isa_bw_image", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
+    "isa_bw_image", "isa_prealign_burst", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
@@ -234,6 +234,27 @@ class Merger:
         op = ctypes.c_void_p(out_host.data_ptr()) if hasattr(out_host, "data_ptr") else out_host.ctypes.data_as(ctypes.c_void_p)
         check(lib().isa_merge_burst_host(self.ctx, rp, n, ctypes.byref(info), ctypes.byref(pre), op, stream_ptr(stream)))
         return out_host
+
+    def prealign(self, raw, info: IsaRawInfo, increment=0.1, range_deg=1.0, roll=None, stream=None):
+        """Global pre-alignment (isa_prealign_burst) of a device burst n x H x W.
+
+        Returns (shifts n x 2, rotations_deg n, reference, scan n x 4): the
+        PreAlignmentStore outputs that `merge(..., shifts=, rotations=,
+        reference=)` takes, and the raw per-frame scan results against frame 0."""
+        n, H, W = raw.shape
+        shifts = np.zeros((n, 2), np.float32)
+        rots = np.zeros(n, np.float32)
+        scan = np.zeros((n, 4), np.float64)
+        ref = ctypes.c_int(-1)
+        rl = None
+        if roll is not None:
+            rl = np.ascontiguousarray(roll, dtype=np.float32)
+        check(lib().isa_prealign_burst(self.ctx, vp(raw), ctypes.c_size_t(W * 2), ctypes.c_size_t(W * H * 2), n, ctypes.byref(info),
+                                       ctypes.c_float(increment), ctypes.c_float(range_deg),
+                                       rl.ctypes.data_as(ctypes.c_void_p) if rl is not None else None,
+                                       shifts.ctypes.data_as(ctypes.c_void_p), rots.ctypes.data_as(ctypes.c_void_p), ctypes.byref(ref),
+                                       scan.ctypes.data_as(ctypes.c_void_p), stream_ptr(stream)))
+        return shifts, rots, ref.value, scan
 
     def stage_times(self):
         ms = (ctypes.c_float * 8)()

@@ -181,6 +181,23 @@ ISA_API int isa_gamma_srgb(float* img, size_t pitch, int width, int height, void
  * PreAlignment.cs:268-281), Gaussian. Needs ctx for the FFT plan/scratch. */
 ISA_API int isa_bw_image(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, int width, int height, const isa_raw_info* info,
                  float sigma, int high_pass, float* out, size_t out_pitch, void* stream);
+/* Global pre-alignment of a burst (ComputePreAlignment, controller
+ * :1451-1528): the tracking image of every frame, then for every frame
+ * i >= 1 PreAlignment.ScanAngles (PreAlignment.cs:176-261) against frame 0
+ * -- a coarse scan of rotation angles over [zero - range, zero + range] in
+ * steps of 5 * increment and a fine scan of +-10 increments around the coarse
+ * best, each angle a cubic rotation about the frame centre, a full-frame FFT
+ * cross-correlation and the position of its maximum -- with
+ * zero = roll[0] - roll[i] (camera roll angles in degrees; NULL = 0). The
+ * results go through PreAlignmentStore (PreAlignmentStore.cs:36-110):
+ * shifts (n x 2), rotations_deg (n) and the reference index that minimises
+ * the total shift, the inputs of isa_prealign. scan (optional, n x 4): the
+ * raw ScanAngles results (x, y, angle, correlation) of each frame against
+ * frame 0. Host outputs; synchronises `stream`. Frames need at least 4096
+ * pixels. Reference controller defaults: increment 0.1, range 1.0. */
+ISA_API int isa_prealign_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                               float increment_deg, float range_deg, const float* roll_deg, float* shifts, float* rotations_deg, int* reference,
+                               double* scan, void* stream);
 /* fourierFilterKernel (BasicKernels.cs:81-100) on a (width/2+1) x height
  * half spectrum (float2), times post_scale. */
 ISA_API int isa_fourier_filter(void* spectrum, size_t pitch, int width, int height, float lp, float hp, float lps, float hps, int clear_axis,

@@ -502,3 +502,110 @@ def accumulate_canvas_ref(lib, raw, cfa, acc, wsum, mask, kp4, flow, white, blac
     mc = np.zeros((H, W, 4), lib.dtype)
     mc[oy // 2:oy // 2 + H // 2, ox // 2:ox // 2 + W // 2] = mask
     lib.accumulate_ref(canvas_raw, cfa, acc, wsum, mc, kpc, flc, white, black, True)
+
+
+# ---- global pre-alignment (checker) -------------------------------------------
+# PreAlignment.ScanAngles (PEFStudioDX/PreAlignment.cs:176-261) and
+# PreAlignmentStore (PEFStudioDX/PreAlignmentStore.cs:36-110), in FP64. The
+# reference rotates with NPP WarpAffine (InterpolationMode.Cubic); NPP's cubic
+# kernel and pixel-centre convention are not published, so this restatement
+# defines them: Keys' cubic convolution (a = -0.5) on a 4 x 4 neighbourhood with
+# clamped taps, integer pixel centres, rotation about (W/2, H/2) as
+# Matrix3x3.RotAroundCenter (Matrix.cs:93-99) composes it, destination pixels
+# whose source falls outside the frame left at 0 (the Set(0) before the warp).
+
+def _keys(t, a=-0.5):
+    t = np.abs(t)
+    return np.where(t <= 1, ((a + 2) * t - (a + 3)) * t * t + 1,
+                    np.where(t < 2, ((a * t - 5 * a) * t + 8 * a) * t - 4 * a, 0.0))
+
+
+def rotate_cubic(img, angle_deg):
+    H, W = img.shape
+    r = angle_deg / 180.0 * np.pi
+    ca, sa = np.cos(r), np.sin(r)
+    y, x = np.mgrid[0:H, 0:W].astype(np.float64)
+    dx, dy = x - W / 2.0, y - H / 2.0
+    sx, sy = ca * dx - sa * dy + W / 2.0, sa * dx + ca * dy + H / 2.0
+    inside = (sx >= 0) & (sx <= W - 1) & (sy >= 0) & (sy <= H - 1)
+    x0, y0 = np.floor(sx), np.floor(sy)
+    ax, ay = sx - x0, sy - y0
+    x0, y0 = x0.astype(np.int64), y0.astype(np.int64)
+    out = np.zeros((H, W))
+    for j in range(4):
+        wy = _keys(ay - (j - 1))
+        yy = np.clip(y0 - 1 + j, 0, H - 1)
+        row = np.zeros((H, W))
+        for i in range(4):
+            xx = np.clip(x0 - 1 + i, 0, W - 1)
+            row += _keys(ax - (i - 1)) * img[yy, xx]
+        out += wy * row
+    return np.where(inside, out, 0.0)
+
+
+def scan_angles(ref_img, img, incr, rng, zero):
+    """(x, y, angle, value) of `img` against `ref_img` (PreAlignment.cs:176-261)."""
+    H, W = img.shape
+    R = np.fft.rfft2(ref_img)
+    max_val, max_ang, max_x, max_y = -np.finfo(np.float64).max, 0.0, 0, 0
+    for phase in range(2):
+        step = 5 * incr if phase == 0 else incr
+        ang = zero - rng
+        while ang <= zero + rng:
+            T = np.fft.rfft2(rotate_cubic(img, ang))
+            cc = np.fft.irfft2(np.conj(R) * T, s=(H, W))
+            k = int(np.argmax(cc))
+            v = cc.flat[k]  # numpy's inverse already divides by W * H, as the reference's Div after cuFFT does
+            if v > max_val:
+                max_val, max_ang, max_x, max_y = v, ang, k % W, k // W
+            ang += step
+        zero, rng = max_ang, 10 * incr
+    if max_x > W // 2:
+        max_x -= W
+    if max_y > H // 2:
+        max_y -= H
+    return (-float(max_x), -float(max_y), max_ang, max_val)
+
+
+def prealign_store(init):
+    """PreAlignmentStore constructor: shifts (n x 2), rotations (n), reference index."""
+    n = len(init)
+    basic = [(0.0, 0.0, 0.0)] * n
+    for i in range(1, n):
+        basic[i - 1] = (init[i][0] - init[i - 1][0], init[i][1] - init[i - 1][1], init[i][2] - init[i - 1][2])
+    min_index, min_shift = -1, np.finfo(np.float64).max
+    for i in range(n - 1):
+        ax = ay = 0.0
+        for j in range(i):
+            ax -= basic[j][0]; ay -= basic[j][1]
+        bx = by = 0.0
+        for j in range(i, n - 1):
+            bx += basic[j][0]; by += basic[j][1]
+        d = np.sqrt((ax + bx) ** 2 + (ay + by) ** 2)
+        if d < min_shift:
+            min_shift, min_index = d, i
+    shifts = np.zeros((n, 2), np.float32)
+    rots = np.zeros(n, np.float32)
+    for i in range(n):
+        a = [0.0, 0.0, 0.0]
+        for j in range(i, min_index):
+            for c in range(3):
+                a[c] -= basic[j][c]
+        for j in range(min_index, i):
+            for c in range(3):
+                a[c] += basic[j][c]
+        shifts[i] = (a[0], a[1])
+        rots[i] = a[2]
+    return shifts, rots, min_index
+
+
+def prealign_images(images, incr=float(np.float32(0.1)), rng=float(np.float32(1.0)), rolls=None):
+    """ComputePreAlignment (controller :1451-1528) on tracking images n x H x W."""
+    n = len(images)
+    init = [(0.0, 0.0, 0.0, 0.0)] * n
+    r0 = -float(rolls[0]) if rolls is not None else 0.0
+    for i in range(1, n):
+        rt = -float(rolls[i]) if rolls is not None else 0.0
+        zero = float(np.float32(rt) - np.float32(r0))
+        init[i] = scan_angles(images[0], images[i], incr, rng, zero)
+    return init, prealign_store(init)
