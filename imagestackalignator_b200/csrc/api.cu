@@ -193,6 +193,11 @@ struct isa_ctx {
     float *half_ref = nullptr, *half_mov = nullptr;
     float4 *ref_mr = nullptr, *ref_sr = nullptr, *mov_box = nullptr;  // robustness statistics (half resolution)
     float4* masks = nullptr;
+    // adjoint scratch (allocated by the first isa_merge_backward)
+    void* adj = nullptr;
+    float* adj_gkp = nullptr;
+    float4 *adj_gmask = nullptr, *adj_m = nullptr, *adj_aux = nullptr, *adj_gm = nullptr;
+    double* adj_acc = nullptr;
     float *st3 = nullptr, *kparam = nullptr;
     float *acc = nullptr, *wsum = nullptr, *out_stage = nullptr;
     isa_frame_in* frame_in = nullptr;
@@ -853,6 +858,7 @@ int isa_ctx_destroy(isa_ctx* c)
     if (c->ev_copied) cudaEventDestroy(c->ev_copied);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->arena) cudaFree(c->arena);
+    if (c->adj) cudaFree(c->adj);
     delete c;
     return ISA_OK;
 }
@@ -874,6 +880,80 @@ int isa_merge_burst(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t fr
 {
     if (!c) return fail(ISA_EINVAL, "ctx is NULL");
     return run_merge(c, raw, raw_pitch, frame_stride, n, info, pre, out, out_pitch, S(stream));
+}
+
+int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                       const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch, float* out,
+                       size_t out_pitch, double* loss, double* grad, void* stream)
+{
+    if (!c || !raw || !target || !out || !loss || !grad) return fail(ISA_EINVAL, "NULL argument");
+    ISA_TRY(check_info(info));
+    const isa_params* p = &c->p;
+    const int W = info->width, H = info->height;
+    isa_accum_geom g;
+    float thr;
+    accum_geom(p, W, H, g, thr);
+    if (thr != 0.f) return fail(ISA_EINVAL, "the adjoint covers the merge_scale and super-resolution modes (normalisation threshold 0)");
+    if (!p->fused_accumulate) return fail(ISA_EINVAL, "the adjoint needs fused_accumulate");
+    if (target_pitch < (size_t)g.Wo * 12) return fail(ISA_EINVAL, "target pitch %zu < %d", target_pitch, g.Wo * 12);
+    if (weight && weight_pitch < (size_t)g.Wo * 4) return fail(ISA_EINVAL, "weight pitch %zu < %d", weight_pitch, g.Wo * 4);
+    cudaStream_t st = S(stream);
+    // forward (keeps flows, masks, kernel parameters, structure tensor, sums and the frame table)
+    ISA_TRY(run_merge(c, raw, raw_pitch, frame_stride, n, info, pre, out, out_pitch, st));
+    const size_t fsz = (size_t)W * H, mw = (size_t)c->max_w, mh = (size_t)c->max_h;
+    const int Wh = W / 2, Hh = H / 2;
+    const size_t hsz = (size_t)Wh * Hh, hp4 = (size_t)Wh * 16, hp3 = (size_t)Wh * 12, fp = (size_t)W * sizeof(float2), p3 = (size_t)W * 12,
+                 p4 = (size_t)W * 16, op = (size_t)g.Wo * 12;
+    if (!c->adj) {
+        const size_t hmax = (mw / 2) * (mh / 2);
+        const size_t b_gkp = mw * mh * 12, b_gmask = hmax * 16 * c->max_n, b_h = hmax * 16;
+        const size_t total = b_gkp + b_gmask + 3 * b_h + 16 * sizeof(double) + 4 * 256;
+        if (cudaMalloc(&c->adj, total) != cudaSuccess) { c->adj = nullptr; return fail(ISA_ENOMEM, "adjoint scratch of %.2f GB", total / 1e9); }
+        char* q = (char*)c->adj;
+        auto take = [&](size_t bytes) { char* r = q; q += (bytes + 255) / 256 * 256; return r; };
+        c->adj_gkp = (float*)take(b_gkp);
+        c->adj_gmask = (float4*)take(b_gmask);
+        c->adj_m = (float4*)take(b_h);
+        c->adj_aux = (float4*)take(b_h);
+        c->adj_gm = (float4*)take(b_h);
+        c->adj_acc = (double*)take(16 * sizeof(double));
+    }
+    ISA_CK(cudaMemsetAsync(c->adj_gkp, 0, fsz * 12, st));
+    ISA_CK(cudaMemsetAsync(c->adj_gmask, 0, hsz * 16 * n, st));
+    ISA_CK(cudaMemsetAsync(c->adj_acc, 0, 16 * sizeof(double), st));
+    float black[3], white[3], scale[3], divisor[3];
+    color_consts(info, black, white, scale, divisor);
+    const unsigned cfa = pack_cfa(info->cfa);
+    const int ref = pre ? pre->reference : 0;
+    // output -> kernel parameters and mask certainties (all frames at once)
+    ISA_LAUNCH(c, isa_launch_accumulate_bwd(g, cfa, c->frame_in, n, raw_pitch, fp, hp4, c->kparam, p4, white, black, out, out_pitch, c->wsum, op, target,
+                                            target_pitch, weight, weight_pitch, c->adj_gkp, c->adj_gmask, hsz, c->adj_acc + 8, st));
+    // kernel parameters -> kDetail, kDenoise, Dth, Dtr, kStretch, kShrink
+    ISA_LAUNCH(c, isa_launch_kparam_bwd(c->st3, p3, W, H, c->adj_gkp, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
+                                        c->adj_acc, st));
+    // mask certainties -> erosion -> robustness s, t (per frame, recomputing the un-eroded mask)
+    float maxv = 0.f;
+    for (int ch = 0; ch < 3; ch++) maxv = std::max(maxv, white[ch] + black[ch]);
+    int f = 1;
+    for (int i = 0; i < n; i++) {
+        if (i == ref) continue;
+        const uint16_t* fr = (const uint16_t*)((const char*)raw + (size_t)i * frame_stride);
+        const float2* flow = c->flows + (size_t)i * fsz;
+        ISA_LAUNCH(c, isa_launch_subsample(fr, raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
+        ISA_LAUNCH(c, isa_launch_box3(c->half_mov, hp3, Wh, Hh, c->mov_box, hp4, st));
+        ISA_LAUNCH(c, isa_launch_mask_store(c->ref_mr, c->ref_sr, c->mov_box, hp4, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha,
+                                            info->noise_beta, p->threshold_m, p->robust_s, p->robust_t, c->adj_m, c->adj_aux, st));
+        ISA_CK(cudaMemsetAsync(c->adj_gm, 0, hsz * 16, st));
+        ISA_LAUNCH(c, isa_launch_erode_route(c->adj_m, c->adj_gmask + (size_t)f * hsz, hp4, Wh, Hh, p->erode_size, c->adj_gm, st));
+        ISA_LAUNCH(c, isa_launch_mask_param_bwd(c->adj_m, c->adj_aux, c->adj_gm, hp4, Wh, Hh, p->robust_t, c->adj_acc + 6, st));
+        f++;
+    }
+    double h[9];
+    ISA_CK(cudaMemcpyAsync(h, c->adj_acc, sizeof(h), cudaMemcpyDeviceToHost, st));
+    ISA_CK(cudaStreamSynchronize(st));
+    *loss = h[8];
+    for (int k = 0; k < 8; k++) grad[k] = h[k];
+    return ISA_OK;
 }
 
 int isa_merge_burst_host(isa_ctx* c, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre, float* host_out,

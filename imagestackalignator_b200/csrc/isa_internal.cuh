@@ -118,6 +118,14 @@ cudaError_t isa_launch_conj_mul(const float2* a, float2* b, size_t n, cudaStream
 size_t isa_argmax_scratch_bytes();
 cudaError_t isa_launch_argmax(const float* img, int n, void* scratch, void* out, cudaStream_t st);
 
+// adjoint of the merge (robust.cu, merge.cu)
+cudaError_t isa_launch_mask_store(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch, int Wh,
+                                  int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s,
+                                  float t, float4* m_out, float4* aux_out, cudaStream_t st);
+cudaError_t isa_launch_erode_route(const float4* m, const float4* g_eroded, size_t sp, int Wh, int Hh, int size, float4* g_mask, cudaStream_t st);
+cudaError_t isa_launch_mask_param_bwd(const float4* m, const float4* aux, const float4* g_mask, size_t sp, int Wh, int Hh, float t, double* grad2,
+                                      cudaStream_t st);
+
 // merge.cu
 struct isa_accum_geom {
     int W, H;          // input frame
@@ -149,3 +157,11 @@ cudaError_t isa_launch_accumulate_x2(const isa_accum_geom& g, unsigned cfa, cons
                                      cudaStream_t st);
 cudaError_t isa_launch_apply_weighting(float* img, size_t img_pitch, const float* acc, const float* wsum, size_t pitch, int W, int H,
                                        float thr, cudaStream_t st);
+
+cudaError_t isa_launch_accumulate_bwd(const isa_accum_geom& g, unsigned cfa, const isa_frame_in* frames, int nframes, size_t raw_pitch,
+                                      size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch, const float* white,
+                                      const float* black, const float* out, size_t out_pitch, const float* wsum, size_t ws_pitch, const float* target,
+                                      size_t tg_pitch, const float* weight, size_t wt_pitch, float* gkp, float4* gmask, size_t gmask_stride, double* loss,
+                                      cudaStream_t st);
+cudaError_t isa_launch_kparam_bwd(const float* st3, size_t st_pitch, int W, int H, const float* gkp, float Dth, float Dtr, float kDetail,
+                                  float kDenoise, float kStretch, float kShrink, double* grad6, cudaStream_t st);

@@ -204,6 +204,208 @@ __global__ void k_apply_weighting(float* img, size_t img_pitch, const float* __r
     }
 }
 
+// ---- adjoint of the merge for an L2 loss --------------------------------------
+// L = sum over output pixels and channels of (out - target)^2 with
+// out_c = acc_c / wsum_c (ApplyWeighting with threshold 0). With
+// g_c = 2 (out_c - target_c) and h_c = g_c / wsum_c, a tap t of frame f with
+// normalised sample v, certainty c and weight w contributes
+//   dL/dw_t += c h_c (v - out_c),   dL/dcert += w h_c (v - out_c),
+// the weights w_t = exp(-q_t / 2) of the kernel parameters k give
+// dL/dk = sum_t dL/dw_t dw_t/dk, and the bilinear lookup of k scatters it to
+// the kernel-parameter image. Certainty gradients are scattered to the
+// frame's mask cell (atomic adds; their order is not fixed).
+template <int KC>
+__global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsigned cfa, const isa_frame_in* __restrict__ frames, int nframes,
+                                                       size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* __restrict__ kparam,
+                                                       size_t kp_pitch, F3 white, F3 black, const float* __restrict__ out, size_t out_pitch,
+                                                       const float* __restrict__ wsum, size_t ws_pitch, const float* __restrict__ target,
+                                                       size_t tg_pitch, const float* __restrict__ weight, size_t wt_pitch, float* __restrict__ gkp,
+                                                       float4* __restrict__ gmask, size_t gmask_stride, double* __restrict__ loss)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    double lsum = 0.0;
+    if (x < g.Wo && y < g.Ho) {
+        const float* op = isa::row_ptr(out, out_pitch, y) + 3 * x;
+        const float* wp = isa::row_ptr(wsum, ws_pitch, y) + 3 * x;
+        const float* tp = isa::row_ptr(target, tg_pitch, y) + 3 * x;
+        const float om = weight ? isa::row_ptr(weight, wt_pitch, y)[x] : 1.f;
+        float o[3], h[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            o[c] = op[c];
+            const float d = o[c] - tp[c];
+            lsum += (double)om * d * d;
+            h[c] = wp[c] != 0.f ? 2.f * om * d / wp[c] : 0.f;
+        }
+        if (x >= 1 && y >= 1 && x < g.Wo - 1 && y < g.Ho - 1 && (h[0] != 0.f || h[1] != 0.f || h[2] != 0.f)) {
+            const float xb = ((float)x + 0.5f + (float)g.ox) / g.s - 0.5f;
+            const float yb = ((float)y + 0.5f + (float)g.oy) / g.s - 0.5f;
+            float k[3];
+            kparam_sample<KC>(kparam, kp_pitch, g.W, g.H, xb, yb, k);
+            float wt[25], G[25];
+            bool live[25];
+#pragma unroll
+            for (int py = -2; py <= 2; py++)
+#pragma unroll
+                for (int px = -2; px <= 2; px++) {
+                    const int t = (py + 2) * 5 + px + 2;
+                    float q = px * px * k[0] + 2 * px * py * k[2] + py * py * k[1];
+                    float v = expf(-0.5f * q);
+                    live[t] = isfinite(v);  // the fallback weight does not depend on k
+                    if (!live[t]) v = px * py == 0 ? 1.f : 0.f;
+                    wt[t] = v;
+                    G[t] = 0.f;
+                }
+            int ux[5], uy[5];
+#pragma unroll
+            for (int d = 0; d < 5; d++) {
+                ux[d] = isa::clampi(floor_div_s(x + d - 2 + g.ox, g), g.cx0, g.cx1) >> 1;
+                uy[d] = isa::clampi(floor_div_s(y + d - 2 + g.oy, g), g.cy0, g.cy1) >> 1;
+            }
+            for (int f = 0; f < nframes; f++) {
+                const isa_frame_in fr = frames[f];
+                int sx = 0, sy = 0;
+                if (fr.flow) {
+                    float2 fl = flow_sample(fr.flow, flow_pitch, g.W, g.H, xb, yb);
+                    sx = (int)roundf(fl.x * g.s);
+                    sy = (int)roundf(fl.y * g.s);
+                }
+                float4* gm = gmask + (size_t)f * gmask_stride;
+#pragma unroll
+                for (int py = 0; py < 5; py++) {
+                    const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
+                    const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
+                    const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
+#pragma unroll
+                    for (int px = 0; px < 5; px++) {
+                        const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
+                        const int c = isa::cfa_at(cfa, qx, qy);
+                        if (c > 2) continue;
+                        float raw = (float)__ldg(rr + qx);
+                        raw = (raw - black.v[c]) / white.v[c];
+                        const float hc = c == 0 ? h[0] : (c == 1 ? h[1] : h[2]);
+                        const float oc = c == 0 ? o[0] : (c == 1 ? o[1] : o[2]);
+                        const float r = hc * (raw - oc);
+                        float cert = 1.f;
+                        if (mr) {
+                            const float4 m = __ldg(mr + ux[px]);
+                            cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
+                            if (!isfinite(cert)) cert = 0.f;
+                            else {
+                                float* dst = (float*)(isa::row_ptr(gm, mask_pitch, uy[py]) + ux[px]) + c;
+                                atomicAdd(dst, wt[py * 5 + px] * r);
+                            }
+                        }
+                        G[py * 5 + px] += cert * r;
+                    }
+                }
+            }
+            // dL/dk, then the transpose of the bilinear lookup (clamp addressing, zero weights skipped as in lerp2)
+            float gk[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int py = -2; py <= 2; py++)
+#pragma unroll
+                for (int px = -2; px <= 2; px++) {
+                    const int t = (py + 2) * 5 + px + 2;
+                    if (!live[t]) continue;
+                    const float gw = G[t] * wt[t];
+                    gk[0] += -0.5f * (float)(px * px) * gw;
+                    gk[1] += -0.5f * (float)(py * py) * gw;
+                    gk[2] += -(float)(px * py) * gw;
+                }
+            const float fx = floorf(xb), fy = floorf(yb);
+            const int i = (int)fx, j = (int)fy;
+            const float a = xb - fx, b = yb - fy;
+            const int i0 = isa::clampi(i, 0, g.W - 1), i1 = isa::clampi(i + 1, 0, g.W - 1), j0 = isa::clampi(j, 0, g.H - 1), j1 = isa::clampi(j + 1, 0, g.H - 1);
+            const float w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                atomicAdd(gkp + ((size_t)j0 * g.W + i0) * 3 + c, w00 * gk[c]);
+                if (a != 0.f) atomicAdd(gkp + ((size_t)j0 * g.W + i1) * 3 + c, w10 * gk[c]);
+                if (b != 0.f) atomicAdd(gkp + ((size_t)j1 * g.W + i0) * 3 + c, w01 * gk[c]);
+                if (a != 0.f && b != 0.f) atomicAdd(gkp + ((size_t)j1 * g.W + i1) * 3 + c, w11 * gk[c]);
+            }
+        }
+    }
+    // block sum of the loss, one atomic per block
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    __shared__ double sl[8];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((tid & 31) == 0) sl[tid >> 5] = lsum;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; w++) t += sl[w];
+        atomicAdd(loss, t);
+    }
+}
+
+// dL/d(kDetail, kDenoise, Dth, Dtr, kStretch, kShrink) from dL/dkparam: the
+// chain rule through k_kernel_param's FP64 arithmetic, summed over pixels.
+__global__ void __launch_bounds__(256) k_kparam_bwd(const float* __restrict__ st3, size_t st_pitch, int W, int H, const float* __restrict__ gkp,
+                                                   float Dth, float Dtr, float kDetail, float kDenoise, float kStretch, float kShrink,
+                                                   double* __restrict__ grad)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    double gp[6] = {0, 0, 0, 0, 0, 0};
+    if (x < W && y < H) {
+        const float* gk = gkp + ((size_t)y * W + x) * 3;
+        const double g0 = gk[0], g1 = gk[1], g2 = gk[2];
+        if (g0 != 0.0 || g1 != 0.0 || g2 != 0.0) {
+            const float* gs = isa::row_ptr(st3, st_pitch, y) + 3 * x;
+            double a11 = gs[0], a22 = gs[1], a12 = gs[2];
+            double hlp = sqrt((a22 - a11) * (a22 - a11) + 4.0 * a12 * a12);
+            double c = 2.0 * a12, s = a22 - a11 + hlp;
+            double nrm = sqrt(c * c + s * s);
+            if (nrm > 0) { c /= nrm; s /= nrm; } else { c = 1; s = 0; }
+            double l1 = (a11 + a22 + hlp) / 2.0, l2 = (a11 + a22 - hlp) / 2.0;
+            double A = 1 + sqrt((l1 - l2) * (l1 - l2) / ((l1 + l2) * (l1 + l2)));
+            double Draw = 1 - sqrt(l1) / (double)Dtr + (double)Dth;
+            double D = fmax(fmin(1.0, Draw), 0.0);
+            const double kd = kDetail, kst = kStretch, ksh = kShrink, kdn = kDenoise;
+            double u1 = (1.0 - D) * (kd * kst * A) + D * kd * kdn;
+            double u2 = (1.0 - D) * (kd / ksh * A) + D * kd * kdn;
+            double k1 = u1 * u1, k2 = u2 * u2;
+            double x2 = c, y2 = s, x1 = s, y1 = -c;
+            double b11 = k1 * x1 * x1 + x2 * x2 * k2;
+            double b12 = k1 * x1 * y1 + x2 * y2 * k2;
+            double b22 = k1 * y1 * y1 + y2 * y2 * k2;
+            double det = b11 * b22 - b12 * b12 + (double)0.0000000001f;
+            double id = 1.0 / det, id2 = id * id;
+            // out0 = b22/det, out1 = b11/det, out2 = -b12/det; d(det) = b22 db11 + b11 db22 - 2 b12 db12
+            double gb11 = g0 * (-b22 * b22 * id2) + g1 * (id - b11 * b22 * id2) + g2 * (b12 * b22 * id2);
+            double gb22 = g0 * (id - b22 * b11 * id2) + g1 * (-b11 * b11 * id2) + g2 * (b12 * b11 * id2);
+            double gb12 = g0 * (2.0 * b22 * b12 * id2) + g1 * (2.0 * b11 * b12 * id2) + g2 * (-id - 2.0 * b12 * b12 * id2);
+            double gk1 = gb11 * x1 * x1 + gb12 * x1 * y1 + gb22 * y1 * y1;
+            double gk2 = gb11 * x2 * x2 + gb12 * x2 * y2 + gb22 * y2 * y2;
+            double gu1 = 2.0 * u1 * gk1, gu2 = 2.0 * u2 * gk2;
+            gp[0] = gu1 * ((1.0 - D) * kst * A + D * kdn) + gu2 * ((1.0 - D) * A / ksh + D * kdn);
+            gp[1] = (gu1 + gu2) * D * kd;
+            gp[4] = gu1 * (1.0 - D) * kd * A;
+            gp[5] = gu2 * (-(1.0 - D) * kd * A / (ksh * ksh));
+            if (Draw > 0.0 && Draw < 1.0) {
+                double gD = gu1 * (-kd * kst * A + kd * kdn) + gu2 * (-kd * A / ksh + kd * kdn);
+                gp[2] = gD;
+                gp[3] = gD * sqrt(l1) / ((double)Dtr * (double)Dtr);
+            }
+        }
+    }
+    __shared__ double sg[8][6];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        double v = gp[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0) sg[tid >> 5][q] = v;
+    }
+    __syncthreads();
+    if (tid < 6) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += sg[w][tid];
+        atomicAdd(grad + tid, t);
+    }
+}
+
 inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
 
 }  // namespace
@@ -255,5 +457,27 @@ cudaError_t isa_launch_apply_weighting(float* img, size_t img_pitch, const float
 {
     dim3 b(32, 8);
     k_apply_weighting<<<grid2(W, H, b), b, 0, st>>>(img, img_pitch, acc, wsum, pitch, W, H, thr);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_accumulate_bwd(const isa_accum_geom& g, unsigned cfa, const isa_frame_in* frames, int nframes, size_t raw_pitch,
+                                      size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch, const float* white,
+                                      const float* black, const float* out, size_t out_pitch, const float* wsum, size_t ws_pitch, const float* target,
+                                      size_t tg_pitch, const float* weight, size_t wt_pitch, float* gkp, float4* gmask, size_t gmask_stride, double* loss,
+                                      cudaStream_t st)
+{
+    F3 wh, bl;
+    for (int c = 0; c < 3; c++) { wh.v[c] = white[c]; bl.v[c] = black[c]; }
+    dim3 b(32, 8), grd = grid2(g.Wo, g.Ho, b);
+    k_accumulate_bwd<4><<<grd, b, 0, st>>>(g, cfa, frames, nframes, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, out, out_pitch,
+                                           wsum, ws_pitch, target, tg_pitch, weight, wt_pitch, gkp, gmask, gmask_stride, loss);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_kparam_bwd(const float* st3, size_t st_pitch, int W, int H, const float* gkp, float Dth, float Dtr, float kDetail,
+                                  float kDenoise, float kStretch, float kShrink, double* grad6, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_kparam_bwd<<<grid2(W, H, b), b, 0, st>>>(st3, st_pitch, W, H, gkp, Dth, Dtr, kDetail, kDenoise, kStretch, kShrink, grad6);
     return cudaGetLastError();
 }

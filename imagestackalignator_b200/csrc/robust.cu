@@ -184,10 +184,14 @@ struct RobustTabs {
 
 // mask_at with the reference statistics and the moved 3x3 means looked up;
 // a shifted centre outside the image (whose clamped taps differ from the
-// clamped centre's) is summed directly.
-__device__ float4 mask_fast(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
-                            const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m,
-                            float s_lit, float t_lit, int x, int y)
+// clamped centre's) is summed directly. The terms the adjoint needs are
+// returned too: the three exponentials E_c and the gain sg (s, or 0 where
+// M exceeds the threshold), so that mask_c = clamp(sg E_c - t, 0, 1).
+struct MaskTerms { float m[3]; float M; float E[3]; float sg; };
+
+__device__ __forceinline__ MaskTerms mask_terms(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                                                const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
+                                                float thr_m, float s_lit, float t_lit, int x, int y)
 {
     float2 sf = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x, y);
     float2 sl = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x + 2, y + 2);
@@ -213,9 +217,9 @@ __device__ float4 mask_fast(const RobustTabs& tb, const float* __restrict__ mov3
     float md = fabsf(mr[0] - mm[0]) + fabsf(mr[1] - mm[1]) + fabsf(mr[2] - mm[2]);
     md /= 3.0f;
     mxx *= 0.5f * md; mxy *= 0.5f * md; mnx *= 0.5f * md; mny *= 0.5f * md;
-    float M = sqrtf((mxx - mnx) * (mxx - mnx) + (mxy - mny) * (mxy - mny));
-    float sgain = M > thr_m ? 0.f : s_lit;
-    float out[3];
+    MaskTerms r;
+    r.M = sqrtf((mxx - mnx) * (mxx - mnx) + (mxy - mny) * (mxy - mny));
+    r.sg = r.M > thr_m ? 0.f : s_lit;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         float sr = sr3[c];
@@ -224,9 +228,37 @@ __device__ float4 mask_fast(const RobustTabs& tb, const float* __restrict__ mov3
         float dist = fabsf(mr[c] - mm[c]);
         float sig = fmaxf(smd, sr);
         dist = dist * (sr * sr / (sr * sr + smd * smd));
-        out[c] = fmaxf(fminf(sgain * expf(-dist * dist / (sig * sig)) - t_lit, 1.0f), 0.0f);
+        r.E[c] = expf(-dist * dist / (sig * sig));
+        r.m[c] = fmaxf(fminf(r.sg * r.E[c] - t_lit, 1.0f), 0.0f);
     }
-    return make_float4(out[0], out[1], out[2], M);
+    return r;
+}
+
+__device__ __forceinline__ float4 mask_fast(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                                            const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m,
+                                            float s_lit, float t_lit, int x, int y)
+{
+    const MaskTerms r = mask_terms(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s_lit, t_lit, x, y);
+    return make_float4(r.m[0], r.m[1], r.m[2], r.M);
+}
+
+// Adjoint support: the un-eroded mask of every half-res pixel (border 1, as
+// in the forward) and its exponentials and gain (zero on the border, whose
+// value does not depend on s and t).
+__global__ void k_mask_store(RobustTabs tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh, const float2* __restrict__ flow,
+                             size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s, float t, float4* __restrict__ m_out,
+                             float4* __restrict__ aux_out, size_t sp)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wh || y >= Hh) return;
+    float4 m = make_float4(1.f, 1.f, 1.f, 1.f), aux = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (x >= 1 && x < Wh - 1 && y >= 1 && y < Hh - 1) {
+        const MaskTerms r = mask_terms(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, x, y);
+        m = make_float4(r.m[0], r.m[1], r.m[2], r.M);
+        aux = make_float4(r.E[0], r.E[1], r.E[2], r.sg);
+    }
+    isa::row_ptr(m_out, sp, y)[x] = m;
+    isa::row_ptr(aux_out, sp, y)[x] = aux;
 }
 
 // Mask over a 32 x 32 output tile plus the erosion halo in shared memory
@@ -274,6 +306,69 @@ __global__ void __launch_bounds__(256) k_robustness_erode_fast(RobustTabs tb, co
             m.x = fminf(m.x, v.x); m.y = fminf(m.y, v.y); m.z = fminf(m.z, v.z); m.w = fminf(m.w, v.w);
         }
         isa::row_ptr(out, out_pitch, y)[x] = m;
+    }
+}
+
+// Adjoint of the 5x5 erosion: each eroded value's gradient goes to the
+// first pixel of its window (row-major, replicate border) holding the
+// minimum, per channel.
+__global__ void k_erode_route(const float4* __restrict__ m, const float4* __restrict__ g_eroded, size_t sp, int Wh, int Hh, int size,
+                              float4* __restrict__ g_mask)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wh || y >= Hh) return;
+    const float4 ge = isa::row_ptr(g_eroded, sp, y)[x];
+    const float gc[3] = {ge.x, ge.y, ge.z};
+    const int a = size / 2;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (gc[c] == 0.f) continue;
+        float best = INFINITY;
+        int bx = x, by = y;
+        for (int j = 0; j < size; j++) {
+            const int yy = isa::clampi(y + j - a, 0, Hh - 1);
+            for (int i = 0; i < size; i++) {
+                const int xx = isa::clampi(x + i - a, 0, Wh - 1);
+                const float4 v = __ldg(isa::row_ptr(m, sp, yy) + xx);
+                const float vc = c == 0 ? v.x : (c == 1 ? v.y : v.z);
+                if (vc < best) { best = vc; bx = xx; by = yy; }
+            }
+        }
+        atomicAdd((float*)(isa::row_ptr(g_mask, sp, by) + bx) + c, gc[c]);
+    }
+}
+
+// dL/ds and dL/dt from the un-eroded mask's gradient: mask_c = clamp(sg E_c - t, 0, 1).
+__global__ void __launch_bounds__(256) k_mask_param_bwd(const float4* __restrict__ m, const float4* __restrict__ aux, const float4* __restrict__ g_mask,
+                                                       size_t sp, int Wh, int Hh, float t_lit, double* __restrict__ grad2)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    double gs = 0.0, gt = 0.0;
+    if (x >= 1 && x < Wh - 1 && y >= 1 && y < Hh - 1) {
+        const float4 gm = __ldg(isa::row_ptr(g_mask, sp, y) + x);
+        const float4 ax = __ldg(isa::row_ptr(aux, sp, y) + x);
+        const float g[3] = {gm.x, gm.y, gm.z}, E[3] = {ax.x, ax.y, ax.z};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float raw = ax.w * E[c] - t_lit;
+            if (g[c] != 0.f && raw > 0.f && raw < 1.f) {
+                if (ax.w != 0.f) gs += (double)g[c] * E[c];
+                gt -= (double)g[c];
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        gs += __shfl_xor_sync(0xffffffffu, gs, o);
+        gt += __shfl_xor_sync(0xffffffffu, gt, o);
+    }
+    __shared__ double sh[8][2];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((tid & 31) == 0) { sh[tid >> 5][0] = gs; sh[tid >> 5][1] = gt; }
+    __syncthreads();
+    if (tid < 2) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += sh[w][tid];
+        atomicAdd(grad2 + tid, t);
     }
 }
 
@@ -333,5 +428,30 @@ cudaError_t isa_launch_robustness_erode_tabs(const float4* mr, const float4* sr,
     dim3 g((Wh + RF_T - 1) / RF_T, (Hh + RF_T - 1) / RF_T);
     k_robustness_erode_fast<<<g, 256, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size, out,
                                                out_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_mask_store(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch, int Wh,
+                                  int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s,
+                                  float t, float4* m_out, float4* aux_out, cudaStream_t st)
+{
+    RobustTabs tb{mr, sr, box, sp};
+    dim3 b(32, 8);
+    k_mask_store<<<grid2(Wh, Hh, b), b, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, m_out, aux_out, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_erode_route(const float4* m, const float4* g_eroded, size_t sp, int Wh, int Hh, int size, float4* g_mask, cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_erode_route<<<grid2(Wh, Hh, b), b, 0, st>>>(m, g_eroded, sp, Wh, Hh, size, g_mask);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_mask_param_bwd(const float4* m, const float4* aux, const float4* g_mask, size_t sp, int Wh, int Hh, float t, double* grad2,
+                                      cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_mask_param_bwd<<<grid2(Wh, Hh, b), b, 0, st>>>(m, aux, g_mask, sp, Wh, Hh, t, grad2);
     return cudaGetLastError();
 }

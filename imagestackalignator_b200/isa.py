@@ -70,7 +70,7 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
-    "isa_bw_image", "isa_prealign_burst", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
+    "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
@@ -222,6 +222,25 @@ class Merger:
         check(lib().isa_merge_burst(self.ctx, vp(raw), ctypes.c_size_t(W * 2), ctypes.c_size_t(W * H * 2), n, ctypes.byref(info),
                                     ctypes.byref(pre), vp(out), ctypes.c_size_t(Wo * 12), stream_ptr(stream)))
         return out
+
+    def backward(self, raw, info: IsaRawInfo, target, weight=None, out=None, shifts=None, rotations=None, reference=0, stream=None):
+        """Forward merge and the adjoint of sum(weight * (out - target)^2) (isa_merge_backward).
+
+        Returns (out, loss, grad) with grad = d loss / d (k_detail, k_denoise,
+        dth, dtr, k_stretch, k_shrink, robust_s, robust_t) as float64."""
+        import torch
+        n, H, W = raw.shape
+        Wo, Ho = self.output_size(W, H)
+        if out is None:
+            out = torch.empty((Ho, Wo, 3), dtype=torch.float32, device=raw.device)
+        pre, keep = self._pre(n, shifts, rotations, reference)
+        loss = ctypes.c_double()
+        grad = np.zeros(8, np.float64)
+        check(lib().isa_merge_backward(self.ctx, vp(raw), ctypes.c_size_t(W * 2), ctypes.c_size_t(W * H * 2), n, ctypes.byref(info),
+                                       ctypes.byref(pre), vp(target), ctypes.c_size_t(Wo * 12), vp(weight) if weight is not None else None,
+                                       ctypes.c_size_t(Wo * 4), vp(out), ctypes.c_size_t(Wo * 12),
+                                       ctypes.byref(loss), grad.ctypes.data_as(ctypes.c_void_p), stream_ptr(stream)))
+        return out, loss.value, grad
 
     def merge_host(self, raw_host, info: IsaRawInfo, out_host=None, shifts=None, rotations=None, reference=0, stream=None):
         """raw_host: host uint16 array/tensor (pinned for full speed); returns host float32 Ho x Wo x 3."""

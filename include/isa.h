@@ -146,6 +146,32 @@ ISA_API long isa_launch_count(isa_ctx* ctx);
  * raw_pitch. out: float3 image of isa_output_size() with out_pitch. */
 ISA_API int isa_merge_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
                     const isa_prealign* pre, float* out, size_t out_pitch, void* stream);
+/* Forward merge plus the adjoint of the weighted L2 loss
+ *   L = sum over output pixels p and channels c of weight_p (out - target)^2
+ * with respect to the merge parameters, in this order: k_detail, k_denoise,
+ * dth, dtr, k_stretch, k_shrink (through the kernel shape,
+ * kernel.cu:628-700, and the kernel weights of the accumulation,
+ * DeBayerKernels.cu:290-468) and robust_s, robust_t (through the robustness
+ * mask, RobustnessModell.cu:29-157, and its erosion). No counterpart in the
+ * reference, which has no gradients. Runs isa_merge_burst into `out`
+ * (output size, out_pitch), then the adjoint with tile-level recomputation
+ * of the masks instead of stored per-frame weights; writes *loss and
+ * grad[8] (host) and synchronises `stream`. target: float3 image of the
+ * output size; weight: one float per output pixel (NULL = all 1).
+ * The loss is piecewise smooth: an output channel whose certainty-weighted
+ * weight sum reaches exactly zero is set to 0 (ApplyWeighting), a jump, and
+ * the mask clamps and the erosion's minimum have kinks; the gradient is
+ * that of the smooth piece at the parameters (a zero weight excludes pixels
+ * near such jumps). The gradient with respect to the flow is zero almost
+ * everywhere -- the accumulation and the mask read the frames at
+ * round(s * flow) and round(flow / 2) and the mask's flow term M only
+ * switches the gain at a threshold -- so none is returned. Covers the
+ * merge_scale and super-resolution modes (normalisation threshold 0) with
+ * fused_accumulate; the first call allocates the adjoint scratch in the
+ * context. */
+ISA_API int isa_merge_backward(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                               const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch,
+                               float* out, size_t out_pitch, double* loss, double* grad, void* stream);
 /* The same with host buffers: frames are copied in and the image copied out
  * on `stream` (pinned host memory gives full PCIe speed). */
 ISA_API int isa_merge_burst_host(isa_ctx* ctx, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre,
