@@ -187,6 +187,46 @@ def run_reference(args):
     return 0
 
 
+ADJ = dict(width=4000, height=3000, frames=10, scale=1.5)  # the differentiable-merge workload (10 x 4000x3000 at 1.5x)
+
+
+def adjoint_ratio(args):
+    """Forward merge vs forward + adjoint (isa_merge_backward) of an L2 loss on
+    the differentiable-merge workload, device time per call, same warm-up and
+    step counts as the main measurement."""
+    import torch
+    from imagestackalignator_b200 import isa, synthetic
+    W, H, n = ADJ["width"], ADJ["height"], ADJ["frames"]
+    b = synthetic.make_burst(W, H, n, seed=2000, max_shift=WORKLOAD["max_shift"], max_rot_deg=WORKLOAD["max_rot_deg"],
+                             noise_a=WORKLOAD["noise_a"], noise_b=WORKLOAD["noise_b"], device="cuda")
+    p = merge_params()
+    p.merge_scale = ADJ["scale"]
+    m = isa.Merger(W, H, n, p)
+    info = isa.make_info(b)
+    raw = torch.from_numpy(b.raw.view(np.int16)).cuda()
+    out = m.merge(raw, info)
+    target = (0.9 * out + 0.03).contiguous()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    fwd = timed(lambda: m.merge(raw, info, out))
+    both = timed(lambda: m.backward(raw, info, target, out=out))
+    m.close()
+    return {"workload": f"{n}x{W}x{H} merged at {ADJ['scale']}x, L2 loss, gradients of the 8 merge parameters", "fwd_ms": fwd,
+            "fwd_adj_ms": both, "ratio": both / fwd}
+
+
 def run_ours(args):
     import torch
     from imagestackalignator_b200 import isa
@@ -282,6 +322,9 @@ def run_ours(args):
         cpu = {"value": px / 1e6 / dt, "unit": UNIT, "cores": threads, "kind": "reference",
                "sample": f"{WORKLOAD['frames']} frames of {SAMPLE['width']}x{SAMPLE['height']} (same statistics) merged at 2x by the "
                          f"reference kernels compiled for the host (FP32, OpenMP), {dt:.1f} s wall"}
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = adjoint_ratio(args)
     names = ["tracking_images", "tile_alignment", "kernel_params", "lk_and_robustness", "accumulation", "finalize"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -293,6 +336,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "fwd_adjoint": adjoint,
         "clocks": clocks,
     }
     if rank == 0:
@@ -313,6 +357,7 @@ def main():
     ap.add_argument("--per-frame", action="store_true", help="accumulate frame by frame (reference layout) instead of fused")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--size", default=None, help="WxH override for profiling runs on a smaller burst (not a bench line)")
     ap.add_argument("--frames", type=int, default=None, help="frame-count override for profiling runs (not a bench line)")
     args = ap.parse_args()
