@@ -86,34 +86,57 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
     tile_offset(tx, ty, T, Wl, Hl, pd.base_trk_x, pd.base_trk_y, pd.rot_trk, pre.x, pre.y, oxt, oyt);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = L::NT / 32;
-    // stage the template and the search block: clamped columns once per lane, one row per warp iteration
+    // stage the template and the search block, one row per warp iteration; all loads of a warp are
+    // issued before any store, so their latencies overlap
     constexpr int TX = (T + 31) / 32, BX = (B + 31) / 32;
-    int cr[TX], ct[BX];
-#pragma unroll
-    for (int k = 0; k < TX; k++) cr[k] = isa::clampi(tx * T + S + lane + 32 * k + oxr, 0, Wl - 1);
-#pragma unroll
-    for (int k = 0; k < BX; k++) ct[k] = isa::clampi(tx * T + lane + 32 * k + oxt, 0, Wl - 1);
-    // all loads of a warp are issued before any store, so their latencies overlap
     constexpr int TR = (T + NW - 1) / NW, BR = (B + NW - 1) / NW;
     float vt[TR][TX], vb[BR][BX];
+    const int xr0 = tx * T + S + oxr, yr0 = ty * T + S + oyr, xt0 = tx * T + oxt, yt0 = ty * T + oyt;
+    if (xr0 >= 0 && xr0 + T <= Wl && yr0 >= 0 && yr0 + T <= Hl && xt0 >= 0 && xt0 + B <= Wl && yt0 >= 0 && yt0 + B <= Hl) {
+        // both regions inside the level image: no clamping, rows a fixed stride apart
+        const char* pr = (const char*)(imr + xr0 + lane) + (size_t)(yr0 + warp) * pitch;
+        const char* pt = (const char*)(imt + xt0 + lane) + (size_t)(yt0 + warp) * pitch;
+        const size_t step = (size_t)NW * pitch;
 #pragma unroll
-    for (int i = 0; i < TR; i++) {
-        const int y = warp + i * NW;
-        if (y < T) {
-            const float* row = isa::row_ptr(imr, pitch, isa::clampi(ty * T + S + y + oyr, 0, Hl - 1));
+        for (int i = 0; i < TR; i++)
+            if (warp + i * NW < T) {
 #pragma unroll
-            for (int k = 0; k < TX; k++)
-                if (lane + 32 * k < T) vt[i][k] = __ldg(row + cr[k]);
+                for (int k = 0; k < TX; k++)
+                    if (lane + 32 * k < T) vt[i][k] = __ldg((const float*)(pr + i * step) + 32 * k);
+            }
+#pragma unroll
+        for (int i = 0; i < BR; i++)
+            if (warp + i * NW < B) {
+#pragma unroll
+                for (int k = 0; k < BX; k++)
+                    if (lane + 32 * k < B) vb[i][k] = __ldg((const float*)(pt + i * step) + 32 * k);
+            }
+    } else {
+        // clamped columns once per lane, clamped rows per iteration (replicate border)
+        int cr[TX], ct[BX];
+#pragma unroll
+        for (int k = 0; k < TX; k++) cr[k] = isa::clampi(xr0 + lane + 32 * k, 0, Wl - 1);
+#pragma unroll
+        for (int k = 0; k < BX; k++) ct[k] = isa::clampi(xt0 + lane + 32 * k, 0, Wl - 1);
+#pragma unroll
+        for (int i = 0; i < TR; i++) {
+            const int y = warp + i * NW;
+            if (y < T) {
+                const float* row = isa::row_ptr(imr, pitch, isa::clampi(yr0 + y, 0, Hl - 1));
+#pragma unroll
+                for (int k = 0; k < TX; k++)
+                    if (lane + 32 * k < T) vt[i][k] = __ldg(row + cr[k]);
+            }
         }
-    }
 #pragma unroll
-    for (int i = 0; i < BR; i++) {
-        const int y = warp + i * NW;
-        if (y < B) {
-            const float* row = isa::row_ptr(imt, pitch, isa::clampi(ty * T + y + oyt, 0, Hl - 1));
+        for (int i = 0; i < BR; i++) {
+            const int y = warp + i * NW;
+            if (y < B) {
+                const float* row = isa::row_ptr(imt, pitch, isa::clampi(yt0 + y, 0, Hl - 1));
 #pragma unroll
-            for (int k = 0; k < BX; k++)
-                if (lane + 32 * k < B) vb[i][k] = __ldg(row + ct[k]);
+                for (int k = 0; k < BX; k++)
+                    if (lane + 32 * k < B) vb[i][k] = __ldg(row + ct[k]);
+            }
         }
     }
 #pragma unroll
