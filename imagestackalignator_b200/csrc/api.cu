@@ -460,6 +460,16 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     float2* grids_tmp = c->grids_tmp;
     ISA_CK(cudaMemsetAsync(grids, 0, gstride * strat.m, st));
     int tcx0 = 0, tcy0 = 0;
+    // levels with resize 2, 4 and 8 (the default pyramid) from one read of each tracking image
+    int lv_of[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
+    for (int li = 0; li < L; li++)
+        if (p->levels[li].resize_level >= 1 && p->levels[li].resize_level <= 8) lv_of[p->levels[li].resize_level] = li;
+    const bool fused_pyramid = lv_of[2] >= 0 && lv_of[4] >= 0 && lv_of[8] >= 0;
+    if (fused_pyramid)
+        for (int i = 0; i < n; i++)
+            ISA_LAUNCH(c, isa_launch_pyramid248(c->bw_track + i * fsz, pitch, W, H, c->pyr[lv_of[2]] + (size_t)i * (W / 2) * (H / 2), bw_pitch(W / 2),
+                                                c->pyr[lv_of[4]] + (size_t)i * (W / 4) * (H / 4), bw_pitch(W / 4),
+                                                c->pyr[lv_of[8]] + (size_t)i * (W / 8) * (H / 8), bw_pitch(W / 8), st));
     for (int li = L - 1; li >= 0; li--) {
         const isa_level& lv = p->levels[li];
         const int Wl = W / lv.resize_level, Hl = H / lv.resize_level;
@@ -475,9 +485,10 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         size_t lpitch = bw_pitch(Wl);
         if (lv.resize_level > 1) {
             float* base = c->pyr[li];
+            const bool done = fused_pyramid && (lv.resize_level == 2 || lv.resize_level == 4 || lv.resize_level == 8) && lv_of[lv.resize_level] == li;
             for (int i = 0; i < n; i++) {
                 float* dst = base + (size_t)i * Wl * Hl;
-                ISA_LAUNCH(c, isa_launch_resize_box(c->bw_track + i * fsz, pitch, W, H, lv.resize_level, dst, lpitch, st));
+                if (!done) ISA_LAUNCH(c, isa_launch_resize_box(c->bw_track + i * fsz, pitch, W, H, lv.resize_level, dst, lpitch, st));
                 fptr[i] = dst;
             }
         } else {

@@ -252,12 +252,34 @@ __global__ void __launch_bounds__(256) k_gauss2d(const float* __restrict__ in, s
     float t[NT];
 #pragma unroll
     for (int k = 0; k < NT; k++) t[k] = taps.t[k];
-    for (int yy = tid >> 5; yy < SH; yy += 8) {
-        const float* row = isa::row_ptr(in, in_pitch, isa::clampi(y0 - R + yy, 0, H - 1));
-        for (int xx = tid & 31; xx < SW; xx += 32) {
-            float v = __ldg(row + isa::clampi(x0 - R + xx, 0, W - 1));
-            if (clamp_in) v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
-            s_in[yy][xx] = v;
+    // all loads of a thread are issued before its stores (compile-time trip counts)
+    constexpr int RY = (SH + 7) / 8, RX = (SW + 31) / 32;
+    float v[RY][RX];
+    const int lane = tid & 31, wy = tid >> 5;
+    int cx[RX];
+#pragma unroll
+    for (int k = 0; k < RX; k++) cx[k] = isa::clampi(x0 - R + lane + 32 * k, 0, W - 1);
+#pragma unroll
+    for (int j = 0; j < RY; j++) {
+        const int yy = wy + 8 * j;
+        if (yy < SH) {
+            const float* row = isa::row_ptr(in, in_pitch, isa::clampi(y0 - R + yy, 0, H - 1));
+#pragma unroll
+            for (int k = 0; k < RX; k++)
+                if (lane + 32 * k < SW) v[j][k] = __ldg(row + cx[k]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < RY; j++) {
+        const int yy = wy + 8 * j;
+        if (yy < SH) {
+#pragma unroll
+            for (int k = 0; k < RX; k++)
+                if (lane + 32 * k < SW) {
+                    float q = v[j][k];
+                    if (clamp_in) q = q < 0.f ? 0.f : (q > 1.f ? 1.f : q);
+                    s_in[yy][lane + 32 * k] = q;
+                }
         }
     }
     __syncthreads();
@@ -295,6 +317,67 @@ __global__ void k_resize_box(const float* __restrict__ in, size_t in_pitch, int 
         for (int i = 0; i < L; i++) s += r[i];
     }
     isa::row_ptr(out, out_pitch, y)[x] = s / (float)(L * L);
+}
+
+// The 2x, 4x and 8x box means of one image from a single read: a thread owns
+// an 8 x 8 block and sums each output's L x L pixels in the order of
+// k_resize_box (rows, then columns, from 0), so the values are identical.
+__global__ void k_pyramid248(const float* __restrict__ in, size_t in_pitch, int W, int H, float* __restrict__ o2, size_t p2, float* __restrict__ o4,
+                             size_t p4, float* __restrict__ o8, size_t p8)
+{
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y * blockDim.y + threadIdx.y;
+    const int x0 = 8 * bx, y0 = 8 * by;
+    if (x0 >= W - 1 || y0 >= H - 1) return;  // no 2x2 output starts here
+    float v[8][8];
+    const bool full = x0 + 8 <= W && y0 + 8 <= H && ((((uintptr_t)in) | in_pitch) & 15) == 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const float* r = isa::row_ptr(in, in_pitch, min(y0 + j, H - 1)) + x0;
+        if (full) {
+            const float4 a = __ldg((const float4*)r), b = __ldg((const float4*)r + 1);
+            v[j][0] = a.x; v[j][1] = a.y; v[j][2] = a.z; v[j][3] = a.w; v[j][4] = b.x; v[j][5] = b.y; v[j][6] = b.z; v[j][7] = b.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) v[j][i] = x0 + i < W ? __ldg(r + i) : 0.f;
+        }
+    }
+    const int W2 = W / 2, H2 = H / 2, W4 = W / 4, H4 = H / 4, W8 = W / 8, H8 = H / 8;
+#pragma unroll
+    for (int qy = 0; qy < 4; qy++)
+#pragma unroll
+        for (int qx = 0; qx < 4; qx++) {
+            const int x = 4 * bx + qx, y = 4 * by + qy;
+            if (x < W2 && y < H2) {
+                float s = 0.f;
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 2; i++) s += v[2 * qy + j][2 * qx + i];
+                isa::row_ptr(o2, p2, y)[x] = s / 4.0f;
+            }
+        }
+#pragma unroll
+    for (int qy = 0; qy < 2; qy++)
+#pragma unroll
+        for (int qx = 0; qx < 2; qx++) {
+            const int x = 2 * bx + qx, y = 2 * by + qy;
+            if (x < W4 && y < H4) {
+                float s = 0.f;
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) s += v[4 * qy + j][4 * qx + i];
+                isa::row_ptr(o4, p4, y)[x] = s / 16.0f;
+            }
+        }
+    if (bx < W8 && by < H8) {
+        float s = 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+#pragma unroll
+            for (int i = 0; i < 8; i++) s += v[j][i];
+        isa::row_ptr(o8, p8, by)[bx] = s / 64.0f;
+    }
 }
 
 // deBayersSubSample3 (DeBayerKernels.cu:244-283).
@@ -389,5 +472,13 @@ cudaError_t isa_launch_subsample(const uint16_t* raw, size_t raw_pitch, int W, i
 {
     dim3 b(32, 8);
     k_subsample<<<grid2(W / 2, H / 2, b), b, 0, st>>>(raw, raw_pitch, W / 2, H / 2, cfa, max_val, out, out_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_pyramid248(const float* in, size_t in_pitch, int W, int H, float* o2, size_t p2, float* o4, size_t p4, float* o8, size_t p8,
+                                  cudaStream_t st)
+{
+    dim3 b(32, 8);
+    k_pyramid248<<<grid2((W + 7) / 8, (H + 7) / 8, b), b, 0, st>>>(in, in_pitch, W, H, o2, p2, o4, p4, o8, p8);
     return cudaGetLastError();
 }

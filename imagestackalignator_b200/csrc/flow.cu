@@ -83,28 +83,49 @@ __device__ __forceinline__ float2 lk_update(float2 f, double sxx, double sxy, do
     return make_float2((float)((double)f.x + u), (float)((double)f.y + v));
 }
 
-// c, s: cosine and sine of the pre-alignment rotation (uniform, computed once on the host).
+// c, s: cosine and sine of the pre-alignment rotation (uniform, computed once
+// on the host). Each thread writes FF_PX consecutive pixels of a row.
+constexpr int FF_PX = 4;
+
 __global__ void k_flow_from_tiles(const float2* __restrict__ tiles, size_t tile_pitch, int tcx, int tcy, int W, int H, float bx, float by,
                                   float c, float s, float2* __restrict__ flow, size_t flow_pitch)
 {
-    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= W || y >= H) return;
-    float fx = c * -bx - s * -by;
-    float fy = s * -bx + c * -by;
-    float pcx = (float)(x - W / 2), pcy = (float)(y - H / 2);
-    fx += c * pcx - s * pcy - pcx;
-    fy += s * pcx + c * pcy - pcy;
-    float xb = ((float)x + 0.5f) / (float)W * tcx - 0.5f, yb = ((float)y + 0.5f) / (float)H * tcy - 0.5f;
-    float flx = floorf(xb), fly = floorf(yb);
-    int i = (int)flx, j = (int)fly;
-    float a = xb - flx, b = yb - fly;
-    int i0 = isa::clampi(i, 0, tcx - 1), i1 = isa::clampi(i + 1, 0, tcx - 1), j0 = isa::clampi(j, 0, tcy - 1), j1 = isa::clampi(j + 1, 0, tcy - 1);
+    const int xq = (blockIdx.x * blockDim.x + threadIdx.x) * FF_PX, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (xq >= W || y >= H) return;
+    const float pcy = (float)(y - H / 2);
+    const float yb = ((float)y + 0.5f) / (float)H * tcy - 0.5f;
+    const float fly = floorf(yb);
+    const int j = (int)fly;
+    const float b = yb - fly;
+    const int j0 = isa::clampi(j, 0, tcy - 1), j1 = isa::clampi(j + 1, 0, tcy - 1);
     const float2* r0 = isa::row_ptr(tiles, tile_pitch, j0);
     const float2* r1 = isa::row_ptr(tiles, tile_pitch, j1);
-    float2 p00 = r0[i0], p10 = r0[i1], p01 = r1[i0], p11 = r1[i1];
-    fx += isa::lerp2(p00.x, p10.x, p01.x, p11.x, a, b);
-    fy += isa::lerp2(p00.y, p10.y, p01.y, p11.y, a, b);
-    isa::row_ptr(flow, flow_pitch, y)[x] = make_float2(fx, fy);
+    const float fx0 = c * -bx - s * -by, fy0 = s * -bx + c * -by;
+    float2 res[FF_PX];
+#pragma unroll
+    for (int q = 0; q < FF_PX; q++) {
+        const int x = min(xq + q, W - 1);
+        float fx = fx0, fy = fy0;
+        const float pcx = (float)(x - W / 2);
+        fx += c * pcx - s * pcy - pcx;
+        fy += s * pcx + c * pcy - pcy;
+        const float xb = ((float)x + 0.5f) / (float)W * tcx - 0.5f;
+        const float flx = floorf(xb);
+        const int i = (int)flx;
+        const float a = xb - flx;
+        const int i0 = isa::clampi(i, 0, tcx - 1), i1 = isa::clampi(i + 1, 0, tcx - 1);
+        const float2 p00 = __ldg(r0 + i0), p10 = __ldg(r0 + i1), p01 = __ldg(r1 + i0), p11 = __ldg(r1 + i1);
+        fx += isa::lerp2(p00.x, p10.x, p01.x, p11.x, a, b);
+        fy += isa::lerp2(p00.y, p10.y, p01.y, p11.y, a, b);
+        res[q] = make_float2(fx, fy);
+    }
+    float2* o = isa::row_ptr(flow, flow_pitch, y) + xq;
+    if (xq + FF_PX <= W && ((uintptr_t)o & 15) == 0) {
+        ((float4*)o)[0] = make_float4(res[0].x, res[0].y, res[1].x, res[1].y);
+        ((float4*)o)[1] = make_float4(res[2].x, res[2].y, res[3].x, res[3].y);
+    } else {
+        for (int q = 0; q < FF_PX && xq + q < W; q++) o[q] = res[q];
+    }
 }
 
 __global__ void k_warp(const float* __restrict__ img, size_t img_pitch, int W, int H, const float2* __restrict__ flow, size_t flow_pitch,
@@ -331,7 +352,7 @@ cudaError_t isa_launch_flow_from_tiles(const float2* tiles, size_t tile_pitch, i
 {
     dim3 b(32, 8);
     const float c = rot == 0.f ? 1.f : (float)cos((double)rot), s = rot == 0.f ? 0.f : (float)sin((double)rot);
-    k_flow_from_tiles<<<grid2(W, H, b), b, 0, st>>>(tiles, tile_pitch, tcx, tcy, W, H, bx, by, c, s, flow, flow_pitch);
+    k_flow_from_tiles<<<grid2((W + FF_PX - 1) / FF_PX, H, b), b, 0, st>>>(tiles, tile_pitch, tcx, tcy, W, H, bx, by, c, s, flow, flow_pitch);
     return cudaGetLastError();
 }
 

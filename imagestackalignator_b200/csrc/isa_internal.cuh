@@ -64,6 +64,8 @@ cudaError_t isa_launch_gauss(const float* in, size_t in_pitch, float* out, size_
                              int H, int C, const float* taps, int ntaps, int clamp01_input, cudaStream_t st);
 cudaError_t isa_launch_resize_box(const float* in, size_t in_pitch, int W, int H, int L, float* out, size_t out_pitch,
                                   cudaStream_t st);
+cudaError_t isa_launch_pyramid248(const float* in, size_t in_pitch, int W, int H, float* o2, size_t p2, float* o4, size_t p4, float* o8, size_t p8,
+                                  cudaStream_t st);
 cudaError_t isa_launch_subsample(const uint16_t* raw, size_t raw_pitch, int W, int H, unsigned cfa, float max_val, float* out,
                                  size_t out_pitch, cudaStream_t st);
 
