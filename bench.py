@@ -227,6 +227,62 @@ def adjoint_ratio(args):
             "fwd_adj_ms": both, "ratio": both / fwd}
 
 
+BATCH = dict(width=2048, height=1536, frames=8, bursts=16, contexts=4)  # many small bursts (phone-sized) merged at 2x
+
+
+def batch_throughput(args):
+    """Many small bursts: one context on one stream (isa_merge_burst per burst)
+    against isa_merge_batch over several contexts and streams, device time for
+    the whole set of bursts, same warm-up and step counts as the main line."""
+    import torch
+    from imagestackalignator_b200 import isa, synthetic
+    W, H, n, nb, nc = BATCH["width"], BATCH["height"], BATCH["frames"], BATCH["bursts"], BATCH["contexts"]
+    p = merge_params()
+    mergers = [isa.Merger(W, H, n, p) for _ in range(nc)]
+    Wo, Ho = mergers[0].output_size(W, H)
+    items = []
+    for i in range(nb):
+        b = synthetic.make_burst(W, H, n, seed=3000 + i, max_shift=WORKLOAD["max_shift"], max_rot_deg=WORKLOAD["max_rot_deg"],
+                                 noise_a=WORKLOAD["noise_a"], noise_b=WORKLOAD["noise_b"], device="cuda")
+        items.append(dict(raw=torch.from_numpy(b.raw.view(np.int16)).cuda(), info=isa.make_info(b),
+                          out=torch.empty((Ho, Wo, 3), dtype=torch.float32, device="cuda")))
+    main = torch.cuda.current_stream()
+    streams = [torch.cuda.Stream() for _ in range(nc)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def sequential():
+        for it in items:
+            mergers[0].merge(it["raw"], it["info"], it["out"], stream=main)
+
+    def batched():
+        for s in streams:
+            s.wait_stream(main)
+        st = isa.merge_batch(mergers, items, streams)
+        if any(st):
+            raise RuntimeError(f"isa_merge_batch status {st}")
+        for s in streams:
+            main.wait_stream(s)
+
+    def timed(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(main)
+        for _ in range(args.steps):
+            fn()
+        e1.record(main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    seq = timed(sequential)
+    bat = timed(batched)
+    for m in mergers:
+        m.close()
+    mp = nb * Wo * Ho / 1e6
+    return {"workload": f"{nb} bursts of {n}x{W}x{H} merged at 2x", "contexts": nc, "sequential_ms": seq, "batched_ms": bat,
+            "sequential_mp_s": mp / (seq / 1e3), "batched_mp_s": mp / (bat / 1e3), "batched_bursts_s": nb / (bat / 1e3)}
+
+
 def run_ours(args):
     import torch
     from imagestackalignator_b200 import isa
@@ -325,6 +381,9 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = adjoint_ratio(args)
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batch = batch_throughput(args)
     names = ["tracking_images", "tile_alignment", "kernel_params", "lk_and_robustness", "accumulation", "finalize"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -336,7 +395,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint,
+        "fwd_adjoint": adjoint, "batch": batch,
         "clocks": clocks,
     }
     if rank == 0:
@@ -358,6 +417,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
+    ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
     ap.add_argument("--size", default=None, help="WxH override for profiling runs on a smaller burst (not a bench line)")
     ap.add_argument("--frames", type=int, default=None, help="frame-count override for profiling runs (not a bench line)")
     args = ap.parse_args()

@@ -967,6 +967,44 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
     return ISA_OK;
 }
 
+int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, int* status)
+{
+    if (!ctxs || nctx < 1 || (!bursts && nbursts > 0) || nbursts < 0) return fail(ISA_EINVAL, "bad batch arguments");
+    for (int i = 0; i < nctx; i++)
+        if (!ctxs[i]) return fail(ISA_EINVAL, "context %d is NULL", i);
+    std::vector<double> load(nctx, 0.0);
+    int first = ISA_OK;
+    for (int b = 0; b < nbursts; b++) {
+        const isa_burst& u = bursts[b];
+        int rc = ISA_OK;
+        if (!u.info || !u.raw || !u.out) rc = fail(ISA_EINVAL, "burst %d: NULL argument", b);
+        int k = 0;
+        for (int i = 1; i < nctx; i++)
+            if (load[i] < load[k]) k = i;
+        isa_ctx* c = ctxs[k];
+        const isa_params saved = c->p;
+        if (rc == ISA_OK && u.params) {
+            const isa_params& q = *u.params;
+            rc = check_params(&q);
+            bool same = rc == ISA_OK && q.level_count == saved.level_count && q.tracking_strategy == saved.tracking_strategy &&
+                        q.tracking_block_size == saved.tracking_block_size;
+            for (int l = 0; same && l < q.level_count; l++)
+                same = q.levels[l].resize_level == saved.levels[l].resize_level && q.levels[l].tile_size == saved.levels[l].tile_size &&
+                       q.levels[l].max_shift == saved.levels[l].max_shift;
+            if (rc == ISA_OK && !same) rc = fail(ISA_EINVAL, "burst %d: params change the pyramid levels or the tracking strategy", b);
+            if (rc == ISA_OK) c->p = q;
+        }
+        if (rc == ISA_OK) {
+            rc = run_merge(c, u.raw, u.raw_pitch, u.frame_stride, u.n, u.info, u.pre, u.out, u.out_pitch, S(streams ? streams[k] : nullptr));
+            load[k] += (double)u.info->width * u.info->height * u.n;
+        }
+        c->p = saved;
+        if (status) status[b] = rc;
+        if (rc != ISA_OK && first == ISA_OK) first = rc;
+    }
+    return first;
+}
+
 int isa_merge_burst_host(isa_ctx* c, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre, float* host_out,
                          void* stream)
 {

@@ -70,7 +70,7 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
-    "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
+    "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
@@ -300,6 +300,36 @@ class Merger:
         tx, ty = ctypes.c_int(), ctypes.c_int()
         check(lib().isa_debug_shifts(self.ctx, ctypes.byref(p), ctypes.byref(tx), ctypes.byref(ty)))
         return p.value, tx.value, ty.value
+
+
+class IsaBurst(ctypes.Structure):
+    _fields_ = [("raw", ctypes.c_void_p), ("raw_pitch", ctypes.c_size_t), ("frame_stride", ctypes.c_size_t), ("n", ctypes.c_int),
+                ("info", ctypes.c_void_p), ("pre", ctypes.c_void_p), ("params", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                ("out_pitch", ctypes.c_size_t)]
+
+
+def merge_batch(mergers, bursts, streams=None):
+    """isa_merge_batch: `bursts` is a list of dicts with raw (device n x H x W
+    tensor), info (IsaRawInfo), out (device Ho x Wo x 3 tensor) and optionally
+    params (MergeParams); returns the per-burst status list. Work is enqueued
+    on `streams` (one per merger; torch streams or None) and not waited for."""
+    keep = []
+    arr = (IsaBurst * len(bursts))()
+    for i, b in enumerate(bursts):
+        raw, info, out = b["raw"], b["info"], b["out"]
+        n, H, W = raw.shape
+        pp = None
+        if b.get("params") is not None:
+            pp = make_params(b["params"])
+            keep.append(pp)
+        keep.append(info)
+        arr[i] = IsaBurst(raw.data_ptr(), W * 2, W * H * 2, n, ctypes.addressof(info), None,
+                          ctypes.addressof(pp) if pp is not None else None, out.data_ptr(), out.shape[1] * 12)
+    ctxs = (ctypes.c_void_p * len(mergers))(*[m.ctx for m in mergers])
+    sts = (ctypes.c_void_p * len(mergers))(*[stream_ptr(s) for s in (streams or [None] * len(mergers))])
+    status = (ctypes.c_int * max(1, len(bursts)))()
+    lib().isa_merge_batch(ctxs, sts, len(mergers), arr, len(bursts), status)
+    return [status[i] for i in range(len(bursts))]
 
 
 def device_copy(ptr, shape, dtype, device="cuda"):

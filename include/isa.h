@@ -118,6 +118,18 @@ typedef struct isa_prealign {
 
 typedef struct isa_ctx isa_ctx;
 
+/* One burst of a batch (isa_merge_batch). */
+typedef struct isa_burst {
+    const uint16_t* raw;         /* device, n frames; frame i at raw + i * frame_stride bytes, rows at raw_pitch */
+    size_t raw_pitch, frame_stride;
+    int n;
+    const isa_raw_info* info;
+    const isa_prealign* pre;     /* NULL: no pre-alignment */
+    const struct isa_params* params;  /* NULL: the context's parameters */
+    float* out;                  /* device float3 image of isa_output_size(), rows at out_pitch */
+    size_t out_pitch;
+} isa_burst;
+
 /* ---- context, parameters, errors --------------------------------------- */
 ISA_API void isa_params_default(isa_params* p);
 ISA_API const char* isa_last_error(void);
@@ -172,6 +184,19 @@ ISA_API int isa_merge_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch,
 ISA_API int isa_merge_backward(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
                                const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch,
                                float* out, size_t out_pitch, double* loss, double* grad, void* stream);
+/* Many bursts of different sizes, frame counts, CFA layouts, bit depths and
+ * merge scales (no counterpart in the reference, whose controller merges one
+ * burst). Each burst goes to the context with the least work queued so far
+ * (W * H * n, in burst order, deterministic) and is merged on that context's
+ * stream (streams[i] for ctxs[i]); contexts run concurrently, so small
+ * bursts that cannot fill the GPU alone overlap. Returns after enqueuing all
+ * bursts; the caller synchronises the streams. A burst's params may differ
+ * from its context's in the merge mode and scale and in the scalar
+ * parameters, but must keep the context's pyramid levels and tracking
+ * strategy, and its frames and output must fit the context. status[b]
+ * (optional, host) receives each burst's result; the return value is the
+ * first failure, or ISA_OK. */
+ISA_API int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, int* status);
 /* The same with host buffers: frames are copied in and the image copied out
  * on `stream` (pinned host memory gives full PCIe speed). */
 ISA_API int isa_merge_burst_host(isa_ctx* ctx, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre,
