@@ -283,6 +283,38 @@ def batch_throughput(args):
             "sequential_mp_s": mp / (seq / 1e3), "batched_mp_s": mp / (bat / 1e3), "batched_bursts_s": nb / (bat / 1e3)}
 
 
+def post_throughput(args, merged):
+    """Colour/tone post-processing (isa_postprocess, the SaveAs16BitTiff chain)
+    of the merged image to uint16 RGB: device time per call, HBM roofline."""
+    import torch
+    from imagestackalignator_b200 import isa
+    Ho, Wo, _ = merged.shape
+    lx = np.float32(np.round(np.arange(256) / 255.0, 9))
+    ly = np.float32(np.clip(lx + 0.12 * np.sin(2 * np.pi * lx) / (2 * np.pi), 0, 1))
+    cam = np.array([[0.62, 0.24, 0.10], [0.27, 0.69, 0.04], [0.03, 0.12, 0.68]])
+    t1, t2 = isa.color_twists(cam)
+    pp, keep = isa.post_params((0, 0, Wo, Ho), [1.0, 1.0, 1.0], t1, t2, lx, ly, 0.0)
+    out16 = torch.empty((Ho, Wo, 3), dtype=torch.int16, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup)):
+        isa.postprocess(merged, pp, isa.POST_RGB16, out16)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        isa.postprocess(merged, pp, isa.POST_RGB16, out16)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    alg = Wo * Ho * (12 + 6)
+    peak, kind = measured_peak()
+    gbs = alg / (ms / 1e3) / 1e9
+    return {"workload": f"{Wo}x{Ho} float3 -> uint16 RGB (clamp, 2 colour twists, 256-level cubic LUT, exposure, sRGB gamma)",
+            "ms": ms, "mp_s": Wo * Ho / 1e6 / (ms / 1e3), "algorithmic_bytes": alg, "achieved_gbs": gbs, "frac": gbs / peak,
+            "peak_source": f"{kind} hbm_gbs",
+            "l2": f"input {Wo * Ho * 12 / 1e9:.2f} GB {'larger' if Wo * Ho * 12 > 126e6 else 'smaller'} than the 126 MB L2"}
+
+
 def run_ours(args):
     import torch
     from imagestackalignator_b200 import isa
@@ -381,6 +413,9 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = adjoint_ratio(args)
+    post = None
+    if rank == 0 and world == 1 and not args.no_post:
+        post = post_throughput(args, out)
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = batch_throughput(args)
@@ -395,7 +430,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint, "batch": batch,
+        "fwd_adjoint": adjoint, "batch": batch, "postprocess": post,
         "clocks": clocks,
     }
     if rank == 0:
@@ -418,6 +453,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
+    ap.add_argument("--no-post", action="store_true", help="skip the colour/tone post-processing timing")
     ap.add_argument("--size", default=None, help="WxH override for profiling runs on a smaller burst (not a bench line)")
     ap.add_argument("--frames", type=int, default=None, help="frame-count override for profiling runs (not a bench line)")
     args = ap.parse_args()

@@ -1438,3 +1438,238 @@ extern "C" int isa_solve_shifts_static(int n, int ref, int strategy, int block, 
     return ISA_OK;
 }
 
+
+// ---- colour and tone post-processing, TIFF output ----
+
+namespace {
+
+struct M3 { double a[3][3]; };
+
+// DNGMatrix operator * (DNGMatrix.cs:232-254): sums from 0.0 in column order
+M3 mat_mul(const M3& x, const M3& y)
+{
+    M3 r;
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) {
+            double s = 0.0;
+            for (int m = 0; m < 3; m++) s += x.a[j][m] * y.a[m][k];
+            r.a[j][k] = s;
+        }
+    return r;
+}
+
+// DNGMatrix.Invert3x3 (DNGMatrix.cs:440-486): adjugate over the determinant
+bool mat_inv3(const M3& m, M3& out)
+{
+    const double a00 = m.a[0][0], a01 = m.a[0][1], a02 = m.a[0][2], a10 = m.a[1][0], a11 = m.a[1][1], a12 = m.a[1][2], a20 = m.a[2][0],
+                 a21 = m.a[2][1], a22 = m.a[2][2];
+    double t[3][3];
+    t[0][0] = a11 * a22 - a21 * a12;
+    t[0][1] = a21 * a02 - a01 * a22;
+    t[0][2] = a01 * a12 - a11 * a02;
+    t[1][0] = a20 * a12 - a10 * a22;
+    t[1][1] = a00 * a22 - a20 * a02;
+    t[1][2] = a10 * a02 - a00 * a12;
+    t[2][0] = a10 * a21 - a20 * a11;
+    t[2][1] = a20 * a01 - a00 * a21;
+    t[2][2] = a00 * a11 - a10 * a01;
+    const double det = a00 * t[0][0] + a01 * t[1][0] + a02 * t[2][0];
+    if (!(std::fabs(det) >= 1e-10)) return false;  // NEAR_ZERO (DNGMatrix.cs:34)
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) out.a[j][k] = t[j][k] / det;
+    return true;
+}
+
+// DNGColorSpace(toPCS) (DNGColorSpace.cs:45-65): rows scaled so that RGB
+// white (1, 1, 1) maps to the PCS white (D50 xy (0.3457, 0.3585) as XYZ,
+// DNGxyCoord.cs:79-101, 175-181, 211-214); fromPCS is its inverse.
+bool color_space(const M3& toPCS, M3& to, M3& from)
+{
+    const double x = 0.3457, y = 0.3585;  // inside the pinning range of XYtoXYZ, x + y < 0.999999
+    const double W2[3] = {x / y, 1.0, (1.0 - x - y) / y};
+    for (int j = 0; j < 3; j++) {
+        double w1 = 0.0;
+        for (int m = 0; m < 3; m++) w1 += toPCS.a[j][m] * 1.0;
+        const double s = W2[j] / w1;
+        for (int k = 0; k < 3; k++) to.a[j][k] = s * toPCS.a[j][k];
+    }
+    return mat_inv3(to, from);
+}
+
+void twist_of(const M3& m, float t[12])
+{
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) t[i * 4 + j] = (float)m.a[i][j];
+        t[i * 4 + 3] = 0.f;
+    }
+}
+
+int check_post(const isa_post_params* pp, int width, int height)
+{
+    ISA_REQ(pp, "NULL post-processing parameters");
+    ISA_REQ(pp->crop_x >= 0 && pp->crop_y >= 0 && pp->crop_w > 0 && pp->crop_h > 0 && pp->crop_x + pp->crop_w <= width &&
+                pp->crop_y + pp->crop_h <= height,
+            "crop outside the image");
+    if (!(pp->lut_x && pp->lut_y && pp->nlut >= 4 && pp->nlut <= ISA_MAX_LUT)) return fail(ISA_EINVAL, "LUT needs 4 to %d levels", ISA_MAX_LUT);
+    for (int i = 1; i < pp->nlut; i++)
+        if (!(pp->lut_x[i] > pp->lut_x[i - 1])) return fail(ISA_EINVAL, "LUT levels must increase strictly (level %d)", i);
+    for (int i = 0; i < pp->nlut; i++)
+        if (!std::isfinite(pp->lut_x[i]) || !std::isfinite(pp->lut_y[i])) return fail(ISA_EINVAL, "LUT entry %d is not finite", i);
+    return ISA_OK;
+}
+
+// LUTCubic as the cubic through the four nearest levels: for segment k
+// (x[k] <= v < x[k + 1]) the levels i0 .. i0 + 3, i0 = clamp(k - 1, 0, n - 4),
+// in FP64: Newton divided differences on the nodes z_j = x[i0 + j] - x[k],
+// expanded to c0 + c1 t + c2 t^2 + c3 t^3 in t = v - x[k], then rounded to float.
+void lut_coefficients(const float* x, const float* y, int n, float (*c)[4])
+{
+    for (int k = 0; k < n - 1; k++) {
+        const int i0 = std::min(std::max(k - 1, 0), n - 4);
+        double z[4], a[4];
+        for (int j = 0; j < 4; j++) {
+            z[j] = (double)x[i0 + j] - (double)x[k];
+            a[j] = (double)y[i0 + j];
+        }
+        for (int o = 1; o < 4; o++)
+            for (int j = 3; j >= o; j--) a[j] = (a[j] - a[j - 1]) / (z[j] - z[j - o]);
+        // p(t) = a0 + (t - z0)(a1 + (t - z1)(a2 + (t - z2) a3)), expanded from the inside out
+        double p[4] = {a[3], 0.0, 0.0, 0.0};  // coefficients of t^0 .. t^3 of the partial polynomial
+        int deg = 0;
+        for (int j = 2; j >= 0; j--) {
+            // p <- p * (t - z_j) + a_j
+            double q[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int d = 0; d <= deg; d++) {
+                q[d + 1] += p[d];
+                q[d] -= z[j] * p[d];
+            }
+            q[0] += a[j];
+            deg++;
+            for (int d = 0; d < 4; d++) p[d] = q[d];
+        }
+        for (int d = 0; d < 4; d++) c[k][d] = (float)p[d];
+    }
+}
+
+void post_args(const isa_post_params* pp, isa_post_args& a)
+{
+    a.crop_x = pp->crop_x; a.crop_y = pp->crop_y; a.crop_w = pp->crop_w; a.crop_h = pp->crop_h;
+    for (int c = 0; c < 3; c++) a.wb[c] = pp->camera_white[c];
+    for (int i = 0; i < 12; i++) { a.t1[i] = pp->twist1[i]; a.t2[i] = pp->twist2[i]; }
+    a.amp = (float)std::pow(2.0, (double)pp->exposure);  // (float)Math.Pow(2.0, Exposure) (:2243)
+    a.nlut = pp->nlut;
+    a.uniform = 1;
+    lut_coefficients(pp->lut_x, pp->lut_y, pp->nlut, a.lut_c);
+    for (int i = 0; i < pp->nlut; i++) {
+        a.lut_x[i] = pp->lut_x[i];
+        // near-uniform levels (within half a step of i / (n - 1)): the kernel's guess is off by at most one level
+        if (!(std::fabs((double)pp->lut_x[i] - (double)i / (pp->nlut - 1)) <= 0.5 / (pp->nlut - 1))) a.uniform = 0;
+    }
+}
+
+void put16(std::vector<unsigned char>& b, size_t at, uint16_t v) { b[at] = v & 255; b[at + 1] = v >> 8; }
+void put32(std::vector<unsigned char>& b, size_t at, uint32_t v)
+{
+    for (int i = 0; i < 4; i++) b[at + i] = (v >> (8 * i)) & 255;
+}
+
+}  // namespace
+
+int isa_color_twists(const double camera_to_pcs[9], float twist1[12], float twist2[12])
+{
+    ISA_REQ(camera_to_pcs && twist1 && twist2, "NULL argument");
+    // DNGColorSpace.ProPhoto and .sRGB50 (DNGColorSpace.cs:35-42)
+    const M3 prophoto{{{0.7976749, 0.1351917, 0.0313534}, {0.2880402, 0.7118741, 0.0000857}, {0.0000000, 0.0000000, 0.8252100}}};
+    const M3 srgb50{{{0.4360747, 0.3850649, 0.1430804}, {0.2225045, 0.7168786, 0.0606169}, {0.0139322, 0.0971045, 0.7141733}}};
+    M3 pp_to, pp_from, s_to, s_from, cam;
+    ISA_REQ(color_space(prophoto, pp_to, pp_from) && color_space(srgb50, s_to, s_from), "colour space matrix is singular");
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) cam.a[j][k] = camera_to_pcs[j * 3 + k];
+    twist_of(mat_mul(pp_from, cam), twist1);      // ProPhoto.FromPCS * cameraToXYZ (:2227)
+    twist_of(mat_mul(s_from, pp_to), twist2);     // sRGB50.FromPCS * ProPhoto.ToPCS (:2239)
+    return ISA_OK;
+}
+
+int isa_postprocess(const float* img, size_t pitch, int width, int height, const isa_post_params* pp, int format, void* out, size_t out_pitch,
+                    void* stream)
+{
+    ISA_REQ(img && out && width > 0 && height > 0 && pitch >= (size_t)width * 12, "bad image argument");
+    if (format != ISA_POST_RGB16 && format != ISA_POST_BGRA8) return fail(ISA_EINVAL, "unknown output format %d", format);
+    ISA_TRY(check_post(pp, width, height));
+    ISA_REQ(out_pitch >= (size_t)pp->crop_w * (format == ISA_POST_RGB16 ? 6 : 4) && (format == ISA_POST_RGB16 || out_pitch % 4 == 0) &&
+                (format == ISA_POST_RGB16 ? ((uintptr_t)out & 1) == 0 && out_pitch % 2 == 0 : ((uintptr_t)out & 3) == 0),
+            "bad output pitch or alignment");
+    isa_post_args a;
+    post_args(pp, a);
+    ISA_CK(isa_launch_postprocess(img, pitch, a, format, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_save_tiff16(const char* path, const uint16_t* rgb, int width, int height)
+{
+    ISA_REQ(path && rgb && width > 0 && height > 0, "bad argument");
+    const uint64_t nbytes = (uint64_t)width * height * 3 * 2;
+    ISA_REQ(nbytes <= 0xffffffffull - 200, "image too large for a 32-bit TIFF");
+    // header, the IFD of 13 entries in the order of ImageFileDirectory(width, height)
+    // (ImageFileDirectory.cs:75-92), then the out-of-line values in the same
+    // order (BitsPerSample, XResolution, YResolution, Make), then the strip
+    std::vector<unsigned char> b(200, 0);
+    b[0] = 0x49; b[1] = 0x49; b[2] = 0x2A; b[3] = 0; put32(b, 4, 8);
+    put16(b, 8, 13);
+    size_t e = 10;
+    const auto entry = [&](uint16_t tag, uint16_t type, uint32_t count, uint32_t value) {
+        put16(b, e, tag); put16(b, e + 2, type); put32(b, e + 4, count); put32(b, e + 8, value);
+        e += 12;
+    };
+    const uint32_t data_at = 200;
+    entry(256, 4, 1, (uint32_t)width);             // ImageWidth, LONG
+    entry(257, 4, 1, (uint32_t)height);            // ImageLength, LONG
+    entry(258, 3, 3, 170);                         // BitsPerSample 16, 16, 16 (out of line)
+    entry(259, 3, 1, 1);                           // Compression: none
+    entry(262, 3, 1, 2);                           // PhotometricInterpretation: RGB
+    entry(273, 4, 1, data_at);                     // StripOffsets
+    entry(277, 3, 1, 3);                           // SamplesPerPixel
+    entry(278, 4, 1, (uint32_t)height);            // RowsPerStrip
+    entry(279, 4, 1, (uint32_t)nbytes);            // StripByteCounts
+    entry(282, 5, 1, 176);                         // XResolution 720/10
+    entry(283, 5, 1, 184);                         // YResolution 720/10
+    entry(296, 3, 1, 1);                           // ResolutionUnit: none
+    entry(271, 2, 8, 192);                         // Make "MK TIFF\0"
+    put32(b, e, 0);                                // no next IFD; e + 4 == 170
+    put16(b, 170, 16); put16(b, 172, 16); put16(b, 174, 16);
+    put32(b, 176, 720); put32(b, 180, 10);
+    put32(b, 184, 720); put32(b, 188, 10);
+    std::memcpy(&b[192], "MK TIFF", 8);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(ISA_EINVAL, "cannot open %s for writing", path);
+    bool ok = std::fwrite(b.data(), 1, b.size(), f) == b.size();
+    // uint16 little-endian samples (BinaryWriter.Write(ushort))
+    std::vector<unsigned char> row((size_t)width * 6);
+    for (int y = 0; ok && y < height; y++) {
+        const uint16_t* r = rgb + (size_t)y * width * 3;
+        for (size_t i = 0; i < (size_t)width * 3; i++) { row[2 * i] = r[i] & 255; row[2 * i + 1] = r[i] >> 8; }
+        ok = std::fwrite(row.data(), 1, row.size(), f) == row.size();
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(ISA_EINVAL, "writing %s failed", path);
+    return ISA_OK;
+}
+
+int isa_save_as_16bit_tiff(const float* img, size_t pitch, int width, int height, const isa_post_params* pp, const char* path, void* stream)
+{
+    ISA_REQ(path, "NULL path");
+    ISA_TRY(check_post(pp, width, height));
+    const size_t bytes = (size_t)pp->crop_w * pp->crop_h * 6;
+    void* d = nullptr;
+    ISA_CK(cudaMallocAsync(&d, bytes, S(stream)));
+    std::vector<uint16_t> h((size_t)pp->crop_w * pp->crop_h * 3);
+    int rc = isa_postprocess(img, pitch, width, height, pp, ISA_POST_RGB16, d, (size_t)pp->crop_w * 6, stream);
+    if (rc == ISA_OK) {
+        cudaError_t e = cudaMemcpyAsync(h.data(), d, bytes, cudaMemcpyDeviceToHost, S(stream));
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
+        if (e != cudaSuccess) rc = fail(ISA_ECUDA, "copying the image to the host: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(d, S(stream));
+    if (rc != ISA_OK) return rc;
+    return isa_save_tiff16(path, h.data(), pp->crop_w, pp->crop_h);
+}

@@ -3,6 +3,7 @@
 // channels interleaved (float2 flow, float3 RGB, float4 masks/kernels).
 #pragma once
 #include <cuda_runtime.h>
+#include "isa.h"
 #include <stdint.h>
 #include <math.h>
 #include <algorithm>
@@ -167,3 +168,16 @@ cudaError_t isa_launch_accumulate_bwd(const isa_accum_geom& g, unsigned cfa, con
                                       cudaStream_t st);
 cudaError_t isa_launch_kparam_bwd(const float* st3, size_t st_pitch, int W, int H, const float* gkp, float Dth, float Dtr, float kDetail,
                                   float kDenoise, float kStretch, float kShrink, double* grad6, cudaStream_t st);
+
+// post.cu: the post-processing chain (isa_postprocess), arguments by value
+struct isa_post_args {
+    int crop_x, crop_y, crop_w, crop_h;
+    float wb[3];
+    float t1[12], t2[12];
+    float amp;
+    int nlut, uniform;
+    float lut_x[ISA_MAX_LUT];
+    float lut_c[ISA_MAX_LUT - 1][4];  // per segment k: cubic in t = v - lut_x[k], c0 + c1 t + c2 t^2 + c3 t^3
+};
+cudaError_t isa_launch_postprocess(const float* img, size_t pitch, const isa_post_args& a, int format, void* out, size_t out_pitch,
+                                   cudaStream_t st);

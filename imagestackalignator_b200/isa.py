@@ -74,6 +74,7 @@ EXPORTS = [
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
+    "isa_color_twists", "isa_postprocess", "isa_save_tiff16", "isa_save_as_16bit_tiff",
 ]
 
 _lib = None
@@ -300,6 +301,71 @@ class Merger:
         tx, ty = ctypes.c_int(), ctypes.c_int()
         check(lib().isa_debug_shifts(self.ctx, ctypes.byref(p), ctypes.byref(tx), ctypes.byref(ty)))
         return p.value, tx.value, ty.value
+
+
+MAX_LUT = 512
+POST_RGB16, POST_BGRA8 = 0, 1
+
+
+class IsaPostParams(ctypes.Structure):
+    _fields_ = [("crop_x", ctypes.c_int), ("crop_y", ctypes.c_int), ("crop_w", ctypes.c_int), ("crop_h", ctypes.c_int),
+                ("camera_white", ctypes.c_float * 3), ("twist1", ctypes.c_float * 12), ("twist2", ctypes.c_float * 12),
+                ("lut_x", ctypes.c_void_p), ("lut_y", ctypes.c_void_p), ("nlut", ctypes.c_int), ("exposure", ctypes.c_float)]
+
+
+def color_twists(camera_to_pcs):
+    """isa_color_twists: (camera -> ProPhoto, ProPhoto -> sRGB) as float32 3 x 4 arrays."""
+    m = np.ascontiguousarray(camera_to_pcs, np.float64).reshape(9)
+    t1 = np.zeros(12, np.float32)
+    t2 = np.zeros(12, np.float32)
+    check(lib().isa_color_twists(m.ctypes.data_as(ctypes.c_void_p), t1.ctypes.data_as(ctypes.c_void_p), t2.ctypes.data_as(ctypes.c_void_p)))
+    return t1.reshape(3, 4), t2.reshape(3, 4)
+
+
+def post_params(crop, camera_white, twist1, twist2, lut_x, lut_y, exposure=0.0):
+    """(IsaPostParams, arrays to keep alive while it is used)."""
+    lx = np.ascontiguousarray(lut_x, np.float32)
+    ly = np.ascontiguousarray(lut_y, np.float32)
+    pp = IsaPostParams()
+    pp.crop_x, pp.crop_y, pp.crop_w, pp.crop_h = (int(v) for v in crop)
+    for c in range(3):
+        pp.camera_white[c] = float(camera_white[c])
+    for i, v in enumerate(np.asarray(twist1, np.float32).reshape(12)):
+        pp.twist1[i] = float(v)
+    for i, v in enumerate(np.asarray(twist2, np.float32).reshape(12)):
+        pp.twist2[i] = float(v)
+    pp.lut_x = lx.ctypes.data
+    pp.lut_y = ly.ctypes.data
+    pp.nlut = len(lx)
+    pp.exposure = float(exposure)
+    return pp, (lx, ly)
+
+
+def postprocess(img, pp: IsaPostParams, fmt=POST_RGB16, out=None, stream=None):
+    """isa_postprocess on a device float32 H x W x 3 image; returns the crop as
+    uint16 crop_h x crop_w x 3 (RGB16) or uint8 crop_h x crop_w x 4 (BGRA8)."""
+    import torch
+    H, W, _ = img.shape
+    if out is None:
+        shape = (pp.crop_h, pp.crop_w, 3) if fmt == POST_RGB16 else (pp.crop_h, pp.crop_w, 4)
+        out = torch.empty(shape, dtype=torch.int16 if fmt == POST_RGB16 else torch.uint8, device=img.device)
+    row = pp.crop_w * (6 if fmt == POST_RGB16 else 4)
+    check(lib().isa_postprocess(vp(img), ctypes.c_size_t(W * 12), W, H, ctypes.byref(pp), fmt, vp(out), ctypes.c_size_t(row),
+                                stream_ptr(stream)))
+    return out
+
+
+def save_tiff16(path, rgb):
+    """isa_save_tiff16 of a host uint16 H x W x 3 array."""
+    a = np.ascontiguousarray(rgb, np.uint16)
+    h, w, _ = a.shape
+    check(lib().isa_save_tiff16(os.fsencode(path), a.ctypes.data_as(ctypes.c_void_p), w, h))
+
+
+def save_as_16bit_tiff(img, pp: IsaPostParams, path, stream=None):
+    """isa_save_as_16bit_tiff: post-process a device float3 image and write the TIFF."""
+    H, W, _ = img.shape
+    check(lib().isa_save_as_16bit_tiff(vp(img), ctypes.c_size_t(W * 12), W, H, ctypes.byref(pp), os.fsencode(path), stream_ptr(stream)))
 
 
 class IsaBurst(ctypes.Structure):

@@ -359,6 +359,52 @@ ISA_API int isa_accumulate(const uint16_t* raw, size_t raw_pitch, int width, int
 ISA_API int isa_apply_weighting(float* img, const float* acc, const float* wsum, size_t pitch, int width, int height, float threshold,
                         void* stream);
 
+/* ---- Colour and tone post-processing and 16-bit TIFF output ----
+ * The controller's SaveAs16BitTiff (ImageStackAlignatorController.cs:2197-2260)
+ * and ProcessColorsAndShow (:2262-2320) after ApplyWeighting: NPP
+ * ThresholdLTGT to [0, CameraWhite], ColorTwist camera -> ProPhoto,
+ * ThresholdLTGT to [0, 1], LUTCubic (tone curve), ColorTwist ProPhoto ->
+ * sRGB (D50), Mul 2^Exposure, GammasRGB (kernel.cu:290-332), Mul 65535 (or
+ * 255), ROI = the raw file's crop, Convert with NppRoundMode.Near. */
+#define ISA_MAX_LUT 512
+typedef struct isa_post_params {
+    int crop_x, crop_y, crop_w, crop_h;   /* RawFile CropLeft, CropTop, CroppedWidth, CroppedHeight */
+    float camera_white[3];                /* DNGColorSpec.CameraWhite: per-channel upper clamp */
+    float twist1[12];                     /* camera -> ProPhoto, 3 x 4 row-major (isa_color_twists) */
+    float twist2[12];                     /* ProPhoto -> sRGB (D50), 3 x 4 row-major */
+    const float* lut_x;                   /* host: LUT levels, strictly increasing (the controller's LUTx, 256 entries i/255) */
+    const float* lut_y;                   /* host: LUT values at the levels (defaultLUT) */
+    int nlut;                             /* 4 .. ISA_MAX_LUT */
+    float exposure;                       /* Exposure (:793, default 0): the image is scaled by 2^exposure before the gamma */
+} isa_post_params;
+
+enum { ISA_POST_RGB16 = 0,  /* SaveAs16BitTiff: uint16 R, G, B per pixel */
+       ISA_POST_BGRA8 = 1   /* ProcessColorsAndShow: uint8 B, G, R, 255 per pixel (the WPF Bgra32 bitmap) */ };
+
+/* The two 3 x 4 colour twists of SaveAs16BitTiff (:2226-2240) from the
+ * colour spec's CameraToPCS (row-major 3 x 3, camera -> XYZ D50), in FP64 as
+ * DNGColorSpace (DNGColorSpace.cs:36-65: ProPhoto and sRGB50 matrices scaled
+ * so that RGB white maps to the D50 PCS white, inverted with
+ * DNGMatrix.Invert3x3, DNGMatrix.cs:440-486), then cast to float with a zero
+ * offset column (DNGMatrix.GetAs3x4Array, DNGMatrix.cs:181-193). Host only. */
+ISA_API int isa_color_twists(const double camera_to_pcs[9], float twist1[12], float twist2[12]);
+/* The post-processing chain on a float3 image (device, width x height,
+ * pitch bytes) into `out` (device, crop_w x crop_h, format ISA_POST_*,
+ * out_pitch bytes). One fused pass; the LUT is interpolated with the cubic
+ * through the four nearest levels (NPP's LUTCubic does not publish its
+ * polynomial), as per-segment coefficients computed on the host in FP64 and
+ * evaluated in FP32 by Horner's rule. */
+ISA_API int isa_postprocess(const float* img, size_t pitch, int width, int height, const isa_post_params* pp, int format, void* out,
+                            size_t out_pitch, void* stream);
+/* ImageFileDirectory(width, height).SaveAsTiff (PefFile/ImageFileDirectory.cs:75-123):
+ * little-endian baseline TIFF, 13 tags, one strip of uint16 RGB (host,
+ * width x height x 3, row-major). Host only. */
+ISA_API int isa_save_tiff16(const char* path, const uint16_t* rgb, int width, int height);
+/* SaveAs16BitTiff from a device float3 image: isa_postprocess (ISA_POST_RGB16)
+ * on `stream`, copy to the host, isa_save_tiff16. Synchronises `stream`. */
+ISA_API int isa_save_as_16bit_tiff(const float* img, size_t pitch, int width, int height, const isa_post_params* pp, const char* path,
+                                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -148,6 +148,27 @@ EXPORT void orc_gamma_srgb(real* rgb, int W, int H)
     }
 }
 
+/* GammasRGB (kernel.cu:290-332) in float exactly as the reference's float
+ * code: float literals, powf, each operation rounded on its own (no
+ * contraction on this target). Used by the FP32 post-processing restatement
+ * (oracle/post.py). n values in place. */
+EXPORT void orc_gamma_srgb_f32(float* v, size_t n)
+{
+    for (size_t i = 0; i < n; i++) {
+        float x = v[i];
+        if (isnan(x)) x = 0.0f;
+        x = fmaxf(fminf(x, 1.0f), 0.0f);
+        if (x <= 0.0031308f) {
+            x = 12.92f * x;
+        } else {
+            const float p = powf(x, 1.0f / 2.4f);
+            const float g = (1.0f + 0.055f) * p;
+            x = g - 0.055f;
+        }
+        v[i] = x;
+    }
+}
+
 /* A2: NPP ColorToGray (controller :2404-2408): gray = sum_c w_c * rgb_c. */
 EXPORT void orc_color_to_gray(const real* rgb, int W, int H, const real* w, real* gray)
 {
