@@ -21,6 +21,7 @@ the same statistics; under torchrun only rank 0 runs it.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -315,6 +316,45 @@ def post_throughput(args, merged):
             "l2": f"input {Wo * Ho * 12 / 1e9:.2f} GB {'larger' if Wo * Ho * 12 > 126e6 else 'smaller'} than the 126 MB L2"}
 
 
+def raw_decode_throughput(args, frame):
+    """PEF raw decoding (isa_pef_decode) of one frame of the workload,
+    compressed in the reference's stream layout: device time per frame
+    (one launch sequence, no host round trips), with
+    the restated reference decoder on one host core as its CPU baseline."""
+    import torch
+    from imagestackalignator_b200 import isa, synthetic
+    H, W = frame.shape
+    code, lens = synthetic.pef_code_book()
+    stream = synthetic.pef_stream(frame, code, lens)
+    table = isa.pef_huff_table(synthetic.pef_maker_note(code, lens))
+    d = torch.from_numpy(stream).cuda()
+    out = torch.empty((H, W), dtype=torch.int16, device="cuda")
+    scratch = torch.empty(isa.lib().isa_pef_decode_scratch(ctypes.c_size_t(stream.size), W, H), dtype=torch.uint8, device="cuda")
+    stream_t = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup)):
+        isa.pef_decode(d, table, W, H, out, scratch)
+    torch.cuda.synchronize()
+    exact = bool(np.array_equal(out.cpu().numpy().view(np.uint16), frame))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream_t)
+    for _ in range(args.steps):
+        isa.pef_decode(d, table, W, H, out, scratch)
+    e1.record(stream_t)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    res = {"workload": f"one {W}x{H} 14-bit frame of the burst, {stream.size / 1e6:.1f} MB compressed ({stream.size * 8 / frame.size:.2f} bits/px)",
+           "ms": ms, "mp_s": W * H / 1e6 / (ms / 1e3), "compressed_gb_s": stream.size / 1e9 / (ms / 1e3),
+           "exact": exact, "cpu_baseline": None}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import raw as R  # the restated reference decoder (PEFFile.cs:35-111), one host core
+        t0 = time.perf_counter()
+        R.decode(stream, table, W, H)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"mp_s": W * H / 1e6 / dt, "cores": 1, "kind": "port", "sample": f"the same {W}x{H} stream, {dt:.2f} s"}
+    return res
+
+
 def run_ours(args):
     import torch
     from imagestackalignator_b200 import isa
@@ -416,6 +456,9 @@ def run_ours(args):
     post = None
     if rank == 0 and world == 1 and not args.no_post:
         post = post_throughput(args, out)
+    rawdec = None
+    if rank == 0 and world == 1 and not args.no_raw:
+        rawdec = raw_decode_throughput(args, np.ascontiguousarray(burst.raw[1]))
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = batch_throughput(args)
@@ -430,7 +473,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint, "batch": batch, "postprocess": post,
+        "fwd_adjoint": adjoint, "batch": batch, "postprocess": post, "raw_decode": rawdec,
         "clocks": clocks,
     }
     if rank == 0:
@@ -454,6 +497,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
     ap.add_argument("--no-post", action="store_true", help="skip the colour/tone post-processing timing")
+    ap.add_argument("--no-raw", action="store_true", help="skip the PEF raw-decoding timing")
     ap.add_argument("--size", default=None, help="WxH override for profiling runs on a smaller burst (not a bench line)")
     ap.add_argument("--frames", type=int, default=None, help="frame-count override for profiling runs (not a bench line)")
     args = ap.parse_args()

@@ -1673,3 +1673,99 @@ int isa_save_as_16bit_tiff(const float* img, size_t pitch, int width, int height
     if (rc != ISA_OK) return rc;
     return isa_save_tiff16(path, h.data(), pp->crop_w, pp->crop_h);
 }
+
+// ---- PEF raw decoding ----
+
+int isa_pef_huff_table(const uint8_t* mn, size_t n, int big_endian, uint16_t table[4097])
+{
+    ISA_REQ(mn && table, "NULL argument");
+    std::memset(table, 0, 4097 * sizeof(uint16_t));
+    const auto rd16 = [&](size_t i) -> unsigned {
+        return big_endian ? (unsigned)(mn[i] << 8 | mn[i + 1]) : (unsigned)(mn[i + 1] << 8 | mn[i]);
+    };
+    ISA_REQ(n >= 2, "maker note too short");
+    const int dep = (int)((rd16(0) + 12) & 15);
+    if (n < (size_t)(14 + 3 * dep)) return fail(ISA_EINVAL, "maker note too short for %d codes", dep);
+    for (int c = 0; c < dep; c++) {
+        const unsigned code = rd16(14 + 2 * (size_t)c), len = mn[14 + 2 * (size_t)dep + c];
+        // the fill loop of MNHuffmanTable: entries code + 1 .. through the 4096 >> len peeks that start with the code (mod 4096)
+        for (unsigned i = code; i <= ((code + (4096u >> (len & 31)) - 1) & 4095u);) {
+            ++i;
+            if (i > 4096) break;
+            table[i] = (uint16_t)(len << 8 | (unsigned)c);
+        }
+        table[0] = 12;
+    }
+    return dep;
+}
+
+size_t isa_pef_decode_scratch(size_t nbytes, int width, int height)
+{
+    if (width <= 0 || height <= 0) return 0;
+    size_t parts[14];
+    return isa_pef_scratch_layout(nbytes, width, height, parts);
+}
+
+int isa_pef_decode(const uint8_t* data, size_t nbytes, const uint16_t* table, int width, int height, void* scratch, size_t scratch_bytes,
+                   uint16_t* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(data && table && scratch && out && width > 0 && height > 0 && nbytes > 0, "bad argument");
+    ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
+    ISA_REQ(scratch_bytes >= isa_pef_decode_scratch(nbytes, width, height), "scratch too small (isa_pef_decode_scratch)");
+    if ((nbytes * 8 / 1024 + 2 + 255) / 256 > (size_t)isa_pef_max_blocks()) return fail(ISA_EINVAL, "stream of %zu bytes too long", nbytes);
+    ISA_REQ(table[0] == 12, "decode table must peek 12 bits (table[0] == 12)");
+    for (int i = 1; i < 4097; i++) {
+        const unsigned len = table[i] >> 8, cat = table[i] & 255;
+        if (table[i] != 0 && (len < 1 || len > 12 || cat > 15)) return fail(ISA_EINVAL, "unsupported table entry %d (length %u, category %u)", i, len, cat);
+    }
+    ISA_CK(isa_launch_pef_decode(data, nbytes, table, width, height, scratch, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_pef_unpack(const uint8_t* file, size_t file_size, const uint32_t* offsets, const uint32_t* sizes, int nstrips, int rows_per_strip, int width,
+                   int height, int bit_depth, uint16_t* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(file && offsets && sizes && out && width > 0 && height > 0 && rows_per_strip > 0, "bad argument");
+    ISA_REQ(nstrips >= 1 && nstrips <= 512, "1 to 512 strips");
+    ISA_REQ(bit_depth >= 1 && bit_depth <= 16, "bit depth 1 to 16");
+    ISA_REQ((long long)nstrips * rows_per_strip >= height, "the strips do not cover the frame");
+    ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
+    ISA_CK(isa_launch_pef_unpack(file, file_size, offsets, sizes, nstrips, rows_per_strip, width, height, bit_depth, out, out_pitch, S(stream)));
+    return ISA_OK;
+}
+
+int isa_pef_levels(const int cfa[4], const float* black_point, int n_black, float white_level, const float white_point[4], float scaling,
+                   int bit_depth, float black[3], float white[3], float white_balance[3])
+{
+    ISA_REQ(cfa && white_point && black && white && white_balance, "NULL argument");
+    ISA_REQ(cfa_ok(cfa), "CFA codes must be 0, 1, 2");
+    ISA_REQ(n_black == 0 || (black_point && (n_black == 1 || n_black == 3 || n_black == 4)), "1, 3 or 4 black point values");
+    const float white_all = white_level > 0 ? white_level : (float)std::pow(2.0, (double)bit_depth);
+    float b[3] = {0.f, 0.f, 0.f};
+    if (n_black == 1) {
+        b[0] = b[1] = b[2] = black_point[0];
+    } else if (n_black == 3) {
+        b[0] = black_point[0]; b[1] = black_point[1]; b[2] = black_point[2];
+    } else if (n_black == 4) {
+        int ir = -1, ib = -1, ig1 = -1, ig2 = -1;
+        for (int i = 0; i < 4; i++) {
+            if (cfa[i] == 0 && ir < 0) ir = i;
+            if (cfa[i] == 2 && ib < 0) ib = i;
+            // the reference's loop: the first green, then the last green (:240-251)
+            if (cfa[i] == 1 && ig1 < 0) ig1 = i;
+            if (cfa[i] == 1 && ig1 >= 0) ig2 = i;
+        }
+        ISA_REQ(ir >= 0 && ib >= 0 && ig1 >= 0, "CFA without red, green and blue");
+        b[0] = black_point[ir];
+        b[2] = black_point[ib];
+        b[1] = std::max(black_point[ig1], black_point[ig2]);
+    }
+    for (int c = 0; c < 3; c++) {
+        black[c] = b[c];
+        white[c] = white_all - b[c];
+    }
+    white_balance[0] = white_point[0] / scaling;
+    white_balance[1] = white_point[1] / scaling;
+    white_balance[2] = white_point[3] / scaling;
+    return ISA_OK;
+}

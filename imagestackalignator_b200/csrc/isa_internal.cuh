@@ -181,3 +181,11 @@ struct isa_post_args {
 };
 cudaError_t isa_launch_postprocess(const float* img, size_t pitch, const isa_post_args& a, int format, void* out, size_t out_pitch,
                                    cudaStream_t st);
+
+// raw.cu: PEF decoding (isa_pef_decode, isa_pef_unpack)
+size_t isa_pef_scratch_layout(unsigned long long nbytes, int W, int H, size_t* parts);
+cudaError_t isa_launch_pef_decode(const uint8_t* data, unsigned long long nbytes, const unsigned short* table, int W, int H, void* scratch,
+                                  uint16_t* out, size_t out_pitch, cudaStream_t st);
+int isa_pef_max_blocks();
+cudaError_t isa_launch_pef_unpack(const uint8_t* file, unsigned long long fsize, const uint32_t* offsets, const uint32_t* sizes, int nstrips,
+                                  int rows_per_strip, int W, int H, int depth, uint16_t* out, size_t out_pitch, cudaStream_t st);

@@ -1,0 +1,535 @@
+// Raw decoding of Pentax PEF frames on the GPU (PEFFile, PefFile/PEFFile.cs:81-156).
+//
+// Compressed frames are one bitstream of lossless-JPEG style symbols (a
+// Huffman-coded difference category, then that many difference bits) in
+// raster order, each difference relative to the pixel two columns left, or
+// for the first two columns two rows up. The reference decodes it with one
+// sequential bit reader. Here the stream is first copied into zero-padded
+// big-endian 32-bit words (every symbol is then read with two aligned loads
+// and a funnel shift), and cut into chunks of PEF_CHUNK bits. The first
+// symbol boundary at or past a chunk's start lies within PEF_K bits of it
+// (a symbol is at most 12 + 15 bits), so:
+//   1. every chunk is decoded from each of its PEF_K candidate starts (a
+//      warp per chunk, a lane per candidate, positions only) to the first
+//      boundary at or past its end: per candidate the next chunk's
+//      candidate and the symbol count, or "stopped" at an empty table
+//      entry -- a map over PEF_K states. This stream format barely
+//      resynchronises (most of each symbol is raw difference bits), so the
+//      candidates are decoded, not guessed;
+//   2. the maps are chained from chunk 0's state 0 in three levels (32
+//      chunks per warp, 32 warps per block, blocks in order), then walked
+//      back down: every chunk's true start, count and local offset;
+//   3. a scan of the block totals gives each chunk's first pixel, and every
+//      chunk decodes again from its true start, writing its differences;
+//   4. column prefix sums (first two columns, per row parity) and row prefix
+//      sums (per column parity) undo the prediction, in 32-bit wrap-around
+//      arithmetic, stored as the low 16 bits.
+// Reads past the end of the data see zero bytes, as the reference's bit
+// reader does at the end of its file region; an empty table entry consumes
+// nothing, after which every remaining pixel repeats the last value (the
+// reference's reader then returns zero differences).
+//
+// Uncompressed frames (`isa_pef_unpack`): W values of `depth` bits per row,
+// MSB first, strips of rows_per_strip rows whose bit buffer carries over from
+// one strip to the next; one thread per value.
+#include "isa_internal.cuh"
+
+namespace {
+
+constexpr int PEF_NT = 256;
+constexpr unsigned long long PEF_CHUNK = 1024;  // bits per chunk
+constexpr int PEF_MAX_STRIPS = 512;
+constexpr int PEF_K = 27;          // candidate starts per chunk: a symbol is at most 12 + 15 bits
+constexpr int PEF_CB = 1024;       // chunks per block of the map composition (32 warps x 32 chunks)
+constexpr unsigned PEF_STOP = 255; // state after an empty table entry
+
+struct PefTable {
+    unsigned short t[4097];
+};
+
+// Zero-padded big-endian words of the stream: word i = bytes 4i .. 4i + 3.
+__global__ void k_pef_words(const uint8_t* __restrict__ data, unsigned long long nbytes, unsigned long long nwords, unsigned* __restrict__ words)
+{
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < nwords; i += (unsigned long long)gridDim.x * blockDim.x) {
+        unsigned w = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const unsigned long long b = 4 * i + k;
+            w = (w << 8) | (b < nbytes ? (unsigned)__ldg(data + b) : 0u);
+        }
+        words[i] = w;
+    }
+}
+
+// The 32 bits starting at bit p, MSB first (zero past the padded copy).
+__device__ __forceinline__ unsigned bits32(const unsigned* __restrict__ words, unsigned long long nwords, unsigned long long p)
+{
+    const unsigned long long w = p >> 5;
+    const unsigned hi = w < nwords ? __ldg(words + w) : 0u, lo = w + 1 < nwords ? __ldg(words + w + 1) : 0u;
+    return __funnelshift_l(lo, hi, (unsigned)(p & 31));
+}
+
+// One symbol at bit p: the table entry's code length and category (0 length: empty entry).
+__device__ __forceinline__ int pef_decode_at(unsigned x, const unsigned short* tab, int& adv)
+{
+    const unsigned t = tab[1 + (x >> 20)];
+    const int clen = (int)(t >> 8), ssss = (int)(t & 255);
+    adv = clen == 0 ? 0 : clen + ssss;
+    if (ssss == 0) return 0;
+    int v = (int)((x << clen) >> (32 - ssss));
+    if ((v & (1 << (ssss - 1))) == 0) v -= (1 << ssss) - 1;
+    return v;
+}
+
+// The decode table and the advance table (code length + category, 0 for an
+// empty entry) into device memory once, so that every CTA copies them from
+// global memory (coalesced) rather than from kernel parameters read with a
+// different address per thread.
+__global__ void k_pef_tables(const __grid_constant__ PefTable T, unsigned short* __restrict__ tab, uint8_t* __restrict__ adv)
+{
+    for (int i = threadIdx.x; i < 4097; i += blockDim.x) {
+        const unsigned t = T.t[i];
+        tab[i] = (unsigned short)t;
+        if (i > 0) adv[i - 1] = (t >> 8) == 0 ? 0 : (uint8_t)((t >> 8) + (t & 255));
+    }
+}
+
+__device__ __forceinline__ void load_table(unsigned short* s, const unsigned short* __restrict__ g)
+{
+    for (int i = threadIdx.x; i < 4097; i += blockDim.x) s[i] = g[i];
+    __syncthreads();
+}
+
+// Step 1: a warp per chunk (grid-stride): the chunk's 33 words staged in
+// shared memory, lane k < PEF_K follows candidate start k (advance table only).
+constexpr int PEF_CW = 34;  // words a chunk's decode reads: 32, the next one, and one spare
+
+__global__ void __launch_bounds__(PEF_NT) k_pef_map(const unsigned* __restrict__ words, const uint8_t* __restrict__ gadv, int nchunks,
+                                                    uint8_t* __restrict__ nextk, uint16_t* __restrict__ cntk)
+{
+    __shared__ __align__(16) uint8_t adv[4096];
+    __shared__ unsigned cw[PEF_NT / 32][PEF_CW];
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) ((unsigned*)adv)[i] = ((const unsigned*)gadv)[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, k = threadIdx.x & 31;
+    for (int i = blockIdx.x * (PEF_NT / 32) + warp; i < nchunks; i += gridDim.x * (PEF_NT / 32)) {
+        for (int t = k; t < PEF_CW; t += 32) cw[warp][t] = __ldg(words + (size_t)i * 32 + t);
+        __syncwarp();
+        if (k < PEF_K) {
+            unsigned p = (unsigned)k, c = 0;
+            bool stop = false;
+            while (p < PEF_CHUNK) {
+                const unsigned w = p >> 5;
+                const unsigned a = adv[__funnelshift_l(cw[warp][w + 1], cw[warp][w], p & 31) >> 20];
+                if (a == 0) { stop = true; break; }
+                p += a;
+                c++;
+            }
+            nextk[(size_t)i * 32 + k] = stop ? PEF_STOP : (uint8_t)(p - PEF_CHUNK);
+            cntk[(size_t)i * 32 + k] = (uint16_t)c;
+        }
+        __syncwarp();
+    }
+}
+
+// Step 2a: per block of PEF_CB = 32 x 32 chunks, the 32-chunk map of each
+// warp (lane j follows state j) and the block's map.
+__global__ void __launch_bounds__(1024) k_pef_compose(const uint8_t* __restrict__ nextk, int nchunks, uint8_t* __restrict__ sub_map,
+                                                      uint8_t* __restrict__ block_map)
+{
+    __shared__ uint8_t m[PEF_CB][32];
+    __shared__ uint8_t sm[32][32];
+    const int c0 = blockIdx.x * PEF_CB, n = min(PEF_CB, nchunks - c0);
+    for (int t = threadIdx.x; t < n * 32; t += blockDim.x) m[t >> 5][t & 31] = nextk[(size_t)c0 * 32 + t];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, j = threadIdx.x & 31;
+    unsigned s = j < PEF_K ? (unsigned)j : PEF_STOP;
+    for (int q = warp * 32; q < min(n, warp * 32 + 32) && s != PEF_STOP; q++) s = m[q][s];
+    sm[warp][j] = (uint8_t)s;
+    sub_map[((size_t)blockIdx.x * 32 + warp) * 32 + j] = (uint8_t)s;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned b = j < PEF_K ? (unsigned)j : PEF_STOP;
+        for (int w = 0; w < 32 && b != PEF_STOP; w++) b = sm[w][b];
+        block_map[(size_t)blockIdx.x * 32 + j] = (uint8_t)b;
+    }
+}
+
+// Step 2b: one thread walks the block maps from state 0: every block's entry state and the state after the last chunk.
+__global__ void k_pef_chain(const uint8_t* __restrict__ block_map, int nblocks, uint8_t* __restrict__ block_in, unsigned* __restrict__ final_state)
+{
+    extern __shared__ uint8_t bm[];
+    for (int t = threadIdx.x; t < nblocks * 32; t += blockDim.x) bm[t] = block_map[t];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    unsigned s = 0;
+    for (int b = 0; b < nblocks; b++) {
+        block_in[b] = (uint8_t)s;
+        if (s != PEF_STOP) s = bm[b * 32 + s];
+    }
+    *final_state = s;
+}
+
+// Step 2c: down the levels. Warp entry states from the block's entry state,
+// then lane 0 of each warp walks its 32 chunks (true start, count); the
+// counts are scanned within the block (local offsets and the block total).
+// After a stop every later chunk has count 0, so totals need no stop flag.
+__global__ void __launch_bounds__(1024) k_pef_walk(const uint8_t* __restrict__ nextk, const uint16_t* __restrict__ cntk, const uint8_t* __restrict__ sub_map,
+                                                   const uint8_t* __restrict__ block_in, int nchunks, unsigned long long* __restrict__ start,
+                                                   unsigned* __restrict__ loc, unsigned* __restrict__ block_total)
+{
+    __shared__ uint8_t wentry[32];
+    __shared__ unsigned wtot[32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c0 = blockIdx.x * PEF_CB, n = min(PEF_CB, nchunks - c0);
+    if (threadIdx.x == 0) {
+        unsigned s = block_in[blockIdx.x];
+        for (int w = 0; w < 32; w++) {
+            wentry[w] = (uint8_t)s;
+            if (s != PEF_STOP) s = sub_map[((size_t)blockIdx.x * 32 + w) * 32 + s];
+        }
+    }
+    __syncthreads();
+    if (lane == 0) {
+        unsigned s = wentry[warp];
+        for (int q = 0; q < 32; q++) {
+            const int ci = warp * 32 + q;
+            if (ci >= n) break;
+            const int i = c0 + ci;
+            if (s == PEF_STOP) {
+                start[i] = (unsigned long long)i * PEF_CHUNK;
+                loc[i] = 0;
+                continue;
+            }
+            start[i] = (unsigned long long)i * PEF_CHUNK + s;
+            loc[i] = cntk[(size_t)i * 32 + s];
+            s = nextk[(size_t)i * 32 + s];
+        }
+    }
+    __syncwarp();
+    const int ci = warp * 32 + lane;
+    const unsigned my = ci < n ? loc[c0 + ci] : 0u;
+    unsigned x = my;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wtot[warp] = x;
+    __syncthreads();
+    unsigned wpre = 0;
+    for (int w = 0; w < warp; w++) wpre += wtot[w];
+    if (ci < n) loc[c0 + ci] = wpre + x - my;
+    if (threadIdx.x == 0) {
+        unsigned tot = 0;
+        for (int w = 0; w < 32; w++) tot += wtot[w];
+        block_total[blockIdx.x] = tot;
+    }
+}
+
+// Step 3a: exclusive scan of the block totals (one CTA); boff[nblocks] = all symbols.
+__global__ void __launch_bounds__(1024) k_pef_scan(const unsigned* __restrict__ block_total, int nblocks, unsigned long long* __restrict__ boff)
+{
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < nblocks; base += 1024) {
+        const int i = base + threadIdx.x;
+        const unsigned long long v = i < nblocks ? block_total[i] : 0ull;
+        unsigned long long x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        if (i < nblocks) boff[i] = carry + (warp ? wsum[warp - 1] : 0ull) + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += wsum[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) boff[nblocks] = carry;
+}
+
+// Step 3b: the differences of every chunk at its pixel offset (one thread
+// per chunk; the CTA's 256 consecutive chunks staged in shared memory with
+// one skew word per 32, so that the lanes' chunks fall in different banks).
+__global__ void __launch_bounds__(PEF_NT) k_pef_emit(const unsigned* __restrict__ words, unsigned long long nwords, const unsigned short* __restrict__ gtab,
+                                                     int nchunks, int nblocks, const unsigned long long* __restrict__ start,
+                                                     const unsigned* __restrict__ loc, const unsigned long long* __restrict__ boff,
+                                                     unsigned long long npix, int16_t* __restrict__ diff)
+{
+    __shared__ unsigned short tab[4097];
+    __shared__ unsigned cw[PEF_NT * 33 + 2];
+    const int c0 = blockIdx.x * PEF_NT;
+    for (int j = threadIdx.x; j < PEF_NT * 32 + 2; j += PEF_NT) {
+        const unsigned long long g = (unsigned long long)c0 * 32 + j;
+        cw[j + (j >> 5)] = g < nwords ? __ldg(words + g) : 0u;
+    }
+    load_table(tab, gtab);
+    const int t = threadIdx.x, i = c0 + t;
+    if (i >= nchunks) return;
+    const unsigned long long total = boff[nblocks], limit = total < npix ? total : npix;
+    unsigned long long o = boff[i / PEF_CB] + loc[i];
+    if (o >= limit) return;
+    unsigned p = (unsigned)(start[i] - (unsigned long long)i * PEF_CHUNK);
+    const unsigned* cb = cw + 33 * t;
+    while (p < PEF_CHUNK && o < limit) {
+        const unsigned w = p >> 5;
+        const unsigned x = __funnelshift_l(cb[w + 1 + ((w + 1) >> 5)], cb[w], p & 31);
+        int a;
+        const int d = pef_decode_at(x, tab, a);
+        if (a == 0) break;
+        p += a;
+        diff[o++] = (int16_t)d;
+    }
+}
+
+// After the last chunk: pixels the chunks did not reach (a stream that ends
+// early reads zero bytes; after a stop the differences are zero). One thread.
+__global__ void k_pef_tail(const unsigned* __restrict__ words, unsigned long long nwords, const unsigned short* __restrict__ gtab, int nchunks, int nblocks,
+                           const unsigned* __restrict__ final_state, const unsigned long long* __restrict__ boff, unsigned long long npix,
+                           int16_t* __restrict__ diff)
+{
+    unsigned long long o = boff[nblocks];
+    if (o >= npix) return;
+    const unsigned s = *final_state;
+    if (s != PEF_STOP) {
+        unsigned long long p = (unsigned long long)nchunks * PEF_CHUNK + s;
+        while (o < npix) {
+            int a;
+            const int d = pef_decode_at(bits32(words, nwords, p), gtab, a);
+            if (a == 0) break;
+            p += a;
+            diff[o++] = (int16_t)d;
+        }
+    }
+    for (; o < npix; o++) diff[o] = 0;
+}
+
+// Prediction of the first two columns: running sums down the rows of one
+// parity (vpred[row & 1][col]), one warp per (row parity, column).
+__global__ void k_pef_cols(const int16_t* __restrict__ diff, int W, int H, int* __restrict__ colsum)
+{
+    const int lane = threadIdx.x & 31, seq = threadIdx.x >> 5;  // 4 warps: (parity, column)
+    const int par = seq >> 1, col = seq & 1;
+    if (col >= W) return;
+    unsigned carry = 0;
+    for (int base = par; base < H; base += 64) {
+        const int row = base + 2 * lane;
+        unsigned x = row < H ? (unsigned)diff[(size_t)row * W + col] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (row < H) colsum[(size_t)row * 2 + col] = (int)(carry + x);
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+}
+
+// Row prediction: value(row, col) = colsum(row, col & 1) + sum of the row's
+// differences at columns 2 .. col of the same parity. One CTA per row.
+__global__ void __launch_bounds__(PEF_NT) k_pef_rows(const int16_t* __restrict__ diff, const int* __restrict__ colsum, int W, int H,
+                                                     uint16_t* __restrict__ out, size_t out_pitch)
+{
+    __shared__ unsigned ws[2][PEF_NT / 32];
+    __shared__ unsigned carry[2];
+    const int row = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int16_t* drow = diff + (size_t)row * W;
+    uint16_t* orow = isa::row_ptr(out, out_pitch, row);
+    if (threadIdx.x < 2) carry[threadIdx.x] = threadIdx.x < W ? (unsigned)colsum[(size_t)row * 2 + threadIdx.x] : 0u;
+    __syncthreads();
+    // columns in pairs: thread t of a pass owns columns 2 (base + t) and 2 (base + t) + 1
+    for (int base = 1; 2 * base < W; base += PEF_NT) {
+        const int c0 = 2 * (base + threadIdx.x);
+        unsigned e = c0 < W ? (unsigned)drow[c0] : 0u, od = c0 + 1 < W ? (unsigned)drow[c0 + 1] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned ye = __shfl_up_sync(0xffffffffu, e, o), yo = __shfl_up_sync(0xffffffffu, od, o);
+            if (lane >= o) { e += ye; od += yo; }
+        }
+        if (lane == 31) { ws[0][warp] = e; ws[1][warp] = od; }
+        __syncthreads();
+        unsigned pe = carry[0], po = carry[1];
+        for (int w = 0; w < warp; w++) { pe += ws[0][w]; po += ws[1][w]; }
+        if (c0 < W) orow[c0] = (uint16_t)(pe + e);
+        if (c0 + 1 < W) orow[c0 + 1] = (uint16_t)(po + od);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned te = 0, to = 0;
+            for (int w = 0; w < PEF_NT / 32; w++) { te += ws[0][w]; to += ws[1][w]; }
+            carry[0] += te;
+            carry[1] += to;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 2 && threadIdx.x < W) orow[threadIdx.x] = (uint16_t)colsum[(size_t)row * 2 + threadIdx.x];
+}
+
+// Uncompressed strips: value v of strip s (v = line * W + px) is bits
+// [v * depth, + depth) of the strip's virtual stream: the carry_bits bits
+// the previous strip left in the reader's buffer, then the strip's bytes.
+struct UnpackStrip {
+    unsigned long long off, size;   // the strip's bytes in the file
+    unsigned long long carry_src;   // file byte whose low carry_bits bits precede the strip's bytes (~0: zero bits)
+    unsigned carry_bits;
+};
+
+struct UnpackArgs {
+    int nstrips;
+    UnpackStrip s[PEF_MAX_STRIPS];
+};
+
+__device__ __forceinline__ unsigned file_byte(const uint8_t* __restrict__ file, unsigned long long fsize, unsigned long long i)
+{
+    return i < fsize ? (unsigned)__ldg(file + i) : 0u;
+}
+
+__device__ __forceinline__ unsigned strip_bits(const uint8_t* __restrict__ file, unsigned long long fsize, const UnpackStrip& s,
+                                               unsigned long long b, int depth)
+{
+    unsigned long long v = 0;
+    int got = 0;
+    while (got < depth) {
+        const unsigned long long p = b + got;
+        if (p < s.carry_bits) {
+            const unsigned cv = s.carry_src == ~0ull ? 0u : file_byte(file, fsize, s.carry_src);
+            const int take = (int)min((unsigned long long)(depth - got), s.carry_bits - p);
+            const int lo = (int)(s.carry_bits - p) - take;  // bit index (from 0 = LSB) of the last bit taken
+            v = (v << take) | ((cv >> lo) & ((1u << take) - 1));
+            got += take;
+            continue;
+        }
+        const unsigned long long q = p - s.carry_bits, byte = q >> 3;
+        const int sh = (int)(q & 7), take = min(8 - sh, depth - got);
+        const unsigned x = byte < s.size ? file_byte(file, fsize, s.off + byte) : 0u;
+        v = (v << take) | ((x >> (8 - sh - take)) & ((1u << take) - 1));
+        got += take;
+    }
+    return (unsigned)v;
+}
+
+__global__ void k_pef_unpack(const uint8_t* __restrict__ file, unsigned long long fsize, const __grid_constant__ UnpackArgs A, int rows_per_strip,
+                             int W, int H, int depth, uint16_t* __restrict__ out, size_t out_pitch)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W || y >= H) return;
+    const int s = y / rows_per_strip, line = y - s * rows_per_strip;
+    const unsigned long long b = ((unsigned long long)line * W + x) * depth;
+    isa::row_ptr(out, out_pitch, y)[x] = (uint16_t)strip_bits(file, fsize, A.s[s], b, depth);
+}
+
+}  // namespace
+
+size_t isa_pef_scratch_layout(unsigned long long nbytes, int W, int H, size_t* parts)
+{
+    const unsigned long long nchunks = (nbytes * 8 + PEF_CHUNK - 1) / PEF_CHUNK + 1;
+    const unsigned long long nblocks = (nchunks + PEF_CB - 1) / PEF_CB;
+    const unsigned long long nwords = nchunks * 32 + 64;  // every chunk's staged words lie inside
+    size_t o = 0;
+    const auto take = [&](int k, size_t bytes) { parts[k] = o; o += (bytes + 255) / 256 * 256; };
+    take(0, nwords * 4);           // big-endian words of the stream
+    take(1, nchunks * 8);          // true start of each chunk
+    take(2, nchunks * 32);         // next state per (chunk, candidate)
+    take(3, nchunks * 64);         // count per (chunk, candidate)
+    take(4, nchunks * 4);          // local offsets
+    take(5, nblocks * 32 * 32);    // warp (32-chunk) maps
+    take(6, nblocks * 32);         // block maps
+    take(7, nblocks + 32);         // block entry states, then the final state at the next 16-byte boundary
+    take(8, nblocks * 4);          // block totals
+    take(9, (nblocks + 1) * 8);    // block offsets, total
+    take(10, (size_t)W * H * 2);   // differences (|d| < 2^15)
+    take(11, (size_t)H * 2 * 4);   // column sums
+    take(12, 4097 * 2);            // decode table
+    take(13, 4096);                // advance table
+    return o;
+}
+
+int isa_pef_max_blocks() { return (227 * 1024) / 32; }
+
+cudaError_t isa_launch_pef_decode(const uint8_t* data, unsigned long long nbytes, const unsigned short* table, int W, int H, void* scratch,
+                                  uint16_t* out, size_t out_pitch, cudaStream_t st)
+{
+    size_t part[14];
+    isa_pef_scratch_layout(nbytes, W, H, part);
+    char* base = (char*)scratch;
+    const int nchunks = (int)((nbytes * 8 + PEF_CHUNK - 1) / PEF_CHUNK) + 1;  // one spare chunk past the data
+    const int nblocks = (nchunks + PEF_CB - 1) / PEF_CB;
+    const unsigned long long nwords = (unsigned long long)nchunks * 32 + 64;
+    if (nblocks > isa_pef_max_blocks()) return cudaErrorInvalidValue;
+    unsigned* words = (unsigned*)(base + part[0]);
+    unsigned long long* start = (unsigned long long*)(base + part[1]);
+    uint8_t* nextk = (uint8_t*)(base + part[2]);
+    uint16_t* cntk = (uint16_t*)(base + part[3]);
+    unsigned* loc = (unsigned*)(base + part[4]);
+    uint8_t* sub_map = (uint8_t*)(base + part[5]);
+    uint8_t* block_map = (uint8_t*)(base + part[6]);
+    uint8_t* block_in = (uint8_t*)(base + part[7]);
+    unsigned* final_state = (unsigned*)(base + part[7] + (nblocks + 15) / 16 * 16);
+    unsigned* block_total = (unsigned*)(base + part[8]);
+    unsigned long long* boff = (unsigned long long*)(base + part[9]);
+    int16_t* diff = (int16_t*)(base + part[10]);
+    int* colsum = (int*)(base + part[11]);
+    unsigned short* gtab = (unsigned short*)(base + part[12]);
+    uint8_t* gadv = (uint8_t*)(base + part[13]);
+    PefTable T;
+    for (int i = 0; i < 4097; i++) T.t[i] = table[i];
+    k_pef_tables<<<1, 1024, 0, st>>>(T, gtab, gadv);
+    k_pef_words<<<(unsigned)std::min<unsigned long long>((nwords + 255) / 256, 148 * 16), 256, 0, st>>>(data, nbytes, nwords, words);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned mapg = (unsigned)std::min<long long>((nchunks + PEF_NT / 32 - 1) / (PEF_NT / 32), (long long)sms * 8);
+    k_pef_map<<<mapg, PEF_NT, 0, st>>>(words, gadv, nchunks, nextk, cntk);
+    k_pef_compose<<<nblocks, 1024, 0, st>>>(nextk, nchunks, sub_map, block_map);
+    const size_t chain_smem = (size_t)nblocks * 32;
+    cudaError_t e = cudaFuncSetAttribute(k_pef_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(chain_smem, 1));
+    if (e != cudaSuccess) return e;
+    k_pef_chain<<<1, 256, chain_smem, st>>>(block_map, nblocks, block_in, final_state);
+    k_pef_walk<<<nblocks, 1024, 0, st>>>(nextk, cntk, sub_map, block_in, nchunks, start, loc, block_total);
+    k_pef_scan<<<1, 1024, 0, st>>>(block_total, nblocks, boff);
+    const unsigned long long npix = (unsigned long long)W * H;
+    k_pef_emit<<<(unsigned)((nchunks + PEF_NT - 1) / PEF_NT), PEF_NT, 0, st>>>(words, nwords, gtab, nchunks, nblocks, start, loc, boff, npix, diff);
+    k_pef_tail<<<1, 1, 0, st>>>(words, nwords, gtab, nchunks, nblocks, final_state, boff, npix, diff);
+    k_pef_cols<<<1, 128, 0, st>>>(diff, W, H, colsum);
+    k_pef_rows<<<H, PEF_NT, 0, st>>>(diff, colsum, W, H, out, out_pitch);
+    return cudaGetLastError();
+}
+
+// Strip descriptors from the file layout: strip s starts at offsets[s] with
+// the bits the previous strips left in the reader's buffer (PEFFile.cs:124-155).
+cudaError_t isa_launch_pef_unpack(const uint8_t* file, unsigned long long fsize, const uint32_t* offsets, const uint32_t* sizes, int nstrips,
+                                  int rows_per_strip, int W, int H, int depth, uint16_t* out, size_t out_pitch, cudaStream_t st)
+{
+    if (nstrips < 1 || nstrips > PEF_MAX_STRIPS) return cudaErrorInvalidValue;
+    UnpackArgs A;
+    A.nstrips = nstrips;
+    unsigned long long carry_src = ~0ull;
+    unsigned carry_bits = 0;
+    const unsigned long long need = (unsigned long long)rows_per_strip * W * depth;
+    for (int s = 0; s < nstrips; s++) {
+        A.s[s] = UnpackStrip{offsets[s], sizes[s], carry_src, carry_bits};
+        // bytes this strip consumes; the bits left over are the low bits of the last one
+        const unsigned long long bytes = need > carry_bits ? (need - carry_bits + 7) / 8 : 0;
+        const unsigned long long left = carry_bits + bytes * 8 - need;
+        if (bytes > 0) carry_src = bytes <= sizes[s] ? (unsigned long long)offsets[s] + bytes - 1 : ~0ull;
+        carry_bits = (unsigned)left;
+    }
+    dim3 b(256), g((W + 255) / 256, H);
+    k_pef_unpack<<<g, b, 0, st>>>(file, fsize, A, rows_per_strip, W, H, depth, out, out_pitch);
+    return cudaGetLastError();
+}

@@ -75,6 +75,7 @@ EXPORTS = [
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
     "isa_color_twists", "isa_postprocess", "isa_save_tiff16", "isa_save_as_16bit_tiff",
+    "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
 ]
 
 _lib = None
@@ -97,6 +98,7 @@ def lib():
             if name not in ("isa_last_error", "isa_version", "isa_params_default"):
                 f.restype = ctypes.c_int
         L.isa_launch_count.restype = ctypes.c_long
+        L.isa_pef_decode_scratch.restype = ctypes.c_size_t
         _lib = L
     return _lib
 
@@ -366,6 +368,59 @@ def save_as_16bit_tiff(img, pp: IsaPostParams, path, stream=None):
     """isa_save_as_16bit_tiff: post-process a device float3 image and write the TIFF."""
     H, W, _ = img.shape
     check(lib().isa_save_as_16bit_tiff(vp(img), ctypes.c_size_t(W * 12), W, H, ctypes.byref(pp), os.fsencode(path), stream_ptr(stream)))
+
+
+def pef_huff_table(maker_note: bytes, big_endian=False):
+    """isa_pef_huff_table: the 4097-entry decode table from the HuffmanTable maker-note bytes."""
+    buf = np.frombuffer(bytes(maker_note), np.uint8).copy()
+    t = np.zeros(4097, np.uint16)
+    n = lib().isa_pef_huff_table(buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(buf.size), int(big_endian), t.ctypes.data_as(ctypes.c_void_p))
+    check(n if n < 0 else 0)
+    return t
+
+
+def pef_decode(data, table, width, height, out=None, scratch=None, stream=None):
+    """isa_pef_decode of a device uint8 stream; returns the uint16 height x
+    width frame as an int16 tensor."""
+    import torch
+    nbytes = data.numel()
+    need = lib().isa_pef_decode_scratch(ctypes.c_size_t(nbytes), width, height)
+    if scratch is None or scratch.numel() < need:
+        scratch = torch.empty(need, dtype=torch.uint8, device=data.device)
+    if out is None:
+        out = torch.empty((height, width), dtype=torch.int16, device=data.device)
+    t = np.ascontiguousarray(table, np.uint16)
+    check(lib().isa_pef_decode(vp(data), ctypes.c_size_t(nbytes), t.ctypes.data_as(ctypes.c_void_p), width, height, vp(scratch),
+                               ctypes.c_size_t(scratch.numel()), vp(out), ctypes.c_size_t(out.stride(0) * 2), stream_ptr(stream)))
+    return out
+
+
+def pef_unpack(file, offsets, sizes, rows_per_strip, width, height, bit_depth, out=None, stream=None):
+    """isa_pef_unpack of a device uint8 file image; returns the frame (int16 tensor holding uint16)."""
+    import torch
+    off = np.ascontiguousarray(offsets, np.uint32)
+    sz = np.ascontiguousarray(sizes, np.uint32)
+    if out is None:
+        out = torch.empty((height, width), dtype=torch.int16, device=file.device)
+    check(lib().isa_pef_unpack(vp(file), ctypes.c_size_t(file.numel()), off.ctypes.data_as(ctypes.c_void_p), sz.ctypes.data_as(ctypes.c_void_p),
+                               len(off), rows_per_strip, width, height, bit_depth, vp(out), ctypes.c_size_t(out.stride(0) * 2),
+                               stream_ptr(stream)))
+    return out
+
+
+def pef_levels(cfa, black_point, white_level, white_point, scaling, bit_depth):
+    """isa_pef_levels: (black[3], white[3], white_balance[3]) as float32 arrays."""
+    c = np.ascontiguousarray(cfa, np.int32)
+    bp = np.ascontiguousarray([] if black_point is None else black_point, np.float32)
+    wp = np.ascontiguousarray(white_point, np.float32)
+    b = np.zeros(3, np.float32)
+    w = np.zeros(3, np.float32)
+    wb = np.zeros(3, np.float32)
+    check(lib().isa_pef_levels(c.ctypes.data_as(ctypes.c_void_p), bp.ctypes.data_as(ctypes.c_void_p) if bp.size else None, int(bp.size),
+                               ctypes.c_float(-1.0 if white_level is None else float(white_level)), wp.ctypes.data_as(ctypes.c_void_p),
+                               ctypes.c_float(scaling), bit_depth, b.ctypes.data_as(ctypes.c_void_p), w.ctypes.data_as(ctypes.c_void_p),
+                               wb.ctypes.data_as(ctypes.c_void_p)))
+    return b, w, wb
 
 
 class IsaBurst(ctypes.Structure):

@@ -156,3 +156,72 @@ def make_burst(width=2048, height=1536, frames=8, seed=0, max_shift=6.0, max_rot
     w = float(white_max - black)
     return Burst(raw=raw, cfa=codes, black=(float(black),) * 3, white=(w, w, w), noise_a=noise_a, noise_b=noise_b,
                  shifts=shifts, rotations=rots, truth=truth)
+
+
+# ---- PEF-style compressed streams (inputs for isa_pef_decode) ----
+# The reference only decodes; these build streams in the layout its decoder
+# reads (PefFile/PEFFile.cs:81-111): per pixel in raster order a prefix code
+# for the difference category (bit length of |diff|), then the difference in
+# that many bits (negative values as diff - 1), the difference taken to the
+# pixel two columns left, or two rows up in the first two columns.
+
+PEF_CODE_LENGTHS = (2, 3, 3, 3, 3, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12)
+
+
+def pef_code_book(lengths=PEF_CODE_LENGTHS):
+    """Canonical prefix code for the category lengths: (code words left-aligned in 12 bits, lengths)."""
+    order = sorted(range(len(lengths)), key=lambda c: (lengths[c], c))
+    code = [0] * len(lengths)
+    nxt, prev = 0, lengths[order[0]]
+    for i, c in enumerate(order):
+        if i:
+            nxt = (nxt + 1) << (lengths[c] - prev)
+        prev = lengths[c]
+        code[c] = nxt << (12 - lengths[c])
+    return np.array(code, np.uint16), np.array(lengths, np.uint8)
+
+
+def pef_maker_note(code, lens, big_endian=False):
+    """The HuffmanTable maker-note payload (PefFile/PentaxMakerNotesEntry.cs:4555-4613)."""
+    import struct
+    e = ">" if big_endian else "<"
+    dep = len(code)
+    return (struct.pack(e + "H", (dep - 12) & 0xFFFF) + bytes(12) + struct.pack(e + f"{dep}H", *[int(c) for c in code]) +
+            bytes(int(v) for v in lens))
+
+
+def pef_stream(img, code, lens):
+    """Compressed stream of a uint16 H x W frame (numpy, vectorised)."""
+    v = np.asarray(img, np.int64)
+    H, W = v.shape
+    d = np.empty_like(v)
+    d[:, 2:] = v[:, 2:] - v[:, :-2]
+    d[:2, :2] = v[:2, :2]
+    d[2:, :2] = v[2:, :2] - v[:-2, :2]
+    d = d.reshape(-1)
+    mag = np.abs(d)
+    ssss = np.zeros(mag.shape, np.int64)
+    while True:
+        m = (mag >> ssss) != 0
+        if not m.any():
+            break
+        ssss += m
+    if ssss.max() >= len(code):
+        raise ValueError("difference outside the code book")
+    clen = np.asarray(lens, np.int64)[ssss]
+    cword = np.asarray(code, np.int64)[ssss] >> (12 - clen)
+    dbits = np.where(d >= 0, d, d - 1) & ((np.int64(1) << ssss) - 1)
+    field = (cword << ssss) | dbits          # code then difference, MSB first
+    flen = clen + ssss
+    start = np.concatenate([[0], np.cumsum(flen)[:-1]])
+    total = int(start[-1] + flen[-1])
+    # each field (at most 26 bits) lies in the 64-bit big-endian pair of 32-bit words (w, w + 1)
+    w = start >> 5
+    val = (field << (64 - (start & 31) - flen)).astype(np.uint64)
+    hi = val >> np.uint64(32)
+    lo = val & np.uint64(0xFFFFFFFF)
+    words = np.zeros(int(w[-1]) + 2, np.uint64)
+    first = np.concatenate([[0], np.flatnonzero(np.diff(w)) + 1])
+    words[w[first]] |= np.bitwise_or.reduceat(hi, first)
+    words[w[first] + 1] |= np.bitwise_or.reduceat(lo, first)
+    return np.frombuffer(words.astype(">u4").tobytes(), np.uint8)[: (total + 7) // 8].copy()

@@ -405,6 +405,40 @@ ISA_API int isa_save_tiff16(const char* path, const uint16_t* rgb, int width, in
 ISA_API int isa_save_as_16bit_tiff(const float* img, size_t pitch, int width, int height, const isa_post_params* pp, const char* path,
                                    void* stream);
 
+/* ---- Raw decoding of Pentax PEF frames ----
+ * The pixel data of PEFFile (PefFile/PEFFile.cs:81-156) and the levels of
+ * PEFFile.SetMembers (:176-280). The TIFF/Exif/maker-note container is
+ * parsed by the host; these entry points take the parsed values. */
+/* MNHuffmanTable (PefFile/PentaxMakerNotesEntry.cs:4555-4613): the decode
+ * table (4097 entries, table[0] = 12) from the HuffmanTable maker-note
+ * bytes, in the file's byte order. Returns the number of codes (>= 0) or
+ * ISA_EINVAL. Host only. */
+ISA_API int isa_pef_huff_table(const uint8_t* maker_note, size_t n, int big_endian, uint16_t table[4097]);
+/* Device scratch isa_pef_decode needs for `nbytes` of stream and a width x height frame. */
+ISA_API size_t isa_pef_decode_scratch(size_t nbytes, int width, int height);
+/* The compressed strip (PEFFile.cs:81-111) of one frame: `data` (device,
+ * nbytes) is the strip, `table` (host) from isa_pef_huff_table (code
+ * lengths 1..12, categories 0..15), `out` uint16 width x height (device).
+ * Decodes in parallel without host round trips: 1024-bit chunks decoded
+ * from each of their 27 candidate starts, the start maps chained, a scan of
+ * the symbol counts, the differences, then prefix sums that undo the
+ * prediction. Reads past the data see zeros. Streams up to about 1.9 Gbit. */
+ISA_API int isa_pef_decode(const uint8_t* data, size_t nbytes, const uint16_t* table, int width, int height, void* scratch, size_t scratch_bytes,
+                           uint16_t* out, size_t out_pitch, void* stream);
+/* The uncompressed branch (PEFFile.cs:116-156): `file` (device, file_size
+ * bytes) holds nstrips strips at offsets[s], sizes[s] (host arrays, at most
+ * 512 strips) of rows_per_strip rows of `bit_depth`-bit values (1..16), MSB
+ * first; the reader's left-over bits carry from one strip to the next. */
+ISA_API int isa_pef_unpack(const uint8_t* file, size_t file_size, const uint32_t* offsets, const uint32_t* sizes, int nstrips, int rows_per_strip,
+                           int width, int height, int bit_depth, uint16_t* out, size_t out_pitch, void* stream);
+/* PEFFile.SetMembers levels (PEFFile.cs:199-260): black per R, G, B from
+ * one, three or four (per CFA position; green = max of the two greens)
+ * BlackPoint values, white = WhiteLevel (or 2^bit_depth when white_level
+ * <= 0) minus black, white balance = WhitePoint[0, 1, 3] / DataScaling.
+ * cfa as isa_raw_info. Host only. */
+ISA_API int isa_pef_levels(const int cfa[4], const float* black_point, int n_black, float white_level, const float white_point[4], float scaling,
+                           int bit_depth, float black[3], float white[3], float white_balance[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -842,3 +842,144 @@ EXPORT void orc_apply_weighting(real* img, const real* acc, const real* wsum, in
         img[i] = w != 0 ? v / w : 0;
     }
 }
+
+/* ---- Raw decoding (PEF) ----
+ * MNHuffmanTable (PefFile/PentaxMakerNotesEntry.cs:4555-4613): the maker
+ * note's bytes hold a u16 (dep - 12), 12 bytes not used, dep u16 code words
+ * left-aligned in 12 bits and dep u8 code lengths (all u16 in the file's
+ * byte order). The decode table has table[0] = 12 and, for each code c,
+ * table[1 + i] = len << 8 | c over the 4096 >> len peeks i that start with
+ * the code. */
+EXPORT int orc_pef_huff_table(const uint8_t* mn, int n, int big_endian, uint16_t* table)
+{
+    uint16_t code[16], len[16];
+    memset(table, 0, 4097 * sizeof(uint16_t));
+    if (n < 2) return -1;
+#define RD16(p) (big_endian ? (uint16_t)((p)[0] << 8 | (p)[1]) : (uint16_t)((p)[1] << 8 | (p)[0]))
+    const int dep = (RD16(mn) + 12) & 15;
+    if (n < 14 + 3 * dep) return -1;
+    for (int c = 0; c < dep; c++) code[c] = RD16(mn + 14 + 2 * c);
+    for (int c = 0; c < dep; c++) len[c] = mn[14 + 2 * dep + c];
+#undef RD16
+    for (int c = 0; c < dep; c++) {
+        for (int i = code[c]; i <= ((code[c] + (4096 >> len[c]) - 1) & 4095);) table[++i] = (uint16_t)(len[c] << 8 | c);
+        table[0] = 12;
+    }
+    return dep;
+}
+
+/* The bit reader of PEFFile (getbithuff, PEFFile.cs:35-69): bytes are
+ * appended to a 32-bit buffer while fewer than nbits are valid; reads past
+ * the end of the data give zero bytes. */
+typedef struct { const uint8_t* d; size_t n, pos; uint32_t buf; int vbits; } orc_bits;
+
+static uint32_t orc_getbithuff(orc_bits* b, int nbits, const uint16_t* huff)
+{
+    if (nbits > 25) return 0;
+    if (nbits == 0 || b->vbits < 0) return 0;
+    while (b->vbits < nbits) {
+        uint32_t c = b->pos < b->n ? b->d[b->pos] : 0;
+        b->pos++;
+        b->buf = (b->buf << 8) + (uint8_t)c;
+        b->vbits += 8;
+    }
+    uint32_t c = b->buf << (32 - b->vbits) >> (32 - nbits);
+    if (huff) {
+        b->vbits -= huff[c] >> 8;
+        c = (uint8_t)huff[c];
+    } else {
+        b->vbits -= nbits;
+    }
+    return c;
+}
+
+/* PEFFile(aFileName) compressed branch (PEFFile.cs:81-111): one strip,
+ * ljpeg_diff per pixel in raster order, the first two columns predicted
+ * from the pixel two rows up (vpred), the others from the pixel two
+ * columns left (hpred), stored as (ushort). The shift by len - 1 uses the
+ * 5-bit shift count of C# (len = 0 gives diff = 0). */
+EXPORT void orc_pef_decode(const uint8_t* data, size_t n, const uint16_t* huff, int W, int H, uint16_t* out)
+{
+    orc_bits b = {data, n, 0, 0, 0};
+    int vpred[2][2] = {{0, 0}, {0, 0}}, hpred[2] = {0, 0};
+    for (int row = 0; row < H; row++)
+        for (int col = 0; col < W; col++) {
+            const int len = (int)orc_getbithuff(&b, huff[0], huff + 1);
+            int diff = (int)orc_getbithuff(&b, len, NULL);
+            if ((diff & (int)(1u << ((len - 1) & 31))) == 0) diff -= (int)((1u << (len & 31)) - 1);
+            if (col < 2) hpred[col] = vpred[row & 1][col] += diff;
+            else hpred[col & 1] += diff;
+            out[(size_t)row * W + col] = (uint16_t)hpred[col & 1];
+        }
+}
+
+/* PEFFile(aFileName) uncompressed branch (PEFFile.cs:116-156): per strip,
+ * rows_per_strip rows of W values of `depth` bits, MSB first; the bit
+ * buffer and its count carry over from one strip to the next. Rows past H
+ * are not written (the reference would throw there). */
+EXPORT void orc_pef_unpack(const uint8_t* file, size_t file_size, const uint32_t* offsets, const uint32_t* sizes, int nstrips, int rows_per_strip,
+                           int W, int H, int depth, uint16_t* out)
+{
+    uint32_t bitbuf = 0;
+    int bitoff = 0;
+    for (int s = 0; s < nstrips; s++) {
+        const uint8_t* d = file + offsets[s];
+        const size_t nd = offsets[s] < file_size ? (size_t)sizes[s] : 0;
+        size_t pos = 0;
+        for (int line = 0; line < rows_per_strip; line++)
+            for (int px = 0; px < W; px++) {
+                const int row = s * rows_per_strip + line;
+                while (bitoff < depth) {
+                    uint32_t v = pos < nd ? d[pos] : 0;
+                    bitbuf = (bitbuf << 8) + v;
+                    bitoff += 8;
+                    pos++;
+                }
+                uint32_t v = bitbuf << (32 - bitoff) >> (32 - depth);
+                bitoff -= depth;
+                if (row < H) out[(size_t)row * W + px] = (uint16_t)v;
+            }
+    }
+}
+
+/* Test-stream synthesis (not part of the reference, which only decodes):
+ * the inverse of orc_pef_decode for a code book (code[c] left-aligned in 12
+ * bits, len[c]) covering categories 0 .. ncodes-1. Returns the bytes
+ * written, or -1 if `cap` is too small or a difference needs a category
+ * the book lacks. The last byte is zero-padded. */
+EXPORT long orc_pef_encode(const uint16_t* img, int W, int H, const uint16_t* code, const uint8_t* len, int ncodes, uint8_t* out, size_t cap)
+{
+    uint64_t acc = 0;
+    int nacc = 0;
+    size_t w = 0;
+    int vpred[2][2] = {{0, 0}, {0, 0}}, hpred[2] = {0, 0};
+#define PUT(v, nb)                                                   \
+    do {                                                             \
+        acc = (acc << (nb)) | ((uint64_t)(v) & ((1ull << (nb)) - 1)); \
+        nacc += (nb);                                                \
+        while (nacc >= 8) {                                          \
+            if (w >= cap) return -1;                                 \
+            out[w++] = (uint8_t)(acc >> (nacc - 8));                 \
+            nacc -= 8;                                               \
+        }                                                            \
+    } while (0)
+    for (int row = 0; row < H; row++)
+        for (int col = 0; col < W; col++) {
+            const int v = img[(size_t)row * W + col];
+            const int pred = col < 2 ? vpred[row & 1][col] : hpred[col & 1];
+            const int diff = v - pred;
+            int ssss = 0;
+            while ((abs(diff) >> ssss) != 0) ssss++;
+            if (ssss >= ncodes || len[ssss] == 0) return -1;
+            PUT(code[ssss] >> (12 - len[ssss]), len[ssss]);
+            if (ssss > 0) PUT(diff >= 0 ? diff : diff - 1, ssss);
+            if (col < 2) hpred[col] = vpred[row & 1][col] = v;
+            else hpred[col & 1] = v;
+        }
+    if (nacc > 0) {
+        if (w >= cap) return -1;
+        out[w++] = (uint8_t)(acc << (8 - nacc));
+    }
+#undef PUT
+    return (long)w;
+}
