@@ -1769,3 +1769,328 @@ int isa_pef_levels(const int cfa[4], const float* black_point, int n_black, floa
     white_balance[2] = white_point[3] / scaling;
     return ISA_OK;
 }
+
+// ---- DNG colour specification (CameraToPCS and CameraWhite) ----
+// Restates DNGColorSpec (PefFile/DNGColorSpec.cs:31-647), DNGTemperature
+// (PefFile/DNGTemperature.cs, xy -> temperature) and DNGxyCoord
+// (PefFile/DNGxyCoord.cs), all in FP64 with the reference's operation order.
+
+namespace {
+
+// Robertson's isotemperature lines (Robertson 1968, as tabulated in
+// Wyszecki & Stiles): reciprocal megakelvin, u, v, slope.
+const double kRobertson[31][4] = {
+    {0, 0.18006, 0.26352, -0.24341},   {10, 0.18066, 0.26589, -0.25479},  {20, 0.18133, 0.26846, -0.26876},  {30, 0.18208, 0.27119, -0.28539},
+    {40, 0.18293, 0.27407, -0.30470},  {50, 0.18388, 0.27709, -0.32675},  {60, 0.18494, 0.28021, -0.35156},  {70, 0.18611, 0.28342, -0.37915},
+    {80, 0.18740, 0.28668, -0.40955},  {90, 0.18880, 0.28997, -0.44278},  {100, 0.19032, 0.29326, -0.47888}, {125, 0.19462, 0.30141, -0.58204},
+    {150, 0.19962, 0.30921, -0.70471}, {175, 0.20525, 0.31647, -0.84901}, {200, 0.21142, 0.32312, -1.0182},  {225, 0.21807, 0.32909, -1.2168},
+    {250, 0.22511, 0.33439, -1.4512},  {275, 0.23247, 0.33904, -1.7298},  {300, 0.24010, 0.34308, -2.0637},  {325, 0.24702, 0.34655, -2.4681},
+    {350, 0.25591, 0.34951, -2.9641},  {375, 0.26400, 0.35200, -3.5814},  {400, 0.27218, 0.35407, -4.3633},  {425, 0.28039, 0.35577, -5.3762},
+    {450, 0.28863, 0.35714, -6.7262},  {475, 0.29685, 0.35823, -8.5955},  {500, 0.30505, 0.35907, -11.324},  {525, 0.31320, 0.35968, -15.628},
+    {550, 0.32129, 0.36011, -23.325},  {575, 0.32931, 0.36038, -40.770},  {600, 0.33724, 0.36051, -116.45}};
+
+struct XY { double x, y; };
+const XY kD50{0.3457, 0.3585};
+
+struct V3 { double v[3]; };
+
+V3 xy_to_xyz(XY c)
+{
+    double x = std::max(0.000001, std::min(c.x, 0.999999)), y = std::max(0.000001, std::min(c.y, 0.999999));
+    if (x + y > 0.999999) {
+        const double s = 0.999999 / (x + y);
+        x *= s;
+        y *= s;
+    }
+    return V3{{x / y, 1.0, (1.0 - x - y) / y}};
+}
+
+XY xyz_to_xy(const V3& c)
+{
+    const double total = c.v[0] + c.v[1] + c.v[2];
+    if (total > 0.0) return XY{c.v[0] / total, c.v[1] / total};
+    return kD50;
+}
+
+V3 mat_vec(const M3& m, const V3& a)
+{
+    V3 r;
+    for (int j = 0; j < 3; j++) {
+        double s = 0.0;
+        for (int k = 0; k < 3; k++) s += m.a[j][k] * a.v[k];
+        r.v[j] = s;
+    }
+    return r;
+}
+
+double max3(const V3& a) { return std::max(a.v[0], std::max(a.v[1], a.v[2])); }
+
+M3 diag(const V3& a)
+{
+    M3 m{};
+    for (int j = 0; j < 3; j++) m.a[j][j] = a.v[j];
+    return m;
+}
+
+M3 ident3() { return diag(V3{{1.0, 1.0, 1.0}}); }
+
+M3 scaled(double s, const M3& m)
+{
+    M3 r = m;
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) r.a[j][k] *= s;
+    return r;
+}
+
+M3 mat_add(const M3& a, const M3& b)
+{
+    M3 r = a;
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) r.a[j][k] += b.a[j][k];
+    return r;
+}
+
+M3 inv_or_throw(const M3& m, bool& ok)
+{
+    M3 r{};
+    if (!mat_inv3(m, r)) ok = false;
+    return r;
+}
+
+// DNGTemperature.xyCoord setter (DNGTemperature.cs:181-258): the temperature only.
+double temperature_of(XY c)
+{
+    const double u = 2.0 * c.x / (1.5 - c.x + 6.0 * c.y);
+    const double v = 3.0 * c.y / (1.5 - c.x + 6.0 * c.y);
+    double last_dt = 0.0;
+    for (int index = 1; index <= 30; index++) {
+        double du = 1.0, dv = kRobertson[index][3];
+        const double len = std::sqrt(1.0 + dv * dv);
+        du /= len;
+        dv /= len;
+        const double uu = u - kRobertson[index][1], vv = v - kRobertson[index][2];
+        double dt = -uu * dv + vv * du;
+        if (dt <= 0.0 || index == 30) {
+            if (dt > 0.0) dt = 0.0;
+            dt = -dt;
+            const double f = index == 1 ? 0.0 : dt / (last_dt + dt);
+            return 1.0E6 / (kRobertson[index - 1][0] * f + kRobertson[index][0] * (1.0 - f));
+        }
+        last_dt = dt;
+    }
+    return 0.0;
+}
+
+// ConvertIlluminantToTemperature (DNGColorSpec.cs:122-172), EXIF LightSource codes.
+double illuminant_temperature(int code)
+{
+    switch (code) {
+    case 1: return 5500.0;                        // daylight
+    case 2: return (3800.0 + 4500.0) * 0.5;       // fluorescent
+    case 3: return 2850.0;                        // tungsten
+    case 4: return 5500.0;                        // flash
+    case 9: return 5500.0;                        // fine weather
+    case 10: return 6500.0;                       // cloudy
+    case 11: return 7500.0;                       // shade
+    case 12: return (5700.0 + 7100.0) * 0.5;      // daylight fluorescent
+    case 13: return (4600.0 + 5500.0) * 0.5;      // day white fluorescent
+    case 14: return (3800.0 + 4500.0) * 0.5;      // cool white fluorescent
+    case 15: return (3250.0 + 3800.0) * 0.5;      // white fluorescent
+    case 16: return (2600.0 + 3250.0) * 0.5;      // warm white fluorescent
+    case 17: return 2850.0;                       // standard light A
+    case 18: return 5500.0;                       // B
+    case 19: return 6500.0;                       // C
+    case 20: return 5500.0;                       // D55
+    case 21: return 6500.0;                       // D65
+    case 22: return 7500.0;                       // D75
+    case 23: return 5000.0;                       // D50
+    case 24: return 3200.0;                       // ISO studio tungsten
+    default: return 0.0;                          // unknown, other
+    }
+}
+
+// MapWhiteMatrix (DNGColorSpec.cs:38-65): linearised Bradford adaptation white1 -> white2.
+M3 map_white(XY w1, XY w2, bool& ok)
+{
+    const M3 Mb{{{0.8951, 0.2664, -0.1614}, {-0.7502, 1.7135, 0.0367}, {0.0389, -0.0685, 1.0296}}};
+    V3 a = mat_vec(Mb, xy_to_xyz(w1)), b = mat_vec(Mb, xy_to_xyz(w2));
+    for (int j = 0; j < 3; j++) {
+        a.v[j] = std::max(a.v[j], 0.0);
+        b.v[j] = std::max(b.v[j], 0.0);
+    }
+    M3 A{};
+    for (int j = 0; j < 3; j++) A.a[j][j] = std::max(0.1, std::min(a.v[j] > 0.0 ? b.v[j] / a.v[j] : 10.0, 10.0));
+    return mat_mul(mat_mul(inv_or_throw(Mb, ok), A), Mb);
+}
+
+struct ColorSpec {
+    double t1, t2;
+    M3 cm1, cm2, fm1, fm2, cc1, cc2, ab;
+    bool cm2_set, fm1_set, fm2_set;
+};
+
+// NormalizeForwardMatrix (DNGColorSpec.cs:105-120)
+M3 normalize_forward(const M3& m, bool& ok)
+{
+    const V3 xyz = mat_vec(m, V3{{1.0, 1.0, 1.0}});
+    return mat_mul(mat_mul(diag(xy_to_xyz(kD50)), inv_or_throw(diag(xyz), ok)), m);
+}
+
+// FindXYZtoCamera (DNGColorSpec.cs:531-645); forward / calibration optional outputs.
+M3 find_xyz_to_camera(const ColorSpec& s, XY white, M3* fm, bool* fm_set, M3* cc)
+{
+    const double T = temperature_of(white);
+    double g;
+    if (T <= s.t1) g = 1.0;
+    else if (T >= s.t2) g = 0.0;
+    else {
+        const double invT = 1.0 / T;
+        g = (invT - (1.0 / s.t2)) / ((1.0 / s.t1) - (1.0 / s.t2));
+    }
+    const auto mix = [&](const M3& a, const M3& b) { return g >= 1.0 ? a : (g <= 0.0 ? b : mat_add(scaled(g, a), scaled(1.0 - g, b))); };
+    if (fm) {
+        if (s.fm1_set && s.fm2_set) { *fm = mix(s.fm1, s.fm2); *fm_set = true; }
+        else if (s.fm1_set) { *fm = s.fm1; *fm_set = true; }
+        else if (s.fm2_set) { *fm = s.fm2; *fm_set = true; }
+        else *fm_set = false;
+    }
+    if (cc) *cc = mix(s.cc1, s.cc2);
+    return mix(s.cm1, s.cm2);
+}
+
+// NeutralToXY (DNGColorSpec.cs:490-529)
+XY neutral_to_xy(const ColorSpec& s, const V3& neutral, bool& ok)
+{
+    XY last = kD50;
+    for (int pass = 0; pass < 30; pass++) {
+        const M3 xyz_to_cam = find_xyz_to_camera(s, last, nullptr, nullptr, nullptr);
+        XY next = xyz_to_xy(mat_vec(inv_or_throw(xyz_to_cam, ok), neutral));
+        if (std::fabs(next.x - last.x) + std::fabs(next.y - last.y) < 0.0000001) return next;
+        if (pass == 29) {
+            next.x = (last.x + next.x) * 0.5;
+            next.y = (last.y + next.y) * 0.5;
+        }
+        last = next;
+    }
+    return last;
+}
+
+// The WhiteXY setter (DNGColorSpec.cs:404-466) for three channels.
+void set_white(const ColorSpec& s, XY white, M3& camera_to_pcs, V3& camera_white, bool& ok)
+{
+    M3 fm{}, cc{};
+    bool fm_set = false;
+    const M3 cm = find_xyz_to_camera(s, white, &fm, &fm_set, &cc);
+    camera_white = mat_vec(cm, xy_to_xyz(white));
+    const double ws = 1.0 / max3(camera_white);
+    for (int j = 0; j < 3; j++) camera_white.v[j] = std::max(0.001, std::min(ws * camera_white.v[j], 1.0));
+    M3 pcs_to_camera = mat_mul(cm, map_white(kD50, white, ok));
+    const double scale = max3(mat_vec(pcs_to_camera, xy_to_xyz(kD50)));
+    pcs_to_camera = scaled(1.0 / scale, pcs_to_camera);
+    if (fm_set) {
+        const M3 ind_to_ref = inv_or_throw(mat_mul(s.ab, cc), ok);
+        const V3 ref_white = mat_vec(ind_to_ref, camera_white);
+        camera_to_pcs = mat_mul(mat_mul(fm, inv_or_throw(diag(ref_white), ok)), ind_to_ref);
+    } else {
+        camera_to_pcs = inv_or_throw(pcs_to_camera, ok);
+    }
+}
+
+M3 m3_of(const double* p)
+{
+    M3 m;
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) m.a[j][k] = p[j * 3 + k];
+    return m;
+}
+
+int color_spec_out(const ColorSpec& s, XY white, double camera_to_pcs[9], double camera_white[3], double white_xy[2])
+{
+    bool ok = true;
+    M3 c2p{};
+    V3 cw{};
+    set_white(s, white, c2p, cw, ok);
+    if (!ok) return fail(ISA_ESINGULAR, "a colour matrix is singular");
+    for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) camera_to_pcs[j * 3 + k] = c2p.a[j][k];
+    for (int j = 0; j < 3; j++) camera_white[j] = cw.v[j];
+    if (white_xy) { white_xy[0] = white.x; white_xy[1] = white.y; }
+    return ISA_OK;
+}
+
+}  // namespace
+
+int isa_dng_color_spec(const isa_dng_color_tags* t, double camera_to_pcs[9], double camera_white[3], double white_xy[2])
+{
+    ISA_REQ(t && camera_to_pcs && camera_white, "NULL argument");
+    ISA_REQ(t->as_shot_white_xy || t->as_shot_neutral, "one of AsShotWhiteXY and AsShotNeutral is needed (DNG specification)");
+    bool ok = true;
+    ColorSpec s;
+    s.t1 = illuminant_temperature(t->illuminant1);
+    s.t2 = illuminant_temperature(t->illuminant2);
+    s.cm1 = t->color_matrix1 ? m3_of(t->color_matrix1) : ident3();
+    s.cm2_set = t->color_matrix2 != nullptr;
+    s.cm2 = s.cm2_set ? m3_of(t->color_matrix2) : M3{};
+    s.fm1_set = t->forward_matrix1 != nullptr;
+    s.fm2_set = t->forward_matrix2 != nullptr;
+    s.fm1 = s.fm1_set ? m3_of(t->forward_matrix1) : M3{};
+    s.fm2 = s.fm2_set ? m3_of(t->forward_matrix2) : M3{};
+    s.cc1 = t->camera_calibration1 ? m3_of(t->camera_calibration1) : ident3();
+    s.cc2 = t->camera_calibration2 ? m3_of(t->camera_calibration2) : ident3();
+    s.ab = t->analog_balance ? diag(V3{{t->analog_balance[0], t->analog_balance[1], t->analog_balance[2]}}) : ident3();
+    if (s.fm1_set) s.fm1 = normalize_forward(s.fm1, ok);
+    s.cm1 = mat_mul(mat_mul(s.ab, s.cc1), s.cm1);
+    if (!s.cm2_set || s.t1 <= 0.0 || s.t2 <= 0.0 || s.t1 == s.t2) {
+        s.t1 = s.t2 = 5000.0;
+        s.cm2 = s.cm1;
+        s.fm2 = s.fm1;
+        s.fm2_set = s.fm1_set;
+        s.cc2 = s.cc1;
+    } else {
+        if (s.fm2_set) s.fm2 = normalize_forward(s.fm2, ok);
+        s.cm2 = mat_mul(mat_mul(s.ab, s.cc2), s.cm2);
+        if (s.t1 > s.t2) {
+            std::swap(s.t1, s.t2);
+            std::swap(s.cm1, s.cm2);
+            std::swap(s.fm1, s.fm2);
+            std::swap(s.fm1_set, s.fm2_set);
+            std::swap(s.cc1, s.cc2);
+        }
+    }
+    XY white;
+    if (t->as_shot_white_xy) {
+        white = XY{t->as_shot_white_xy[0], t->as_shot_white_xy[1]};
+    } else {
+        V3 vec{{t->as_shot_neutral[0], t->as_shot_neutral[1], t->as_shot_neutral[2]}};
+        const double unify = 1.0 / max3(vec);
+        for (int j = 0; j < 3; j++) vec.v[j] = unify * vec.v[j];
+        white = neutral_to_xy(s, vec, ok);
+    }
+    if (!ok) return fail(ISA_ESINGULAR, "a colour matrix is singular");
+    return color_spec_out(s, white, camera_to_pcs, camera_white, white_xy);
+}
+
+int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2])
+{
+    ISA_REQ(white_balance && camera_to_pcs && camera_white, "NULL argument");
+    for (int c = 0; c < 3; c++)
+        if (!(white_balance[c] > 0.f) || !std::isfinite(white_balance[c])) return fail(ISA_EINVAL, "white balance must be positive");
+    // PEFFile.SetMembers (PEFFile.cs:276-278): identity colour matrices under D50 for both illuminants
+    bool ok = true;
+    ColorSpec s;
+    s.t1 = s.t2 = 5000.0;
+    s.cm1 = s.cm2 = ident3();
+    s.cm2_set = true;
+    s.fm1_set = s.fm2_set = false;
+    s.fm1 = s.fm2 = M3{};
+    s.cc1 = s.cc2 = ident3();
+    s.ab = ident3();
+    // DNGColorSpec(..., float[] whiteBalance) (DNGColorSpec.cs:248-266): neutral = 1 / wb in float, scaled by 1 / max
+    V3 vec;
+    for (int c = 0; c < 3; c++) vec.v[c] = (double)(1.0f / white_balance[c]);
+    const double unify = 1.0 / max3(vec);
+    for (int c = 0; c < 3; c++) vec.v[c] = unify * vec.v[c];
+    const XY white = neutral_to_xy(s, vec, ok);
+    if (!ok) return fail(ISA_ESINGULAR, "a colour matrix is singular");
+    return color_spec_out(s, white, camera_to_pcs, camera_white, white_xy);
+}

@@ -76,6 +76,7 @@ EXPORTS = [
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
     "isa_color_twists", "isa_postprocess", "isa_save_tiff16", "isa_save_as_16bit_tiff",
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
+    "isa_dng_color_spec", "isa_pef_color_spec",
 ]
 
 _lib = None
@@ -421,6 +422,47 @@ def pef_levels(cfa, black_point, white_level, white_point, scaling, bit_depth):
                                ctypes.c_float(scaling), bit_depth, b.ctypes.data_as(ctypes.c_void_p), w.ctypes.data_as(ctypes.c_void_p),
                                wb.ctypes.data_as(ctypes.c_void_p)))
     return b, w, wb
+
+
+class IsaDngColorTags(ctypes.Structure):
+    _fields_ = [("color_matrix1", ctypes.c_void_p), ("color_matrix2", ctypes.c_void_p), ("illuminant1", ctypes.c_int),
+                ("illuminant2", ctypes.c_int), ("forward_matrix1", ctypes.c_void_p), ("forward_matrix2", ctypes.c_void_p),
+                ("camera_calibration1", ctypes.c_void_p), ("camera_calibration2", ctypes.c_void_p), ("analog_balance", ctypes.c_void_p),
+                ("as_shot_neutral", ctypes.c_void_p), ("as_shot_white_xy", ctypes.c_void_p)]
+
+
+def dng_color_spec(color_matrix1=None, color_matrix2=None, illuminant1=0, illuminant2=0, forward_matrix1=None, forward_matrix2=None,
+                   camera_calibration1=None, camera_calibration2=None, analog_balance=None, as_shot_neutral=None, as_shot_white_xy=None):
+    """isa_dng_color_spec: (camera_to_pcs 3 x 3, camera_white 3, white xy 2) as float64."""
+    keep = []
+
+    def arr(v, n):
+        if v is None:
+            return None
+        a = np.ascontiguousarray(v, np.float64).reshape(n)
+        keep.append(a)
+        return a.ctypes.data
+
+    t = IsaDngColorTags(arr(color_matrix1, 9), arr(color_matrix2, 9), int(illuminant1), int(illuminant2), arr(forward_matrix1, 9),
+                        arr(forward_matrix2, 9), arr(camera_calibration1, 9), arr(camera_calibration2, 9), arr(analog_balance, 3),
+                        arr(as_shot_neutral, 3), arr(as_shot_white_xy, 2))
+    c2p = np.zeros(9)
+    cw = np.zeros(3)
+    xy = np.zeros(2)
+    check(lib().isa_dng_color_spec(ctypes.byref(t), c2p.ctypes.data_as(ctypes.c_void_p), cw.ctypes.data_as(ctypes.c_void_p),
+                                   xy.ctypes.data_as(ctypes.c_void_p)))
+    return c2p.reshape(3, 3), cw, xy
+
+
+def pef_color_spec(white_balance):
+    """isa_pef_color_spec: the colour spec of a PEF file from its white balance."""
+    wb = np.ascontiguousarray(white_balance, np.float32)
+    c2p = np.zeros(9)
+    cw = np.zeros(3)
+    xy = np.zeros(2)
+    check(lib().isa_pef_color_spec(wb.ctypes.data_as(ctypes.c_void_p), c2p.ctypes.data_as(ctypes.c_void_p), cw.ctypes.data_as(ctypes.c_void_p),
+                                   xy.ctypes.data_as(ctypes.c_void_p)))
+    return c2p.reshape(3, 3), cw, xy
 
 
 class IsaBurst(ctypes.Structure):

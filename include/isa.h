@@ -439,6 +439,31 @@ ISA_API int isa_pef_unpack(const uint8_t* file, size_t file_size, const uint32_t
 ISA_API int isa_pef_levels(const int cfa[4], const float* black_point, int n_black, float white_level, const float white_point[4], float scaling,
                            int bit_depth, float black[3], float white[3], float white_balance[3]);
 
+/* ---- DNG colour specification ----
+ * DNGColorSpec (PefFile/DNGColorSpec.cs:31-647) with DNGTemperature and
+ * DNGxyCoord, in FP64: the colour matrix (and forward matrix, camera
+ * calibration) interpolated by the white point's temperature between the
+ * two calibration illuminants, the white point from AsShotWhiteXY or found
+ * from AsShotNeutral, then CameraWhite and CameraToPCS (camera -> XYZ D50),
+ * the inputs of isa_color_twists and isa_post_params. Host only. */
+typedef struct isa_dng_color_tags {
+    const double* color_matrix1;        /* 9, row-major (ColorMatrix1); NULL = identity */
+    const double* color_matrix2;        /* 9 or NULL */
+    int illuminant1, illuminant2;       /* CalibrationIlluminant1/2, EXIF LightSource codes; 0 = absent/unknown */
+    const double* forward_matrix1;      /* 9 or NULL */
+    const double* forward_matrix2;      /* 9 or NULL */
+    const double* camera_calibration1;  /* 9 or NULL = identity (the reference reads CameraCalibration1 for both) */
+    const double* camera_calibration2;  /* 9 or NULL = identity */
+    const double* analog_balance;       /* 3 or NULL = 1 */
+    const double* as_shot_neutral;      /* 3 or NULL */
+    const double* as_shot_white_xy;     /* 2 or NULL; used when given */
+} isa_dng_color_tags;
+ISA_API int isa_dng_color_spec(const isa_dng_color_tags* tags, double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
+/* The colour spec PEFFile.SetMembers builds (PEFFile.cs:276-278): identity
+ * colour matrices under D50 and the white point of the neutral 1 / white
+ * balance (isa_pef_levels' white_balance). */
+ISA_API int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
+
 #ifdef __cplusplus
 }
 #endif

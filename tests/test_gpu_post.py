@@ -115,3 +115,41 @@ def test_postprocess_large_crop_edges(cuda):
         got = isa.postprocess(torch.from_numpy(img).cuda(), pp, isa.POST_RGB16)
         torch.cuda.synchronize()
         close(got.cpu().numpy().view(np.uint16), PO.postprocess(img, crop, [1, 1, 1], t1, t2, lx, lx, 0.0))
+
+
+def test_pef_file_to_tiff_chain(cuda, tmp_path):
+    """The reference's flow from PEF pixel data to the 16-bit TIFF: frames
+    decoded from the compressed stream layout (isa_pef_decode), merged, the
+    colour spec of PEFFile.SetMembers from the white balance
+    (isa_pef_color_spec), its camera white and twists into SaveAs16BitTiff."""
+    import torch
+    from imagestackalignator_b200 import synthetic as S
+    import raw as R
+    import colorspec as CS
+    b = synthetic.make_burst(512, 384, 3, seed=12, max_shift=3, max_rot_deg=0.0)
+    code, lens = S.pef_code_book()
+    table = isa.pef_huff_table(S.pef_maker_note(code, lens))
+    frames = []
+    for f in range(b.n):
+        stream = S.pef_stream(b.raw[f], code, lens)
+        out = isa.pef_decode(torch.from_numpy(stream).cuda(), table, b.width, b.height)
+        frames.append(out)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint16), R.decode(stream, R.huff_table(S.pef_maker_note(code, lens)), b.width, b.height))
+    raw = torch.stack(frames)
+    assert np.array_equal(raw.cpu().numpy().view(np.uint16), b.raw)
+    m = isa.Merger(b.width, b.height, b.n, P.MergeParams())
+    merged = m.merge(raw, isa.make_info(b))
+    torch.cuda.synchronize()
+    wb = np.float32([1.9, 1.0, 1.6])
+    c2p, cw, xy = isa.pef_color_spec(wb)
+    want_spec = CS.pef_color_spec(wb)
+    assert np.array_equal(c2p, want_spec[0]) and np.array_equal(cw, want_spec[1])
+    t1, t2 = isa.color_twists(c2p)
+    lx = lut_levels()
+    crop = (2, 2, b.width - 4, b.height - 4)   # the PEF crop (PEFFile.cs:266-270)
+    pp, keep = isa.post_params(crop, np.float32(cw), t1, t2, lx, tone(lx), 0.0)
+    path = tmp_path / "burst.tif"
+    isa.save_as_16bit_tiff(merged, pp, str(path))
+    tags, img = PO.parse_tiff16(path.read_bytes())
+    close(img, PO.postprocess(merged.cpu().numpy(), crop, np.float32(cw), t1, t2, lx, tone(lx), 0.0))
