@@ -196,8 +196,11 @@ __global__ void k_lk_sums(float2* flow, size_t flow_pitch, const float* __restri
 // owns image column x0 - R + t (R = h + 2, mirrored at the border) and walks
 // down the strip one row at a time:
 //   1. the warped source and the reference at (column, row) go into a
-//      five-row ring in shared memory; the global loads for the next rows
-//      are issued one and two rows ahead (flow, then the bilinear samples);
+//      six-row ring in shared memory (one row more than the derivatives
+//      read, so a slot is rewritten only after the next row's barrier and
+//      the step needs no barrier at its end); the global loads for the next
+//      rows are issued one and two rows ahead (flow, then the bilinear
+//      samples);
 //   2. five-tap derivatives at the ring's centre row (neighbouring columns
 //      from shared memory), FP32 products, and per-column vertical window
 //      sums in FP64 registers (the product leaving the window comes from a
@@ -212,7 +215,7 @@ template <int H>
 struct LkStream {
     static constexpr int R = H + 2, SW = LKS_NT - 2 * R, WIN = 2 * H + 1;
     static constexpr int NSEG = (SW + 1) / 2;
-    static constexpr size_t E_BYTES = (size_t)2 * 5 * LKS_NT * 4;
+    static constexpr size_t E_BYTES = (size_t)2 * 6 * LKS_NT * 4;
     static constexpr size_t P_BYTES = (size_t)WIN * 5 * LKS_NT * 4;
     static constexpr size_t OFF_P = E_BYTES, OFF_C = (OFF_P + P_BYTES + 15) / 16 * 16;
     static constexpr size_t TOTAL = OFF_C + (size_t)2 * 5 * LKS_NT * 8;
@@ -226,8 +229,8 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
     using L = LkStream<H>;
     constexpr int R = L::R, SW = L::SW, WIN = L::WIN, NT = LKS_NT;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* Ew = (float*)smem;            // [5][NT]
-    float* Er = Ew + 5 * NT;              // [5][NT]
+    float* Ew = (float*)smem;            // [6][NT]
+    float* Er = Ew + 6 * NT;              // [6][NT]
     float* Pr = (float*)(smem + L::OFF_P);    // [WIN][5][NT]
     double* Cs = (double*)(smem + L::OFF_C);  // [2][5][NT]
     const int t = threadIdx.x;
@@ -254,7 +257,7 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
     if (nE > 1) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(1)) + col);
     double cs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     // ring slots of rows e, e-1, e-2, e-3, e-4 (mod 5) and of the product row (mod WIN), advanced incrementally
-    int r0 = 0, r1 = 4, r2 = 3, r3 = 2, r4 = 1, pw = 0;
+    int r0 = 0, r1 = 5, r2 = 4, r3 = 3, r4 = 2, pw = 0;
     for (int e = 0; e < nE; e++) {
         Ew[r0 * NT + t] = isa::lerp2(s00, s10, s01, s11, sa, sb);
         Er[r0 * NT + t] = sref;
@@ -326,8 +329,7 @@ __global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__
                 }
             }
         }
-        __syncthreads();
-        r4 = r3; r3 = r2; r2 = r1; r1 = r0; r0 = r0 + 1 == 5 ? 0 : r0 + 1;
+        r4 = r3; r3 = r2; r2 = r1; r1 = r0; r0 = r0 + 1 == 6 ? 0 : r0 + 1;
     }
 }
 
