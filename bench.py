@@ -355,6 +355,41 @@ def raw_decode_throughput(args, frame):
     return res
 
 
+def dng_decode_throughput(args, frame):
+    """DNG raw decoding (isa_dng_decode) of one frame of the workload stored
+    as 256 x 256 lossless-JPEG tiles (two interleaved components, predictor
+    1): time per frame through the entry point (host header parsing, one
+    thread per tile, synchronised), with the restated reference reader on
+    one host core as its CPU baseline."""
+    import torch
+    from imagestackalignator_b200 import isa, synthetic
+    H, W = frame.shape
+    f, offs, cnts = synthetic.dng_tiled_file(frame)
+    dev = torch.from_numpy(f).cuda()
+    kw = dict(tiled=True, tile_w=256, tile_h=256, file_dev=dev)
+    out = isa.dng_decode(f, W, H, offs, cnts, **kw)
+    torch.cuda.synchronize()
+    exact = bool(np.array_equal(out.cpu().numpy().view(np.uint16), frame))
+    stream_t = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream_t)
+    for _ in range(args.steps):
+        isa.dng_decode(f, W, H, offs, cnts, **kw)
+    e1.record(stream_t)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    res = {"workload": f"one {W}x{H} 14-bit frame as {len(offs)} lossless-JPEG tiles of 256x256, {f.size / 1e6:.1f} MB", "ms": ms,
+           "mp_s": W * H / 1e6 / (ms / 1e3), "exact": exact, "cpu_baseline": None}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import raw as R  # the restated reference reader (DNGFile.cs:40-600), one host core
+        t0 = time.perf_counter()
+        R.dng_decode(f, W, H, offs, cnts, tiled=True, tile_w=256, tile_h=256)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"mp_s": W * H / 1e6 / dt, "cores": 1, "kind": "port", "sample": f"the same file, {dt:.2f} s"}
+    return res
+
+
 def run_ours(args):
     import torch
     from imagestackalignator_b200 import isa
@@ -459,6 +494,9 @@ def run_ours(args):
     rawdec = None
     if rank == 0 and world == 1 and not args.no_raw:
         rawdec = raw_decode_throughput(args, np.ascontiguousarray(burst.raw[1]))
+    dngdec = None
+    if rank == 0 and world == 1 and not args.no_raw:
+        dngdec = dng_decode_throughput(args, np.ascontiguousarray(burst.raw[1]))
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = batch_throughput(args)
@@ -473,7 +511,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint, "batch": batch, "postprocess": post, "raw_decode": rawdec,
+        "fwd_adjoint": adjoint, "batch": batch, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec,
         "clocks": clocks,
     }
     if rank == 0:
@@ -497,7 +535,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
     ap.add_argument("--no-post", action="store_true", help="skip the colour/tone post-processing timing")
-    ap.add_argument("--no-raw", action="store_true", help="skip the PEF raw-decoding timing")
+    ap.add_argument("--no-raw", action="store_true", help="skip the PEF and DNG raw-decoding timings")
     ap.add_argument("--size", default=None, help="WxH override for profiling runs on a smaller burst (not a bench line)")
     ap.add_argument("--frames", type=int, default=None, help="frame-count override for profiling runs (not a bench line)")
     args = ap.parse_args()

@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -2093,4 +2094,224 @@ int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], do
     const XY white = neutral_to_xy(s, vec, ok);
     if (!ok) return fail(ISA_ESINGULAR, "a colour matrix is singular");
     return color_spec_out(s, white, camera_to_pcs, camera_white, white_xy);
+}
+
+// ---- DNG pixel data ----
+
+namespace {
+
+// ljpeg_start (DNGFile.cs:94-170) on the host: the frame header, the
+// Huffman tables (make_decoder_ref, :73-92) and the entropy data's offset.
+struct Lj92Header {
+    int algo = 0, bits = 0, high = 0, wide = 0, clrs = 0, sraw = 0, psv = 0, restart = 0x7fffffff;
+    std::vector<uint16_t> huff[20];
+    int huff_of[20];
+    size_t data = 0;
+};
+
+bool lj92_start(const uint8_t* d, size_t n, Lj92Header& h)
+{
+    size_t pos = 0;
+    const auto rd = [&]() -> int { return pos < n ? d[pos++] : (pos++, -1); };
+    for (int c = 0; c < 20; c++) h.huff_of[c] = -1;
+    rd();
+    if (rd() != 0xd8) return false;
+    std::vector<uint8_t> data(0x10000);
+    int tag;
+    do {
+        for (int k = 0; k < 4; k++) {
+            const int b = rd();
+            if (b < 0) return false;
+            data[k] = (uint8_t)b;
+        }
+        tag = data[0] << 8 | data[1];
+        const int len = (data[2] << 8 | data[3]) - 2;
+        if (tag <= 0xff00) return false;
+        for (int got = 0; got < len; got++) {
+            const int b = rd();
+            if (b < 0) { pos--; break; }
+            data[got] = (uint8_t)b;
+        }
+        switch (tag) {
+        case 0xffc3:
+            h.sraw = ((data[7] >> 4) * (data[7] & 15) - 1) & 3;
+            h.algo = tag & 0xff;
+            h.bits = data[0];
+            h.high = data[1] << 8 | data[2];
+            h.wide = data[3] << 8 | data[4];
+            h.clrs = data[5] + h.sraw;
+            break;
+        case 0xffc1:
+        case 0xffc0:
+            h.algo = tag & 0xff;
+            h.bits = data[0];
+            h.high = data[1] << 8 | data[2];
+            h.wide = data[3] << 8 | data[4];
+            h.clrs = data[5] + h.sraw;
+            break;
+        case 0xffc4: {
+            size_t dp = 0;
+            int c;
+            while (dp < (size_t)std::max(len, 0) && ((c = data[dp++]) & -20) == 0) {
+                // make_decoder_ref: counts of lengths 1..16, then the values; 1 + 2^max entries
+                const size_t cnt0 = dp;
+                dp += 16;
+                int max;
+                for (max = 16; max > 0 && data[cnt0 + max - 1] == 0; max--) ;
+                std::vector<uint16_t> t((size_t)1 + ((size_t)1 << max), 0);
+                t[0] = (uint16_t)max;
+                int hh = 1;
+                for (int ln = 1; ln <= max; ln++)
+                    for (int i = 0; i < data[cnt0 + ln - 1]; i++, ++dp)
+                        for (int j = 0; j < 1 << (max - ln); j++)
+                            if (hh <= 1 << max) t[hh++] = (uint16_t)(ln << 8 | (dp < data.size() ? data[dp] : 0));
+                h.huff[c] = t;
+                h.huff_of[c] = c;
+            }
+            break;
+        }
+        case 0xffda:
+            h.psv = data[1 + data[0] * 2];
+            h.bits -= data[3 + data[0] * 2] & 15;
+            break;
+        case 0xffdd:
+            h.restart = data[0] << 8 | data[1];
+            break;
+        }
+    } while (tag != 0xffda);
+    for (int c = 0; c < 19; c++)
+        if (h.huff_of[c + 1] < 0) h.huff_of[c + 1] = h.huff_of[c];
+    h.data = pos;
+    return true;
+}
+
+struct DngPlan {
+    std::vector<unsigned char> parts;       // Lj92Part records
+    std::vector<uint16_t> tables;           // distinct tables, concatenated
+    size_t row_samples = 0;                 // two-row buffers of all parts, in uint16
+    int nparts = 0;
+};
+
+int dng_plan(const uint8_t* file, size_t fsize, const isa_dng_layout* L, int W, int H, DngPlan& plan)
+{
+    plan.nparts = L->n;
+    plan.parts.assign((size_t)L->n * isa_dng_part_bytes(), 0);
+    std::map<std::vector<uint16_t>, int> seen;
+    int row = 0, col = 0;
+    for (int t = 0; t < L->n; t++) {
+        const size_t o = L->offsets[t];
+        const size_t end = std::min<size_t>(fsize, o + (size_t)L->byte_counts[t]);
+        Lj92Header h;
+        const bool ok = o < fsize && lj92_start(file + o, end - o, h) && h.algo == 0xc3;
+        int hdr[7] = {h.bits, h.high, h.wide, h.clrs, h.sraw, h.psv, h.restart};
+        int tab[6] = {0, 0, 0, 0, 0, 0};
+        bool skip = !ok;
+        if (ok) {
+            if (h.clrs < 1 || h.clrs > 6 || h.wide < 1 || h.high < 0 || h.bits < 1 || h.bits > 16 || h.restart <= 0)
+                return fail(ISA_EINVAL, "part %d: unsupported lossless-JPEG header (%d components, %d bits)", t, h.clrs, h.bits);
+            for (int c = 0; c < h.clrs; c++) {
+                const int k = h.huff_of[c];
+                if (k < 0) return fail(ISA_EINVAL, "part %d: no Huffman table for component %d", t, c);
+                auto it = seen.find(h.huff[k]);
+                if (it == seen.end()) {
+                    it = seen.emplace(h.huff[k], (int)plan.tables.size()).first;
+                    plan.tables.insert(plan.tables.end(), h.huff[k].begin(), h.huff[k].end());
+                }
+                tab[c] = it->second;
+            }
+        }
+        const int orow = L->tiled ? row : t * L->rows_per_strip, ocol = L->tiled ? col : 0;
+        const unsigned long long rb = plan.row_samples;
+        if (ok) plan.row_samples += (size_t)2 * h.wide * h.clrs + 8;
+        isa_dng_part_set(plan.parts.data(), t, (unsigned long long)(o + h.data), (unsigned long long)end, skip ? 1 : 0, hdr, orow, ocol, tab, rb);
+        if (L->tiled) {
+            col += L->tile_width;
+            if (col >= W) { col = 0; row += L->tile_height; }
+        }
+    }
+    (void)H;
+    return ISA_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+}  // namespace
+
+int isa_dng_check(const isa_dng_layout* L, int width, int height)
+{
+    ISA_REQ(L && width > 0 && height > 0 && L->n >= 1 && L->offsets && L->byte_counts, "bad DNG layout");
+    ISA_REQ(L->compression == 7 || (L->compression == 1 && !L->tiled), "lossless JPEG tiles/strips or uncompressed strips only");
+    ISA_REQ(!L->tiled || (L->tile_width > 0 && L->tile_height > 0), "tile size");
+    ISA_REQ(L->tiled || L->rows_per_strip > 0, "rows per strip");
+    ISA_REQ(L->compression != 1 || (L->bit_depth >= 1 && L->bit_depth <= 16), "bit depth 1 to 16");
+    ISA_REQ(!L->linearization || L->nlin > 0, "empty linearisation table");
+    return ISA_OK;
+}
+
+size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size, const isa_dng_layout* L, int width, int height)
+{
+    if (!file_host || isa_dng_check(L, width, height) != ISA_OK) return 0;
+    size_t s = align256((size_t)L->n * 16) + align256((size_t)L->n * 8) + align256((size_t)L->n * 8) + align256(64);
+    s += align256((size_t)width * 2) + align256((size_t)height * 2) + align256((size_t)std::max(L->nlin, 1) * 2);
+    if (L->compression == 7) {
+        DngPlan plan;
+        if (dng_plan(file_host, file_size, L, width, height, plan) != ISA_OK) return 0;
+        s += align256(plan.parts.size()) + align256(plan.tables.size() * 2 + 2) + align256(plan.row_samples * 2 + 16);
+    }
+    return s;
+}
+
+int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height,
+                   void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream)
+{
+    ISA_REQ(file_host && file_dev && scratch && out, "NULL argument");
+    ISA_TRY(isa_dng_check(L, width, height));
+    ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
+    const size_t need = isa_dng_decode_scratch(file_host, file_size, L, width, height);
+    if (need == 0) return fail(ISA_EINVAL, "%s", g_err.empty() ? "unsupported DNG layout" : g_err.c_str());
+    ISA_REQ(scratch_bytes >= need, "scratch too small (isa_dng_decode_scratch)");
+    cudaStream_t st = S(stream);
+    char* base = (char*)scratch;
+    size_t o = 0;
+    const auto take = [&](size_t bytes) { char* p = base + o; o += align256(bytes); return p; };
+    take((size_t)L->n * 16);
+    unsigned long long* d_offs = (unsigned long long*)take((size_t)L->n * 8);
+    unsigned long long* d_cnts = (unsigned long long*)take((size_t)L->n * 8);
+    int* d_err = (int*)take(64);
+    uint16_t* d_bh = (uint16_t*)take((size_t)width * 2);
+    uint16_t* d_bv = (uint16_t*)take((size_t)height * 2);
+    uint16_t* d_lin = (uint16_t*)take((size_t)std::max(L->nlin, 1) * 2);
+    std::vector<unsigned long long> offs(L->n), cnts(L->n);
+    for (int i = 0; i < L->n; i++) { offs[i] = L->offsets[i]; cnts[i] = L->byte_counts[i]; }
+    ISA_CK(cudaMemcpyAsync(d_offs, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(d_cnts, cnts.data(), cnts.size() * 8, cudaMemcpyHostToDevice, st));
+    const int err0 = 0x7fffffff;
+    ISA_CK(cudaMemcpyAsync(d_err, &err0, sizeof(int), cudaMemcpyHostToDevice, st));
+    if (L->black_h) ISA_CK(cudaMemcpyAsync(d_bh, L->black_h, (size_t)width * 2, cudaMemcpyHostToDevice, st));
+    if (L->black_v) ISA_CK(cudaMemcpyAsync(d_bv, L->black_v, (size_t)height * 2, cudaMemcpyHostToDevice, st));
+    if (L->linearization) ISA_CK(cudaMemcpyAsync(d_lin, L->linearization, (size_t)L->nlin * 2, cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemset2DAsync(out, out_pitch, 0, (size_t)width * 2, height, st));
+    const void* d_parts = nullptr;
+    const uint16_t* d_tables = nullptr;
+    uint16_t* d_rows = nullptr;
+    int nparts = L->n;
+    DngPlan plan;
+    if (L->compression == 7) {
+        ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));
+        void* p = take(plan.parts.size());
+        uint16_t* tb = (uint16_t*)take(plan.tables.size() * 2 + 2);
+        d_rows = (uint16_t*)take(plan.row_samples * 2 + 16);
+        ISA_CK(cudaMemcpyAsync(p, plan.parts.data(), plan.parts.size(), cudaMemcpyHostToDevice, st));
+        if (!plan.tables.empty()) ISA_CK(cudaMemcpyAsync(tb, plan.tables.data(), plan.tables.size() * 2, cudaMemcpyHostToDevice, st));
+        d_parts = p;
+        d_tables = tb;
+    }
+    ISA_CK(isa_launch_dng(file_dev, file_size, L->compression, d_parts, nparts, d_tables, d_rows, d_offs, d_cnts, L->rows_per_strip, L->bit_depth,
+                          L->linearization ? d_lin : nullptr, L->nlin, L->black_h ? d_bh : nullptr, L->black_v ? d_bv : nullptr, width, height,
+                          L->dng_version_large, out, out_pitch, d_err, st));
+    int err = err0;
+    ISA_CK(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ISA_CK(cudaStreamSynchronize(st));
+    if (err != err0) return fail(ISA_EINVAL, "part %d: a decoded sample exceeds the frame's bit depth (the reference stops there)", err);
+    return ISA_OK;
 }

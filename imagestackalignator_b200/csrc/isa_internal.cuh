@@ -189,3 +189,12 @@ cudaError_t isa_launch_pef_decode(const uint8_t* data, unsigned long long nbytes
 int isa_pef_max_blocks();
 cudaError_t isa_launch_pef_unpack(const uint8_t* file, unsigned long long fsize, const uint32_t* offsets, const uint32_t* sizes, int nstrips,
                                   int rows_per_strip, int W, int H, int depth, uint16_t* out, size_t out_pitch, cudaStream_t st);
+
+// raw.cu: DNG pixel data (isa_dng_decode)
+size_t isa_dng_part_bytes();
+void isa_dng_part_set(void* dst, int i, unsigned long long pos, unsigned long long end, int skip, const int* hdr, int out_row, int out_col,
+                      const int* table, unsigned long long rowbuf);
+cudaError_t isa_launch_dng(const uint8_t* file, unsigned long long fsize, int compression, const void* parts, int nparts, const uint16_t* tables,
+                           uint16_t* rows, const unsigned long long* offs, const unsigned long long* cnts, int rps, int depth, const uint16_t* lin,
+                           int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large, uint16_t* out, size_t out_pitch, int* error,
+                           cudaStream_t st);

@@ -533,3 +533,209 @@ cudaError_t isa_launch_pef_unpack(const uint8_t* file, unsigned long long fsize,
     k_pef_unpack<<<g, b, 0, st>>>(file, fsize, A, rows_per_strip, W, H, depth, out, out_pitch);
     return cudaGetLastError();
 }
+
+// ---- DNG pixel data (DNGFile, PefFile/DNGFile.cs:372-600) ----
+//
+// Lossless-JPEG tiles or strips: one thread per tile / strip decodes its
+// stream sequentially with the reference's reader (dcraw's ljpeg_row,
+// getbithuff and ljpeg_diff: the byte after a 0xFF is skipped, restart
+// markers are searched from two bytes back, predictors 1..7, the first
+// column from vpred), headers parsed and Huffman tables built on the host.
+// Values then pass the linearisation table and the black-level deltas:
+// out = max(0, lin[min(v, n - 1)] - black_h[col] - black_v[row]).
+// Uncompressed strips: one thread per value.
+
+namespace {
+
+struct Lj92Part {
+    unsigned long long pos, end;   // entropy data start and end of the part's bytes in the file
+    int skip;                      // ljpeg_start failed or not a lossless frame: nothing written
+    int bits, high, wide, clrs, sraw, psv, restart;
+    int out_row, out_col;          // where the part's first sample goes
+    int table[6];                  // table offsets (in uint16) per component
+    unsigned long long rowbuf;     // offset (in uint16) of the part's two-row buffer
+};
+
+struct DngArgs {
+    const uint8_t* file;
+    unsigned long long fsize;
+    const Lj92Part* parts;
+    int nparts;
+    const uint16_t* tables;
+    uint16_t* rows;
+    const uint16_t* lin;
+    int nlin;
+    const uint16_t* bh;
+    const uint16_t* bv;
+    int W, H, large;
+    uint16_t* out;
+    size_t out_pitch;
+    int* error;
+};
+
+__device__ __forceinline__ uint16_t dng_value(const DngArgs& A, unsigned v, int row, int col)
+{
+    const int black = (A.bh ? (int)A.bh[col] : 0) + (A.bv ? (int)A.bv[row] : 0);
+    const int x = A.lin ? (int)A.lin[v < (unsigned)A.nlin ? v : (unsigned)(A.nlin - 1)] : (int)v;
+    return (uint16_t)(x - black > 0 ? x - black : 0);
+}
+
+struct DngReader {
+    const uint8_t* d;
+    long long n, pos;
+    unsigned bitbuf;
+    int vbits;
+    __device__ __forceinline__ int byte() { return pos >= 0 && pos < n ? (int)__ldg(d + pos++) : (pos++, -1); }
+    __device__ __forceinline__ unsigned bits(int nbits, const uint16_t* huff)
+    {
+        if (nbits > 25) return 0;
+        if (nbits == 0 || vbits < 0) return 0;
+        while (vbits < nbits) {
+            const int c = byte();
+            if (c == 255) byte();
+            bitbuf = (bitbuf << 8) + (uint8_t)c;
+            vbits += 8;
+        }
+        unsigned c = bitbuf << (32 - vbits) >> (32 - nbits);
+        if (huff) {
+            vbits -= huff[c] >> 8;
+            c = (uint8_t)huff[c];
+        } else {
+            vbits -= nbits;
+        }
+        return c;
+    }
+    __device__ __forceinline__ int diff(const uint16_t* huff, int large)
+    {
+        const int len = (int)bits(huff[0], huff + 1);
+        if (len == 16 && large) return -32768;
+        int d = (int)bits(len, nullptr);
+        if ((d & (int)(1u << ((len - 1) & 31))) == 0) d -= (int)((1u << (len & 31)) - 1);
+        return d;
+    }
+};
+
+__global__ void k_dng_lj92(const DngArgs A)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.nparts) return;
+    const Lj92Part P = A.parts[t];
+    if (P.skip) return;
+    DngReader r{A.file + P.pos, (long long)(P.end - P.pos), 0, 0u, 0};
+    uint16_t* rowbuf = A.rows + P.rowbuf + 4;  // 4 spare samples before the buffer: row[0][-clrs] at column 0 is never read
+    const int jwide = P.wide * P.clrs;
+    int vpred[6];
+    for (int jrow = 0; jrow < P.high; jrow++) {
+        if ((long long)jrow * P.wide % P.restart == 0) {
+            for (int c = 0; c < 6; c++) vpred[c] = 1 << (P.bits - 1);
+            if (jrow > 0) {
+                r.pos -= 2;
+                unsigned short mark = 0;
+                int c;
+                do mark = (unsigned short)((mark << 8) + (c = r.byte()));
+                while (r.pos < r.n - 1 && mark >> 4 != 0xffd);
+            }
+            r.bitbuf = 0;
+            r.vbits = 0;
+        }
+        uint16_t* row0 = rowbuf + (size_t)jwide * (jrow & 1);
+        uint16_t* row1 = rowbuf + (size_t)jwide * ((jrow + 1) & 1);
+        int spred = 0;
+        for (int col = 0; col < P.wide; col++)
+            for (int c = 0; c < P.clrs; c++) {
+                const int d = r.diff(A.tables + P.table[c < 6 ? c : 5], A.large);
+                int pred;
+                if (P.sraw > 0 && c <= P.sraw && (col | c) > 0) pred = spred;
+                else if (col > 0) pred = row0[-P.clrs];
+                else pred = (vpred[c] += d) - d;
+                if (jrow > 0 && col > 0) switch (P.psv) {
+                    case 1: break;
+                    case 2: pred = row1[0]; break;
+                    case 3: pred = row1[-P.clrs]; break;
+                    case 4: pred = pred + row1[0] - row1[-P.clrs]; break;
+                    case 5: pred = pred + ((row1[0] - row1[-P.clrs]) >> 1); break;
+                    case 6: pred = row1[0] + ((pred - row1[-P.clrs]) >> 1); break;
+                    case 7: pred = (pred + row1[0]) >> 1; break;
+                    default: pred = 0; break;
+                    }
+                const uint16_t v = (uint16_t)(pred + d);
+                *row0 = v;
+                if (v >> P.bits) {
+                    atomicMin(A.error, t);
+                    return;
+                }
+                if (c <= P.sraw) spred = v;
+                row0++;
+                row1++;
+            }
+        const uint16_t* rp = rowbuf + (size_t)jwide * (jrow & 1);
+        const int orow = P.out_row + jrow;
+        if (orow >= A.H) continue;
+        uint16_t* o = isa::row_ptr(A.out, A.out_pitch, orow);
+        for (int jcol = 0; jcol < jwide; jcol++) {
+            const int ocol = P.out_col + jcol;
+            if (ocol < A.W) o[ocol] = dng_value(A, rp[jcol], orow, ocol);
+        }
+    }
+}
+
+// Uncompressed strips: 16-bit little-endian samples filling rows strip by
+// strip, or MSB-first samples of `depth` bits with the bit count reset at
+// each strip.
+__global__ void k_dng_plain(const DngArgs A, const unsigned long long* __restrict__ offs, const unsigned long long* __restrict__ cnts, int rps,
+                            int depth)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= A.W || y >= A.H) return;
+    const int s = y / rps, line = y - s * rps;
+    if (s >= A.nparts) return;
+    const unsigned long long v = (unsigned long long)line * A.W + x;
+    unsigned val;
+    if (depth == 16) {
+        if (2 * v + 1 >= cnts[s]) return;  // the strip holds data.Length / 2 samples
+        const unsigned long long b = offs[s] + 2 * v;
+        const unsigned lo = b < A.fsize ? __ldg(A.file + b) : 0u, hi = b + 1 < A.fsize ? __ldg(A.file + b + 1) : 0u;
+        val = lo | hi << 8;
+    } else {
+        const unsigned long long bit = v * depth;
+        unsigned long long acc = 0;
+        for (unsigned long long q = bit >> 3; q <= (bit + depth - 1) >> 3; q++) {
+            const unsigned long long b = offs[s] + q;
+            acc = (acc << 8) | ((q < cnts[s] && b < A.fsize) ? __ldg(A.file + b) : 0u);
+        }
+        const unsigned long long nb = (((bit + depth - 1) >> 3) - (bit >> 3) + 1) * 8;
+        val = (unsigned)((acc >> (nb - (bit & 7) - depth)) & ((1ull << depth) - 1));
+    }
+    isa::row_ptr(A.out, A.out_pitch, y)[x] = dng_value(A, val, y, x);
+}
+
+}  // namespace
+
+size_t isa_dng_part_bytes() { return sizeof(Lj92Part); }
+
+void isa_dng_part_set(void* dst, int i, unsigned long long pos, unsigned long long end, int skip, const int* hdr, int out_row, int out_col,
+                      const int* table, unsigned long long rowbuf)
+{
+    Lj92Part P{};
+    P.pos = pos; P.end = end; P.skip = skip;
+    P.bits = hdr[0]; P.high = hdr[1]; P.wide = hdr[2]; P.clrs = hdr[3]; P.sraw = hdr[4]; P.psv = hdr[5]; P.restart = hdr[6];
+    P.out_row = out_row; P.out_col = out_col;
+    for (int c = 0; c < 6; c++) P.table[c] = table[c];
+    P.rowbuf = rowbuf;
+    ((Lj92Part*)dst)[i] = P;
+}
+
+cudaError_t isa_launch_dng(const uint8_t* file, unsigned long long fsize, int compression, const void* parts, int nparts, const uint16_t* tables,
+                           uint16_t* rows, const unsigned long long* offs, const unsigned long long* cnts, int rps, int depth, const uint16_t* lin,
+                           int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large, uint16_t* out, size_t out_pitch, int* error,
+                           cudaStream_t st)
+{
+    DngArgs A{file, fsize, (const Lj92Part*)parts, nparts, tables, rows, lin, nlin, bh, bv, W, H, large, out, out_pitch, error};
+    if (compression == 7) {
+        k_dng_lj92<<<(nparts + 63) / 64, 64, 0, st>>>(A);
+    } else {
+        dim3 g((W + 255) / 256, H);
+        k_dng_plain<<<g, 256, 0, st>>>(A, offs, cnts, rps, depth);
+    }
+    return cudaGetLastError();
+}

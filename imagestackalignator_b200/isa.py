@@ -76,7 +76,7 @@ EXPORTS = [
     "isa_robustness_erode", "isa_structure_tensor", "isa_kernel_param", "isa_accumulate", "isa_apply_weighting",
     "isa_color_twists", "isa_postprocess", "isa_save_tiff16", "isa_save_as_16bit_tiff",
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
-    "isa_dng_color_spec", "isa_pef_color_spec",
+    "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
 ]
 
 _lib = None
@@ -100,6 +100,7 @@ def lib():
                 f.restype = ctypes.c_int
         L.isa_launch_count.restype = ctypes.c_long
         L.isa_pef_decode_scratch.restype = ctypes.c_size_t
+        L.isa_dng_decode_scratch.restype = ctypes.c_size_t
         _lib = L
     return _lib
 
@@ -463,6 +464,39 @@ def pef_color_spec(white_balance):
     check(lib().isa_pef_color_spec(wb.ctypes.data_as(ctypes.c_void_p), c2p.ctypes.data_as(ctypes.c_void_p), cw.ctypes.data_as(ctypes.c_void_p),
                                    xy.ctypes.data_as(ctypes.c_void_p)))
     return c2p.reshape(3, 3), cw, xy
+
+
+class IsaDngLayout(ctypes.Structure):
+    _fields_ = [("tiled", ctypes.c_int), ("tile_width", ctypes.c_int), ("tile_height", ctypes.c_int), ("rows_per_strip", ctypes.c_int),
+                ("n", ctypes.c_int), ("offsets", ctypes.c_void_p), ("byte_counts", ctypes.c_void_p), ("compression", ctypes.c_int),
+                ("bit_depth", ctypes.c_int), ("dng_version_large", ctypes.c_int), ("linearization", ctypes.c_void_p), ("nlin", ctypes.c_int),
+                ("black_h", ctypes.c_void_p), ("black_v", ctypes.c_void_p)]
+
+
+def dng_decode(file, width, height, offsets, counts, compression=7, tiled=True, tile_w=0, tile_h=0, rows_per_strip=0, bit_depth=16, large=True,
+               linearization=None, black_h=None, black_v=None, file_dev=None, stream=None):
+    """isa_dng_decode of a DNG file image (host uint8 array; copied to the
+    device unless file_dev is given); returns the frame (int16 tensor holding uint16)."""
+    import torch
+    f = np.ascontiguousarray(file, np.uint8)
+    keep = [np.ascontiguousarray(offsets, np.uint32), np.ascontiguousarray(counts, np.uint32)]
+    lin = None if linearization is None else np.ascontiguousarray(linearization, np.uint16)
+    bh = None if black_h is None else np.ascontiguousarray(black_h, np.uint16)
+    bv = None if black_v is None else np.ascontiguousarray(black_v, np.uint16)
+    keep += [lin, bh, bv]
+    L = IsaDngLayout(int(tiled), tile_w, tile_h, rows_per_strip, len(keep[0]), keep[0].ctypes.data, keep[1].ctypes.data, compression, bit_depth,
+                     int(large), None if lin is None else lin.ctypes.data, 0 if lin is None else lin.size,
+                     None if bh is None else bh.ctypes.data, None if bv is None else bv.ctypes.data)
+    fp = f.ctypes.data_as(ctypes.c_void_p)
+    need = lib().isa_dng_decode_scratch(fp, ctypes.c_size_t(f.size), ctypes.byref(L), width, height)
+    if need == 0:
+        raise IsaError(ISA_EINVAL, lib().isa_last_error().decode())
+    dev = file_dev if file_dev is not None else torch.from_numpy(f).cuda()
+    scratch = torch.empty(need, dtype=torch.uint8, device=dev.device)
+    out = torch.empty((height, width), dtype=torch.int16, device=dev.device)
+    check(lib().isa_dng_decode(fp, vp(dev), ctypes.c_size_t(f.size), ctypes.byref(L), width, height, vp(scratch), ctypes.c_size_t(need), vp(out),
+                               ctypes.c_size_t(width * 2), stream_ptr(stream)))
+    return out
 
 
 class IsaBurst(ctypes.Structure):

@@ -225,3 +225,99 @@ def pef_stream(img, code, lens):
     words[w[first]] |= np.bitwise_or.reduceat(hi, first)
     words[w[first] + 1] |= np.bitwise_or.reduceat(lo, first)
     return np.frombuffer(words.astype(">u4").tobytes(), np.uint8)[: (total + 7) // 8].copy()
+
+
+# ---- Lossless-JPEG (DNG) tiles, inputs for isa_dng_decode ----
+
+LJ92_CODE_LENGTHS = (2, 3, 3, 3, 3, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13)
+
+
+def _bits_to_bytes(field, flen):
+    """Concatenate MSB-first bit fields (each at most 26 bits) into bytes, the last one padded with ones."""
+    field = np.asarray(field, np.int64)
+    flen = np.asarray(flen, np.int64)
+    start = np.concatenate([[0], np.cumsum(flen)[:-1]])
+    total = int(start[-1] + flen[-1]) if len(flen) else 0
+    pad = (-total) % 8
+    if pad:
+        field = np.concatenate([field, [(1 << pad) - 1]])
+        flen = np.concatenate([flen, [pad]])
+        start = np.concatenate([start, [total]])
+        total += pad
+    w = start >> 5
+    val = (field << (64 - (start & 31) - flen)).astype(np.uint64)
+    hi = val >> np.uint64(32)
+    lo = val & np.uint64(0xFFFFFFFF)
+    words = np.zeros(int(w[-1]) + 2, np.uint64)
+    first = np.concatenate([[0], np.flatnonzero(np.diff(w)) + 1])
+    words[w[first]] |= np.bitwise_or.reduceat(hi, first)
+    words[w[first] + 1] |= np.bitwise_or.reduceat(lo, first)
+    return np.frombuffer(words.astype(">u4").tobytes(), np.uint8)[: total // 8].copy()
+
+
+def lj92_tile(img, clrs=2, bits=14, lengths=LJ92_CODE_LENGTHS):
+    """One lossless-JPEG tile (predictor 1, one Huffman table for all
+    components, no restart interval) of a uint16 high x (wide * clrs) block
+    whose components are interleaved, in the layout DNGFile's reader
+    (PefFile/DNGFile.cs:94-285) decodes."""
+    v = np.asarray(img, np.int64)
+    high, W = v.shape
+    wide = W // clrs
+    pred = np.empty_like(v)
+    pred[:, clrs:] = v[:, :-clrs]                       # left sample of the same component
+    pred[0, :clrs] = 1 << (bits - 1)                     # vpred at the first row
+    pred[1:, :clrs] = v[:-1, :clrs]                      # the first column from the row above
+    d = (v - pred) & 0xFFFF
+    d = np.where(d >= 32768, d - 65536, d).reshape(-1)
+    mag = np.abs(d)
+    ssss = np.zeros(mag.shape, np.int64)
+    while True:
+        m = (mag >> ssss) != 0
+        if not m.any():
+            break
+        ssss += m
+    lens = np.asarray(lengths, np.int64)
+    if ssss.max() >= len(lens):
+        raise ValueError("difference outside the code book")
+    code = np.zeros(len(lens), np.int64)
+    c = 0
+    for ln in range(1, 17):
+        for k in range(len(lens)):
+            if lens[k] == ln:
+                code[k] = c
+                c += 1
+        c <<= 1
+    clen = lens[ssss]
+    dbits = np.where(d >= 0, d, d - 1) & ((np.int64(1) << ssss) - 1)
+    data = _bits_to_bytes((code[ssss] << ssss) | dbits, clen + ssss)
+    stuffed = np.insert(data, np.flatnonzero(data == 0xFF) + 1, 0)   # a zero byte after every 0xFF
+    counts = [int((lens == ln).sum()) for ln in range(1, 17)]
+    values = [k for ln in range(1, 17) for k in range(len(lens)) if lens[k] == ln]
+    hdr = bytearray([0xFF, 0xD8, 0xFF, 0xC3, 0, 8 + 3 * clrs, bits, high >> 8, high & 255, wide >> 8, wide & 255, clrs])
+    for c in range(clrs):
+        hdr += bytes([c + 1, 0x11, 0])
+    hdr += bytes([0xFF, 0xC4, 0, 3 + 16 + len(values), 0x00]) + bytes(counts) + bytes(values)
+    hdr += bytes([0xFF, 0xDA, 0, 6 + 2 * clrs, clrs])
+    for c in range(clrs):
+        hdr += bytes([c + 1, 0x00])
+    hdr += bytes([1, 0, 0])
+    return np.concatenate([np.frombuffer(bytes(hdr), np.uint8), stuffed, np.array([0xFF, 0xD9], np.uint8)])
+
+
+def dng_tiled_file(img, tile_w=256, tile_h=256, clrs=2, bits=14, head=64):
+    """A file image holding `img` as lossless-JPEG tiles in row-major order
+    after `head` bytes: (file, offsets, byte counts)."""
+    H, W = img.shape
+    parts = [np.zeros(head, np.uint8)]
+    offs, cnts, pos = [], [], head
+    for ty in range(0, H, tile_h):
+        for tx in range(0, W, tile_w):
+            t = np.zeros((tile_h, tile_w), np.uint16)
+            blk = img[ty:ty + tile_h, tx:tx + tile_w]
+            t[: blk.shape[0], : blk.shape[1]] = blk
+            s = lj92_tile(t, clrs, bits)
+            offs.append(pos)
+            cnts.append(len(s))
+            parts.append(s)
+            pos += len(s)
+    return np.concatenate(parts), offs, cnts

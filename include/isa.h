@@ -464,6 +464,38 @@ ISA_API int isa_dng_color_spec(const isa_dng_color_tags* tags, double camera_to_
  * balance (isa_pef_levels' white_balance). */
 ISA_API int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
 
+/* ---- Raw decoding of DNG frames ----
+ * The pixel data of DNGFile (PefFile/DNGFile.cs:372-600): lossless-JPEG
+ * (compression 7) tiles or strips, decoded with the reference's dcraw
+ * reader (predictors 1..7, restart markers, 0xFF byte skipping), or
+ * uncompressed strips (compression 1: 16-bit little-endian samples, or
+ * packed MSB-first samples of bit_depth bits); then the linearisation
+ * table and the black-level deltas: out = max(0, lin[min(v, nlin - 1)] -
+ * black_h[col] - black_v[row]). Lossless-JPEG headers are parsed from
+ * `file_host`; the data is read from `file_dev` (the same bytes on the
+ * device) by one thread per tile. */
+typedef struct isa_dng_layout {
+    int tiled;                       /* 1: TileWidth/TileLength/TileOffsets/TileByteCounts; 0: strips */
+    int tile_width, tile_height;     /* tiles */
+    int rows_per_strip;              /* strips */
+    int n;                           /* tiles or strips */
+    const uint32_t* offsets;         /* host: n byte offsets in the file */
+    const uint32_t* byte_counts;     /* host: n byte counts */
+    int compression;                 /* 7 = lossless JPEG, 1 = none (strips only) */
+    int bit_depth;                   /* BitsPerSample of uncompressed strips */
+    int dng_version_large;           /* DNGVersion absent or its second byte > 1 (a category-16 code means -32768) */
+    const uint16_t* linearization;   /* host LinearizationTable or NULL */
+    int nlin;
+    const uint16_t* black_h;         /* host, width entries: BlackLevelDeltaH placed in the active area, or NULL */
+    const uint16_t* black_v;         /* host, height entries: BlackLevelDeltaV, or NULL */
+} isa_dng_layout;
+ISA_API size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size, const isa_dng_layout* layout, int width, int height);
+/* Decodes into `out` (device, uint16 width x height; pixels no part covers
+ * are 0) and synchronises `stream`; ISA_EINVAL where the reference would
+ * stop (a sample above the frame's bit depth). */
+ISA_API int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* layout, int width, int height,
+                           void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

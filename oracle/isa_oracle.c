@@ -983,3 +983,352 @@ EXPORT long orc_pef_encode(const uint16_t* img, int W, int H, const uint16_t* co
 #undef PUT
     return (long)w;
 }
+
+/* ---- Raw decoding (DNG) ----
+ * The lossless-JPEG reader of DNGFile (PefFile/DNGFile.cs:40-285, dcraw's
+ * ljpeg_start / ljpeg_row / getbithuff / ljpeg_diff) and the tile / strip
+ * assembly with black-level deltas and linearisation (:323-600). A stream
+ * is a byte range; ReadByte past its end gives -1. */
+typedef struct {
+    const uint8_t* d;
+    long n, pos;
+    uint32_t bitbuf;
+    int vbits;
+} orc_mstream;
+
+static int ms_byte(orc_mstream* s) { return s->pos >= 0 && s->pos < s->n ? s->d[s->pos++] : (s->pos++, -1); }
+
+typedef struct {
+    int algo, bits, high, wide, clrs, sraw, psv, restart;
+    int vpred[6];
+    uint16_t* huff[20];
+    uint16_t* own[20];
+} orc_jhead;
+
+/* make_decoder_ref (DNGFile.cs:73-92): the 1 + 2^max lookup table. */
+static uint16_t* orc_make_decoder(const uint8_t** source, const uint8_t* end)
+{
+    const uint8_t* count = (*source += 16) - 17;
+    int max;
+    for (max = 16; max > 0 && count[max] == 0; max--) ;
+    uint16_t* huff = (uint16_t*)calloc((size_t)1 + ((size_t)1 << max), sizeof(uint16_t));
+    huff[0] = (uint16_t)max;
+    int h = 1;
+    for (int len = 1; len <= max; len++)
+        for (int i = 0; i < count[len]; i++, ++*source)
+            for (int j = 0; j < 1 << (max - len); j++)
+                if (h <= 1 << max) huff[h++] = (uint16_t)(len << 8 | (*source < end ? **source : 0));
+    return huff;
+}
+
+static void orc_jhead_free(orc_jhead* jh)
+{
+    for (int c = 0; c < 20; c++) free(jh->own[c]);
+}
+
+/* ljpeg_start (DNGFile.cs:94-170). Returns 1 and leaves s at the entropy data, or 0. */
+static int orc_ljpeg_start(orc_jhead* jh, orc_mstream* s)
+{
+    static uint8_t data[0x10000];
+    memset(jh, 0, sizeof(*jh));
+    jh->restart = 0x7fffffff;
+    ms_byte(s);
+    if (ms_byte(s) != 0xd8) return 0;
+    int tag;
+    do {
+        for (int k = 0; k < 4; k++) {
+            const int b = ms_byte(s);
+            if (b < 0) return 0;
+            data[k] = (uint8_t)b;
+        }
+        tag = data[0] << 8 | data[1];
+        const int len = (data[2] << 8 | data[3]) - 2;
+        if (tag <= 0xff00) return 0;
+        int got = 0;
+        for (; got < len; got++) {
+            const int b = ms_byte(s);
+            if (b < 0) { s->pos--; break; }
+            data[got] = (uint8_t)b;
+        }
+        switch (tag) {
+        case 0xffc3:
+            jh->sraw = ((data[7] >> 4) * (data[7] & 15) - 1) & 3;
+            jh->algo = tag & 0xff;
+            jh->bits = data[0];
+            jh->high = data[1] << 8 | data[2];
+            jh->wide = data[3] << 8 | data[4];
+            jh->clrs = data[5] + jh->sraw;
+            break;
+        case 0xffc1:
+        case 0xffc0:
+            jh->algo = tag & 0xff;
+            jh->bits = data[0];
+            jh->high = data[1] << 8 | data[2];
+            jh->wide = data[3] << 8 | data[4];
+            jh->clrs = data[5] + jh->sraw;
+            break;
+        case 0xffc4: {
+            const uint8_t* dp = data;
+            int c;
+            while (dp < data + len && ((c = *dp++) & -20) == 0) {
+                free(jh->own[c]);
+                jh->own[c] = jh->huff[c] = orc_make_decoder(&dp, data + len);
+            }
+            break;
+        }
+        case 0xffda:
+            jh->psv = data[1 + data[0] * 2];
+            jh->bits -= data[3 + data[0] * 2] & 15;
+            break;
+        case 0xffdd:
+            jh->restart = data[0] << 8 | data[1];
+            break;
+        }
+    } while (tag != 0xffda);
+    for (int c = 0; c < 19; c++)
+        if (!jh->huff[c + 1]) jh->huff[c + 1] = jh->huff[c];
+    return 1;
+}
+
+/* getbithuff of DNGFile (:234-268): the byte after a 0xFF is skipped; past the end 0xFF bytes. */
+static uint32_t orc_dng_bits(orc_mstream* s, int nbits, const uint16_t* huff)
+{
+    if (nbits > 25) return 0;
+    if (nbits < 0) { s->vbits = 0; s->bitbuf = 0; return 0; }
+    if (nbits == 0 || s->vbits < 0) return 0;
+    while (s->vbits < nbits) {
+        const int c = ms_byte(s);
+        if (c == 255) ms_byte(s);
+        s->bitbuf = (s->bitbuf << 8) + (uint8_t)c;
+        s->vbits += 8;
+    }
+    uint32_t c = s->bitbuf << (32 - s->vbits) >> (32 - nbits);
+    if (huff) {
+        s->vbits -= huff[c] >> 8;
+        c = (uint8_t)huff[c];
+    } else {
+        s->vbits -= nbits;
+    }
+    return c;
+}
+
+static int orc_ljpeg_diff(orc_mstream* s, const uint16_t* huff, int large)
+{
+    const int len = (int)orc_dng_bits(s, huff[0], huff + 1);
+    if (len == 16 && large) return -32768;
+    int diff = (int)orc_dng_bits(s, len, NULL);
+    if ((diff & (int)(1u << ((len - 1) & 31))) == 0) diff -= (int)((1u << (len & 31)) - 1);
+    return diff;
+}
+
+/* ljpeg_row (DNGFile.cs:173-228) into rowbuf (2 rows of wide * clrs). Returns the row or NULL. */
+static uint16_t* orc_ljpeg_row(orc_jhead* jh, orc_mstream* s, int jrow, uint16_t* rowbuf, int large)
+{
+    if ((long)jrow * jh->wide % jh->restart == 0) {
+        for (int c = 0; c < 6; c++) jh->vpred[c] = 1 << (jh->bits - 1);
+        if (jrow > 0) {
+            s->pos -= 2;
+            uint16_t mark = 0;
+            int c;
+            do mark = (uint16_t)((mark << 8) + (c = ms_byte(s)));
+            while (s->pos < s->n - 1 && mark >> 4 != 0xffd);
+        }
+        orc_dng_bits(s, -1, NULL);
+    }
+    uint16_t* row[3];
+    for (int c = 0; c < 3; c++) row[c] = rowbuf + (size_t)jh->wide * jh->clrs * ((jrow + c) & 1);
+    int spred = 0;
+    for (int col = 0; col < jh->wide; col++)
+        for (int c = 0; c < jh->clrs; c++) {
+            const int diff = orc_ljpeg_diff(s, jh->huff[c], large);
+            int pred;
+            if (jh->sraw > 0 && c <= jh->sraw && (col | c) > 0) pred = spred;
+            else if (col > 0) pred = row[0][-jh->clrs];
+            else pred = (jh->vpred[c] += diff) - diff;
+            if (jrow > 0 && col > 0) switch (jh->psv) {
+                case 1: break;
+                case 2: pred = row[1][0]; break;
+                case 3: pred = row[1][-jh->clrs]; break;
+                case 4: pred = pred + row[1][0] - row[1][-jh->clrs]; break;
+                case 5: pred = pred + ((row[1][0] - row[1][-jh->clrs]) >> 1); break;
+                case 6: pred = row[1][0] + ((pred - row[1][-jh->clrs]) >> 1); break;
+                case 7: pred = (pred + row[1][0]) >> 1; break;
+                default: pred = 0; break;
+                }
+            if ((*row[0] = (uint16_t)(pred + diff)) >> jh->bits) return NULL;
+            if (c <= jh->sraw) spred = *row[0];
+            row[0]++; row[1]++;
+        }
+    return row[2];
+}
+
+static inline uint16_t orc_dng_value(unsigned v, int row, int col, const uint16_t* lin, int nlin, const uint16_t* bh, const uint16_t* bv)
+{
+    const int black = (bh ? bh[col] : 0) + (bv ? bv[row] : 0);
+    const int x = lin ? (int)lin[v < (unsigned)nlin ? v : (unsigned)(nlin - 1)] : (int)v;
+    return (uint16_t)(x - black > 0 ? x - black : 0);
+}
+
+/* DNGFile pixel data (:372-600). compression 7 = lossless JPEG, 1 = none.
+ * tiled: tiles of tw x th in row-major tile order; else strips of rps rows.
+ * Returns 0, or -1 where the reference would stop with an exception. */
+EXPORT int orc_dng_decode(const uint8_t* file, size_t file_size, int tiled, int tw, int th, int rps, int nparts, const uint32_t* offsets,
+                          const uint32_t* counts, int compression, int bit_depth, int large, const uint16_t* lin, int nlin,
+                          const uint16_t* bh, const uint16_t* bv, int W, int H, uint16_t* out)
+{
+    memset(out, 0, (size_t)W * H * 2);
+    int row = 0, col = 0;
+    for (int t = 0; t < nparts; t++) {
+        const long o = offsets[t];
+        const long n = (o + (long)counts[t] <= (long)file_size) ? (long)counts[t] : (o < (long)file_size ? (long)file_size - o : 0);
+        if (compression == 7) {
+            orc_mstream s = {file + o, n, 0, 0, 0};
+            orc_jhead jh;
+            int ret = orc_ljpeg_start(&jh, &s);
+            if (ret > 0 && jh.algo == 0xc3) {
+                const int jwide = jh.wide * jh.clrs;
+                uint16_t* rowbuf = (uint16_t*)calloc((size_t)jh.wide * jh.clrs * 2 + 8, sizeof(uint16_t));
+                for (int jrow = 0; jrow < jh.high; jrow++) {
+                    const uint16_t* rp = orc_ljpeg_row(&jh, &s, jrow, rowbuf + 4, large);
+                    if (!rp) { free(rowbuf); orc_jhead_free(&jh); return -1; }
+                    for (int jcol = 0; jcol < jwide; jcol++) {
+                        const int r = tiled ? row + jrow : t * rps + jrow, c = tiled ? col + jcol : jcol;
+                        if (c < W && r < H) out[(size_t)r * W + c] = orc_dng_value(rp[jcol], r, c, lin, nlin, bh, bv);
+                    }
+                }
+                free(rowbuf);
+            }
+            orc_jhead_free(&jh);
+            if (tiled) {
+                col += tw;
+                if (col >= W) { col = 0; row += th; }
+            }
+        } else if (compression == 1 && !tiled) {
+            const uint8_t* d = file + o;
+            if (bit_depth == 16) {
+                for (long p = 0; p < n / 2; p++) {
+                    const int r = t * rps + (int)(p / W), c = (int)(p % W);
+                    if (r >= H) return -1;
+                    out[(size_t)r * W + c] = orc_dng_value((unsigned)(d[2 * p] | d[2 * p + 1] << 8), r, c, lin, nlin, bh, bv);
+                }
+            } else if (bit_depth < 16) {
+                uint32_t bitbuf = 0;
+                int offset = 0;
+                long pos = 0;
+                for (int line = 0; line < rps; line++)
+                    for (int px = 0; px < W; px++) {
+                        const int r = t * rps + line;
+                        while (offset < bit_depth) {
+                            const uint32_t v = pos < n ? d[pos] : 0;
+                            bitbuf = (bitbuf << 8) + v;
+                            offset += 8;
+                            pos++;
+                        }
+                        const uint32_t v = bitbuf << (32 - offset) >> (32 - bit_depth);
+                        offset -= bit_depth;
+                        if (r >= H) continue;
+                        out[(size_t)r * W + px] = orc_dng_value(v, r, px, lin, nlin, bh, bv);
+                    }
+            }
+        } else {
+            return -1;
+        }
+    }
+    return 0;
+}
+
+/* Test-tile synthesis (the reference only decodes): one lossless-JPEG tile
+ * of `wide` x `high` samples with `clrs` components (interleaved), one DC
+ * table of the given code lengths per category for all components,
+ * predictor psv, optional restart interval (in MCUs, a multiple of wide),
+ * with byte stuffing and RSTn markers. Returns bytes written or -1. */
+EXPORT long orc_lj92_encode(const uint16_t* img, int wide, int high, int clrs, int bits, int psv, int restart, const uint8_t* lens, int ncat,
+                            uint8_t* out, size_t cap)
+{
+    size_t w = 0;
+#define OUTB(b) do { if (w >= cap) return -1; out[w++] = (uint8_t)(b); } while (0)
+    /* canonical codes from the lengths */
+    uint16_t code[17];
+    {
+        int c = 0;
+        for (int len = 1; len <= 16; len++) {
+            for (int k = 0; k < ncat; k++)
+                if (lens[k] == len) code[k] = (uint16_t)c++;
+            c <<= 1;
+        }
+    }
+    OUTB(0xFF); OUTB(0xD8);
+    /* SOF3 */
+    OUTB(0xFF); OUTB(0xC3);
+    const int lsof = 8 + 3 * clrs;
+    OUTB(lsof >> 8); OUTB(lsof & 255); OUTB(bits); OUTB(high >> 8); OUTB(high & 255); OUTB(wide >> 8); OUTB(wide & 255); OUTB(clrs);
+    for (int c = 0; c < clrs; c++) { OUTB(c + 1); OUTB(0x11); OUTB(0); }
+    /* DHT: table 0 */
+    int nv = 0;
+    for (int k = 0; k < ncat; k++) nv += lens[k] > 0;
+    OUTB(0xFF); OUTB(0xC4);
+    const int ldht = 2 + 1 + 16 + nv;
+    OUTB(ldht >> 8); OUTB(ldht & 255); OUTB(0x00);
+    for (int len = 1; len <= 16; len++) {
+        int cnt = 0;
+        for (int k = 0; k < ncat; k++) cnt += lens[k] == len;
+        OUTB(cnt);
+    }
+    for (int len = 1; len <= 16; len++)
+        for (int k = 0; k < ncat; k++)
+            if (lens[k] == len) OUTB(k);
+    if (restart > 0) { OUTB(0xFF); OUTB(0xDD); OUTB(0); OUTB(4); OUTB(restart >> 8); OUTB(restart & 255); }
+    /* SOS */
+    OUTB(0xFF); OUTB(0xDA);
+    const int lsos = 6 + 2 * clrs;
+    OUTB(lsos >> 8); OUTB(lsos & 255); OUTB(clrs);
+    for (int c = 0; c < clrs; c++) { OUTB(c + 1); OUTB(0x00); }
+    OUTB(psv); OUTB(0); OUTB(0);
+    uint64_t acc = 0;
+    int nacc = 0, rst = 0;
+#define PUTBITS(v, nb) do { acc = (acc << (nb)) | ((uint64_t)(v) & ((1ull << (nb)) - 1)); nacc += (nb); \
+        while (nacc >= 8) { const uint8_t b_ = (uint8_t)(acc >> (nacc - 8)); nacc -= 8; OUTB(b_); if (b_ == 0xFF) OUTB(0x00); } } while (0)
+#define FLUSH() do { if (nacc > 0) { const int pad_ = 8 - nacc; PUTBITS((1u << pad_) - 1, pad_); } } while (0)
+    const int W = wide * clrs;
+    for (int r = 0; r < high; r++) {
+        if (restart > 0 && r > 0 && ((long)r * wide) % restart == 0) {
+            FLUSH();
+            OUTB(0xFF); OUTB(0xD0 + (rst & 7));
+            rst++;
+        }
+        const int fresh = restart > 0 ? ((long)r * wide) % restart == 0 : r == 0;
+        for (int col = 0; col < wide; col++)
+            for (int c = 0; c < clrs; c++) {
+                const int x = img[(size_t)r * W + col * clrs + c];
+                int pred;
+                const int left = col > 0 ? img[(size_t)r * W + (col - 1) * clrs + c] : 0;
+                const int up = r > 0 ? img[(size_t)(r - 1) * W + col * clrs + c] : 0;
+                const int ul = (r > 0 && col > 0) ? img[(size_t)(r - 1) * W + (col - 1) * clrs + c] : 0;
+                if (col == 0) pred = fresh ? 1 << (bits - 1) : up;   /* vpred: reset at restarts */
+                else pred = left;
+                if (r > 0 && col > 0) switch (psv) {                     /* the previous row survives restarts */
+                    case 1: break;
+                    case 2: pred = up; break;
+                    case 3: pred = ul; break;
+                    case 4: pred = left + up - ul; break;
+                    case 5: pred = left + ((up - ul) >> 1); break;
+                    case 6: pred = up + ((left - ul) >> 1); break;
+                    case 7: pred = (left + up) >> 1; break;
+                    default: pred = 0; break;
+                    }
+                int diff = (x - pred) & 0xFFFF;
+                if (diff >= 32768) diff -= 65536;
+                int ssss = 0;
+                while ((abs(diff) >> ssss) != 0) ssss++;
+                if (ssss >= ncat || lens[ssss] == 0) return -1;
+                PUTBITS(code[ssss], lens[ssss]);
+                if (ssss > 0) PUTBITS(diff >= 0 ? diff : diff - 1, ssss);
+            }
+    }
+    FLUSH();
+    OUTB(0xFF); OUTB(0xD9);
+#undef PUTBITS
+#undef FLUSH
+#undef OUTB
+    return (long)w;
+}

@@ -127,3 +127,59 @@ def levels(bayer, black_point, white_level, white_point, scaling, bit_depth):
     s = np.float32(scaling)
     wb = [np.float32(np.float32(white_point[0]) / s), np.float32(np.float32(white_point[1]) / s), np.float32(np.float32(white_point[3]) / s)]
     return black, white, wb
+
+
+# ---- DNG (lossless JPEG tiles / strips, uncompressed strips) ----
+
+def lj92_encode(img, clrs=1, bits=14, psv=1, restart=0, lens=(2, 3, 3, 3, 3, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13)):
+    """A lossless-JPEG tile (SOI, SOF3, DHT, DRI, SOS, data, EOI) of img (high x wide*clrs, interleaved components)."""
+    img = np.ascontiguousarray(img, np.uint16)
+    high, W = img.shape
+    wide = W // clrs
+    L = lib()
+    L.orc_lj92_encode.restype = ctypes.c_long
+    cap = img.size * 5 + 1024
+    out = np.zeros(cap, np.uint8)
+    ln = np.ascontiguousarray(lens, np.uint8)
+    n = L.orc_lj92_encode(_p(img), wide, high, clrs, bits, psv, restart, _p(ln), len(ln), _p(out), ctypes.c_size_t(cap))
+    if n < 0:
+        raise ValueError("difference outside the code book")
+    return out[:n].copy()
+
+
+def dng_decode(file, W, H, offsets, counts, compression=7, tiled=True, tile_w=0, tile_h=0, rows_per_strip=0, bit_depth=16, large=True,
+               linearization=None, black_h=None, black_v=None):
+    """DNGFile pixel data of a file image (uint8): returns (status, uint16 H x W)."""
+    f = np.ascontiguousarray(file, np.uint8)
+    off = np.ascontiguousarray(offsets, np.uint32)
+    cnt = np.ascontiguousarray(counts, np.uint32)
+    lin = None if linearization is None else np.ascontiguousarray(linearization, np.uint16)
+    bh = None if black_h is None else np.ascontiguousarray(black_h, np.uint16)
+    bv = None if black_v is None else np.ascontiguousarray(black_v, np.uint16)
+    out = np.zeros((H, W), np.uint16)
+    L = lib()
+    L.orc_dng_decode.restype = ctypes.c_int
+    st = L.orc_dng_decode(_p(f), ctypes.c_size_t(f.size), int(tiled), tile_w, tile_h, rows_per_strip, len(off), _p(off), _p(cnt), compression,
+                          bit_depth, int(large), None if lin is None else _p(lin), 0 if lin is None else lin.size,
+                          None if bh is None else _p(bh), None if bv is None else _p(bv), W, H, _p(out))
+    return st, out
+
+
+def dng_tiles(img, tile_w, tile_h, clrs=1, bits=14, psv=1, restart=0, head=32):
+    """A file image with the frame cut into lossless-JPEG tiles (tile_w pixels = tile_w / clrs samples of clrs components),
+    tiles in row-major order after `head` bytes; returns (file, offsets, counts)."""
+    H, W = img.shape
+    parts = [np.full(head, 0x42, np.uint8)]
+    offs, cnts = [], []
+    pos = head
+    for ty in range(0, H, tile_h):
+        for tx in range(0, W, tile_w):
+            t = np.zeros((tile_h, tile_w), np.uint16)
+            blk = img[ty:ty + tile_h, tx:tx + tile_w]
+            t[:blk.shape[0], :blk.shape[1]] = blk
+            s = lj92_encode(t, clrs, bits, psv, restart)
+            offs.append(pos)
+            cnts.append(len(s))
+            parts.append(s)
+            pos += len(s)
+    return np.concatenate(parts), offs, cnts

@@ -103,3 +103,29 @@ def test_pef_argument_checks():
     assert lib.isa_pef_unpack(fake, ctypes.c_size_t(10), p(off), p(sz), 1, 4, 8, 8, 12, fake, ctypes.c_size_t(16), None) == isa.ISA_EINVAL
     assert lib.isa_pef_unpack(fake, ctypes.c_size_t(10), p(off), p(sz), 1, 8, 8, 8, 17, fake, ctypes.c_size_t(16), None) == isa.ISA_EINVAL
     assert lib.isa_pef_huff_table(p(np.zeros(4, np.uint8)), ctypes.c_size_t(4), 0, p(np.zeros(4097, np.uint16))) == isa.ISA_EINVAL
+
+
+def test_synthesisers_match_the_oracle_encoders():
+    """The numpy stream builders bench.py uses (imagestackalignator_b200/synthetic.py)
+    write the same bytes as the oracle's encoders, which the restated readers invert."""
+    from imagestackalignator_b200 import synthetic as S
+    rng = np.random.default_rng(8)
+    code, lens = S.pef_code_book()
+    for shape in [(1, 1), (8, 2), (37, 53)]:
+        img = rng.integers(0, 16384, shape).astype(np.uint16)
+        assert np.array_equal(S.pef_stream(img, code, lens), R.encode(img, code, lens))
+    for clrs in (1, 2):
+        img = np.clip(rng.normal(3000, 700, (24, 32)), 0, 16383).astype(np.uint16)
+        t = S.lj92_tile(img, clrs, 14)
+        assert np.array_equal(t, R.lj92_encode(img, clrs, 14, 1, 0))
+        st, out = R.dng_decode(np.concatenate([np.zeros(8, np.uint8), t]), 32, 24, [8], [len(t)], tiled=True, tile_w=32, tile_h=24)
+        assert st == 0 and np.array_equal(out, img)
+
+
+@pytest.mark.parametrize("psv", [1, 4, 7])
+def test_oracle_dng_tiles_round_trip(psv):
+    rng = np.random.default_rng(psv)
+    img = np.clip(rng.normal(3000, 400, (50, 70)), 0, 16383).astype(np.uint16)
+    f, offs, cnts = R.dng_tiles(img, 32, 32, clrs=2, bits=14, psv=psv)
+    st, out = R.dng_decode(f, 70, 50, offs, cnts, tiled=True, tile_w=32, tile_h=32)
+    assert st == 0 and np.array_equal(out, img)
