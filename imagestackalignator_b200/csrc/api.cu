@@ -2190,6 +2190,7 @@ struct DngPlan {
     std::vector<uint16_t> tables;           // distinct tables, concatenated
     size_t row_samples = 0;                 // two-row buffers of all parts, in uint16
     int nparts = 0;
+    int jwide_max = 1;                      // the widest row of samples
 };
 
 int dng_plan(const uint8_t* file, size_t fsize, const isa_dng_layout* L, int W, int H, DngPlan& plan)
@@ -2222,7 +2223,10 @@ int dng_plan(const uint8_t* file, size_t fsize, const isa_dng_layout* L, int W, 
         }
         const int orow = L->tiled ? row : t * L->rows_per_strip, ocol = L->tiled ? col : 0;
         const unsigned long long rb = plan.row_samples;
-        if (ok) plan.row_samples += (size_t)2 * h.wide * h.clrs + 8;
+        if (ok) {
+            plan.row_samples += (size_t)2 * h.wide * h.clrs + 8;
+            plan.jwide_max = std::max(plan.jwide_max, h.wide * h.clrs);
+        }
         isa_dng_part_set(plan.parts.data(), t, (unsigned long long)(o + h.data), (unsigned long long)end, skip ? 1 : 0, hdr, orow, ocol, tab, rb);
         if (L->tiled) {
             col += L->tile_width;
@@ -2298,6 +2302,8 @@ int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t fil
     DngPlan plan;
     if (L->compression == 7) {
         ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));
+        if ((size_t)4 * (4096 + 4 * (size_t)plan.jwide_max + 64) > 227 * 1024)
+            return fail(ISA_EINVAL, "rows of %d samples exceed the decoder's shared-memory row buffers", plan.jwide_max);
         void* p = take(plan.parts.size());
         uint16_t* tb = (uint16_t*)take(plan.tables.size() * 2 + 2);
         d_rows = (uint16_t*)take(plan.row_samples * 2 + 16);
@@ -2308,7 +2314,7 @@ int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t fil
     }
     ISA_CK(isa_launch_dng(file_dev, file_size, L->compression, d_parts, nparts, d_tables, d_rows, d_offs, d_cnts, L->rows_per_strip, L->bit_depth,
                           L->linearization ? d_lin : nullptr, L->nlin, L->black_h ? d_bh : nullptr, L->black_v ? d_bv : nullptr, width, height,
-                          L->dng_version_large, out, out_pitch, d_err, st));
+                          L->dng_version_large, out, out_pitch, d_err, st, plan.jwide_max, (int)plan.tables.size()));
     int err = err0;
     ISA_CK(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     ISA_CK(cudaStreamSynchronize(st));

@@ -197,4 +197,4 @@ void isa_dng_part_set(void* dst, int i, unsigned long long pos, unsigned long lo
 cudaError_t isa_launch_dng(const uint8_t* file, unsigned long long fsize, int compression, const void* parts, int nparts, const uint16_t* tables,
                            uint16_t* rows, const unsigned long long* offs, const unsigned long long* cnts, int rps, int depth, const uint16_t* lin,
                            int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large, uint16_t* out, size_t out_pitch, int* error,
-                           cudaStream_t st);
+                           cudaStream_t st, int jwide_max, int ntables);

@@ -580,12 +580,26 @@ __device__ __forceinline__ uint16_t dng_value(const DngArgs& A, unsigned v, int 
     return (uint16_t)(x - black > 0 ? x - black : 0);
 }
 
+// The reader of one tile, run by lane 0 of the tile's warp. The warp keeps
+// a DNG_WIN-byte window of the tile's bytes in shared memory (loaded with
+// coalesced reads by all lanes) and slides it whenever fewer than
+// DNG_MARGIN bytes remain ahead of the reader: one column of samples reads
+// at most 6 components x 2 calls x 8 bytes.
+constexpr int DNG_WIN = 4096, DNG_MARGIN = 256, DNG_WARPS = 4;
+
 struct DngReader {
-    const uint8_t* d;
-    long long n, pos;
+    const uint8_t* win;    // shared window: bytes [base, base + DNG_WIN) of the tile
+    long long base, n, pos;
     unsigned bitbuf;
     int vbits;
-    __device__ __forceinline__ int byte() { return pos >= 0 && pos < n ? (int)__ldg(d + pos++) : (pos++, -1); }
+    __device__ __forceinline__ int byte()
+    {
+        long long i = pos - base;
+        i = i < 0 ? 0 : (i >= DNG_WIN ? DNG_WIN - 1 : i);  // the margin keeps i in range; the clamp only guards the memory
+        const int v = (pos >= 0 && pos < n) ? (int)win[i] : -1;
+        pos++;
+        return v;
+    }
     __device__ __forceinline__ unsigned bits(int nbits, const uint16_t* huff)
     {
         if (nbits > 25) return 0;
@@ -615,68 +629,127 @@ struct DngReader {
     }
 };
 
-__global__ void k_dng_lj92(const DngArgs A)
+// Warp per tile: lane 0 decodes sample by sample (the reference's order and
+// arithmetic), the warp keeps the byte window filled and converts and stores
+// each finished row. Row buffers live in shared memory.
+__global__ void __launch_bounds__(32 * DNG_WARPS) k_dng_lj92(const DngArgs A, int jwide_max, int ntab)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= A.nparts) return;
-    const Lj92Part P = A.parts[t];
-    if (P.skip) return;
-    DngReader r{A.file + P.pos, (long long)(P.end - P.pos), 0, 0u, 0};
-    uint16_t* rowbuf = A.rows + P.rowbuf + 4;  // 4 spare samples before the buffer: row[0][-clrs] at column 0 is never read
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // all Huffman tables of the frame when they fit (ntab > 0 entries), then per warp the window and the rows
+    uint16_t* stab = (uint16_t*)dsm;
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) stab[i] = A.tables[i];
+    __syncthreads();
+    const uint16_t* tabs = ntab > 0 ? stab : A.tables;
+    uint8_t* win = dsm + (size_t)(ntab * 2 + 15) / 16 * 16 + (size_t)warp * (DNG_WIN + 4 * (size_t)jwide_max + 64);
+    uint16_t* rowbuf = (uint16_t*)(win + DNG_WIN);
+    int* svpred = (int*)(win + DNG_WIN + 4 * (size_t)jwide_max);        // 6 predictors
+    int* stable = svpred + 8;                                             // 6 table offsets
+    const int t = blockIdx.x * DNG_WARPS + warp;
+    if (t >= A.nparts) return;  // whole warp
+    const Lj92Part* PP = A.parts + t;
+    if (PP->skip) return;
+    if (lane < 6) stable[lane] = PP->table[lane];
+    struct {
+        unsigned long long pos, end;
+        int bits, high, wide, clrs, sraw, psv, restart, out_row, out_col;
+    } P{PP->pos, PP->end, PP->bits, PP->high, PP->wide, PP->clrs, PP->sraw, PP->psv, PP->restart, PP->out_row, PP->out_col};
+    __syncwarp();
+    const uint8_t* src = A.file + P.pos;
+    const long long n = (long long)(P.end - P.pos);
+    long long base = 0;
+    const auto load = [&](long long b) {
+        __syncwarp();
+        base = b;
+        for (int i = lane; i < DNG_WIN; i += 32) {
+            const long long q = b + i;
+            win[i] = (q >= 0 && q < n) ? __ldg(src + q) : (uint8_t)0;
+        }
+        __syncwarp();
+    };
+    load(0);
+    DngReader r{win, 0, n, 0, 0u, 0};
     const int jwide = P.wide * P.clrs;
-    int vpred[6];
+    bool failed = false;
     for (int jrow = 0; jrow < P.high; jrow++) {
-        if ((long long)jrow * P.wide % P.restart == 0) {
-            for (int c = 0; c < 6; c++) vpred[c] = 1 << (P.bits - 1);
-            if (jrow > 0) {
-                r.pos -= 2;
-                unsigned short mark = 0;
-                int c;
-                do mark = (unsigned short)((mark << 8) + (c = r.byte()));
-                while (r.pos < r.n - 1 && mark >> 4 != 0xffd);
+        const bool restart = (long long)jrow * P.wide % P.restart == 0;
+        if (restart && jrow > 0) {
+            // seek back 2 bytes, then read until a 0xFFDx marker (or the last byte)
+            long long p = __shfl_sync(0xffffffffu, r.pos, 0) - 2;
+            if (p < base || p + DNG_MARGIN > base + DNG_WIN) load(p - 8);
+            if (lane == 0) { r.base = base; r.pos = p; }
+            unsigned short mark = 0;
+            while (true) {
+                bool done = false;
+                if (lane == 0) {
+                    while (r.pos < base + DNG_WIN - 8) {
+                        const int c = r.byte();
+                        mark = (unsigned short)((mark << 8) + c);
+                        if (!(r.pos < r.n - 1 && mark >> 4 != 0xffd)) { done = true; break; }
+                    }
+                }
+                if (__shfl_sync(0xffffffffu, done, 0)) break;
+                load(__shfl_sync(0xffffffffu, r.pos, 0) - 8);
+                if (lane == 0) r.base = base;
             }
+        }
+        if (lane == 0 && restart) {
+            for (int c = 0; c < 6; c++) svpred[c] = 1 << (P.bits - 1);
             r.bitbuf = 0;
             r.vbits = 0;
         }
         uint16_t* row0 = rowbuf + (size_t)jwide * (jrow & 1);
-        uint16_t* row1 = rowbuf + (size_t)jwide * ((jrow + 1) & 1);
+        const uint16_t* row1 = rowbuf + (size_t)jwide * ((jrow + 1) & 1);
         int spred = 0;
-        for (int col = 0; col < P.wide; col++)
-            for (int c = 0; c < P.clrs; c++) {
-                const int d = r.diff(A.tables + P.table[c < 6 ? c : 5], A.large);
-                int pred;
-                if (P.sraw > 0 && c <= P.sraw && (col | c) > 0) pred = spred;
-                else if (col > 0) pred = row0[-P.clrs];
-                else pred = (vpred[c] += d) - d;
-                if (jrow > 0 && col > 0) switch (P.psv) {
-                    case 1: break;
-                    case 2: pred = row1[0]; break;
-                    case 3: pred = row1[-P.clrs]; break;
-                    case 4: pred = pred + row1[0] - row1[-P.clrs]; break;
-                    case 5: pred = pred + ((row1[0] - row1[-P.clrs]) >> 1); break;
-                    case 6: pred = row1[0] + ((pred - row1[-P.clrs]) >> 1); break;
-                    case 7: pred = (pred + row1[0]) >> 1; break;
-                    default: pred = 0; break;
-                    }
-                const uint16_t v = (uint16_t)(pred + d);
-                *row0 = v;
-                if (v >> P.bits) {
-                    atomicMin(A.error, t);
-                    return;
-                }
-                if (c <= P.sraw) spred = v;
-                row0++;
-                row1++;
+        for (int col = 0; col < P.wide; col++) {
+            const long long p = __shfl_sync(0xffffffffu, r.pos, 0);
+            if (p + DNG_MARGIN > base + DNG_WIN) {
+                load(p - 8);
+                if (lane == 0) r.base = base;
             }
-        const uint16_t* rp = rowbuf + (size_t)jwide * (jrow & 1);
-        const int orow = P.out_row + jrow;
-        if (orow >= A.H) continue;
-        uint16_t* o = isa::row_ptr(A.out, A.out_pitch, orow);
-        for (int jcol = 0; jcol < jwide; jcol++) {
-            const int ocol = P.out_col + jcol;
-            if (ocol < A.W) o[ocol] = dng_value(A, rp[jcol], orow, ocol);
+            if (lane == 0) {
+                for (int c = 0; c < P.clrs; c++) {
+                    const int d = r.diff(tabs + stable[c], A.large);
+                    int pred;
+                    if (P.sraw > 0 && c <= P.sraw && (col | c) > 0) pred = spred;
+                    else if (col > 0) pred = row0[col * P.clrs + c - P.clrs];
+                    else pred = (svpred[c] += d) - d;
+                    if (jrow > 0 && col > 0) {
+                        const int up = row1[col * P.clrs + c], ul = row1[col * P.clrs + c - P.clrs];
+                        switch (P.psv) {
+                        case 1: break;
+                        case 2: pred = up; break;
+                        case 3: pred = ul; break;
+                        case 4: pred = pred + up - ul; break;
+                        case 5: pred = pred + ((up - ul) >> 1); break;
+                        case 6: pred = up + ((pred - ul) >> 1); break;
+                        case 7: pred = (pred + up) >> 1; break;
+                        default: pred = 0; break;
+                        }
+                    }
+                    const uint16_t v = (uint16_t)(pred + d);
+                    row0[col * P.clrs + c] = v;
+                    if (v >> P.bits) { failed = true; break; }
+                    if (c <= P.sraw) spred = v;
+                }
+            }
+            if (__shfl_sync(0xffffffffu, failed, 0)) break;
         }
+        failed = __shfl_sync(0xffffffffu, failed, 0);
+        if (failed) break;
+        __syncwarp();
+        // the finished row, converted and stored by the whole warp
+        const int orow = P.out_row + jrow;
+        if (orow < A.H) {
+            uint16_t* o = isa::row_ptr(A.out, A.out_pitch, orow);
+            for (int jcol = lane; jcol < jwide; jcol += 32) {
+                const int ocol = P.out_col + jcol;
+                if (ocol < A.W) o[ocol] = dng_value(A, row0[jcol], orow, ocol);
+            }
+        }
+        __syncwarp();
     }
+    if (failed && lane == 0) atomicMin(A.error, t);
 }
 
 // Uncompressed strips: 16-bit little-endian samples filling rows strip by
@@ -728,11 +801,18 @@ void isa_dng_part_set(void* dst, int i, unsigned long long pos, unsigned long lo
 cudaError_t isa_launch_dng(const uint8_t* file, unsigned long long fsize, int compression, const void* parts, int nparts, const uint16_t* tables,
                            uint16_t* rows, const unsigned long long* offs, const unsigned long long* cnts, int rps, int depth, const uint16_t* lin,
                            int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large, uint16_t* out, size_t out_pitch, int* error,
-                           cudaStream_t st)
+                           cudaStream_t st, int jwide_max, int ntables)
 {
     DngArgs A{file, fsize, (const Lj92Part*)parts, nparts, tables, rows, lin, nlin, bh, bv, W, H, large, out, out_pitch, error};
     if (compression == 7) {
-        k_dng_lj92<<<(nparts + 63) / 64, 64, 0, st>>>(A);
+        const size_t per_warp = (size_t)DNG_WARPS * (DNG_WIN + 4 * (size_t)jwide_max + 64);
+        if (per_warp > 227 * 1024) return cudaErrorInvalidValue;
+        // the tables go to shared memory too when they fit beside the warps' buffers
+        const int ntab = ((size_t)ntables * 2 + 16 + per_warp <= 200 * 1024) ? ntables : 0;
+        const size_t smem = (size_t)(ntab * 2 + 15) / 16 * 16 + per_warp;
+        cudaError_t e = cudaFuncSetAttribute(k_dng_lj92, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_dng_lj92<<<(nparts + DNG_WARPS - 1) / DNG_WARPS, 32 * DNG_WARPS, smem, st>>>(A, jwide_max, ntab);
     } else {
         dim3 g((W + 255) / 256, H);
         k_dng_plain<<<g, 256, 0, st>>>(A, offs, cnts, rps, depth);
