@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -2076,7 +2077,7 @@ int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], do
     ISA_REQ(white_balance && camera_to_pcs && camera_white, "NULL argument");
     for (int c = 0; c < 3; c++)
         if (!(white_balance[c] > 0.f) || !std::isfinite(white_balance[c])) return fail(ISA_EINVAL, "white balance must be positive");
-    // PEFFile.SetMembers (PEFFile.cs:276-278): identity colour matrices under D50 for both illuminants
+    // PEFFile.SetMembers (PEFFile.cs:310-312): identity colour matrices under D50 for both illuminants
     bool ok = true;
     ColorSpec s;
     s.t1 = s.t2 = 5000.0;
@@ -2094,6 +2095,241 @@ int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], do
     const XY white = neutral_to_xy(s, vec, ok);
     if (!ok) return fail(ISA_ESINGULAR, "a colour matrix is singular");
     return color_spec_out(s, white, camera_to_pcs, camera_white, white_xy);
+}
+
+int isa_profile_color_spec(const double* color_matrix1, const double* color_matrix2, int illuminant1, int illuminant2,
+                           const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2])
+{
+    ISA_REQ(white_balance && camera_to_pcs && camera_white, "NULL argument");
+    for (int c = 0; c < 3; c++)
+        if (!(white_balance[c] > 0.f) || !std::isfinite(white_balance[c])) return fail(ISA_EINVAL, "white balance must be positive");
+    // DNGColorSpec.cs:175-266 is the tag constructor without forward matrices,
+    // calibration and analog balance, its neutral being 1 / wb in float
+    double neutral[3];
+    for (int c = 0; c < 3; c++) neutral[c] = (double)(1.0f / white_balance[c]);
+    isa_dng_color_tags t{};
+    t.color_matrix1 = color_matrix1;
+    t.color_matrix2 = color_matrix2;
+    t.illuminant1 = illuminant1;
+    t.illuminant2 = illuminant2;
+    t.as_shot_neutral = neutral;
+    return isa_dng_color_spec(&t, camera_to_pcs, camera_white, white_xy);
+}
+
+// ---- Raw-file metadata ----
+
+int isa_noise_model(int iso, const int* isos, const double* alpha, const double* beta, int n, double ab[2])
+{
+    ISA_REQ(ab && n >= 0 && (n == 0 || (isos && alpha && beta)), "NULL argument or negative count");
+    if (n == 0) {
+        ab[0] = ab[1] = 0.0;
+        return ISA_OK;
+    }
+    int index = -1;  // the last ISO not above the asked one (ExtraCameraProfiles.cs:171-179)
+    for (int i = n - 1; i >= 0; i--)
+        if (isos[i] <= iso) {
+            index = i;
+            break;
+        }
+    if (index == n - 1) {
+        ab[0] = alpha[n - 1];
+        ab[1] = beta[n - 1];
+    } else if (index < 0) {
+        ab[0] = alpha[0];
+        ab[1] = beta[0];
+    } else {
+        const double w = ((double)iso - (double)isos[index + 1]) / ((double)isos[index] - (double)isos[index + 1]);
+        ab[0] = w * alpha[index] + (1.0 - w) * alpha[index + 1];
+        ab[1] = w * beta[index] + (1.0 - w) * beta[index + 1];
+    }
+    return ISA_OK;
+}
+
+int isa_crop_window(int left, int top, int cropped_width, int cropped_height, int width, int height, int crop[4])
+{
+    ISA_REQ(crop, "NULL argument");
+    crop[0] = std::max(2, left);
+    crop[1] = std::max(2, top);
+    crop[2] = cropped_width - std::max(0, (left + cropped_width) - (width - 2));
+    crop[3] = cropped_height - std::max(0, (top + cropped_height) - (height - 2));
+    return ISA_OK;
+}
+
+namespace {
+
+// C#'s Math.Max(float, float): NaN when either is NaN.
+float cs_maxf(float a, float b)
+{
+    if (a != a || b != b) return std::numeric_limits<float>::quiet_NaN();
+    return a > b ? a : b;
+}
+
+// (int) of a tag's rational, truncated toward zero; false when it does not fit.
+bool to_int(double v, int& out)
+{
+    if (!(v > -2147483649.0 && v < 2147483648.0)) return false;
+    out = (int)v;
+    return true;
+}
+
+}  // namespace
+
+int isa_dng_levels(const isa_dng_level_tags* t, isa_raw_levels* out, uint16_t* black_h, uint16_t* black_v)
+{
+    ISA_REQ(t && out && t->cfa_pattern && t->camera_white, "NULL argument");
+    ISA_REQ(t->width > 0 && t->height > 0, "bad size");
+    ISA_REQ(t->cfa_repeat_w == 2 && t->cfa_repeat_h == 2, "the CFA repeat pattern must be 2 x 2 (DNGFile.cs:706-712)");
+    const int W = t->width, H = t->height;
+    int cfa[4];
+    for (int i = 0; i < 4; i++) cfa[i] = t->cfa_pattern[i];
+    ISA_REQ(cfa_ok(cfa), "CFA codes must be 0, 1, 2");
+    // CFAPlaneColor: plane order and the reordering twist (:719-746)
+    int plane[3] = {0, 1, 2};
+    float twist[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+    int identity = 1;
+    if (t->plane_color) {
+        ISA_REQ(t->n_plane_color == 3, "CFAPlaneColor must hold three planes");
+        for (int k = 0; k < 12; k++) twist[k] = 0.f;
+        for (int i = 0; i < 3; i++) {
+            const int color = t->plane_color[i];
+            ISA_REQ(color >= 0 && color <= 2, "CFAPlaneColor names a colour other than red, green, blue");
+            plane[i] = color;
+            twist[color * 4 + i] = 1.f;
+            if (color != i) identity = 0;
+        }
+    }
+    // BlackLevel (:757-824), on the CFA as stored (before the active-area shift)
+    float black[3] = {0.f, 0.f, 0.f};
+    if (t->black_level) {
+        const double* bl = t->black_level;
+        if (t->n_black == 1) {
+            black[0] = black[1] = black[2] = (float)bl[0];
+        } else if (t->n_black == 3) {
+            for (int i = 0; i < 3; i++) black[plane[i]] = (float)bl[i];
+        } else if (t->n_black == 4) {
+            int ir = -1, ib = -1, ig1 = -1, ig2 = -1;
+            for (int i = 0; i < 4; i++)
+                if (cfa[i] == 0) { ir = i; break; }
+            for (int i = 0; i < 4; i++)
+                if (cfa[i] == 2) { ib = i; break; }
+            for (int i = 0; i < 4; i++) {  // the first green, then the last (:809-818)
+                if (cfa[i] == 1 && ig1 == -1) ig1 = i;
+                if (cfa[i] == 1 && ig1 != -1) ig2 = i;
+            }
+            ISA_REQ(ir >= 0 && ib >= 0 && ig1 >= 0, "a CFA without red, green and blue has no per-position black levels");
+            black[0] = (float)bl[ir];
+            black[2] = (float)bl[ib];
+            black[1] = cs_maxf((float)bl[ig1], (float)bl[ig2]);
+        }
+    }
+    const float white_all = (float)t->white_level;
+    float white[3];
+    for (int c = 0; c < 3; c++) white[c] = white_all - black[c];
+    float wb[3];
+    for (int i = 0; i < 3; i++) wb[plane[i]] = 1.0f / (float)t->camera_white[i];
+    // ActiveArea and DefaultCrop (:861-948)
+    int crop_left = 0, crop_top = 0, crop_w = W, crop_h = H;
+    const int* aa = t->active_area;
+    if (aa) {
+        const int top = aa[0], left = aa[1], bottom = aa[2], right = aa[3];
+        crop_left += left;
+        crop_top += top;
+        crop_w = right - left;
+        crop_h = bottom - top;
+        if (top % 2 != 0) {
+            const int c0 = cfa[0], c1 = cfa[1];
+            cfa[0] = cfa[2];
+            cfa[1] = cfa[3];
+            cfa[2] = c0;
+            cfa[3] = c1;
+        }
+        if (left % 2 != 0) {
+            const int c0 = cfa[0], c2 = cfa[2];
+            cfa[0] = cfa[1];
+            cfa[2] = cfa[3];
+            cfa[1] = c0;
+            cfa[3] = c2;
+        }
+    }
+    if (t->default_crop_origin && t->default_crop_size) {
+        int left, top, w, h;  // entry 0 of each tag for both coordinates, as the reference reads them (:910-915)
+        ISA_REQ(to_int(t->default_crop_origin[0], left) && to_int(t->default_crop_size[0], w), "crop out of range");
+        top = left;
+        h = w;
+        crop_left += left;
+        crop_top += top;
+        crop_w = w;
+        crop_h = h;
+    }
+    int crop[4];
+    isa_crop_window(crop_left, crop_top, crop_w, crop_h, W, H, crop);
+    // NoiseProfile (:950-967), then an ExtraCameraProfiles noise model with alpha != 0 (:296-320)
+    float alpha = 0.f, beta = 0.f;
+    if (t->noise_profile) {
+        ISA_REQ(t->n_noise >= 2, "NoiseProfile needs two values");
+        if (t->n_noise > 2) {
+            ISA_REQ(plane[1] * 2 + 1 < t->n_noise, "NoiseProfile too short for the green plane");
+            alpha = (float)t->noise_profile[plane[1] * 2];
+            beta = (float)t->noise_profile[plane[1] * 2 + 1];
+        } else {
+            alpha = (float)t->noise_profile[0];
+            beta = (float)t->noise_profile[1];
+        }
+    }
+    if (t->n_profile > 0) {
+        double ab[2];
+        if (isa_noise_model(t->iso, t->profile_iso, t->profile_alpha, t->profile_beta, t->n_profile, ab) != ISA_OK) return ISA_EINVAL;
+        if (ab[0] != 0.0) {
+            alpha = (float)ab[0];
+            beta = (float)ab[1];
+        }
+    }
+    // BlackLevelDeltaV / H placed in the active area (:324-372); the white
+    // level loses the largest black of a decoded pixel (:607-609), which for
+    // non-negative deltas over a fully decoded frame is max(V) + max(H)
+    const int off_v = aa ? aa[0] : 0, off_h = aa ? aa[1] : 0;
+    const int border_bottom = aa ? H - aa[2] : 0, border_right = aa ? W - aa[3] : 0;
+    int max_v = 0, max_h = 0;
+    if (black_v) std::memset(black_v, 0, sizeof(uint16_t) * (size_t)H);
+    if (black_h) std::memset(black_h, 0, sizeof(uint16_t) * (size_t)W);
+    if (t->black_delta_v) {
+        ISA_REQ(t->n_delta_v + off_v + border_bottom == H && off_v >= 0 && t->n_delta_v >= 0, "BlackLevelDeltaV does not fit the image height");
+        for (int i = 0; i < t->n_delta_v; i++) {
+            const double v = t->black_delta_v[i];
+            ISA_REQ(v > -1.0 && v < 65536.0, "BlackLevelDeltaV value outside 0..65535");
+            const int u = (uint16_t)(int)v;
+            max_v = std::max(max_v, u);
+            if (black_v) black_v[off_v + i] = (uint16_t)u;
+        }
+    }
+    if (t->black_delta_h) {
+        ISA_REQ(t->n_delta_h + off_h + border_right == W && off_h >= 0 && t->n_delta_h >= 0, "BlackLevelDeltaH does not fit the image width");
+        for (int i = 0; i < t->n_delta_h; i++) {
+            const double v = t->black_delta_h[i];
+            ISA_REQ(v > -1.0 && v < 65536.0, "BlackLevelDeltaH value outside 0..65535");
+            const int u = (uint16_t)(int)v;
+            max_h = std::max(max_h, u);
+            if (black_h) black_h[off_h + i] = (uint16_t)u;
+        }
+    }
+    const int max_black = max_v + max_h;
+    isa_raw_levels r{};
+    r.info.width = W;
+    r.info.height = H;
+    for (int i = 0; i < 4; i++) r.info.cfa[i] = cfa[i];
+    for (int c = 0; c < 3; c++) {
+        r.info.black[c] = black[c];
+        r.info.white[c] = white[c] - (float)max_black;
+        r.info.camera_white[c] = (float)t->camera_white[c];
+        r.white_balance[c] = wb[c];
+    }
+    r.info.noise_alpha = alpha;
+    r.info.noise_beta = beta;
+    for (int k = 0; k < 12; k++) r.color_twist[k] = twist[k];
+    r.color_twist_identity = identity;
+    for (int k = 0; k < 4; k++) r.crop[k] = crop[k];
+    *out = r;
+    return ISA_OK;
 }
 
 // ---- DNG pixel data ----

@@ -77,6 +77,7 @@ EXPORTS = [
     "isa_color_twists", "isa_postprocess", "isa_save_tiff16", "isa_save_as_16bit_tiff",
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
     "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
+    "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec",
 ]
 
 _lib = None
@@ -464,6 +465,101 @@ def pef_color_spec(white_balance):
     check(lib().isa_pef_color_spec(wb.ctypes.data_as(ctypes.c_void_p), c2p.ctypes.data_as(ctypes.c_void_p), cw.ctypes.data_as(ctypes.c_void_p),
                                    xy.ctypes.data_as(ctypes.c_void_p)))
     return c2p.reshape(3, 3), cw, xy
+
+
+def profile_color_spec(white_balance, color_matrix1=None, color_matrix2=None, illuminant1=0, illuminant2=0):
+    """isa_profile_color_spec: the colour spec of a camera profile (matrices, illuminants) and a white balance."""
+    keep = []
+
+    def arr(v):
+        if v is None:
+            return None
+        a = np.ascontiguousarray(v, np.float64).reshape(9)
+        keep.append(a)
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    wb = np.ascontiguousarray(white_balance, np.float32)
+    c2p = np.zeros(9)
+    cw = np.zeros(3)
+    xy = np.zeros(2)
+    check(lib().isa_profile_color_spec(arr(color_matrix1), arr(color_matrix2), int(illuminant1), int(illuminant2),
+                                       wb.ctypes.data_as(ctypes.c_void_p), c2p.ctypes.data_as(ctypes.c_void_p),
+                                       cw.ctypes.data_as(ctypes.c_void_p), xy.ctypes.data_as(ctypes.c_void_p)))
+    return c2p.reshape(3, 3), cw, xy
+
+
+def noise_model(iso, isos, alpha, beta):
+    """isa_noise_model: (alpha, beta) of a camera profile's noise model at `iso`."""
+    i = np.ascontiguousarray(isos, np.int32)
+    a = np.ascontiguousarray(alpha, np.float64)
+    b = np.ascontiguousarray(beta, np.float64)
+    ab = np.zeros(2)
+    check(lib().isa_noise_model(int(iso), i.ctypes.data_as(ctypes.c_void_p), a.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p),
+                                int(i.size), ab.ctypes.data_as(ctypes.c_void_p)))
+    return float(ab[0]), float(ab[1])
+
+
+def crop_window(left, top, cropped_width, cropped_height, width, height):
+    """isa_crop_window: (left, top, width, height) kept at least two pixels off the frame's edges."""
+    c = (ctypes.c_int * 4)()
+    check(lib().isa_crop_window(int(left), int(top), int(cropped_width), int(cropped_height), int(width), int(height), c))
+    return tuple(c)
+
+
+class IsaDngLevelTags(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("cfa_pattern", ctypes.c_void_p), ("cfa_repeat_w", ctypes.c_int),
+                ("cfa_repeat_h", ctypes.c_int), ("plane_color", ctypes.c_void_p), ("n_plane_color", ctypes.c_int),
+                ("black_level", ctypes.c_void_p), ("n_black", ctypes.c_int), ("white_level", ctypes.c_double),
+                ("camera_white", ctypes.c_void_p), ("active_area", ctypes.c_void_p), ("default_crop_origin", ctypes.c_void_p),
+                ("default_crop_size", ctypes.c_void_p), ("noise_profile", ctypes.c_void_p), ("n_noise", ctypes.c_int),
+                ("black_delta_h", ctypes.c_void_p), ("n_delta_h", ctypes.c_int), ("black_delta_v", ctypes.c_void_p),
+                ("n_delta_v", ctypes.c_int), ("iso", ctypes.c_int), ("profile_iso", ctypes.c_void_p), ("profile_alpha", ctypes.c_void_p),
+                ("profile_beta", ctypes.c_void_p), ("n_profile", ctypes.c_int)]
+
+
+class IsaRawLevels(ctypes.Structure):
+    _fields_ = [("info", IsaRawInfo), ("white_balance", ctypes.c_float * 3), ("color_twist", ctypes.c_float * 12),
+                ("color_twist_identity", ctypes.c_int), ("crop", ctypes.c_int * 4)]
+
+
+def dng_levels(width, height, cfa_pattern, white_level, camera_white, cfa_repeat=(2, 2), plane_color=None, black_level=None,
+               active_area=None, default_crop_origin=None, default_crop_size=None, noise_profile=None, black_delta_h=None,
+               black_delta_v=None, iso=0, profile_noise=None):
+    """isa_dng_levels. profile_noise = (isos, alphas, betas) of an ExtraCameraProfiles entry, or None.
+    Returns a dict of the levels plus the placed black deltas (uint16 width and height entries)."""
+    keep = []
+
+    def arr(v, dt):
+        if v is None:
+            return None, 0
+        a = np.ascontiguousarray(v, dt).reshape(-1)
+        keep.append(a)
+        return a.ctypes.data, int(a.size)
+
+    cfa, _ = arr(cfa_pattern, np.uint8)
+    pc, npc = arr(plane_color, np.int32)
+    bl, nbl = arr(black_level, np.float64)
+    cw, _ = arr(camera_white, np.float64)
+    aa, _ = arr(active_area, np.int32)
+    co, _ = arr(default_crop_origin, np.float64)
+    cs, _ = arr(default_crop_size, np.float64)
+    npf, nn = arr(noise_profile, np.float64)
+    dh, ndh = arr(black_delta_h, np.float64)
+    dv, ndv = arr(black_delta_v, np.float64)
+    pi, npi = arr(None if profile_noise is None else profile_noise[0], np.int32)
+    pa, _ = arr(None if profile_noise is None else profile_noise[1], np.float64)
+    pb, _ = arr(None if profile_noise is None else profile_noise[2], np.float64)
+    t = IsaDngLevelTags(width, height, cfa, cfa_repeat[0], cfa_repeat[1], pc, npc, bl, nbl, float(white_level), cw, aa, co, cs, npf, nn, dh, ndh,
+                        dv, ndv, int(iso), pi, pa, pb, npi)
+    r = IsaRawLevels()
+    bh = np.zeros(width, np.uint16)
+    bv = np.zeros(height, np.uint16)
+    check(lib().isa_dng_levels(ctypes.byref(t), ctypes.byref(r), bh.ctypes.data_as(ctypes.c_void_p), bv.ctypes.data_as(ctypes.c_void_p)))
+    i = r.info
+    return dict(cfa=list(i.cfa), black=np.array(i.black, np.float32), white=np.array(i.white, np.float32),
+                camera_white=np.array(i.camera_white, np.float32), noise=(np.float32(i.noise_alpha), np.float32(i.noise_beta)),
+                white_balance=np.array(r.white_balance, np.float32), color_twist=np.array(r.color_twist, np.float32).reshape(3, 4),
+                color_twist_identity=bool(r.color_twist_identity), crop=tuple(r.crop), black_h=bh, black_v=bv, info=i)
 
 
 class IsaDngLayout(ctypes.Structure):

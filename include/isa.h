@@ -459,7 +459,7 @@ typedef struct isa_dng_color_tags {
     const double* as_shot_white_xy;     /* 2 or NULL; used when given */
 } isa_dng_color_tags;
 ISA_API int isa_dng_color_spec(const isa_dng_color_tags* tags, double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
-/* The colour spec PEFFile.SetMembers builds (PEFFile.cs:276-278): identity
+/* The colour spec PEFFile.SetMembers builds (PEFFile.cs:310-312): identity
  * colour matrices under D50 and the white point of the neutral 1 / white
  * balance (isa_pef_levels' white_balance). */
 ISA_API int isa_pef_color_spec(const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
@@ -495,6 +495,71 @@ ISA_API size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size
  * stop (a sample above the frame's bit depth). */
 ISA_API int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* layout, int width, int height,
                            void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream);
+
+/* ---- Raw-file metadata: DNG levels, camera profiles ----
+ * DNGFile.SetMembers (PefFile/DNGFile.cs:714-951) and the DNGFile
+ * constructor (:288-372, :607-609): CFA layout, black and white per colour,
+ * white balance, plane reordering, crop window and noise model, from the
+ * parsed tag values. Host only. */
+typedef struct isa_dng_level_tags {
+    int width, height;                /* ImageWidth, ImageLength of the raw IFD */
+    const uint8_t* cfa_pattern;       /* CFAPattern, 4 codes (0 red, 1 green, 2 blue) */
+    int cfa_repeat_w, cfa_repeat_h;   /* CFARepeatPatternDim; anything but 2 x 2 is rejected (:706-712) */
+    const int* plane_color;           /* CFAPlaneColor or NULL (= 0, 1, 2) */
+    int n_plane_color;                /* must be 3 when given (:727-730) */
+    const double* black_level;        /* BlackLevel values or NULL; 1, 3 (per plane) or 4 (per CFA position) are used */
+    int n_black;
+    double white_level;               /* WhiteLevel[0] */
+    const double* camera_white;       /* 3: CameraWhite of the colour spec (isa_dng_color_spec) */
+    const int* active_area;           /* ActiveArea top, left, bottom, right, or NULL */
+    const double* default_crop_origin;/* DefaultCropOrigin or NULL (the reference reads entry 0 for left and top) */
+    const double* default_crop_size;  /* DefaultCropSize or NULL (entry 0 for width and height) */
+    const double* noise_profile;      /* NoiseProfile of the raw IFD, else of IFD 0, or NULL */
+    int n_noise;                      /* >= 2 */
+    const double* black_delta_h;      /* BlackLevelDeltaH values or NULL (truncated to uint16) */
+    int n_delta_h;                    /* must equal the active area's width (:358-365) */
+    const double* black_delta_v;      /* BlackLevelDeltaV values or NULL */
+    int n_delta_v;                    /* must equal the active area's height (:341-350) */
+    /* ExtraCameraProfiles noise model for this camera (:296-320): used when it gives alpha != 0 */
+    int iso;                          /* ISOSpeedRatings */
+    const int* profile_iso;           /* NoiseModel.Iso ascending, or NULL */
+    const double* profile_alpha;
+    const double* profile_beta;
+    int n_profile;
+} isa_dng_level_tags;
+
+typedef struct isa_raw_levels {
+    isa_raw_info info;                /* width, height, cfa (shifted for an odd active-area origin), black,
+                                         white (WhiteLevel - black - the largest black delta), camera_white, noise */
+    float white_balance[3];           /* 1 / CameraWhite, per plane (:836-841) */
+    float color_twist[12];            /* 3 x 4 plane reordering of CFAPlaneColor (identity when absent) */
+    int color_twist_identity;
+    int crop[4];                      /* CropLeft, CropTop, CroppedWidth, CroppedHeight (at least 2 pixels off each edge) */
+} isa_raw_levels;
+
+/* Fills `out` and, when not NULL, black_h (width entries) and black_v
+ * (height entries) with the black-level deltas placed in the active area,
+ * as isa_dng_layout takes them. ISA_EINVAL where the reference throws. */
+ISA_API int isa_dng_levels(const isa_dng_level_tags* tags, isa_raw_levels* out, uint16_t* black_h, uint16_t* black_v);
+
+/* NoiseModel.GetValue (PefFile/ExtraCameraProfiles.cs:164-199): alpha and
+ * beta at `iso` from a profile's ascending ISO list, linear between the two
+ * neighbours, clamped to the ends; (0, 0) for an empty list. */
+ISA_API int isa_noise_model(int iso, const int* isos, const double* alpha, const double* beta, int n, double ab[2]);
+
+/* The crop rule of DNGFile.SetMembers (:944-948) and
+ * RawFile.LoadExtraCameraProfile (PefFile/RawFile.cs:246-261): at least two
+ * pixels off the left and top, the size shortened to end two pixels before
+ * the right and bottom edges. crop = left, top, width, height. */
+ISA_API int isa_crop_window(int left, int top, int cropped_width, int cropped_height, int width, int height, int crop[4]);
+
+/* DNGColorSpec(colorMatrix1, colorMatrix2, illuminant1, illuminant2,
+ * whiteBalance) (PefFile/DNGColorSpec.cs:175-266), the colour spec of an
+ * ExtraCameraProfiles entry (RawFile.cs:264-268): color_matrix2 may be NULL,
+ * illuminants are EXIF LightSource codes, the white point is that of the
+ * neutral 1 / white_balance. isa_pef_color_spec is the identity / D50 case. */
+ISA_API int isa_profile_color_spec(const double* color_matrix1, const double* color_matrix2, int illuminant1, int illuminant2,
+                                   const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
 
 #ifdef __cplusplus
 }

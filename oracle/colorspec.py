@@ -3,7 +3,7 @@ tests/ use it): DNGColorSpec (PefFile/DNGColorSpec.cs:31-647), the xy ->
 temperature conversion of DNGTemperature (PefFile/DNGTemperature.cs:181-258)
 and DNGxyCoord (PefFile/DNGxyCoord.cs:79-115), in Python floats (IEEE double)
 with the reference's operation order, plus the PEF colour spec of
-PEFFile.SetMembers (PefFile/PEFFile.cs:276-278).
+PEFFile.SetMembers (PefFile/PEFFile.cs:310-312).
 
 Parity is unpinned: the reference's C# cannot run here and its tests hold
 no colour vectors; the restatement is checked against libisa.so's host

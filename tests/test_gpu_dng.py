@@ -94,3 +94,57 @@ def test_uncompressed_strips(cuda, depth):
     st, want = R.dng_decode(f, W, H, offs, cnts, **kw)
     assert st == 0 and np.array_equal(want, img)
     assert np.array_equal(run(f, W, H, offs, cnts, **kw), want)
+
+
+def test_dng_file_to_tiff_chain(cuda, tmp_path):
+    """The reference's flow from DNG tags and pixel data to the 16-bit TIFF:
+    levels and geometry of DNGFile.SetMembers (isa_dng_levels, with an active
+    area and black-level deltas), tiles decoded with the placed deltas
+    (isa_dng_decode), the burst merged with those levels, the colour spec from
+    the tags (isa_dng_color_spec), SaveAs16BitTiff with the DNG crop."""
+    import torch
+    from imagestackalignator_b200 import params as P, synthetic
+    import post as PO
+    import rawmeta as RM
+    b = synthetic.make_burst(512, 384, 3, seed=21, max_shift=3, max_rot_deg=0.0)
+    W, H = b.width, b.height
+    aa = [2, 4, H - 2, W - 4]
+    rng = np.random.default_rng(8)
+    dv = rng.integers(0, 6, aa[2] - aa[0]).astype(float)
+    dh = rng.integers(0, 4, aa[3] - aa[1]).astype(float)
+    cm1 = [0.9, -0.2, -0.1, -0.4, 1.2, 0.2, -0.05, 0.2, 0.6]
+    c2p, cw, xy = isa.dng_color_spec(color_matrix1=cm1, illuminant1=21, as_shot_neutral=[0.5, 1.0, 0.7])
+    tags = dict(width=W, height=H, cfa_pattern=list(b.cfa), white_level=16383.0, camera_white=cw, black_level=[512, 512, 512, 512],
+                active_area=aa, black_delta_v=dv, black_delta_h=dh, noise_profile=[b.noise_a, b.noise_b])
+    lv = isa.dng_levels(**tags)
+    want = RM.dng_levels(**tags)
+    assert np.array_equal(lv["black_h"], want["black_h"]) and np.array_equal(lv["white"], want["white"])
+    assert lv["cfa"] == list(b.cfa)           # even active-area origin: the CFA stays
+    frames = []
+    for f in range(b.n):
+        file, offs, cnts = R.dng_tiles(b.raw[f], 128, 128, clrs=2, bits=14, psv=1)
+        kw = dict(tiled=True, tile_w=128, tile_h=128, black_h=lv["black_h"], black_v=lv["black_v"])
+        st, ref = R.dng_decode(file, W, H, offs, cnts, **kw)
+        assert st == 0
+        got = isa.dng_decode(file, W, H, offs, cnts, **kw)
+        torch.cuda.synchronize()
+        assert np.array_equal(got.cpu().numpy().view(np.uint16), ref)
+        frames.append(got)
+    raw = torch.stack(frames)
+    m = isa.Merger(W, H, b.n, P.MergeParams())
+    merged = m.merge(raw, lv["info"])
+    torch.cuda.synchronize()
+    assert np.isfinite(merged.cpu().numpy()).all()
+    t1, t2 = isa.color_twists(c2p)
+    lx = np.float32(np.round(np.arange(256) / 255.0, 9))
+    x, y, w, h = lv["crop"]
+    crop = (x, y, min(w, W - x), min(h, H - y))
+    pp, keep = isa.post_params(crop, np.float32(cw), t1, t2, lx, lx, 0.0)
+    path = tmp_path / "dng.tif"
+    isa.save_as_16bit_tiff(merged, pp, str(path))
+    tags_out, img = PO.parse_tiff16(path.read_bytes())
+    assert img.shape == (crop[3], crop[2], 3)
+    wantimg = PO.postprocess(merged.cpu().numpy(), crop, np.float32(cw), t1, t2, lx, lx, 0.0)
+    d = np.abs(img.astype(np.int64) - wantimg.astype(np.int64))
+    assert d.max() <= 1 and (d > 0).sum() <= max(3, 2e-3 * d.size)
+    assert img.std() > 100
