@@ -22,6 +22,7 @@
 namespace {
 
 thread_local std::string g_err;
+thread_local int g_dng_path = -1;  // decoder of the calling thread's last isa_dng_decode: 1 parallel, 0 per part
 
 int fail(int code, const char* fmt, ...)
 {
@@ -2340,9 +2341,36 @@ namespace {
 // Huffman tables (make_decoder_ref, :73-92) and the entropy data's offset.
 struct Lj92Header {
     int algo = 0, bits = 0, high = 0, wide = 0, clrs = 0, sraw = 0, psv = 0, restart = 0x7fffffff;
-    std::vector<uint16_t> huff[20];
+    std::string huff[20];   // per table: the 16 code-length counts and the values make_decoder_ref reads
     int huff_of[20];
     size_t data = 0;
+};
+
+// make_decoder_ref's table (1 + 2^max entries, entry 0 = max) from a table's counts and values.
+std::vector<uint16_t> lj92_table(const std::string& spec)
+{
+    const uint8_t* cnt = (const uint8_t*)spec.data();
+    int max;
+    for (max = 16; max > 0 && cnt[max - 1] == 0; max--) ;
+    std::vector<uint16_t> t((size_t)1 + ((size_t)1 << max), 0);
+    t[0] = (uint16_t)max;
+    size_t dp = 16;
+    int hh = 1;
+    for (int ln = 1; ln <= max; ln++)
+        for (int i = 0; i < cnt[ln - 1]; i++, ++dp)
+            for (int j = 0; j < 1 << (max - ln); j++)
+                if (hh <= 1 << max) t[hh++] = (uint16_t)(ln << 8 | (uint8_t)spec[dp]);
+    return t;
+}
+
+// The reader's segment buffer: zero at every call's start, as the reference
+// allocates a fresh one (DNGFile.cs:98); the bytes a call wrote are cleared
+// when it returns.
+struct SegmentBuffer {
+    std::vector<uint8_t>& data;
+    size_t used = 0;
+    explicit SegmentBuffer(std::vector<uint8_t>& d) : data(d) {}
+    ~SegmentBuffer() { std::memset(data.data(), 0, std::min(used, data.size())); }
 };
 
 bool lj92_start(const uint8_t* d, size_t n, Lj92Header& h)
@@ -2352,9 +2380,12 @@ bool lj92_start(const uint8_t* d, size_t n, Lj92Header& h)
     for (int c = 0; c < 20; c++) h.huff_of[c] = -1;
     rd();
     if (rd() != 0xd8) return false;
-    std::vector<uint8_t> data(0x10000);
+    static thread_local std::vector<uint8_t> buffer(0x10000);
+    SegmentBuffer seg(buffer);
+    std::vector<uint8_t>& data = buffer;
     int tag;
     do {
+        seg.used = std::max<size_t>(seg.used, 4);
         for (int k = 0; k < 4; k++) {
             const int b = rd();
             if (b < 0) return false;
@@ -2363,6 +2394,7 @@ bool lj92_start(const uint8_t* d, size_t n, Lj92Header& h)
         tag = data[0] << 8 | data[1];
         const int len = (data[2] << 8 | data[3]) - 2;
         if (tag <= 0xff00) return false;
+        seg.used = std::max<size_t>(seg.used, (size_t)std::max(len, 0));
         for (int got = 0; got < len; got++) {
             const int b = rd();
             if (b < 0) { pos--; break; }
@@ -2389,19 +2421,15 @@ bool lj92_start(const uint8_t* d, size_t n, Lj92Header& h)
             size_t dp = 0;
             int c;
             while (dp < (size_t)std::max(len, 0) && ((c = data[dp++]) & -20) == 0) {
-                // make_decoder_ref: counts of lengths 1..16, then the values; 1 + 2^max entries
+                // make_decoder_ref: counts of lengths 1..16, then the values (expanded by lj92_table)
                 const size_t cnt0 = dp;
                 dp += 16;
                 int max;
                 for (max = 16; max > 0 && data[cnt0 + max - 1] == 0; max--) ;
-                std::vector<uint16_t> t((size_t)1 + ((size_t)1 << max), 0);
-                t[0] = (uint16_t)max;
-                int hh = 1;
+                std::string spec((const char*)&data[cnt0], 16);
                 for (int ln = 1; ln <= max; ln++)
-                    for (int i = 0; i < data[cnt0 + ln - 1]; i++, ++dp)
-                        for (int j = 0; j < 1 << (max - ln); j++)
-                            if (hh <= 1 << max) t[hh++] = (uint16_t)(ln << 8 | (dp < data.size() ? data[dp] : 0));
-                h.huff[c] = t;
+                    for (int i = 0; i < data[cnt0 + ln - 1]; i++, ++dp) spec.push_back((char)(dp < data.size() ? data[dp] : 0));
+                h.huff[c] = spec;
                 h.huff_of[c] = c;
             }
             break;
@@ -2433,7 +2461,7 @@ int dng_plan(const uint8_t* file, size_t fsize, const isa_dng_layout* L, int W, 
 {
     plan.nparts = L->n;
     plan.parts.assign((size_t)L->n * isa_dng_part_bytes(), 0);
-    std::map<std::vector<uint16_t>, int> seen;
+    std::map<std::string, int> seen;
     int row = 0, col = 0;
     for (int t = 0; t < L->n; t++) {
         const size_t o = L->offsets[t];
@@ -2452,7 +2480,8 @@ int dng_plan(const uint8_t* file, size_t fsize, const isa_dng_layout* L, int W, 
                 auto it = seen.find(h.huff[k]);
                 if (it == seen.end()) {
                     it = seen.emplace(h.huff[k], (int)plan.tables.size()).first;
-                    plan.tables.insert(plan.tables.end(), h.huff[k].begin(), h.huff[k].end());
+                    const std::vector<uint16_t> t = lj92_table(h.huff[k]);
+                    plan.tables.insert(plan.tables.end(), t.begin(), t.end());
                 }
                 tab[c] = it->second;
             }
@@ -2488,27 +2517,42 @@ int isa_dng_check(const isa_dng_layout* L, int width, int height)
     return ISA_OK;
 }
 
-size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size, const isa_dng_layout* L, int width, int height)
+namespace {
+
+// Scratch of isa_dng_decode for a checked layout and, for lossless JPEG, its plan.
+size_t dng_scratch_bytes(const isa_dng_layout* L, int width, int height, const DngPlan& plan)
 {
-    if (!file_host || isa_dng_check(L, width, height) != ISA_OK) return 0;
     size_t s = align256((size_t)L->n * 16) + align256((size_t)L->n * 8) + align256((size_t)L->n * 8) + align256(64);
     s += align256((size_t)width * 2) + align256((size_t)height * 2) + align256((size_t)std::max(L->nlin, 1) * 2);
     if (L->compression == 7) {
-        DngPlan plan;
-        if (dng_plan(file_host, file_size, L, width, height, plan) != ISA_OK) return 0;
         s += align256(plan.parts.size()) + align256(plan.tables.size() * 2 + 2) + align256(plan.row_samples * 2 + 16);
+        s += align256(isa_dngf_scratch(plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(), L->dng_version_large));
     }
     return s;
 }
 
+}  // namespace
+
+size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size, const isa_dng_layout* L, int width, int height)
+{
+    if (!file_host || isa_dng_check(L, width, height) != ISA_OK) return 0;
+    DngPlan plan;
+    if (L->compression == 7 && dng_plan(file_host, file_size, L, width, height, plan) != ISA_OK) return 0;
+    return dng_scratch_bytes(L, width, height, plan);
+}
+
+int isa_dng_decode_path(void) { return g_dng_path; }
+
 int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height,
                    void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream)
 {
+    g_dng_path = -1;
     ISA_REQ(file_host && file_dev && scratch && out, "NULL argument");
     ISA_TRY(isa_dng_check(L, width, height));
     ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
-    const size_t need = isa_dng_decode_scratch(file_host, file_size, L, width, height);
-    if (need == 0) return fail(ISA_EINVAL, "%s", g_err.empty() ? "unsupported DNG layout" : g_err.c_str());
+    DngPlan plan;
+    if (L->compression == 7) ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));
+    const size_t need = dng_scratch_bytes(L, width, height, plan);
     ISA_REQ(scratch_bytes >= need, "scratch too small (isa_dng_decode_scratch)");
     cudaStream_t st = S(stream);
     char* base = (char*)scratch;
@@ -2535,9 +2579,7 @@ int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t fil
     const uint16_t* d_tables = nullptr;
     uint16_t* d_rows = nullptr;
     int nparts = L->n;
-    DngPlan plan;
     if (L->compression == 7) {
-        ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));
         if ((size_t)4 * (4096 + 4 * (size_t)plan.jwide_max + 64) > 227 * 1024)
             return fail(ISA_EINVAL, "rows of %d samples exceed the decoder's shared-memory row buffers", plan.jwide_max);
         void* p = take(plan.parts.size());
@@ -2547,7 +2589,27 @@ int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t fil
         if (!plan.tables.empty()) ISA_CK(cudaMemcpyAsync(tb, plan.tables.data(), plan.tables.size() * 2, cudaMemcpyHostToDevice, st));
         d_parts = p;
         d_tables = tb;
+        const size_t fast = isa_dngf_scratch(plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(), L->dng_version_large);
+        if (fast > 0) {
+            // the parallel decoder; its flag sends the frame to the per-part reader
+            void* fs = take(fast);
+            int anomaly = 1;
+            ISA_CK(isa_launch_dngf(file_dev, file_size, plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(),
+                                   L->linearization ? d_lin : nullptr, L->nlin, L->black_h ? d_bh : nullptr, L->black_v ? d_bv : nullptr, width,
+                                   height, L->dng_version_large, out, out_pitch, d_err, fs, fast, &anomaly, st));
+            ISA_CK(cudaStreamSynchronize(st));
+            if (anomaly == 0) {
+                int err = err0;
+                ISA_CK(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+                g_dng_path = 1;
+                if (err != err0) return fail(ISA_EINVAL, "part %d: a decoded sample exceeds the frame's bit depth (the reference stops there)", err);
+                return ISA_OK;
+            }
+            ISA_CK(cudaMemcpyAsync(d_err, &err0, sizeof(int), cudaMemcpyHostToDevice, st));
+            ISA_CK(cudaMemset2DAsync(out, out_pitch, 0, (size_t)width * 2, height, st));
+        }
     }
+    g_dng_path = L->compression == 7 ? 0 : -1;
     ISA_CK(isa_launch_dng(file_dev, file_size, L->compression, d_parts, nparts, d_tables, d_rows, d_offs, d_cnts, L->rows_per_strip, L->bit_depth,
                           L->linearization ? d_lin : nullptr, L->nlin, L->black_h ? d_bh : nullptr, L->black_v ? d_bv : nullptr, width, height,
                           L->dng_version_large, out, out_pitch, d_err, st, plan.jwide_max, (int)plan.tables.size()));

@@ -34,6 +34,9 @@
 // one strip to the next; one thread per value.
 #include "isa_internal.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace {
 
 constexpr int PEF_NT = 256;
@@ -818,4 +821,559 @@ cudaError_t isa_launch_dng(const uint8_t* file, unsigned long long fsize, int co
         k_dng_plain<<<g, 256, 0, st>>>(A, offs, cnts, rps, depth);
     }
     return cudaGetLastError();
+}
+
+// ---- DNG lossless-JPEG parts in parallel ----
+//
+// The per-part reader above decodes each tile or strip sequentially, so a
+// frame of a few hundred tiles keeps only a few hundred lanes busy. Parts
+// whose decode is a pure bit-offset recurrence -- predictor 1, no restart
+// inside the part, one Huffman table for every component and part,
+// categories up to 16 -- are decoded instead with the scheme of the PEF
+// decoder:
+//   1. each part's bytes go to its own 128-byte-aligned region of one
+//      stream with the reader's byte skipping applied (the byte after a data
+//      0xFF is dropped, so a byte is dropped exactly when the run of 0xFF
+//      bytes before it within the part is odd); the rest of the region is
+//      0xFF, which is what the reader sees past a part's end;
+//   2. every 1024-bit chunk is decoded from each of its 32 candidate starts
+//      (a symbol is at most 16 + 16 bits); a part's first chunk starts at
+//      its bit 0 whatever state enters it;
+//   3. the start maps are chained in three levels as for PEF, with "stopped"
+//      (an empty table entry: the reader no longer advances and every later
+//      difference of the part is 0) as a 33rd state;
+//   4. each chunk's differences go to its part's sample order, the first
+//      column is summed down the rows per component (vpred), each row along
+//      itself per component, then the values are checked against the bit
+//      depth and converted as above.
+// A part whose data runs out inside its region without stopping, or a run
+// of more than 64 0xFF bytes, raises a flag, and the host decodes the frame
+// with the per-part reader instead.
+
+namespace {
+
+constexpr int DF_K = 32;           // candidate starts per chunk: one lane each
+static_assert(DF_K == 32, "a warp holds the candidates of one chunk");
+constexpr unsigned DF_STOP = 32;   // state of a stopped reader
+constexpr int DF_MS = 40;          // bytes per 33-state map (padded)
+constexpr int DF_NT = 256;
+constexpr int DF_CB = 1024;        // chunks per block of the map composition
+constexpr int DF_FF_RUN = 64;      // longest 0xFF run the byte skipping looks back over
+constexpr int DF_MAX_CLRS = 4;
+
+struct DngfPart {
+    unsigned long long pos, n;     // the part's entropy bytes in the file
+    unsigned long long reg;        // its region of the byte-skipped stream (bytes, a multiple of 128)
+    unsigned long long sbase;      // its first sample in the difference buffer
+    int cs;                        // its first chunk
+    int high, jwide, clrs, bits;
+    int out_row, out_col;
+    int pad;
+};
+
+__device__ __forceinline__ unsigned bswap32(unsigned x) { return __byte_perm(x, 0, 0x0123); }
+
+// Step 1: one CTA per part, 4 bytes per thread per pass; kept bytes placed by a block scan.
+__global__ void __launch_bounds__(1024) k_dngf_unstuff(const uint8_t* __restrict__ file, const DngfPart* __restrict__ parts, uint8_t* __restrict__ us,
+                                                       uint8_t* __restrict__ first, int* __restrict__ anomaly)
+{
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned long long carry;
+    const DngfPart P = parts[blockIdx.x];
+    if (threadIdx.x == 0) {
+        carry = 0;
+        first[P.cs] = 1;
+    }
+    __syncthreads();
+    const uint8_t* src = file + P.pos;
+    const long long n = (long long)P.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (long long b0 = 0; b0 < n; b0 += 4096) {
+        const long long i0 = b0 + 4 * (long long)threadIdx.x;
+        uint8_t v[4] = {0, 0, 0, 0};
+        unsigned keep = 0;
+        if (i0 < n) {
+            int run = 0;  // 0xFF bytes just before i0 within the part
+            for (long long j = i0 - 1; j >= 0 && run <= DF_FF_RUN; j--) {
+                if (__ldg(src + j) != 0xFF) break;
+                run++;
+            }
+            if (run > DF_FF_RUN) atomicExch(anomaly, 1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (i0 + k < n) {
+                    v[k] = __ldg(src + i0 + k);
+                    if ((run & 1) == 0) keep |= 1u << k;
+                    run = v[k] == 0xFF ? run + 1 : 0;
+                }
+            }
+        }
+        const unsigned c = __popc(keep);
+        unsigned x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        unsigned long long o = carry + (warp ? wsum[warp - 1] : 0u) + x - c;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (keep >> k & 1) us[P.reg + o++] = v[k];
+        __syncthreads();
+        if (threadIdx.x == 0) carry += wsum[31];
+        __syncthreads();
+    }
+}
+
+// Step 2: a warp per chunk (grid-stride), its 34 words staged big-endian in
+// shared memory; lane k follows candidate start k (0 for a part's first chunk).
+__global__ void __launch_bounds__(DF_NT) k_dngf_map(const unsigned* __restrict__ us, const uint8_t* __restrict__ gadv, int hmax, int adv_smem,
+                                                    const uint8_t* __restrict__ first, int nchunks, uint8_t* __restrict__ nextk,
+                                                    uint16_t* __restrict__ cntk)
+{
+    extern __shared__ __align__(16) unsigned char dfm[];
+    unsigned* cwall = (unsigned*)dfm;
+    uint8_t* sadv = dfm + (DF_NT / 32) * 34 * 4;
+    if (adv_smem) {
+        const int nw = ((1 << hmax) + 3) / 4;
+        for (int i = threadIdx.x; i < nw; i += blockDim.x) ((unsigned*)sadv)[i] = ((const unsigned*)gadv)[i];
+    }
+    __syncthreads();
+    const uint8_t* adv = adv_smem ? sadv : gadv;
+    const int warp = threadIdx.x >> 5, k = threadIdx.x & 31, sh = 32 - hmax;
+    unsigned* cw = cwall + warp * 34;
+    for (int i = blockIdx.x * (DF_NT / 32) + warp; i < nchunks; i += gridDim.x * (DF_NT / 32)) {
+        for (int t = k; t < 34; t += 32) cw[t] = bswap32(__ldg(us + (size_t)i * 32 + t));
+        __syncwarp();
+        unsigned p = first[i] ? 0u : (unsigned)k, c = 0;
+        bool stop = false;
+        while (p < 1024) {
+            const unsigned w = p >> 5;
+            const unsigned a = adv[__funnelshift_l(cw[w + 1], cw[w], p & 31) >> sh];
+            if (a == 0) {
+                stop = true;
+                break;
+            }
+            p += a;
+            c++;
+        }
+        nextk[(size_t)i * 32 + k] = stop ? (uint8_t)DF_STOP : (uint8_t)(p - 1024);
+        cntk[(size_t)i * 32 + k] = (uint16_t)c;
+        __syncwarp();
+    }
+}
+
+// Step 3a: per block of DF_CB = 32 x 32 chunks, the 33-state map of each warp's 32 chunks and the block's map.
+__global__ void __launch_bounds__(1024) k_dngf_compose(const uint8_t* __restrict__ nextk, const uint8_t* __restrict__ first, int nchunks,
+                                                       uint8_t* __restrict__ sub_map, uint8_t* __restrict__ block_map)
+{
+    __shared__ uint8_t m[DF_CB][33];
+    __shared__ uint8_t sm[32][DF_MS];
+    const int c0 = blockIdx.x * DF_CB, n = min(DF_CB, nchunks - c0);
+    for (int t = threadIdx.x; t < n * 32; t += blockDim.x) m[t >> 5][t & 31] = nextk[(size_t)c0 * 32 + t];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) m[q][32] = first[c0 + q] ? m[q][0] : (uint8_t)DF_STOP;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, j = threadIdx.x & 31;
+    for (int e = j; e < 33; e += 32) {
+        unsigned s = (unsigned)e;
+        for (int q = warp * 32; q < min(n, warp * 32 + 32); q++) s = m[q][s];
+        sm[warp][e] = (uint8_t)s;
+        sub_map[((size_t)blockIdx.x * 32 + warp) * DF_MS + e] = (uint8_t)s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int e = j; e < 33; e += 32) {
+            unsigned b = (unsigned)e;
+            for (int w = 0; w < 32; w++) b = sm[w][b];
+            block_map[(size_t)blockIdx.x * DF_MS + e] = (uint8_t)b;
+        }
+    }
+}
+
+// Step 3b: one thread walks the block maps: every block's entry state (chunk 0 starts a part).
+__global__ void k_dngf_chain(const uint8_t* __restrict__ block_map, int nblocks, uint8_t* __restrict__ block_in)
+{
+    extern __shared__ uint8_t dbm[];
+    for (int t = threadIdx.x; t < nblocks * DF_MS; t += blockDim.x) dbm[t] = block_map[t];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    unsigned s = 0;
+    for (int b = 0; b < nblocks; b++) {
+        block_in[b] = (uint8_t)s;
+        s = dbm[b * DF_MS + s];
+    }
+}
+
+// Step 3c: warp entry states, then lane 0 of each warp walks its chunks
+// (entry state, count); the counts are scanned within the block.
+__global__ void __launch_bounds__(1024) k_dngf_walk(const uint8_t* __restrict__ nextk, const uint16_t* __restrict__ cntk,
+                                                    const uint8_t* __restrict__ sub_map, const uint8_t* __restrict__ block_in,
+                                                    const uint8_t* __restrict__ first, int nchunks, uint8_t* __restrict__ sin,
+                                                    unsigned* __restrict__ loc, unsigned* __restrict__ block_total)
+{
+    __shared__ uint8_t wentry[32];
+    __shared__ unsigned wtot[32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c0 = blockIdx.x * DF_CB, n = min(DF_CB, nchunks - c0);
+    if (threadIdx.x == 0) {
+        unsigned s = block_in[blockIdx.x];
+        for (int w = 0; w < 32; w++) {
+            wentry[w] = (uint8_t)s;
+            s = sub_map[((size_t)blockIdx.x * 32 + w) * DF_MS + s];
+        }
+    }
+    __syncthreads();
+    if (lane == 0) {
+        unsigned s = wentry[warp];
+        for (int q = 0; q < 32; q++) {
+            const int ci = warp * 32 + q;
+            if (ci >= n) break;
+            const int i = c0 + ci;
+            if (first[i]) s = 0;
+            sin[i] = (uint8_t)s;
+            if (s == DF_STOP) {
+                loc[i] = 0;
+                continue;
+            }
+            loc[i] = cntk[(size_t)i * 32 + s];
+            s = nextk[(size_t)i * 32 + s];
+        }
+    }
+    __syncwarp();
+    const int ci = warp * 32 + lane;
+    const unsigned my = ci < n ? loc[c0 + ci] : 0u;
+    unsigned x = my;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wtot[warp] = x;
+    __syncthreads();
+    unsigned wpre = 0;
+    for (int w = 0; w < warp; w++) wpre += wtot[w];
+    if (ci < n) loc[c0 + ci] = wpre + x - my;
+    if (threadIdx.x == 0) {
+        unsigned tot = 0;
+        for (int w = 0; w < 32; w++) tot += wtot[w];
+        block_total[blockIdx.x] = tot;
+    }
+}
+
+__device__ __forceinline__ unsigned long long df_sym(const unsigned long long* __restrict__ boff, const unsigned* __restrict__ loc, int nchunks,
+                                                     int nblocks, int i)
+{
+    return i < nchunks ? boff[i / DF_CB] + loc[i] : boff[nblocks];
+}
+
+// Per part: its first symbol's index in the chunk scan; a part that ends
+// short of its samples without stopping ran out of its region (flag).
+__global__ void k_dngf_parts(const DngfPart* __restrict__ parts, int nparts, int nchunks, int nblocks, const uint8_t* __restrict__ nextk,
+                             const uint8_t* __restrict__ sin, const unsigned* __restrict__ loc, const unsigned long long* __restrict__ boff,
+                             unsigned long long* __restrict__ g0, int* __restrict__ anomaly)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nparts) return;
+    const int a = parts[t].cs, e = t + 1 < nparts ? parts[t + 1].cs : nchunks;
+    const unsigned long long ga = df_sym(boff, loc, nchunks, nblocks, a), ge = df_sym(boff, loc, nchunks, nblocks, e);
+    g0[t] = ga;
+    const unsigned long long S = (unsigned long long)parts[t].high * parts[t].jwide;
+    if (ge - ga < S) {
+        const unsigned s = sin[e - 1];
+        const unsigned exit = s == DF_STOP ? DF_STOP : nextk[(size_t)(e - 1) * 32 + s];
+        if (exit != DF_STOP) atomicExch(anomaly, 1);
+    }
+}
+
+// Step 4a: every chunk's differences (as 16-bit residues) at its part's
+// sample offsets; one thread per chunk, the CTA's chunks staged with one
+// skew word per 32.
+__global__ void __launch_bounds__(DF_NT) k_dngf_emit(const unsigned* __restrict__ us, unsigned long long nwords, const DngfPart* __restrict__ parts,
+                                                     const int* __restrict__ cs, int nparts, int nchunks, int nblocks, const uint8_t* __restrict__ sin,
+                                                     const unsigned* __restrict__ loc, const unsigned long long* __restrict__ boff,
+                                                     const unsigned long long* __restrict__ g0, const uint16_t* __restrict__ gtab, int hmax,
+                                                     int tab_smem, int large, uint16_t* __restrict__ diff)
+{
+    extern __shared__ __align__(16) unsigned char dfe[];
+    unsigned* cw = (unsigned*)dfe;
+    uint16_t* stab = (uint16_t*)(dfe + (DF_NT * 33 + 4) * 4);
+    const int c0 = blockIdx.x * DF_NT;
+    for (int j = threadIdx.x; j < DF_NT * 32 + 2; j += DF_NT) {
+        const unsigned long long g = (unsigned long long)c0 * 32 + j;
+        cw[j + (j >> 5)] = g < nwords ? bswap32(__ldg(us + g)) : 0xffffffffu;
+    }
+    if (tab_smem)
+        for (int i = threadIdx.x; i <= (1 << hmax); i += DF_NT) stab[i] = gtab[i];
+    __syncthreads();
+    const uint16_t* tab = (tab_smem ? stab : gtab) + 1;
+    const int i = c0 + threadIdx.x;
+    if (i >= nchunks) return;
+    unsigned p = sin[i];
+    if (p == DF_STOP) return;
+    int lo = 0, hi = nparts - 1;  // the last part whose first chunk is <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(cs + mid) <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    const DngfPart& P = parts[lo];
+    const unsigned long long S = (unsigned long long)P.high * P.jwide;
+    unsigned long long o = df_sym(boff, loc, nchunks, nblocks, i) - g0[lo];
+    if (o >= S) return;
+    const unsigned* cb = cw + 33 * threadIdx.x;
+    const int sh = 32 - hmax;
+    while (p < 1024 && o < S) {
+        const unsigned w = p >> 5;
+        const unsigned x = __funnelshift_l(cb[w + 1 + ((w + 1) >> 5)], cb[w], p & 31);
+        const unsigned e = tab[x >> sh];
+        const int clen = (int)(e >> 8), cat = (int)(e & 255);
+        if (clen == 0) break;
+        int d;
+        if (cat == 16 && large) {
+            d = -32768;
+            p += clen;
+        } else {
+            d = cat ? (int)((x << clen) >> (32 - cat)) : 0;
+            if (cat && ((d >> (cat - 1)) & 1) == 0) d -= (1 << cat) - 1;
+            p += clen + cat;
+        }
+        diff[P.sbase + o++] = (uint16_t)d;
+    }
+}
+
+// Step 4b: the first column of each component summed down the rows from
+// 1 << (bits - 1), written back as values; a warp per (part, component).
+__global__ void k_dngf_cols(const DngfPart* __restrict__ parts, int nparts, uint16_t* __restrict__ diff)
+{
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int t = gw / DF_MAX_CLRS, c = gw % DF_MAX_CLRS;
+    if (t >= nparts) return;
+    const DngfPart P = parts[t];
+    if (c >= P.clrs) return;
+    unsigned carry = 1u << (P.bits - 1);
+    for (int base = 0; base < P.high; base += 32) {
+        const int r = base + lane;
+        const size_t at = P.sbase + (size_t)r * P.jwide + c;
+        unsigned x = r < P.high ? diff[at] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (r < P.high) diff[at] = (uint16_t)(carry + x);
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+}
+
+// Step 4c: a warp per (part, row): per component the running sum along the
+// row, the bit-depth check, the conversion and the store.
+__global__ void __launch_bounds__(256) k_dngf_rows(const DngArgs A, const DngfPart* __restrict__ parts, const uint16_t* __restrict__ diff)
+{
+    const int t = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const DngfPart& P = parts[t];
+    const int r = blockIdx.x * 8 + warp;
+    if (r >= P.high) return;
+    const uint16_t* drow = diff + P.sbase + (size_t)r * P.jwide;
+    const int orow = P.out_row + r;
+    uint16_t* o = orow < A.H ? isa::row_ptr(A.out, A.out_pitch, orow) : nullptr;
+    const int clrs = P.clrs, jwide = P.jwide;
+    unsigned carry[DF_MAX_CLRS] = {0u, 0u, 0u, 0u};
+    bool bad = false;
+    for (int base = 0; base < jwide; base += 32 * clrs) {
+#pragma unroll
+        for (int c = 0; c < DF_MAX_CLRS; c++) {
+            if (c >= clrs) break;
+            const int j = base + lane * clrs + c;
+            unsigned x = j < jwide ? drow[j] : 0u;
+#pragma unroll
+            for (int q = 1; q < 32; q <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, x, q);
+                if (lane >= q) x += y;
+            }
+            const uint16_t v = (uint16_t)(carry[c] + x);
+            carry[c] += __shfl_sync(0xffffffffu, x, 31);
+            if (j < jwide) {
+                if (v >> P.bits) bad = true;
+                const int ocol = P.out_col + j;
+                if (o && ocol < A.W) o[ocol] = dng_value(A, v, orow, ocol);
+            }
+        }
+    }
+    if (bad) atomicMin(A.error, t);
+}
+
+struct DngfPlan {
+    std::vector<DngfPart> parts;
+    std::vector<int> cs;
+    std::vector<uint8_t> adv;
+    const uint16_t* table = nullptr;   // 1 + 2^hmax entries
+    int hmax = 0, nchunks = 0, nblocks = 0;
+    unsigned long long samples = 0;
+    size_t part[20] = {};
+    size_t bytes = 0;
+};
+
+size_t df_align(size_t v) { return (v + 255) / 256 * 256; }
+
+bool dngf_plan(const Lj92Part* L, int nparts, const uint16_t* tables, size_t ntables, int large, DngfPlan& pl)
+{
+    if (nparts < 1 || nparts > 65535 || ntables == 0) return false;
+    const int tab = L[0].table[0];
+    pl.parts.resize(nparts);
+    pl.cs.resize(nparts + 1);
+    unsigned long long reg = 0, sbase = 0;
+    for (int t = 0; t < nparts; t++) {
+        const Lj92Part& p = L[t];
+        if (p.skip || p.psv != 1 || p.sraw != 0 || p.clrs < 1 || p.clrs > DF_MAX_CLRS || p.bits < 1 || p.bits > 16) return false;
+        if ((long long)p.restart < (long long)p.high * p.wide) return false;  // a restart inside the part
+        for (int c = 0; c < p.clrs; c++)
+            if (p.table[c] != tab) return false;
+        DngfPart& q = pl.parts[t];
+        q.pos = p.pos;
+        q.n = p.end > p.pos ? p.end - p.pos : 0;
+        q.reg = reg;
+        q.sbase = sbase;
+        q.cs = (int)(reg / 128);
+        q.high = p.high;
+        q.jwide = p.wide * p.clrs;
+        q.clrs = p.clrs;
+        q.bits = p.bits;
+        q.out_row = p.out_row;
+        q.out_col = p.out_col;
+        pl.cs[t] = q.cs;
+        reg += (q.n + 256 + 127) / 128 * 128;
+        sbase += (unsigned long long)q.high * q.jwide;
+    }
+    if (reg / 128 > 0x7fffffffull) return false;
+    pl.nchunks = (int)(reg / 128);
+    pl.cs[nparts] = pl.nchunks;
+    pl.nblocks = (pl.nchunks + DF_CB - 1) / DF_CB;
+    if ((size_t)pl.nblocks * DF_MS > 200 * 1024) return false;
+    pl.samples = sbase;
+    if ((size_t)tab >= ntables) return false;
+    pl.hmax = tables[tab];
+    if (pl.hmax < 1 || pl.hmax > 16 || (size_t)tab + 1 + ((size_t)1 << pl.hmax) > ntables) return false;
+    pl.table = tables + tab;
+    pl.adv.assign(std::max<size_t>((size_t)1 << pl.hmax, 4), 0);
+    for (int i = 0; i < 1 << pl.hmax; i++) {
+        const int e = pl.table[1 + i], clen = e >> 8, cat = e & 255;
+        if (clen == 0) continue;
+        if (cat > 16) return false;
+        pl.adv[i] = (uint8_t)(clen + ((cat == 16 && large) ? 0 : cat));
+    }
+    // scratch layout
+    const size_t sizes[] = {
+        (size_t)nparts * sizeof(DngfPart),               // 0 parts
+        (size_t)(nparts + 1) * 4,                        // 1 cs
+        (size_t)pl.nchunks * 128 + 256,                  // 2 byte-skipped stream (0xFF past each part)
+        (size_t)pl.nchunks,                              // 3 first
+        (size_t)pl.nchunks * 32,                         // 4 nextk
+        (size_t)pl.nchunks * 64,                         // 5 cntk
+        (size_t)pl.nchunks,                              // 6 sin
+        (size_t)pl.nchunks * 4,                          // 7 loc
+        (size_t)pl.nblocks * 32 * DF_MS,                 // 8 sub_map
+        (size_t)pl.nblocks * DF_MS,                      // 9 block_map
+        (size_t)pl.nblocks,                              // 10 block_in
+        (size_t)pl.nblocks * 4,                          // 11 block_total
+        (size_t)(pl.nblocks + 1) * 8,                    // 12 boff
+        (size_t)nparts * 8,                              // 13 g0
+        (size_t)pl.samples * 2 + 16,                     // 14 differences
+        ((size_t)1 + ((size_t)1 << pl.hmax)) * 2,        // 15 table
+        pl.adv.size(),                                   // 16 advance table
+        16,                                              // 17 flag
+    };
+    size_t o = 0;
+    for (int k = 0; k < 18; k++) {
+        pl.part[k] = o;
+        o += df_align(sizes[k]);
+    }
+    pl.bytes = o;
+    return true;
+}
+
+}  // namespace
+
+size_t isa_dngf_scratch(const void* parts, int nparts, const uint16_t* tables, size_t ntables, int large)
+{
+    DngfPlan pl;
+    return dngf_plan((const Lj92Part*)parts, nparts, tables, ntables, large, pl) ? pl.bytes : 0;
+}
+
+cudaError_t isa_launch_dngf(const uint8_t* file, unsigned long long fsize, const void* parts_host, int nparts, const uint16_t* tables_host,
+                            size_t ntables, const uint16_t* lin, int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large,
+                            uint16_t* out, size_t out_pitch, int* error, void* scratch, size_t scratch_bytes, int* anomaly_host, cudaStream_t st)
+{
+    DngfPlan pl;
+    if (!dngf_plan((const Lj92Part*)parts_host, nparts, tables_host, ntables, large, pl) || scratch_bytes < pl.bytes) return cudaErrorInvalidValue;
+    char* base = (char*)scratch;
+    DngfPart* d_parts = (DngfPart*)(base + pl.part[0]);
+    int* d_cs = (int*)(base + pl.part[1]);
+    uint8_t* us = (uint8_t*)(base + pl.part[2]);
+    uint8_t* first = (uint8_t*)(base + pl.part[3]);
+    uint8_t* nextk = (uint8_t*)(base + pl.part[4]);
+    uint16_t* cntk = (uint16_t*)(base + pl.part[5]);
+    uint8_t* sin = (uint8_t*)(base + pl.part[6]);
+    unsigned* loc = (unsigned*)(base + pl.part[7]);
+    uint8_t* sub_map = (uint8_t*)(base + pl.part[8]);
+    uint8_t* block_map = (uint8_t*)(base + pl.part[9]);
+    uint8_t* block_in = (uint8_t*)(base + pl.part[10]);
+    unsigned* block_total = (unsigned*)(base + pl.part[11]);
+    unsigned long long* boff = (unsigned long long*)(base + pl.part[12]);
+    unsigned long long* g0 = (unsigned long long*)(base + pl.part[13]);
+    uint16_t* diff = (uint16_t*)(base + pl.part[14]);
+    uint16_t* gtab = (uint16_t*)(base + pl.part[15]);
+    uint8_t* gadv = (uint8_t*)(base + pl.part[16]);
+    int* d_anomaly = (int*)(base + pl.part[17]);
+    for (const DngfPart& p : pl.parts)
+        if (p.pos + p.n > fsize) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(d_parts, pl.parts.data(), pl.parts.size() * sizeof(DngfPart), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(d_cs, pl.cs.data(), pl.cs.size() * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(gtab, pl.table, ((size_t)1 + ((size_t)1 << pl.hmax)) * 2, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(gadv, pl.adv.data(), pl.adv.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(us, 0xFF, (size_t)pl.nchunks * 128 + 256, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(first, 0, (size_t)pl.nchunks, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(diff, 0, (size_t)pl.samples * 2 + 16, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_anomaly, 0, 16, st)) != cudaSuccess) return e;
+    k_dngf_unstuff<<<nparts, 1024, 0, st>>>(file, d_parts, us, first, d_anomaly);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int adv_smem = (1 << pl.hmax) <= 16384;
+    const size_t map_smem = (size_t)(DF_NT / 32) * 34 * 4 + (adv_smem ? pl.adv.size() : 0);
+    if ((e = cudaFuncSetAttribute(k_dngf_map, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)map_smem)) != cudaSuccess) return e;
+    const unsigned mapg = (unsigned)std::min<long long>((pl.nchunks + DF_NT / 32 - 1) / (DF_NT / 32), (long long)sms * 8);
+    k_dngf_map<<<mapg, DF_NT, map_smem, st>>>((const unsigned*)us, gadv, pl.hmax, adv_smem, first, pl.nchunks, nextk, cntk);
+    k_dngf_compose<<<pl.nblocks, 1024, 0, st>>>(nextk, first, pl.nchunks, sub_map, block_map);
+    const size_t chain_smem = (size_t)pl.nblocks * DF_MS;
+    if ((e = cudaFuncSetAttribute(k_dngf_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem)) != cudaSuccess) return e;
+    k_dngf_chain<<<1, 256, chain_smem, st>>>(block_map, pl.nblocks, block_in);
+    k_dngf_walk<<<pl.nblocks, 1024, 0, st>>>(nextk, cntk, sub_map, block_in, first, pl.nchunks, sin, loc, block_total);
+    k_pef_scan<<<1, 1024, 0, st>>>(block_total, pl.nblocks, boff);
+    k_dngf_parts<<<(nparts + 255) / 256, 256, 0, st>>>(d_parts, nparts, pl.nchunks, pl.nblocks, nextk, sin, loc, boff, g0, d_anomaly);
+    const int tab_smem = (1 << pl.hmax) <= 8192;
+    const size_t emit_smem = (size_t)(DF_NT * 33 + 4) * 4 + (tab_smem ? ((size_t)1 + ((size_t)1 << pl.hmax)) * 2 : 0);
+    if ((e = cudaFuncSetAttribute(k_dngf_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emit_smem)) != cudaSuccess) return e;
+    k_dngf_emit<<<(pl.nchunks + DF_NT - 1) / DF_NT, DF_NT, emit_smem, st>>>((const unsigned*)us, (unsigned long long)pl.nchunks * 32 + 64, d_parts, d_cs,
+                                                                          nparts, pl.nchunks, pl.nblocks, sin, loc, boff, g0, gtab, pl.hmax, tab_smem,
+                                                                          large, diff);
+    k_dngf_cols<<<(nparts * DF_MAX_CLRS * 32 + 255) / 256, 256, 0, st>>>(d_parts, nparts, diff);
+    int max_high = 1;
+    for (const DngfPart& p : pl.parts) max_high = std::max(max_high, p.high);
+    DngArgs A{file, fsize, nullptr, nparts, nullptr, nullptr, lin, nlin, bh, bv, W, H, large, out, out_pitch, error};
+    k_dngf_rows<<<dim3((max_high + 7) / 8, nparts), 256, 0, st>>>(A, d_parts, diff);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaMemcpyAsync(anomaly_host, d_anomaly, sizeof(int), cudaMemcpyDeviceToHost, st);
 }

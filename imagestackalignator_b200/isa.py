@@ -77,7 +77,7 @@ EXPORTS = [
     "isa_color_twists", "isa_postprocess", "isa_save_tiff16", "isa_save_as_16bit_tiff",
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
     "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
-    "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec",
+    "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec", "isa_dng_decode_path",
 ]
 
 _lib = None
@@ -562,6 +562,11 @@ def dng_levels(width, height, cfa_pattern, white_level, camera_white, cfa_repeat
                 color_twist_identity=bool(r.color_twist_identity), crop=tuple(r.crop), black_h=bh, black_v=bv, info=i)
 
 
+def dng_decode_path():
+    """isa_dng_decode_path: 1 parallel decoder, 0 per-part reader, -1 none (the calling thread's last isa_dng_decode)."""
+    return int(lib().isa_dng_decode_path())
+
+
 class IsaDngLayout(ctypes.Structure):
     _fields_ = [("tiled", ctypes.c_int), ("tile_width", ctypes.c_int), ("tile_height", ctypes.c_int), ("rows_per_strip", ctypes.c_int),
                 ("n", ctypes.c_int), ("offsets", ctypes.c_void_p), ("byte_counts", ctypes.c_void_p), ("compression", ctypes.c_int),
@@ -570,9 +575,11 @@ class IsaDngLayout(ctypes.Structure):
 
 
 def dng_decode(file, width, height, offsets, counts, compression=7, tiled=True, tile_w=0, tile_h=0, rows_per_strip=0, bit_depth=16, large=True,
-               linearization=None, black_h=None, black_v=None, file_dev=None, stream=None):
+               linearization=None, black_h=None, black_v=None, file_dev=None, stream=None, scratch=None, out=None):
     """isa_dng_decode of a DNG file image (host uint8 array; copied to the
-    device unless file_dev is given); returns the frame (int16 tensor holding uint16)."""
+    device unless file_dev is given); returns the frame (int16 tensor holding
+    uint16). scratch / out: device buffers to reuse (scratch of at least
+    isa_dng_decode_scratch bytes)."""
     import torch
     f = np.ascontiguousarray(file, np.uint8)
     keep = [np.ascontiguousarray(offsets, np.uint32), np.ascontiguousarray(counts, np.uint32)]
@@ -584,15 +591,32 @@ def dng_decode(file, width, height, offsets, counts, compression=7, tiled=True, 
                      int(large), None if lin is None else lin.ctypes.data, 0 if lin is None else lin.size,
                      None if bh is None else bh.ctypes.data, None if bv is None else bv.ctypes.data)
     fp = f.ctypes.data_as(ctypes.c_void_p)
-    need = lib().isa_dng_decode_scratch(fp, ctypes.c_size_t(f.size), ctypes.byref(L), width, height)
+    dev = file_dev if file_dev is not None else torch.from_numpy(f).cuda()
+    if scratch is None:
+        need = lib().isa_dng_decode_scratch(fp, ctypes.c_size_t(f.size), ctypes.byref(L), width, height)
+        if need == 0:
+            raise IsaError(ISA_EINVAL, lib().isa_last_error().decode())
+        scratch = torch.empty(need, dtype=torch.uint8, device=dev.device)
+    if out is None:
+        out = torch.empty((height, width), dtype=torch.int16, device=dev.device)
+    check(lib().isa_dng_decode(fp, vp(dev), ctypes.c_size_t(f.size), ctypes.byref(L), width, height, vp(scratch), ctypes.c_size_t(scratch.numel()),
+                               vp(out), ctypes.c_size_t(out.stride(0) * 2), stream_ptr(stream)))
+    return out
+
+
+def dng_decode_scratch(file, width, height, offsets, counts, compression=7, tiled=True, tile_w=0, tile_h=0, rows_per_strip=0, bit_depth=16,
+                       large=True, linearization=None):
+    """isa_dng_decode_scratch: device bytes isa_dng_decode needs for this file and layout."""
+    f = np.ascontiguousarray(file, np.uint8)
+    off = np.ascontiguousarray(offsets, np.uint32)
+    cnt = np.ascontiguousarray(counts, np.uint32)
+    nlin = 0 if linearization is None else len(linearization)
+    L = IsaDngLayout(int(tiled), tile_w, tile_h, rows_per_strip, len(off), off.ctypes.data, cnt.ctypes.data, compression, bit_depth, int(large),
+                     None, nlin, None, None)
+    need = lib().isa_dng_decode_scratch(f.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(f.size), ctypes.byref(L), width, height)
     if need == 0:
         raise IsaError(ISA_EINVAL, lib().isa_last_error().decode())
-    dev = file_dev if file_dev is not None else torch.from_numpy(f).cuda()
-    scratch = torch.empty(need, dtype=torch.uint8, device=dev.device)
-    out = torch.empty((height, width), dtype=torch.int16, device=dev.device)
-    check(lib().isa_dng_decode(fp, vp(dev), ctypes.c_size_t(f.size), ctypes.byref(L), width, height, vp(scratch), ctypes.c_size_t(need), vp(out),
-                               ctypes.c_size_t(width * 2), stream_ptr(stream)))
-    return out
+    return int(need)
 
 
 class IsaBurst(ctypes.Structure):

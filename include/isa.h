@@ -495,6 +495,13 @@ ISA_API size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size
  * stop (a sample above the frame's bit depth). */
 ISA_API int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* layout, int width, int height,
                            void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream);
+/* Which decoder the calling thread's last isa_dng_decode used: 1 = the
+ * parallel one (lossless-JPEG parts with predictor 1, no restart inside a
+ * part, one Huffman table: chunks decoded from every candidate start, as
+ * isa_pef_decode), 0 = one warp per part with the reference's sequential
+ * reader (every other layout, and frames the parallel decoder hands back),
+ * -1 = none (an argument error or uncompressed strips). */
+ISA_API int isa_dng_decode_path(void);
 
 /* ---- Raw-file metadata: DNG levels, camera profiles ----
  * DNGFile.SetMembers (PefFile/DNGFile.cs:714-951) and the DNGFile

@@ -3,7 +3,11 @@ reader (oracle/raw.py over orc_dng_decode), bit-exact: lossless-JPEG tiles
 with every predictor and one or two interleaved components, strips,
 restart markers, tiles that overhang the frame, linearisation and black-
 level deltas, a sample above the bit depth (the reference stops), and
-uncompressed 16-bit and packed strips."""
+uncompressed 16-bit and packed strips. Predictor-1 frames without restarts
+go through the parallel decoder (isa_dng_decode_path() == 1), the rest
+through the per-part reader; random entropy data (0xFF runs, empty code
+entries, data that ends early) and the hand-back to the per-part reader
+are checked on both."""
 import numpy as np
 import pytest
 
@@ -32,6 +36,67 @@ def test_lj92_tiles(cuda, psv, clrs):
     st, want = R.dng_decode(f, W, H, offs, cnts, **kw)
     assert st == 0 and np.array_equal(want, img)
     assert np.array_equal(run(f, W, H, offs, cnts, **kw), want)
+    assert isa.dng_decode_path() == (1 if psv == 1 else 0)
+
+
+def _data_start(part):
+    """Offset of the entropy data in a lossless-JPEG part (after the SOS segment)."""
+    p = bytes(bytearray(part))
+    pos = 2
+    while True:
+        tag = p[pos] << 8 | p[pos + 1]
+        pos += 2 + (p[pos + 2] << 8 | p[pos + 3])
+        if tag == 0xFFDA:
+            return pos
+
+
+def _random_entropy(f, offs, cnts, seed, ff, nbytes=None, ff_run=0):
+    """The same headers with random entropy bytes (a fraction `ff` of them 0xFF, optionally one long 0xFF run)."""
+    r = np.random.default_rng(seed)
+    parts, no, nc, pos = [f[:offs[0]]], [], [], offs[0]
+    for o, c in zip(offs, cnts):
+        p = f[o:o + c]
+        h = _data_start(p)
+        n = nbytes if nbytes is not None else c - h
+        d = r.integers(0, 256, n).astype(np.uint8)
+        d[r.random(n) < ff] = 0xFF
+        if ff_run:
+            d[n // 2:n // 2 + ff_run] = 0xFF
+        q = np.concatenate([p[:h], d])
+        no.append(pos); nc.append(len(q)); parts.append(q); pos += len(q)
+    return np.concatenate(parts), no, nc
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_lj92_random_entropy_data(cuda, seed):
+    """16-bit frames (every decoded value is in range) whose entropy bytes are random: 0xFF
+    runs for the byte skipping, empty code-book entries that stop a part, data that ends early."""
+    rng = np.random.default_rng(100 + seed)
+    H, W = 120, 200
+    img = rng.integers(0, 32768, (H, W)).astype(np.uint16)  # differences stay inside categories 0..15
+    clrs = 1 + seed % 2
+    f, offs, cnts = R.dng_tiles(img, 64, 40, clrs=clrs, bits=16, psv=1)
+    nbytes = [None, None, None, 50, None, 7, None, None][seed]
+    f, offs, cnts = _random_entropy(f, offs, cnts, seed, ff=[0.02, 0.3, 0.6, 0.0, 0.1, 0.0, 0.45, 0.05][seed], nbytes=nbytes)
+    kw = dict(tiled=True, tile_w=64, tile_h=40, large=seed % 3 != 0)
+    st, want = R.dng_decode(f, W, H, offs, cnts, **kw)
+    assert st == 0
+    assert np.array_equal(run(f, W, H, offs, cnts, **kw), want)
+    assert isa.dng_decode_path() == 1
+
+
+def test_lj92_long_ff_run_goes_to_the_per_part_reader(cuda):
+    """A run of more than 64 0xFF bytes is handed back to the per-part reader: same result."""
+    rng = np.random.default_rng(7)
+    H, W = 80, 128
+    img = rng.integers(0, 32768, (H, W)).astype(np.uint16)  # differences stay inside categories 0..15
+    f, offs, cnts = R.dng_tiles(img, 64, 40, clrs=2, bits=16, psv=1)
+    f, offs, cnts = _random_entropy(f, offs, cnts, 3, ff=0.05, ff_run=101)
+    kw = dict(tiled=True, tile_w=64, tile_h=40)
+    st, want = R.dng_decode(f, W, H, offs, cnts, **kw)
+    assert st == 0
+    assert np.array_equal(run(f, W, H, offs, cnts, **kw), want)
+    assert isa.dng_decode_path() == 0
 
 
 def test_lj92_strips_restart_lin_black(cuda):
@@ -62,6 +127,7 @@ def test_lj92_overhanging_tiles_and_large_frame(cuda):
     st, want = R.dng_decode(f, W, H, offs, cnts, **kw)
     assert st == 0 and np.array_equal(want, img)
     assert np.array_equal(run(f, W, H, offs, cnts, **kw), want)
+    assert isa.dng_decode_path() == 1
 
 
 def test_lj92_sample_above_bit_depth_is_an_error(cuda):
