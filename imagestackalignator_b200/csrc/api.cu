@@ -35,6 +35,17 @@ int fail(int code, const char* fmt, ...)
     return code;
 }
 
+}  // namespace
+
+// The calling thread's error message, for the other host files of the library.
+int isa_set_error(int code, const char* msg)
+{
+    g_err = msg ? msg : "";
+    return code;
+}
+
+namespace {
+
 #define ISA_CK(call)                                                                         \
     do {                                                                                     \
         cudaError_t e_ = (call);                                                             \

@@ -190,6 +190,9 @@ int isa_pef_max_blocks();
 cudaError_t isa_launch_pef_unpack(const uint8_t* file, unsigned long long fsize, const uint32_t* offsets, const uint32_t* sizes, int nstrips,
                                   int rows_per_strip, int W, int H, int depth, uint16_t* out, size_t out_pitch, cudaStream_t st);
 
+// api.cu: sets the calling thread's isa_last_error message and returns code
+int isa_set_error(int code, const char* msg);
+
 // raw.cu: DNG pixel data (isa_dng_decode)
 size_t isa_dng_part_bytes();
 void isa_dng_part_set(void* dst, int i, unsigned long long pos, unsigned long long end, int skip, const int* hdr, int out_row, int out_col,

@@ -78,6 +78,7 @@ EXPORTS = [
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
     "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
     "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec", "isa_dng_decode_path",
+    "isa_dng_open", "isa_dng_close", "isa_dng_file_info",
 ]
 
 _lib = None
@@ -617,6 +618,47 @@ def dng_decode_scratch(file, width, height, offsets, counts, compression=7, tile
     if need == 0:
         raise IsaError(ISA_EINVAL, lib().isa_last_error().decode())
     return int(need)
+
+
+def _arr(ptr, n, ctype):
+    if not ptr or n <= 0:
+        return None
+    return list(ctypes.cast(ptr, ctypes.POINTER(ctype))[:n])
+
+
+def dng_open(file):
+    """isa_dng_open + isa_dng_file_info of a DNG file image (host bytes): a dict
+    with width, height and the keyword arguments of dng_decode ("layout"),
+    dng_levels ("levels", without camera_white) and dng_color_spec ("color")."""
+    f = np.ascontiguousarray(np.frombuffer(bytes(file), np.uint8) if isinstance(file, (bytes, bytearray)) else file, np.uint8)
+    h = ctypes.c_void_p()
+    check(lib().isa_dng_open(f.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(f.size), ctypes.byref(h)))
+    try:
+        L, G, C = IsaDngLayout(), IsaDngLevelTags(), IsaDngColorTags()
+        W, H = ctypes.c_int(), ctypes.c_int()
+        check(lib().isa_dng_file_info(h, ctypes.byref(L), ctypes.byref(G), ctypes.byref(C), ctypes.byref(W), ctypes.byref(H)))
+        layout = dict(tiled=bool(L.tiled), tile_w=L.tile_width, tile_h=L.tile_height, rows_per_strip=L.rows_per_strip,
+                      offsets=_arr(L.offsets, L.n, ctypes.c_uint32), counts=_arr(L.byte_counts, L.n, ctypes.c_uint32),
+                      compression=L.compression, bit_depth=L.bit_depth, large=bool(L.dng_version_large),
+                      linearization=_arr(L.linearization, L.nlin, ctypes.c_uint16))
+        levels = dict(width=G.width, height=G.height, cfa_pattern=_arr(G.cfa_pattern, 4, ctypes.c_uint8),
+                      cfa_repeat=(G.cfa_repeat_w, G.cfa_repeat_h), white_level=G.white_level,
+                      plane_color=_arr(G.plane_color, G.n_plane_color, ctypes.c_int), black_level=_arr(G.black_level, G.n_black, ctypes.c_double),
+                      active_area=_arr(G.active_area, 4, ctypes.c_int), default_crop_origin=_arr(G.default_crop_origin, 2, ctypes.c_double),
+                      default_crop_size=_arr(G.default_crop_size, 2, ctypes.c_double),
+                      noise_profile=_arr(G.noise_profile, G.n_noise, ctypes.c_double),
+                      black_delta_h=_arr(G.black_delta_h, G.n_delta_h, ctypes.c_double),
+                      black_delta_v=_arr(G.black_delta_v, G.n_delta_v, ctypes.c_double), iso=G.iso)
+        color = dict(color_matrix1=_arr(C.color_matrix1, 9, ctypes.c_double), color_matrix2=_arr(C.color_matrix2, 9, ctypes.c_double),
+                     illuminant1=C.illuminant1, illuminant2=C.illuminant2, forward_matrix1=_arr(C.forward_matrix1, 9, ctypes.c_double),
+                     forward_matrix2=_arr(C.forward_matrix2, 9, ctypes.c_double),
+                     camera_calibration1=_arr(C.camera_calibration1, 9, ctypes.c_double),
+                     camera_calibration2=_arr(C.camera_calibration2, 9, ctypes.c_double),
+                     analog_balance=_arr(C.analog_balance, 3, ctypes.c_double), as_shot_neutral=_arr(C.as_shot_neutral, 3, ctypes.c_double),
+                     as_shot_white_xy=_arr(C.as_shot_white_xy, 2, ctypes.c_double))
+        return dict(width=W.value, height=H.value, layout=layout, levels=levels, color=color)
+    finally:
+        lib().isa_dng_close(h)
 
 
 class IsaBurst(ctypes.Structure):

@@ -321,3 +321,114 @@ def dng_tiled_file(img, tile_w=256, tile_h=256, clrs=2, bits=14, head=64):
             parts.append(s)
             pos += len(s)
     return np.concatenate(parts), offs, cnts
+
+
+# ---- DNG files (TIFF container) ----
+
+_TIFF_FMT = {1: "B", 3: "H", 4: "I", 5: "II", 7: "B", 10: "ii", 12: "d"}
+
+
+def _ifd_bytes(entries, at, big, next_off):
+    """One IFD written at file offset `at`: entries (tag, type, values) sorted by
+    tag; values over 4 bytes follow the entry table."""
+    import struct
+    e = ">" if big else "<"
+    entries = sorted(entries, key=lambda x: x[0])
+    table_len = 2 + 12 * len(entries) + 4
+    table = struct.pack(e + "H", len(entries))
+    extra = b""
+    for tag, typ, vals in entries:
+        fmt = _TIFF_FMT[typ]
+        flat = [v for pair in vals for v in pair] if typ in (5, 10) else list(vals)
+        data = struct.pack(e + fmt[0] * len(flat), *flat)
+        if len(data) <= 4:
+            field = data + b"\0" * (4 - len(data))
+        else:
+            field = struct.pack(e + "I", at + table_len + len(extra))
+            extra += data + (b"\0" if len(data) % 2 else b"")
+        table += struct.pack(e + "HHI", tag, typ, len(vals)) + field
+    table += struct.pack(e + "I", next_off)
+    return table + extra
+
+
+def _rat(v, den=1000):
+    return (int(round(v * den)), den)
+
+
+def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False, raw_in_subifd=True, black=(512,), white=16383,
+             active_area=None, crop=None, deltas=None, noise=None, plane_color=None, iso=200, color=None, version=(1, 4, 0, 0),
+             linearization=None, extra_chain_ifd=False):
+    """A DNG file image holding `img` (uint16 H x W Bayer) as lossless-JPEG
+    tiles in a CFA IFD (a SubIFD of IFD 0, or IFD 0 itself), with the tags
+    DNGFile and DNGColorSpec read. color: dict of color_matrix1/2 (9 values),
+    illuminant1/2, forward_matrix1, camera_calibration1, analog_balance,
+    as_shot_neutral, as_shot_white_xy. Rationals are written with
+    denominator 1000 (10000 for matrices)."""
+    import struct
+    H, W = img.shape
+    e = ">" if big_endian else "<"
+    out = bytearray((b"MM" if big_endian else b"II") + struct.pack(e + "HI", 42, 0))
+    offs, cnts = [], []
+    for ty in range(0, H, tile):
+        for tx in range(0, W, tile):
+            t = np.zeros((tile, tile), np.uint16)
+            blk = img[ty:ty + tile, tx:tx + tile]
+            t[:blk.shape[0], :blk.shape[1]] = blk
+            s = lj92_tile(t, clrs, bits)
+            offs.append(len(out))
+            cnts.append(len(s))
+            out += bytes(s)
+            if len(out) % 2:
+                out += b"\0"
+    raw = [(254, 4, [0]), (256, 4, [W]), (257, 4, [H]), (258, 3, [16]), (259, 3, [7]), (262, 3, [32803]), (277, 3, [1]),
+           (322, 3, [tile]), (323, 3, [tile]), (324, 4, offs), (325, 4, cnts), (33421, 3, [2, 2]), (33422, 1, list(cfa)),
+           (50717, 4, [white])]
+    if black is not None:
+        raw.append((50714, 5, [_rat(b) for b in black]))
+    if active_area is not None:
+        raw.append((50829, 4, list(active_area)))
+    if crop is not None:
+        raw.append((50719, 5, [_rat(crop[0]), _rat(crop[1])]))
+        raw.append((50720, 5, [_rat(crop[2]), _rat(crop[3])]))
+    if deltas is not None:
+        raw.append((50715, 10, [_rat(v) for v in deltas[0]]))
+        raw.append((50716, 10, [_rat(v) for v in deltas[1]]))
+    if noise is not None:
+        raw.append((51041, 12, list(noise)))
+    if plane_color is not None:
+        raw.append((50710, 1, list(plane_color)))
+    if linearization is not None:
+        raw.append((50712, 3, [int(v) for v in linearization]))
+    ifd0 = [(254, 4, [1]), (256, 4, [16]), (257, 4, [16]), (271, 2, [0]), (50706, 1, list(version))] if version else [(254, 4, [1])]
+    ifd0 = [x for x in ifd0 if x[0] != 271]
+    c = dict(color or {})
+    for k, tag in (("color_matrix1", 50721), ("color_matrix2", 50722), ("forward_matrix1", 50964), ("forward_matrix2", 50965),
+                   ("camera_calibration1", 50723)):
+        if c.get(k) is not None:
+            ifd0.append((tag, 10, [_rat(v, 10000) for v in c[k]]))
+    for k, tag in (("illuminant1", 50778), ("illuminant2", 50779)):
+        if c.get(k):
+            ifd0.append((tag, 3, [int(c[k])]))
+    for k, tag in (("analog_balance", 50727), ("as_shot_neutral", 50728), ("as_shot_white_xy", 50729)):
+        if c.get(k) is not None:
+            ifd0.append((tag, 5, [_rat(v, 10000) for v in c[k]]))
+    # the Exif IFD with the ISO, then the raw IFD, then IFD 0 (and a trailing chain IFD)
+    exif_at = len(out)
+    out += _ifd_bytes([(34855, 3, [iso])], exif_at, big_endian, 0)
+    ifd0.append((34665, 4, [exif_at]))
+    tail_at = 0
+    if extra_chain_ifd:
+        tail_at = len(out)
+        out += _ifd_bytes([(254, 4, [1]), (256, 4, [8]), (257, 4, [8]), (262, 3, [2])], tail_at, big_endian, 0)
+    if raw_in_subifd:
+        raw_at = len(out)
+        out += _ifd_bytes(raw, raw_at, big_endian, 0)
+        ifd0.append((330, 4, [raw_at]))
+        ifd0.append((262, 3, [2]))
+        entries0 = ifd0
+    else:
+        entries0 = [x for x in ifd0 if x[0] not in (254, 256, 257)] + raw
+    ifd0_at = len(out)
+    out += _ifd_bytes(entries0, ifd0_at, big_endian, tail_at)
+    struct.pack_into(e + "I", out, 4, ifd0_at)
+    return np.frombuffer(bytes(out), np.uint8).copy(), offs, cnts

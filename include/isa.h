@@ -568,6 +568,26 @@ ISA_API int isa_crop_window(int left, int top, int cropped_width, int cropped_he
 ISA_API int isa_profile_color_spec(const double* color_matrix1, const double* color_matrix2, int illuminant1, int illuminant2,
                                    const float white_balance[3], double camera_to_pcs[9], double camera_white[3], double white_xy[2]);
 
+/* ---- DNG container ----
+ * The TIFF structure RawFile reads (PefFile/RawFile.cs:56-90: byte order,
+ * magic 42, the IFD chain), SubIFDs, and the tags DNGFile and DNGColorSpec
+ * read: the raw IFD is the first IFD of the chain whose
+ * PhotometricInterpretation is CFA, else the first CFA SubIFD of the last
+ * IFD of the chain that has one (DNGFile.cs:621-660); colour tags come from
+ * IFD 0, else the raw IFD (DNGColorSpec.cs:94-103), CameraCalibration1
+ * serving both illuminants as the reference reads it; the ISO from the Exif
+ * IFD, else the raw IFD, else IFD 0. Host only; ISA_EINVAL where the
+ * reference cannot read the file. */
+typedef struct isa_dng_file isa_dng_file;
+ISA_API int isa_dng_open(const uint8_t* file, size_t size, isa_dng_file** out);
+ISA_API int isa_dng_close(isa_dng_file* f);
+/* Views into the parsed file, valid until isa_dng_close (any output may be
+ * NULL): the pixel layout for isa_dng_decode (black deltas left NULL: place
+ * them with isa_dng_levels), the level tags for isa_dng_levels (camera_white
+ * left NULL: take it from isa_dng_color_spec) and the colour tags. */
+ISA_API int isa_dng_file_info(const isa_dng_file* f, isa_dng_layout* layout, isa_dng_level_tags* levels, isa_dng_color_tags* color, int* width,
+                              int* height);
+
 #ifdef __cplusplus
 }
 #endif

@@ -214,3 +214,46 @@ def test_dng_file_to_tiff_chain(cuda, tmp_path):
     d = np.abs(img.astype(np.int64) - wantimg.astype(np.int64))
     assert d.max() <= 1 and (d > 0).sum() <= max(3, 2e-3 * d.size)
     assert img.std() > 100
+
+
+def test_dng_files_to_tiff(cuda, tmp_path):
+    """A burst of DNG files through the C ABI alone: isa_dng_open, isa_dng_color_spec,
+    isa_dng_levels, isa_dng_decode (the parallel decoder), the merge with the file's
+    levels and SaveAs16BitTiff with the file's crop and colour spec."""
+    import torch
+    from imagestackalignator_b200 import params as P, synthetic
+    import post as PO
+    b = synthetic.make_burst(512, 384, 3, seed=31, max_shift=3, max_rot_deg=0.0)
+    W, H = b.width, b.height
+    color = dict(color_matrix1=[0.9, -0.2, -0.1, -0.4, 1.2, 0.2, -0.05, 0.2, 0.6], illuminant1=21, as_shot_neutral=[0.52, 1.0, 0.71])
+    dh = [1, 0, 2, 0] * ((W - 8) // 4)
+    dv = [0, 1] * ((H - 4) // 2)
+    frames, lv, c2p, cw = [], None, None, None
+    for f in range(b.n):
+        file, offs, cnts = synthetic.dng_file(b.raw[f], cfa=tuple(b.cfa), tile=128, active_area=[2, 4, H - 2, W - 4], deltas=(dh, dv),
+                                              noise=[b.noise_a, b.noise_b], color=color, big_endian=f == 1)
+        d = isa.dng_open(file)
+        assert (d["width"], d["height"]) == (W, H)
+        c2p, cw, xy = isa.dng_color_spec(**d["color"])
+        lv = isa.dng_levels(camera_white=cw, **d["levels"])
+        got = isa.dng_decode(file, W, H, black_h=lv["black_h"], black_v=lv["black_v"], **d["layout"])
+        torch.cuda.synchronize()
+        assert isa.dng_decode_path() == 1
+        st, want = R.dng_decode(file, W, H, offs, cnts, tiled=True, tile_w=128, tile_h=128, black_h=lv["black_h"], black_v=lv["black_v"])
+        assert st == 0 and np.array_equal(got.cpu().numpy().view(np.uint16), want)
+        frames.append(got)
+    assert lv["cfa"] == list(b.cfa) and lv["noise"] == (np.float32(b.noise_a), np.float32(b.noise_b))
+    merged = isa.Merger(W, H, b.n, P.MergeParams()).merge(torch.stack(frames), lv["info"])
+    torch.cuda.synchronize()
+    t1, t2 = isa.color_twists(c2p)
+    lx = np.float32(np.round(np.arange(256) / 255.0, 9))
+    x, y, w, h = lv["crop"]
+    crop = (x, y, min(w, W - x), min(h, H - y))
+    pp, keep = isa.post_params(crop, np.float32(cw), t1, t2, lx, lx, 0.0)
+    path = tmp_path / "burst.tif"
+    isa.save_as_16bit_tiff(merged, pp, str(path))
+    tags, img = PO.parse_tiff16(path.read_bytes())
+    want = PO.postprocess(merged.cpu().numpy(), crop, np.float32(cw), t1, t2, lx, lx, 0.0)
+    d = np.abs(img.astype(np.int64) - want.astype(np.int64))
+    assert d.max() <= 1 and (d > 0).sum() <= max(3, 2e-3 * d.size)
+    assert img.std() > 100
