@@ -103,3 +103,42 @@ def test_adam_fit_lowers_the_loss(cuda, setup):
         vel = 0.999 * vel + 0.001 * g * g
         theta = theta - lr * (mom / (1 - 0.9 ** step)) / (np.sqrt(vel / (1 - 0.999 ** step)) + 1e-30)
     assert losses[-1] < 0.5 * losses[0], losses
+
+
+def test_autograd_function_adam_fit(cuda, setup):
+    """The same fit through the harness's torch.autograd.Function (tests/merge_autograd.py)
+    and torch.optim.Adam on per-parameter factors; the Function's first gradient is the
+    adjoint's own."""
+    import torch
+    from merge_autograd import MergeLoss, MergeSetup
+    b, p0 = setup
+    info = isa.make_info(b)
+    raw = torch.from_numpy(np.ascontiguousarray(b.raw).view(np.int16)).cuda()
+    m0 = isa.Merger(b.width, b.height, b.n, p0)
+    target = m0.merge(raw, info).clone()
+    torch.cuda.synchronize()
+    Wo, Ho = m0.output_size(b.width, b.height)
+    wsum = isa.device_copy(m0.debug(0)["wsum"], (Ho, Wo, 3), torch.float32)
+    om = (wsum.min(dim=2).values > 0.05).float().contiguous()
+    m0.close()
+    s = MergeSetup(isa.Merger, b.width, b.height, b.n, p0, raw, info, target, om)
+    base = torch.tensor([getattr(p0, n) for n in NAMES], dtype=torch.float64)
+    u = torch.tensor([1.3, 0.8, 1.5, 1.2, 0.8, 1.25, 0.9, 1.3], dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([u], lr=0.02, eps=1e-30)
+    losses = []
+    for step in range(15):
+        opt.zero_grad()
+        loss = MergeLoss.apply(base * u, s)
+        loss.backward()
+        if step == 0:
+            p = s.params((base * u).detach().numpy())
+            m = isa.Merger(b.width, b.height, b.n, p)
+            _, l0, g0 = m.backward(raw, info, target, weight=om)
+            m.close()
+            # a second adjoint call: its float atomics may sum in another order
+            assert np.isclose(l0, loss.item(), rtol=1e-5, atol=0)
+            want = base.numpy() * g0
+            assert np.allclose(u.grad.numpy(), want, rtol=1e-3, atol=1e-6 * np.abs(want).max())
+        opt.step()
+        losses.append(loss.item())
+    assert losses[-1] < 0.5 * losses[0], losses
