@@ -54,6 +54,7 @@ struct Tiff {
     size_t n = 0;
     bool big = false;
     bool ok = true;
+    long long rel = 0;  // subtracted from out-of-line value offsets (maker notes that store file offsets)
     uint32_t u8(size_t p)
     {
         if (p >= n) { ok = false; return 0; }
@@ -81,7 +82,7 @@ struct Tiff {
             en.type = (uint16_t)u16(e + 2);
             en.count = u32(e + 4);
             const size_t bytes = type_size(en.type) * (size_t)en.count;
-            en.at = bytes <= 4 ? e + 8 : (size_t)u32(e + 8);
+            en.at = bytes <= 4 ? e + 8 : (size_t)((long long)u32(e + 8) - rel);
             if (type_size(en.type) != 0 && en.at + bytes <= n) out.tags.emplace((uint16_t)tag, en);
         }
         return u32(o + 2 + 12 * (size_t)cnt);
@@ -346,5 +347,139 @@ int isa_dng_file_info(const isa_dng_file* f, isa_dng_layout* layout, isa_dng_lev
     if (color) *color = f->color;
     if (width) *width = f->width;
     if (height) *height = f->height;
+    return ISA_OK;
+}
+
+// ---- PEF container ----
+// PEFFile.SetMembers (PefFile/PEFFile.cs:176-312): the raw image is IFD 0
+// (size, bit depth, strips); the Exif IFD holds the ISO, the CFA pattern
+// (ExifCFAPattern, PefFile/ExifEntry.cs:2529-2542: repeat counts in bytes 1
+// and 3, the colours from byte 4) and the maker note, which PentaxMakerNotes
+// (PefFile/PentaxMakerNotes.cs:26-198) reads after an "AOC\0" header (its
+// own byte order, entry offsets counted from the file's start) or a
+// "PENTAX \0" header (offsets from the maker note's start). The maker-note
+// entries used: HuffmanTable 0x0220, BlackPoint 0x0200, WhitePoint 0x0201,
+// WhiteLevel 0x007e, DataScaling 0x003d.
+
+struct isa_pef_file {
+    std::vector<uint32_t> offsets, sizes;
+    std::vector<uint8_t> huff;
+    std::vector<float> black;
+    isa_pef_info info{};
+};
+
+namespace {
+
+enum : uint16_t { T_EXIF_CFA = 41730, T_MAKER_NOTE = 37500, MN_BLACK = 0x0200, MN_WHITE_POINT = 0x0201, MN_WHITE_LEVEL = 0x007e,
+                  MN_SCALING = 0x003d, MN_HUFFMAN = 0x0220 };
+
+int open_pef(const uint8_t* file, size_t size, isa_pef_file& f)
+{
+    Tiff t;
+    t.d = file;
+    t.n = size;
+    if (size < 8 || file[0] != file[1] || (file[0] != 'I' && file[0] != 'M')) return fail(ISA_EINVAL, "not a TIFF file (byte order)");
+    t.big = file[0] == 'M';
+    if (t.u16(2) != 42) return fail(ISA_EINVAL, "not a TIFF file (magic number is not 42)");
+    Ifd raw;
+    t.ifd(t.u32(4), raw);
+    if (!t.ok) return fail(ISA_EINVAL, "IFD 0 outside the file");
+    const std::vector<double> w = t.nums(raw.get(T_WIDTH)), h = t.nums(raw.get(T_LENGTH)), bits = t.nums(raw.get(T_BITS));
+    const std::vector<double> offs = t.nums(raw.get(T_STRIP_OFFSETS)), cnts = t.nums(raw.get(T_STRIP_BYTES)), rps = t.nums(raw.get(T_ROWS_PER_STRIP));
+    if (w.empty() || h.empty() || bits.empty()) return fail(ISA_EINVAL, "IFD 0 without size or bit depth");
+    if (offs.empty() || offs.size() != cnts.size()) return fail(ISA_EINVAL, "strip offsets and byte counts do not match");
+    for (size_t i = 0; i < offs.size(); i++) {
+        f.offsets.push_back((uint32_t)offs[i]);
+        f.sizes.push_back((uint32_t)cnts[i]);
+    }
+    const Entry* ex = raw.get(T_EXIF);
+    if (!ex) return fail(ISA_EINVAL, "no Exif IFD");
+    Ifd exif;
+    t.ifd((size_t)t.num(*ex, 0), exif);
+    if (!t.ok) return fail(ISA_EINVAL, "Exif IFD outside the file");
+    const Entry* cfa = exif.get(T_EXIF_CFA);
+    const Entry* mn = exif.get(T_MAKER_NOTE);
+    if (!cfa || cfa->count < 8) return fail(ISA_EINVAL, "no Exif CFA pattern");
+    if (!mn) return fail(ISA_EINVAL, "no maker note");
+    const uint32_t xc = t.u8(cfa->at + 1), yc = t.u8(cfa->at + 3);
+    if (xc != 2 || yc != 2) return fail(ISA_EINVAL, "the CFA pattern is not 2 x 2");
+    isa_pef_info& I = f.info;
+    for (int i = 0; i < 4; i++) I.cfa[i] = (int)t.u8(cfa->at + 4 + i);
+    const std::vector<double> iso = t.nums(exif.get(T_ISO));
+    I.iso = iso.empty() ? 0 : (int)iso[0];
+    // the maker note's own byte order and offset base
+    const size_t mo = mn->at, mlen = (size_t)mn->count * type_size(mn->type);
+    Tiff m;
+    m.d = file + mo;
+    m.n = mlen;
+    size_t ifd_at = 0;
+    if (mlen >= 6 && std::memcmp(m.d, "AOC\0", 4) == 0) {
+        ifd_at = 6;
+        m.rel = (long long)mo;
+    } else if (mlen >= 10 && std::memcmp(m.d, "PENTAX \0", 8) == 0) {
+        ifd_at = 10;
+    } else {
+        return fail(ISA_EINVAL, "not a Pentax maker note");
+    }
+    const uint8_t o0 = m.d[ifd_at - 2], o1 = m.d[ifd_at - 1];
+    if (o0 != o1 || (o0 != 'I' && o0 != 'M')) return fail(ISA_EINVAL, "maker note byte order");
+    m.big = o0 == 'M';
+    Ifd note;
+    m.ifd(ifd_at, note);
+    if (!m.ok) return fail(ISA_EINVAL, "maker note entries outside the maker note");
+    if (const Entry* hu = note.get(MN_HUFFMAN)) {
+        const size_t nb = (size_t)hu->count * type_size(hu->type);
+        f.huff.assign(m.d + hu->at, m.d + hu->at + nb);
+    }
+    for (double v : m.nums(note.get(MN_BLACK))) f.black.push_back((float)v);
+    const std::vector<double> wp = m.nums(note.get(MN_WHITE_POINT)), wl = m.nums(note.get(MN_WHITE_LEVEL)), sc = m.nums(note.get(MN_SCALING));
+    if (wp.size() < 4 || sc.empty()) return fail(ISA_EINVAL, "maker note without WhitePoint or DataScaling");
+    I.width = (int)w[0];
+    I.height = (int)h[0];
+    I.bit_depth = (int)bits[0];
+    I.nstrips = (int)f.offsets.size();
+    I.strip_offsets = f.offsets.data();
+    I.strip_sizes = f.sizes.data();
+    I.rows_per_strip = rps.empty() ? I.height : (int)std::min<double>(rps[0], (double)I.height);
+    I.compressed = !f.huff.empty() && I.nstrips == 1 ? 1 : 0;  // PEFFile.cs:87
+    I.huffman_table = opt(f.huff);
+    I.huffman_bytes = f.huff.size();
+    I.huffman_big_endian = m.big ? 1 : 0;
+    I.black_point = opt(f.black);
+    I.n_black = (int)f.black.size();
+    I.white_level = wl.empty() ? -1.f : (float)wl[0];
+    for (int i = 0; i < 4; i++) I.white_point[i] = (float)wp[i];
+    I.scaling = (float)sc[0];
+    if (!t.ok || !m.ok) return fail(ISA_EINVAL, "a tag's values lie outside the file");
+    return ISA_OK;
+}
+
+}  // namespace
+
+int isa_pef_open(const uint8_t* file, size_t size, isa_pef_file** out)
+{
+    if (!file || !out) return fail(ISA_EINVAL, "NULL argument");
+    *out = nullptr;
+    isa_pef_file* f = new (std::nothrow) isa_pef_file();
+    if (!f) return fail(ISA_ENOMEM, "out of host memory");
+    const int rc = open_pef(file, size, *f);
+    if (rc != ISA_OK) {
+        delete f;
+        return rc;
+    }
+    *out = f;
+    return ISA_OK;
+}
+
+int isa_pef_close(isa_pef_file* f)
+{
+    delete f;
+    return ISA_OK;
+}
+
+int isa_pef_file_info(const isa_pef_file* f, isa_pef_info* info)
+{
+    if (!f || !info) return fail(ISA_EINVAL, "NULL argument");
+    *info = f->info;
     return ISA_OK;
 }

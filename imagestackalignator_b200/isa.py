@@ -78,7 +78,7 @@ EXPORTS = [
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
     "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
     "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec", "isa_dng_decode_path",
-    "isa_dng_open", "isa_dng_close", "isa_dng_file_info",
+    "isa_dng_open", "isa_dng_close", "isa_dng_file_info", "isa_pef_open", "isa_pef_close", "isa_pef_file_info",
 ]
 
 _lib = None
@@ -659,6 +659,35 @@ def dng_open(file):
         return dict(width=W.value, height=H.value, layout=layout, levels=levels, color=color)
     finally:
         lib().isa_dng_close(h)
+
+
+class IsaPefInfo(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("bit_depth", ctypes.c_int), ("cfa", ctypes.c_int * 4),
+                ("nstrips", ctypes.c_int), ("rows_per_strip", ctypes.c_int), ("strip_offsets", ctypes.c_void_p),
+                ("strip_sizes", ctypes.c_void_p), ("compressed", ctypes.c_int), ("huffman_table", ctypes.c_void_p),
+                ("huffman_bytes", ctypes.c_size_t), ("huffman_big_endian", ctypes.c_int), ("black_point", ctypes.c_void_p),
+                ("n_black", ctypes.c_int), ("white_level", ctypes.c_float), ("white_point", ctypes.c_float * 4), ("scaling", ctypes.c_float),
+                ("iso", ctypes.c_int)]
+
+
+def pef_open(file):
+    """isa_pef_open + isa_pef_file_info of a PEF file image (host bytes) as a dict."""
+    f = np.ascontiguousarray(np.frombuffer(bytes(file), np.uint8) if isinstance(file, (bytes, bytearray)) else file, np.uint8)
+    h = ctypes.c_void_p()
+    check(lib().isa_pef_open(f.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(f.size), ctypes.byref(h)))
+    try:
+        I = IsaPefInfo()
+        check(lib().isa_pef_file_info(h, ctypes.byref(I)))
+        huff = None
+        if I.huffman_table:
+            huff = bytes(ctypes.cast(I.huffman_table, ctypes.POINTER(ctypes.c_uint8))[:I.huffman_bytes])
+        return dict(width=I.width, height=I.height, bit_depth=I.bit_depth, cfa=list(I.cfa), nstrips=I.nstrips, rows_per_strip=I.rows_per_strip,
+                    strip_offsets=_arr(I.strip_offsets, I.nstrips, ctypes.c_uint32), strip_sizes=_arr(I.strip_sizes, I.nstrips, ctypes.c_uint32),
+                    compressed=bool(I.compressed), huffman_table=huff, huffman_big_endian=bool(I.huffman_big_endian),
+                    black_point=_arr(I.black_point, I.n_black, ctypes.c_float), white_level=None if I.white_level < 0 else I.white_level,
+                    white_point=list(I.white_point), scaling=I.scaling, iso=I.iso)
+    finally:
+        lib().isa_pef_close(h)
 
 
 class IsaBurst(ctypes.Structure):

@@ -432,3 +432,72 @@ def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False,
     out += _ifd_bytes(entries0, ifd0_at, big_endian, tail_at)
     struct.pack_into(e + "I", out, 4, ifd0_at)
     return np.frombuffer(bytes(out), np.uint8).copy(), offs, cnts
+
+
+def pef_file(img, cfa=(0, 1, 1, 2), compressed=True, big_endian=False, note="AOC", note_big_endian=None, black=(512, 512, 512, 512),
+             white_point=(8192, 8192, 8192, 8192), scaling=8192, white_level=16383, iso=400, bits=14, rows_per_strip=None):
+    """A PEF file image holding `img` (uint16 H x W Bayer): IFD 0 with the
+    strip(s), its Exif IFD with ISO, CFA pattern and a Pentax maker note
+    ("AOC": entry offsets from the file's start, or "PENTAX": from the
+    note's start) holding HuffmanTable (compressed frames), BlackPoint,
+    WhitePoint, WhiteLevel and DataScaling. Uncompressed frames are stored
+    as MSB-first `bits`-bit samples in strips of rows_per_strip rows."""
+    import struct
+    H, W = img.shape
+    e = ">" if big_endian else "<"
+    nb = big_endian if note_big_endian is None else note_big_endian
+    out = bytearray((b"MM" if big_endian else b"II") + struct.pack(e + "HI", 42, 0))
+    code, lens = pef_code_book()
+    offs, cnts = [], []
+    if compressed:
+        data = pef_stream(img, code, lens)
+        offs.append(len(out))
+        cnts.append(len(data))
+        out += bytes(data)
+        rps = H
+    else:
+        rps = rows_per_strip or H
+        for y in range(0, H, rps):
+            blk = np.asarray(img[y:y + rps], np.uint64).reshape(-1)
+            bitsarr = ((blk[:, None] >> np.arange(bits - 1, -1, -1, dtype=np.uint64)) & 1).astype(np.uint8).reshape(-1)
+            data = np.packbits(bitsarr)
+            offs.append(len(out))
+            cnts.append(len(data))
+            out += bytes(data)
+    if len(out) % 2:
+        out += b"\0"
+    entries = []
+    if compressed:
+        entries.append((0x0220, 7, list(pef_maker_note(code, lens, nb))))
+    if black is not None:
+        entries.append((0x0200, 3, list(black)))
+    entries += [(0x0201, 3, list(white_point)), (0x003d, 3, [scaling])]
+    if white_level is not None:
+        entries.append((0x007e, 4, [white_level]))
+    mn_at = len(out)
+    if note == "AOC":
+        head = b"AOC\0" + (b"MM" if nb else b"II")
+        body = _ifd_bytes(entries, mn_at + len(head), nb, 0)   # offsets from the file's start
+    else:
+        head = b"PENTAX \0" + (b"MM" if nb else b"II")
+        body = _ifd_bytes(entries, len(head), nb, 0)            # offsets from the note's start
+    note_bytes = head + body
+    out += note_bytes
+    if len(out) % 2:
+        out += b"\0"
+    exif_at = len(out)
+    exif = [(34855, 3, [iso]), (41730, 7, [0, 2, 0, 2] + list(cfa)), (37500, 7, list(note_bytes))]
+    # the maker note's bytes are already in the file: point the MakerNote entry at them
+    exif_bytes = bytearray(_ifd_bytes(exif, exif_at, big_endian, 0))
+    n = struct.unpack_from(e + "H", exif_bytes, 0)[0]
+    for i in range(n):
+        tag = struct.unpack_from(e + "H", exif_bytes, 2 + 12 * i)[0]
+        if tag == 37500:
+            struct.pack_into(e + "I", exif_bytes, 2 + 12 * i + 8, mn_at)
+    out += exif_bytes
+    ifd0_at = len(out)
+    ifd0 = [(254, 4, [0]), (256, 4, [W]), (257, 4, [H]), (258, 3, [bits]), (259, 3, [65535 if compressed else 1]), (262, 3, [32803]),
+            (273, 4, offs), (278, 4, [rps]), (279, 4, cnts), (34665, 4, [exif_at])]
+    out += _ifd_bytes(ifd0, ifd0_at, big_endian, 0)
+    struct.pack_into(e + "I", out, 4, ifd0_at)
+    return np.frombuffer(bytes(out), np.uint8).copy(), offs, cnts

@@ -588,6 +588,38 @@ ISA_API int isa_dng_close(isa_dng_file* f);
 ISA_API int isa_dng_file_info(const isa_dng_file* f, isa_dng_layout* layout, isa_dng_level_tags* levels, isa_dng_color_tags* color, int* width,
                               int* height);
 
+/* ---- PEF container ----
+ * PEFFile.SetMembers (PefFile/PEFFile.cs:176-312): the raw image of IFD 0,
+ * the Exif IFD's ISO and CFA pattern (ExifCFAPattern,
+ * PefFile/ExifEntry.cs:2529-2542) and the Pentax maker note
+ * (PentaxMakerNotes, PefFile/PentaxMakerNotes.cs:26-198: "AOC\0" or
+ * "PENTAX \0" header, its own byte order) with HuffmanTable, BlackPoint,
+ * WhitePoint, WhiteLevel and DataScaling. The fields feed
+ * isa_pef_huff_table, isa_pef_levels and isa_pef_decode / isa_pef_unpack.
+ * Host only; ISA_EINVAL where the reference cannot read the file. */
+typedef struct isa_pef_file isa_pef_file;
+typedef struct isa_pef_info {
+    int width, height, bit_depth;
+    int cfa[4];
+    int nstrips, rows_per_strip;
+    const uint32_t* strip_offsets;    /* nstrips byte offsets in the file */
+    const uint32_t* strip_sizes;
+    int compressed;                   /* a HuffmanTable and a single strip: the Huffman branch (PEFFile.cs:87) */
+    const uint8_t* huffman_table;     /* the HuffmanTable entry's bytes (isa_pef_huff_table), or NULL */
+    size_t huffman_bytes;
+    int huffman_big_endian;           /* the maker note's byte order */
+    const float* black_point;         /* BlackPoint values or NULL */
+    int n_black;
+    float white_level;                /* WhiteLevel, or -1 when absent (2^bit_depth then) */
+    float white_point[4];             /* WhitePoint */
+    float scaling;                    /* DataScaling */
+    int iso;                          /* ISOSpeedRatings (0 when absent) */
+} isa_pef_info;
+ISA_API int isa_pef_open(const uint8_t* file, size_t size, isa_pef_file** out);
+ISA_API int isa_pef_close(isa_pef_file* f);
+/* The parsed values, valid until isa_pef_close. */
+ISA_API int isa_pef_file_info(const isa_pef_file* f, isa_pef_info* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,3 +153,44 @@ def test_pef_file_to_tiff_chain(cuda, tmp_path):
     isa.save_as_16bit_tiff(merged, pp, str(path))
     tags, img = PO.parse_tiff16(path.read_bytes())
     close(img, PO.postprocess(merged.cpu().numpy(), crop, np.float32(cw), t1, t2, lx, tone(lx), 0.0))
+
+
+def test_pef_files_to_tiff(cuda, tmp_path):
+    """A burst of PEF files through the C ABI alone: isa_pef_open (IFD 0 strip, Exif CFA
+    pattern, Pentax maker note), isa_pef_huff_table, isa_pef_levels, isa_pef_decode of the
+    strip, the merge with those levels, the PEF colour spec and SaveAs16BitTiff."""
+    import torch
+    b = synthetic.make_burst(512, 384, 3, seed=14, max_shift=3, max_rot_deg=0.0)
+    frames = []
+    for f in range(b.n):
+        file, offs, cnts = synthetic.pef_file(b.raw[f], cfa=tuple(b.cfa), big_endian=f == 2, note=["AOC", "PENTAX", "AOC"][f],
+                                              black=(512, 512, 512, 512), white_point=(15000, 8192, 8192, 12000), scaling=8192,
+                                              white_level=16383)
+        d = isa.pef_open(file)
+        assert d["compressed"] and (d["width"], d["height"]) == (b.width, b.height) and d["cfa"] == list(b.cfa)
+        table = isa.pef_huff_table(d["huffman_table"], big_endian=d["huffman_big_endian"])
+        o, n = d["strip_offsets"][0], d["strip_sizes"][0]
+        strip = torch.from_numpy(np.ascontiguousarray(file[o:o + n])).cuda()
+        out = isa.pef_decode(strip, table, b.width, b.height)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint16), b.raw[f])
+        frames.append(out)
+    black, white, wb = isa.pef_levels(d["cfa"], d["black_point"], d["white_level"], d["white_point"], d["scaling"], d["bit_depth"])
+    info = isa.make_info(b)
+    for c in range(3):
+        info.black[c] = float(black[c])
+        info.white[c] = float(white[c])
+    c2p, cw, xy = isa.pef_color_spec(wb)
+    for c in range(3):
+        info.camera_white[c] = float(cw[c])
+    merged = isa.Merger(b.width, b.height, b.n, P.MergeParams()).merge(torch.stack(frames), info)
+    torch.cuda.synchronize()
+    t1, t2 = isa.color_twists(c2p)
+    lx = lut_levels()
+    crop = (2, 2, b.width - 4, b.height - 4)
+    pp, keep = isa.post_params(crop, np.float32(cw), t1, t2, lx, tone(lx), 0.0)
+    path = tmp_path / "pef_burst.tif"
+    isa.save_as_16bit_tiff(merged, pp, str(path))
+    tags, img = PO.parse_tiff16(path.read_bytes())
+    close(img, PO.postprocess(merged.cpu().numpy(), crop, np.float32(cw), t1, t2, lx, tone(lx), 0.0))
+    assert img.std() > 100
