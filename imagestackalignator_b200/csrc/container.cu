@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <new>
 #include <set>
@@ -157,6 +158,20 @@ namespace {
 template <class T>
 const T* opt(const std::vector<T>& v) { return v.empty() ? nullptr : v.data(); }
 
+// A tag value as an integer of type T, truncated toward zero; NaN and values outside T are refused.
+template <class T>
+bool as_int(double v, T& out)
+{
+    if (!(v > (double)std::numeric_limits<T>::min() - 1.0 && v < (double)std::numeric_limits<T>::max() + 1.0)) return false;
+    out = (T)v;
+    return true;
+}
+
+#define ISA_TAG_INT(v, out) \
+    do { \
+        if (!as_int((v), (out))) return fail(ISA_EINVAL, "a tag value is out of range"); \
+    } while (0)
+
 int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
 {
     Tiff t;
@@ -189,8 +204,10 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
             const Entry* s = i.get(T_SUBIFDS);
             if (!s) continue;
             for (uint32_t j = 0; j < s->count && j < 16; j++) {
+                uint32_t at;
+                ISA_TAG_INT(t.num(*s, j), at);
                 subs.emplace_back();
-                t.ifd((size_t)t.num(*s, j), subs.back());
+                t.ifd(at, subs.back());
                 if (!t.ok) return fail(ISA_EINVAL, "SubIFD outside the file");
                 const Entry* p = subs.back().get(T_PHOTOMETRIC);
                 if (p && t.num(*p, 0) == PHOTOMETRIC_CFA) { raw = &subs.back(); break; }
@@ -206,34 +223,42 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
     };
     const std::vector<double> w = raw_nums(T_WIDTH), h = raw_nums(T_LENGTH), bits = raw_nums(T_BITS), comp = raw_nums(T_COMPRESSION);
     if (w.empty() || h.empty() || bits.empty() || comp.empty()) return fail(ISA_EINVAL, "raw IFD without size, bit depth or compression");
-    f.width = (int)w[0];
-    f.height = (int)h[0];
+    ISA_TAG_INT(w[0], f.width);
+    ISA_TAG_INT(h[0], f.height);
     const bool tiled = raw->get(T_TILE_WIDTH) != nullptr;
     const std::vector<double> offs = raw_nums(tiled ? T_TILE_OFFSETS : T_STRIP_OFFSETS), cnts = raw_nums(tiled ? T_TILE_BYTES : T_STRIP_BYTES);
     if (offs.empty() || offs.size() != cnts.size()) return fail(ISA_EINVAL, "tile / strip offsets and byte counts do not match");
     for (size_t i = 0; i < offs.size(); i++) {
-        f.offsets.push_back((uint32_t)offs[i]);
-        f.counts.push_back((uint32_t)cnts[i]);
+        uint32_t o, c;
+        ISA_TAG_INT(offs[i], o);
+        ISA_TAG_INT(cnts[i], c);
+        f.offsets.push_back(o);
+        f.counts.push_back(c);
     }
     const std::vector<double> lin = raw_nums(T_LINEARIZATION);
-    for (double v : lin) f.lin.push_back((uint16_t)v);
+    for (double v : lin) {
+        uint16_t u;
+        ISA_TAG_INT(v, u);
+        f.lin.push_back(u);
+    }
     const std::vector<double> ver = t.nums(ifd0.get(T_DNG_VERSION));
     isa_dng_layout& L = f.layout;
     L.tiled = tiled ? 1 : 0;
     if (tiled) {
         const std::vector<double> tw = raw_nums(T_TILE_WIDTH), th = raw_nums(T_TILE_LENGTH);
         if (th.empty()) return fail(ISA_EINVAL, "TileWidth without TileLength");
-        L.tile_width = (int)tw[0];
-        L.tile_height = (int)th[0];
+        ISA_TAG_INT(tw[0], L.tile_width);
+        ISA_TAG_INT(th[0], L.tile_height);
     } else {
         const std::vector<double> rps = raw_nums(T_ROWS_PER_STRIP);
-        L.rows_per_strip = rps.empty() ? f.height : (int)std::min<double>(rps[0], (double)f.height);
+        L.rows_per_strip = f.height;
+        if (!rps.empty()) ISA_TAG_INT(std::min<double>(rps[0], (double)f.height), L.rows_per_strip);
     }
     L.n = (int)f.offsets.size();
     L.offsets = f.offsets.data();
     L.byte_counts = f.counts.data();
-    L.compression = (int)comp[0];
-    L.bit_depth = (int)bits[0];
+    ISA_TAG_INT(comp[0], L.compression);
+    ISA_TAG_INT(bits[0], L.bit_depth);
     L.dng_version_large = ver.size() < 2 || ver[1] > 1 ? 1 : 0;  // DNGFile constructor (:288-291)
     L.linearization = opt(f.lin);
     L.nlin = (int)f.lin.size();
@@ -241,9 +266,21 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
     const std::vector<double> rep = raw_nums(T_CFA_REPEAT), pat = raw_nums(T_CFA_PATTERN), white = raw_nums(T_WHITE);
     if (rep.size() < 2 || pat.size() < 4) return fail(ISA_EINVAL, "raw IFD without a CFA pattern");
     if (white.empty()) return fail(ISA_EINVAL, "raw IFD without WhiteLevel");
-    for (int i = 0; i < 4; i++) f.cfa.push_back((uint8_t)pat[i]);
-    for (double v : raw_nums(T_CFA_PLANE_COLOR)) f.plane.push_back((int)v);
-    for (double v : raw_nums(T_ACTIVE_AREA)) f.active.push_back((int)v);
+    for (int i = 0; i < 4; i++) {
+        uint8_t c;
+        ISA_TAG_INT(pat[i], c);
+        f.cfa.push_back(c);
+    }
+    for (double v : raw_nums(T_CFA_PLANE_COLOR)) {
+        int c;
+        ISA_TAG_INT(v, c);
+        f.plane.push_back(c);
+    }
+    for (double v : raw_nums(T_ACTIVE_AREA)) {
+        int a;
+        ISA_TAG_INT(v, a);
+        f.active.push_back(a);
+    }
     if (!f.active.empty() && f.active.size() != 4) return fail(ISA_EINVAL, "ActiveArea needs four values");
     f.black = raw_nums(T_BLACK);
     f.crop_origin = raw_nums(T_CROP_ORIGIN);
@@ -256,8 +293,8 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
     G.width = f.width;
     G.height = f.height;
     G.cfa_pattern = f.cfa.data();
-    G.cfa_repeat_w = (int)rep[0];
-    G.cfa_repeat_h = (int)rep[1];
+    ISA_TAG_INT(rep[0], G.cfa_repeat_w);
+    ISA_TAG_INT(rep[1], G.cfa_repeat_h);
     G.plane_color = opt(f.plane);
     G.n_plane_color = (int)f.plane.size();
     G.black_level = opt(f.black);
@@ -277,14 +314,17 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
     std::vector<double> iso;
     if (const Entry* ex = ifd0.get(T_EXIF)) {
         Ifd exif;
-        t.ifd((size_t)t.num(*ex, 0), exif);
+        uint32_t at;
+        ISA_TAG_INT(t.num(*ex, 0), at);
+        t.ifd(at, exif);
         if (!t.ok) return fail(ISA_EINVAL, "Exif IFD outside the file");
         iso = t.nums(exif.get(T_ISO));
     } else {
         iso = raw_nums(T_ISO);
         if (iso.empty()) iso = t.nums(ifd0.get(T_ISO));
     }
-    G.iso = iso.empty() ? 0 : (int)iso[0];
+    G.iso = 0;
+    if (!iso.empty()) ISA_TAG_INT(iso[0], G.iso);
     // colour tags (DNGColorSpec.cs:270-392): CameraCalibration1 serves both illuminants, as the reference reads it
     f.cm1 = color_nums(T_COLOR_MATRIX1);
     f.cm2 = color_nums(T_COLOR_MATRIX2);
@@ -302,8 +342,9 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
     isa_dng_color_tags& C = f.color;
     C.color_matrix1 = opt(f.cm1);
     C.color_matrix2 = opt(f.cm2);
-    C.illuminant1 = il1.empty() ? 0 : (int)il1[0];
-    C.illuminant2 = il2.empty() ? 0 : (int)il2[0];
+    C.illuminant1 = C.illuminant2 = 0;
+    if (!il1.empty()) ISA_TAG_INT(il1[0], C.illuminant1);
+    if (!il2.empty()) ISA_TAG_INT(il2[0], C.illuminant2);
     C.forward_matrix1 = opt(f.fm1);
     C.forward_matrix2 = opt(f.fm2);
     C.camera_calibration1 = opt(f.cc1);
@@ -389,13 +430,18 @@ int open_pef(const uint8_t* file, size_t size, isa_pef_file& f)
     if (w.empty() || h.empty() || bits.empty()) return fail(ISA_EINVAL, "IFD 0 without size or bit depth");
     if (offs.empty() || offs.size() != cnts.size()) return fail(ISA_EINVAL, "strip offsets and byte counts do not match");
     for (size_t i = 0; i < offs.size(); i++) {
-        f.offsets.push_back((uint32_t)offs[i]);
-        f.sizes.push_back((uint32_t)cnts[i]);
+        uint32_t o, c;
+        ISA_TAG_INT(offs[i], o);
+        ISA_TAG_INT(cnts[i], c);
+        f.offsets.push_back(o);
+        f.sizes.push_back(c);
     }
     const Entry* ex = raw.get(T_EXIF);
     if (!ex) return fail(ISA_EINVAL, "no Exif IFD");
     Ifd exif;
-    t.ifd((size_t)t.num(*ex, 0), exif);
+    uint32_t exif_at;
+    ISA_TAG_INT(t.num(*ex, 0), exif_at);
+    t.ifd(exif_at, exif);
     if (!t.ok) return fail(ISA_EINVAL, "Exif IFD outside the file");
     const Entry* cfa = exif.get(T_EXIF_CFA);
     const Entry* mn = exif.get(T_MAKER_NOTE);
@@ -406,7 +452,8 @@ int open_pef(const uint8_t* file, size_t size, isa_pef_file& f)
     isa_pef_info& I = f.info;
     for (int i = 0; i < 4; i++) I.cfa[i] = (int)t.u8(cfa->at + 4 + i);
     const std::vector<double> iso = t.nums(exif.get(T_ISO));
-    I.iso = iso.empty() ? 0 : (int)iso[0];
+    I.iso = 0;
+    if (!iso.empty()) ISA_TAG_INT(iso[0], I.iso);
     // the maker note's own byte order and offset base
     const size_t mo = mn->at, mlen = (size_t)mn->count * type_size(mn->type);
     Tiff m;
@@ -434,13 +481,14 @@ int open_pef(const uint8_t* file, size_t size, isa_pef_file& f)
     for (double v : m.nums(note.get(MN_BLACK))) f.black.push_back((float)v);
     const std::vector<double> wp = m.nums(note.get(MN_WHITE_POINT)), wl = m.nums(note.get(MN_WHITE_LEVEL)), sc = m.nums(note.get(MN_SCALING));
     if (wp.size() < 4 || sc.empty()) return fail(ISA_EINVAL, "maker note without WhitePoint or DataScaling");
-    I.width = (int)w[0];
-    I.height = (int)h[0];
-    I.bit_depth = (int)bits[0];
+    ISA_TAG_INT(w[0], I.width);
+    ISA_TAG_INT(h[0], I.height);
+    ISA_TAG_INT(bits[0], I.bit_depth);
     I.nstrips = (int)f.offsets.size();
     I.strip_offsets = f.offsets.data();
     I.strip_sizes = f.sizes.data();
-    I.rows_per_strip = rps.empty() ? I.height : (int)std::min<double>(rps[0], (double)I.height);
+    I.rows_per_strip = I.height;
+    if (!rps.empty()) ISA_TAG_INT(std::min<double>(rps[0], (double)I.height), I.rows_per_strip);
     I.compressed = !f.huff.empty() && I.nstrips == 1 ? 1 : 0;  // PEFFile.cs:87
     I.huffman_table = opt(f.huff);
     I.huffman_bytes = f.huff.size();

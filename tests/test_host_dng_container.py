@@ -122,3 +122,21 @@ def test_unreadable_files(damage):
     with pytest.raises(isa.IsaError) as e:
         isa.dng_open(bytes(b))
     assert e.value.code == isa.ISA_EINVAL
+
+
+def test_out_of_range_tag_values_are_refused():
+    """Tag values that do not fit the integer they stand for (a rational width of
+    2^32 - 1, a negative strip offset) are ISA_EINVAL, not a wrapped number."""
+    def cfa_file(width_entry, offsets_entry):
+        out = bytearray(b"II" + struct.pack("<HI", 42, 0))
+        ifd = [width_entry, (257, 4, [8]), (258, 3, [16]), (259, 3, [7]), (262, 3, [32803]), offsets_entry, (279, 4, [4]),
+               (33421, 3, [2, 2]), (33422, 1, [0, 1, 1, 2]), (50717, 4, [4095])]
+        at = len(out)
+        out += S._ifd_bytes(ifd, at, False, 0)
+        struct.pack_into("<I", out, 4, at)
+        return bytes(out)
+    assert isa.dng_open(cfa_file((256, 4, [32]), (273, 4, [8])))["width"] == 32
+    for bad in (cfa_file((256, 5, [(2 ** 32 - 1, 1)]), (273, 4, [8])), cfa_file((256, 4, [32]), (273, 10, [(-8, 1)]))):
+        with pytest.raises(isa.IsaError) as e:
+            isa.dng_open(bad)
+        assert e.value.code == isa.ISA_EINVAL
