@@ -134,7 +134,7 @@ enum : uint16_t {
     T_LINEARIZATION = 50712, T_BLACK = 50714, T_BLACK_DH = 50715, T_BLACK_DV = 50716, T_WHITE = 50717, T_CROP_ORIGIN = 50719,
     T_CROP_SIZE = 50720, T_COLOR_MATRIX1 = 50721, T_COLOR_MATRIX2 = 50722, T_CALIBRATION1 = 50723, T_ANALOG_BALANCE = 50727,
     T_AS_SHOT_NEUTRAL = 50728, T_AS_SHOT_WHITE_XY = 50729, T_ILLUMINANT1 = 50778, T_ILLUMINANT2 = 50779, T_ACTIVE_AREA = 50829,
-    T_FORWARD_MATRIX1 = 50964, T_FORWARD_MATRIX2 = 50965, T_NOISE_PROFILE = 51041,
+    T_FORWARD_MATRIX1 = 50964, T_FORWARD_MATRIX2 = 50965, T_NOISE_PROFILE = 51041, T_PRIVATE_DATA = 50740,
 };
 constexpr uint32_t PHOTOMETRIC_CFA = 32803;
 
@@ -142,6 +142,8 @@ constexpr uint32_t PHOTOMETRIC_CFA = 32803;
 
 struct isa_dng_file {
     int width = 0, height = 0;
+    float roll = 0.f;
+    bool roll_present = false;
     std::vector<uint32_t> offsets, counts;
     std::vector<uint16_t> lin;
     std::vector<uint8_t> cfa;
@@ -165,6 +167,60 @@ bool as_int(double v, T& out)
     if (!(v > (double)std::numeric_limits<T>::min() - 1.0 && v < (double)std::numeric_limits<T>::max() + 1.0)) return false;
     out = (T)v;
     return true;
+}
+
+// A Pentax maker note inside `d` (n bytes): PentaxMakerNotes' three headers
+// (PefFile/PentaxMakerNotes.cs:26-170). "AOC\0" + byte order: entries at 6,
+// value offsets counted from the file's start (`at` = the note's file
+// offset); "PENTAX \0" + byte order: entries at 10, offsets from the note's
+// start; "Adobe\0MakN" (a DNG's private data) + count + byte order + the
+// note's original file offset, then one of the two: offsets moved by the
+// 20-byte Adobe header. Returns false for anything else.
+bool pentax_note(const uint8_t* d, size_t n, size_t at, Tiff& m, size_t& ifd_at)
+{
+    m.d = d;
+    m.n = n;
+    m.ok = true;
+    m.rel = 0;
+    size_t order = 0;
+    if (n >= 6 && std::memcmp(d, "AOC\0", 4) == 0) {
+        order = 4;
+        ifd_at = 6;
+        m.rel = (long long)at;
+    } else if (n >= 10 && std::memcmp(d, "PENTAX \0", 8) == 0) {
+        order = 8;
+        ifd_at = 10;
+    } else if (n >= 24 && std::memcmp(d, "Adobe\0MakN", 10) == 0) {
+        if (d[14] != d[15] || (d[14] != 'I' && d[14] != 'M')) return false;
+        m.big = d[14] == 'M';
+        const long long orig = (long long)m.u32(16);
+        if (n >= 26 && std::memcmp(d + 20, "AOC\0", 4) == 0) {
+            order = 24;
+            ifd_at = 26;
+            m.rel = orig - 20;
+        } else if (n >= 30 && std::memcmp(d + 20, "PENTAX \0", 8) == 0) {
+            order = 28;
+            ifd_at = 30;
+            m.rel = -20;
+        } else {
+            return false;
+        }
+    } else {
+        return false;
+    }
+    if (d[order] != d[order + 1] || (d[order] != 'I' && d[order] != 'M')) return false;
+    m.big = d[order] == 'M';
+    return true;
+}
+
+// MNLevelInfo (PefFile/PentaxMakerNotesEntry.cs:4687-4692): the roll angle is -byte 1 / 2 degrees.
+constexpr uint16_t MN_LEVEL_INFO = 0x022b;
+bool roll_angle(Tiff& m, const Ifd& note, float& deg)
+{
+    const Entry* e = note.get(MN_LEVEL_INFO);
+    if (!e || e->count < 2 || type_size(e->type) != 1) return false;
+    deg = (float)(-(int)(int8_t)m.u8(e->at + 1)) / 2.0f;
+    return m.ok;
 }
 
 #define ISA_TAG_INT(v, out) \
@@ -352,11 +408,28 @@ int open_dng(const uint8_t* file, size_t size, isa_dng_file& f)
     C.analog_balance = opt(f.ab);
     C.as_shot_neutral = opt(f.neutral);
     C.as_shot_white_xy = opt(f.white_xy);
+    // the roll angle of a Pentax maker note in DNGPrivateData (DNGFile.cs:676-685)
+    if (const Entry* pd = ifd0.get(T_PRIVATE_DATA)) {
+        Tiff m;
+        size_t ifd_at = 0;
+        if (pentax_note(file + pd->at, (size_t)pd->count * type_size(pd->type), pd->at, m, ifd_at)) {
+            Ifd note;
+            m.ifd(ifd_at, note);
+            if (m.ok) f.roll_present = roll_angle(m, note, f.roll);
+        }
+    }
     if (!t.ok) return fail(ISA_EINVAL, "a tag's values lie outside the file");
     return ISA_OK;
 }
 
 }  // namespace
+
+int isa_dng_roll_angle(const isa_dng_file* f, float* roll_deg)
+{
+    if (!f || !roll_deg) return fail(ISA_EINVAL, "NULL argument");
+    *roll_deg = f->roll_present ? f->roll : 0.f;
+    return f->roll_present ? 1 : 0;
+}
 
 int isa_dng_open(const uint8_t* file, size_t size, isa_dng_file** out)
 {
@@ -457,20 +530,8 @@ int open_pef(const uint8_t* file, size_t size, isa_pef_file& f)
     // the maker note's own byte order and offset base
     const size_t mo = mn->at, mlen = (size_t)mn->count * type_size(mn->type);
     Tiff m;
-    m.d = file + mo;
-    m.n = mlen;
     size_t ifd_at = 0;
-    if (mlen >= 6 && std::memcmp(m.d, "AOC\0", 4) == 0) {
-        ifd_at = 6;
-        m.rel = (long long)mo;
-    } else if (mlen >= 10 && std::memcmp(m.d, "PENTAX \0", 8) == 0) {
-        ifd_at = 10;
-    } else {
-        return fail(ISA_EINVAL, "not a Pentax maker note");
-    }
-    const uint8_t o0 = m.d[ifd_at - 2], o1 = m.d[ifd_at - 1];
-    if (o0 != o1 || (o0 != 'I' && o0 != 'M')) return fail(ISA_EINVAL, "maker note byte order");
-    m.big = o0 == 'M';
+    if (!pentax_note(file + mo, mlen, mo, m, ifd_at)) return fail(ISA_EINVAL, "not a Pentax maker note (header or byte order)");
     Ifd note;
     m.ifd(ifd_at, note);
     if (!m.ok) return fail(ISA_EINVAL, "maker note entries outside the maker note");
@@ -498,6 +559,8 @@ int open_pef(const uint8_t* file, size_t size, isa_pef_file& f)
     I.white_level = wl.empty() ? -1.f : (float)wl[0];
     for (int i = 0; i < 4; i++) I.white_point[i] = (float)wp[i];
     I.scaling = (float)sc[0];
+    I.roll_angle = 0.f;
+    I.roll_angle_present = roll_angle(m, note, I.roll_angle) ? 1 : 0;
     if (!t.ok || !m.ok) return fail(ISA_EINVAL, "a tag's values lie outside the file");
     return ISA_OK;
 }

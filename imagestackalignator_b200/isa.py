@@ -78,7 +78,7 @@ EXPORTS = [
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
     "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
     "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec", "isa_dng_decode_path",
-    "isa_dng_open", "isa_dng_close", "isa_dng_file_info", "isa_pef_open", "isa_pef_close", "isa_pef_file_info",
+    "isa_dng_open", "isa_dng_close", "isa_dng_file_info", "isa_dng_roll_angle", "isa_pef_open", "isa_pef_close", "isa_pef_file_info",
 ]
 
 _lib = None
@@ -656,7 +656,9 @@ def dng_open(file):
                      camera_calibration2=_arr(C.camera_calibration2, 9, ctypes.c_double),
                      analog_balance=_arr(C.analog_balance, 3, ctypes.c_double), as_shot_neutral=_arr(C.as_shot_neutral, 3, ctypes.c_double),
                      as_shot_white_xy=_arr(C.as_shot_white_xy, 2, ctypes.c_double))
-        return dict(width=W.value, height=H.value, layout=layout, levels=levels, color=color)
+        roll = ctypes.c_float()
+        has_roll = lib().isa_dng_roll_angle(h, ctypes.byref(roll))
+        return dict(width=W.value, height=H.value, layout=layout, levels=levels, color=color, roll_angle=float(roll.value) if has_roll == 1 else None)
     finally:
         lib().isa_dng_close(h)
 
@@ -667,7 +669,7 @@ class IsaPefInfo(ctypes.Structure):
                 ("strip_sizes", ctypes.c_void_p), ("compressed", ctypes.c_int), ("huffman_table", ctypes.c_void_p),
                 ("huffman_bytes", ctypes.c_size_t), ("huffman_big_endian", ctypes.c_int), ("black_point", ctypes.c_void_p),
                 ("n_black", ctypes.c_int), ("white_level", ctypes.c_float), ("white_point", ctypes.c_float * 4), ("scaling", ctypes.c_float),
-                ("iso", ctypes.c_int)]
+                ("iso", ctypes.c_int), ("roll_angle", ctypes.c_float), ("roll_angle_present", ctypes.c_int)]
 
 
 def pef_open(file):
@@ -685,7 +687,8 @@ def pef_open(file):
                     strip_offsets=_arr(I.strip_offsets, I.nstrips, ctypes.c_uint32), strip_sizes=_arr(I.strip_sizes, I.nstrips, ctypes.c_uint32),
                     compressed=bool(I.compressed), huffman_table=huff, huffman_big_endian=bool(I.huffman_big_endian),
                     black_point=_arr(I.black_point, I.n_black, ctypes.c_float), white_level=None if I.white_level < 0 else I.white_level,
-                    white_point=list(I.white_point), scaling=I.scaling, iso=I.iso)
+                    white_point=list(I.white_point), scaling=I.scaling, iso=I.iso,
+                    roll_angle=float(I.roll_angle) if I.roll_angle_present else None)
     finally:
         lib().isa_pef_close(h)
 

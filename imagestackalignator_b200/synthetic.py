@@ -357,7 +357,7 @@ def _rat(v, den=1000):
 
 def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False, raw_in_subifd=True, black=(512,), white=16383,
              active_area=None, crop=None, deltas=None, noise=None, plane_color=None, iso=200, color=None, version=(1, 4, 0, 0),
-             linearization=None, extra_chain_ifd=False):
+             linearization=None, extra_chain_ifd=False, private_note=None, roll_byte=0):
     """A DNG file image holding `img` (uint16 H x W Bayer) as lossless-JPEG
     tiles in a CFA IFD (a SubIFD of IFD 0, or IFD 0 itself), with the tags
     DNGFile and DNGColorSpec read. color: dict of color_matrix1/2 (9 values),
@@ -412,6 +412,19 @@ def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False,
     for k, tag in (("analog_balance", 50727), ("as_shot_neutral", 50728), ("as_shot_white_xy", 50729)):
         if c.get(k) is not None:
             ifd0.append((tag, 5, [_rat(v, 10000) for v in c[k]]))
+    if private_note is not None:
+        # DNGPrivateData: "Adobe\0MakN", count, byte order, the note's original file offset, then a Pentax
+        # maker note ("AOC": offsets from the original file's start; "PENTAX": from the note's start)
+        orig = 123456
+        level = [(0x022b, 1, [1, roll_byte & 0xFF, 0, 0, 0, 0, 0, 0, 0, 0]), (0x0201, 3, [8192, 8192, 8192, 8192])]
+        if private_note == "AOC":
+            head = b"AOC\0" + (b"MM" if big_endian else b"II")
+            note_bytes = head + _ifd_bytes(level, orig + len(head), big_endian, 0)
+        else:
+            head = b"PENTAX \0" + (b"MM" if big_endian else b"II")
+            note_bytes = head + _ifd_bytes(level, len(head), big_endian, 0)
+        pdata = b"Adobe\0MakN" + struct.pack(">I", len(note_bytes) + 6) + (b"MM" if big_endian else b"II") + struct.pack(e + "I", orig) + note_bytes
+        ifd0.append((50740, 1, list(pdata)))
     # the Exif IFD with the ISO, then the raw IFD, then IFD 0 (and a trailing chain IFD)
     exif_at = len(out)
     out += _ifd_bytes([(34855, 3, [iso])], exif_at, big_endian, 0)
@@ -435,7 +448,7 @@ def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False,
 
 
 def pef_file(img, cfa=(0, 1, 1, 2), compressed=True, big_endian=False, note="AOC", note_big_endian=None, black=(512, 512, 512, 512),
-             white_point=(8192, 8192, 8192, 8192), scaling=8192, white_level=16383, iso=400, bits=14, rows_per_strip=None):
+             white_point=(8192, 8192, 8192, 8192), scaling=8192, white_level=16383, iso=400, bits=14, rows_per_strip=None, roll_byte=None):
     """A PEF file image holding `img` (uint16 H x W Bayer): IFD 0 with the
     strip(s), its Exif IFD with ISO, CFA pattern and a Pentax maker note
     ("AOC": entry offsets from the file's start, or "PENTAX": from the
@@ -474,6 +487,8 @@ def pef_file(img, cfa=(0, 1, 1, 2), compressed=True, big_endian=False, note="AOC
     entries += [(0x0201, 3, list(white_point)), (0x003d, 3, [scaling])]
     if white_level is not None:
         entries.append((0x007e, 4, [white_level]))
+    if roll_byte is not None:   # LevelInfo: orientation, roll (-2 x degrees), pitch, ...
+        entries.append((0x022b, 1, [1, roll_byte & 0xFF, 0, 0, 0, 0, 0, 0, 0, 0]))
     mn_at = len(out)
     if note == "AOC":
         head = b"AOC\0" + (b"MM" if nb else b"II")

@@ -587,6 +587,11 @@ ISA_API int isa_dng_close(isa_dng_file* f);
  * left NULL: take it from isa_dng_color_spec) and the colour tags. */
 ISA_API int isa_dng_file_info(const isa_dng_file* f, isa_dng_layout* layout, isa_dng_level_tags* levels, isa_dng_color_tags* color, int* width,
                               int* height);
+/* The camera roll angle (degrees) of a Pentax maker note carried in IFD 0's
+ * DNGPrivateData (DNGFile.cs:676-685, MNLevelInfo): 1 and the angle when
+ * present, 0 and 0.0 when not. Per frame, the roll angles are the `roll`
+ * input of isa_prealign_burst, as ComputePreAlignment uses them. */
+ISA_API int isa_dng_roll_angle(const isa_dng_file* f, float* roll_deg);
 
 /* ---- PEF container ----
  * PEFFile.SetMembers (PefFile/PEFFile.cs:176-312): the raw image of IFD 0,
@@ -614,6 +619,8 @@ typedef struct isa_pef_info {
     float white_point[4];             /* WhitePoint */
     float scaling;                    /* DataScaling */
     int iso;                          /* ISOSpeedRatings (0 when absent) */
+    float roll_angle;                 /* LevelInfo roll angle in degrees (PEFFile.cs:278-282), 0 when absent */
+    int roll_angle_present;
 } isa_pef_info;
 ISA_API int isa_pef_open(const uint8_t* file, size_t size, isa_pef_file** out);
 ISA_API int isa_pef_close(isa_pef_file* f);

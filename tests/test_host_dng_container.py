@@ -140,3 +140,13 @@ def test_out_of_range_tag_values_are_refused():
         with pytest.raises(isa.IsaError) as e:
             isa.dng_open(bad)
         assert e.value.code == isa.ISA_EINVAL
+
+
+@pytest.mark.parametrize("note", ["AOC", "PENTAX"])
+@pytest.mark.parametrize("big", [False, True])
+def test_roll_angle_from_private_data(note, big):
+    """The Pentax maker note copied into DNGPrivateData behind the "Adobe\\0MakN" header
+    (offsets from the original file for "AOC", from the note for "PENTAX"): LevelInfo's roll angle."""
+    img = _img(32, 32)
+    assert isa.dng_open(S.dng_file(img, tile=32, big_endian=big, private_note=note, roll_byte=-9)[0])["roll_angle"] == 4.5
+    assert isa.dng_open(S.dng_file(img, tile=32, big_endian=big)[0])["roll_angle"] is None

@@ -73,3 +73,12 @@ def test_unreadable_files(damage):
     with pytest.raises(isa.IsaError) as e:
         isa.pef_open(bytes(b))
     assert e.value.code == isa.ISA_EINVAL
+
+
+@pytest.mark.parametrize("note", ["AOC", "PENTAX"])
+@pytest.mark.parametrize("roll_byte", [None, 0, 7, -12])
+def test_roll_angle_from_level_info(note, roll_byte):
+    """MNLevelInfo: the roll angle is -(signed byte 1) / 2 degrees; absent without the entry."""
+    f, _, _ = S.pef_file(_img(16, 16), note=note, roll_byte=roll_byte, big_endian=note == "PENTAX")
+    got = isa.pef_open(f)["roll_angle"]
+    assert got == (None if roll_byte is None else -roll_byte / 2.0)
