@@ -357,7 +357,7 @@ def _rat(v, den=1000):
 
 def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False, raw_in_subifd=True, black=(512,), white=16383,
              active_area=None, crop=None, deltas=None, noise=None, plane_color=None, iso=200, color=None, version=(1, 4, 0, 0),
-             linearization=None, extra_chain_ifd=False, private_note=None, roll_byte=0):
+             linearization=None, extra_chain_ifd=False, private_note=None, roll_byte=0, threads=1):
     """A DNG file image holding `img` (uint16 H x W Bayer) as lossless-JPEG
     tiles in a CFA IFD (a SubIFD of IFD 0, or IFD 0 itself), with the tags
     DNGFile and DNGColorSpec read. color: dict of color_matrix1/2 (9 values),
@@ -369,17 +369,27 @@ def dng_file(img, cfa=(0, 1, 1, 2), bits=14, tile=128, clrs=2, big_endian=False,
     e = ">" if big_endian else "<"
     out = bytearray((b"MM" if big_endian else b"II") + struct.pack(e + "HI", 42, 0))
     offs, cnts = [], []
-    for ty in range(0, H, tile):
-        for tx in range(0, W, tile):
-            t = np.zeros((tile, tile), np.uint16)
-            blk = img[ty:ty + tile, tx:tx + tile]
-            t[:blk.shape[0], :blk.shape[1]] = blk
-            s = lj92_tile(t, clrs, bits)
-            offs.append(len(out))
-            cnts.append(len(s))
-            out += bytes(s)
-            if len(out) % 2:
-                out += b"\0"
+
+    def encode(pos):
+        ty, tx = pos
+        t = np.zeros((tile, tile), np.uint16)
+        blk = img[ty:ty + tile, tx:tx + tile]
+        t[:blk.shape[0], :blk.shape[1]] = blk
+        return lj92_tile(t, clrs, bits)
+
+    positions = [(ty, tx) for ty in range(0, H, tile) for tx in range(0, W, tile)]
+    if threads > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(threads) as ex:
+            tiles = list(ex.map(encode, positions))
+    else:
+        tiles = [encode(p) for p in positions]
+    for s in tiles:
+        offs.append(len(out))
+        cnts.append(len(s))
+        out += bytes(s)
+        if len(out) % 2:
+            out += b"\0"
     raw = [(254, 4, [0]), (256, 4, [W]), (257, 4, [H]), (258, 3, [16]), (259, 3, [7]), (262, 3, [32803]), (277, 3, [1]),
            (322, 3, [tile]), (323, 3, [tile]), (324, 4, offs), (325, 4, cnts), (33421, 3, [2, 2]), (33422, 1, list(cfa)),
            (50717, 4, [white])]
