@@ -408,7 +408,8 @@ def files_throughput(args, burst, merger, out):
     files = [synthetic.dng_file(np.ascontiguousarray(burst.raw[f]), tile=256, noise=[burst.noise_a, burst.noise_b],
                                 color=dict(as_shot_neutral=[1.0, 1.0, 1.0]), threads=os.cpu_count() or 1)[0] for f in range(n)]
     hosts = [torch.from_numpy(f).pin_memory() for f in files]
-    dev = torch.empty(max(f.size for f in files), dtype=torch.uint8, device="cuda")
+    devs = [torch.empty(f.size, dtype=torch.uint8, device="cuda") for f in files]
+    copy_stream = torch.cuda.Stream()
     frames = torch.empty((n, H, W), dtype=torch.int16, device="cuda")
     need = max(isa.dng_decode_scratch(f, W, H, **isa.dng_open(f)["layout"]) for f in files)
     scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
@@ -416,13 +417,22 @@ def files_throughput(args, burst, merger, out):
     host_out = torch.empty((Ho, Wo, 3), dtype=torch.float32).pin_memory()
 
     def step():
+        # every file's bytes go to the device on a side stream, each decode waiting only for its own file
+        copied = []
+        with torch.cuda.stream(copy_stream):
+            for i in range(n):
+                devs[i].copy_(hosts[i], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy_stream)
+                copied.append(ev)
         info = None
         for i, f in enumerate(files):
             d = isa.dng_open(f)
             c2p, cw, _ = isa.dng_color_spec(**d["color"])
             lv = isa.dng_levels(camera_white=cw, **d["levels"])
-            dev[:f.size].copy_(hosts[i], non_blocking=True)
-            isa.dng_decode(f, W, H, black_h=lv["black_h"], black_v=lv["black_v"], file_dev=dev, scratch=scratch, out=frames[i], **d["layout"])
+            torch.cuda.current_stream().wait_event(copied[i])
+            isa.dng_decode(f, W, H, black_h=lv["black_h"], black_v=lv["black_v"], file_dev=devs[i], scratch=scratch, out=frames[i],
+                           **d["layout"])
             info = lv["info"] if i == 0 else info
         merger.merge(frames, info, out)
         host_out.copy_(out, non_blocking=True)
