@@ -538,6 +538,13 @@ def run_ours(args):
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                 "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
                 "traffic": tr.get("dram_bytes_per_launch") if tr else None}
+    if not args.per_frame and acc_ms:
+        # the reference's layout: one pass per frame reading raw, flow, mask and kernel and reading and
+        # writing the float3 sums, n passes in the time of the fused launch (which is issue-bound, not HBM-bound)
+        ref_bytes = ((2 + 8 + 16 / 4 + 16) / s ** 2 + 48) * Wo * Ho * n
+        ref_gbs = ref_bytes / (stages[4] / 1e3) / 1e9
+        roofline["reference_layout"] = {"bytes_per_step": ref_bytes, "achieved": ref_gbs, "frac": ref_gbs / peak,
+                                        "note": "the per-frame passes of the reference moved in the fused kernel's time"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
