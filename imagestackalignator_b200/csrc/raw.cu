@@ -121,7 +121,19 @@ __global__ void __launch_bounds__(PEF_NT) k_pef_map(const unsigned* __restrict__
         if (k < PEF_K) {
             unsigned p = (unsigned)k, c = 0;
             bool stop = false;
-            while (p < PEF_CHUNK) {
+            // two symbols per step while both must start inside the chunk (a symbol is at most 27 bits)
+            while (p < PEF_CHUNK - 64) {
+                const unsigned w1 = p >> 5;
+                const unsigned a1 = adv[__funnelshift_l(cw[warp][w1 + 1], cw[warp][w1], p & 31) >> 20];
+                if (a1 == 0) { stop = true; break; }
+                p += a1;
+                const unsigned w2 = p >> 5;
+                const unsigned a2 = adv[__funnelshift_l(cw[warp][w2 + 1], cw[warp][w2], p & 31) >> 20];
+                if (a2 == 0) { c += 1; stop = true; break; }
+                p += a2;
+                c += 2;
+            }
+            while (!stop && p < PEF_CHUNK) {
                 const unsigned w = p >> 5;
                 const unsigned a = adv[__funnelshift_l(cw[warp][w + 1], cw[warp][w], p & 31) >> 20];
                 if (a == 0) { stop = true; break; }
@@ -959,7 +971,26 @@ __global__ void __launch_bounds__(DF_NT) k_dngf_map(const unsigned* __restrict__
         __syncwarp();
         unsigned p = first[i] ? 0u : (unsigned)k, c = 0;
         bool stop = false;
-        while (p < 1024) {
+        // two symbols per step while both must start inside the chunk (a symbol is at most 32 bits)
+        while (p < 1024 - 64) {
+            const unsigned w1 = p >> 5;
+            const unsigned a1 = adv[__funnelshift_l(cw[w1 + 1], cw[w1], p & 31) >> sh];
+            if (a1 == 0) {
+                stop = true;
+                break;
+            }
+            p += a1;
+            const unsigned w2 = p >> 5;
+            const unsigned a2 = adv[__funnelshift_l(cw[w2 + 1], cw[w2], p & 31) >> sh];
+            if (a2 == 0) {
+                c += 1;
+                stop = true;
+                break;
+            }
+            p += a2;
+            c += 2;
+        }
+        while (!stop && p < 1024) {
             const unsigned w = p >> 5;
             const unsigned a = adv[__funnelshift_l(cw[w + 1], cw[w], p & 31) >> sh];
             if (a == 0) {
