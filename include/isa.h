@@ -473,7 +473,9 @@ ISA_API int isa_pef_color_spec(const float white_balance[3], double camera_to_pc
  * table and the black-level deltas: out = max(0, lin[min(v, nlin - 1)] -
  * black_h[col] - black_v[row]). Lossless-JPEG headers are parsed from
  * `file_host`; the data is read from `file_dev` (the same bytes on the
- * device) by one thread per tile. */
+ * device), by the parallel decoder for predictor-1 parts without restarts
+ * inside a part and one Huffman table, else by one warp per part
+ * (isa_dng_decode_path). */
 typedef struct isa_dng_layout {
     int tiled;                       /* 1: TileWidth/TileLength/TileOffsets/TileByteCounts; 0: strips */
     int tile_width, tile_height;     /* tiles */
