@@ -2554,79 +2554,165 @@ size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size, const 
 
 int isa_dng_decode_path(void) { return g_dng_path; }
 
+namespace {
+
+constexpr int kDngErr0 = 0x7fffffff;  // no part failed
+
+// The device buffers of one isa_dng_decode call inside its scratch (the order of dng_scratch_bytes).
+struct DngBuffers {
+    unsigned long long* offs;
+    unsigned long long* cnts;
+    int* err;
+    uint16_t *bh, *bv, *lin;
+    void* parts = nullptr;
+    uint16_t* tables = nullptr;
+    uint16_t* rows = nullptr;
+    char* fast = nullptr;
+    size_t fast_bytes = 0;
+};
+
+DngBuffers dng_buffers(char* base, const isa_dng_layout* L, int width, int height, const DngPlan& plan)
+{
+    DngBuffers b;
+    size_t o = 0;
+    const auto take = [&](size_t bytes) { char* p = base + o; o += align256(bytes); return p; };
+    take((size_t)L->n * 16);
+    b.offs = (unsigned long long*)take((size_t)L->n * 8);
+    b.cnts = (unsigned long long*)take((size_t)L->n * 8);
+    b.err = (int*)take(64);
+    b.bh = (uint16_t*)take((size_t)width * 2);
+    b.bv = (uint16_t*)take((size_t)height * 2);
+    b.lin = (uint16_t*)take((size_t)std::max(L->nlin, 1) * 2);
+    if (L->compression == 7) {
+        b.parts = take(plan.parts.size());
+        b.tables = (uint16_t*)take(plan.tables.size() * 2 + 2);
+        b.rows = (uint16_t*)take(plan.row_samples * 2 + 16);
+        b.fast_bytes = isa_dngf_scratch(plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(), L->dng_version_large);
+        if (b.fast_bytes > 0) b.fast = take(b.fast_bytes);
+    }
+    return b;
+}
+
+// Checks, plan and the uploads every decode starts with; the output is cleared.
+int dng_prologue(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height,
+                 void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, cudaStream_t st, DngPlan& plan, DngBuffers& b)
+{
+    ISA_REQ(file_host && file_dev && scratch && out, "NULL argument");
+    ISA_TRY(isa_dng_check(L, width, height));
+    ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
+    if (L->compression == 7) ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));
+    ISA_REQ(scratch_bytes >= dng_scratch_bytes(L, width, height, plan), "scratch too small (isa_dng_decode_scratch)");
+    if (L->compression == 7 && (size_t)4 * (4096 + 4 * (size_t)plan.jwide_max + 64) > 227 * 1024)
+        return fail(ISA_EINVAL, "rows of %d samples exceed the decoder's shared-memory row buffers", plan.jwide_max);
+    b = dng_buffers((char*)scratch, L, width, height, plan);
+    std::vector<unsigned long long> offs(L->n), cnts(L->n);
+    for (int i = 0; i < L->n; i++) { offs[i] = L->offsets[i]; cnts[i] = L->byte_counts[i]; }
+    ISA_CK(cudaMemcpyAsync(b.offs, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(b.cnts, cnts.data(), cnts.size() * 8, cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(b.err, &kDngErr0, sizeof(int), cudaMemcpyHostToDevice, st));
+    if (L->black_h) ISA_CK(cudaMemcpyAsync(b.bh, L->black_h, (size_t)width * 2, cudaMemcpyHostToDevice, st));
+    if (L->black_v) ISA_CK(cudaMemcpyAsync(b.bv, L->black_v, (size_t)height * 2, cudaMemcpyHostToDevice, st));
+    if (L->linearization) ISA_CK(cudaMemcpyAsync(b.lin, L->linearization, (size_t)L->nlin * 2, cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemset2DAsync(out, out_pitch, 0, (size_t)width * 2, height, st));
+    if (L->compression == 7) {
+        ISA_CK(cudaMemcpyAsync(b.parts, plan.parts.data(), plan.parts.size(), cudaMemcpyHostToDevice, st));
+        if (!plan.tables.empty()) ISA_CK(cudaMemcpyAsync(b.tables, plan.tables.data(), plan.tables.size() * 2, cudaMemcpyHostToDevice, st));
+    }
+    return ISA_OK;
+}
+
+int dng_launch_fast(const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height, uint16_t* out, size_t out_pitch,
+                    const DngPlan& plan, const DngBuffers& b, int* anomaly_host, cudaStream_t st)
+{
+    ISA_CK(isa_launch_dngf(file_dev, file_size, plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(),
+                           L->linearization ? b.lin : nullptr, L->nlin, L->black_h ? b.bh : nullptr, L->black_v ? b.bv : nullptr, width, height,
+                           L->dng_version_large, out, out_pitch, b.err, b.fast, b.fast_bytes, anomaly_host, st));
+    return ISA_OK;
+}
+
+int dng_error(int err)
+{
+    if (err != kDngErr0) return fail(ISA_EINVAL, "part %d: a decoded sample exceeds the frame's bit depth (the reference stops there)", err);
+    return ISA_OK;
+}
+
+// The per-part reader (every layout; the frames the parallel decoder hands back), synchronised.
+int dng_sequential(const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height, uint16_t* out, size_t out_pitch,
+                   const DngPlan& plan, const DngBuffers& b, bool clear, cudaStream_t st)
+{
+    if (clear) {
+        ISA_CK(cudaMemcpyAsync(b.err, &kDngErr0, sizeof(int), cudaMemcpyHostToDevice, st));
+        ISA_CK(cudaMemset2DAsync(out, out_pitch, 0, (size_t)width * 2, height, st));
+    }
+    g_dng_path = L->compression == 7 ? 0 : -1;
+    ISA_CK(isa_launch_dng(file_dev, file_size, L->compression, b.parts, L->n, b.tables, b.rows, b.offs, b.cnts, L->rows_per_strip, L->bit_depth,
+                          L->linearization ? b.lin : nullptr, L->nlin, L->black_h ? b.bh : nullptr, L->black_v ? b.bv : nullptr, width, height,
+                          L->dng_version_large, out, out_pitch, b.err, st, plan.jwide_max, (int)plan.tables.size()));
+    int err = kDngErr0;
+    ISA_CK(cudaMemcpyAsync(&err, b.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ISA_CK(cudaStreamSynchronize(st));
+    return dng_error(err);
+}
+
+// After the parallel decoder: its flags, and the per-part reader when it handed the frame back.
+int dng_settle(const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height, uint16_t* out, size_t out_pitch,
+               const DngPlan& plan, const DngBuffers& b, cudaStream_t st)
+{
+    const size_t flag = isa_dngf_flag_offset(plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(), L->dng_version_large);
+    int anomaly = 1, err = kDngErr0;
+    ISA_CK(cudaStreamSynchronize(st));
+    ISA_CK(cudaMemcpy(&anomaly, b.fast + flag, sizeof(int), cudaMemcpyDeviceToHost));
+    ISA_CK(cudaMemcpy(&err, b.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (anomaly == 0) {
+        g_dng_path = 1;
+        return dng_error(err);
+    }
+    return dng_sequential(file_dev, file_size, L, width, height, out, out_pitch, plan, b, true, st);
+}
+
+}  // namespace
+
 int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height,
                    void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream)
 {
     g_dng_path = -1;
+    cudaStream_t st = S(stream);
+    DngPlan plan;
+    DngBuffers b;
+    ISA_TRY(dng_prologue(file_host, file_dev, file_size, L, width, height, scratch, scratch_bytes, out, out_pitch, st, plan, b));
+    if (b.fast) {
+        ISA_TRY(dng_launch_fast(file_dev, file_size, L, width, height, out, out_pitch, plan, b, nullptr, st));
+        return dng_settle(file_dev, file_size, L, width, height, out, out_pitch, plan, b, st);
+    }
+    return dng_sequential(file_dev, file_size, L, width, height, out, out_pitch, plan, b, false, st);
+}
+
+int isa_dng_decode_begin(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height,
+                         void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream)
+{
+    g_dng_path = -1;
+    cudaStream_t st = S(stream);
+    DngPlan plan;
+    DngBuffers b;
+    ISA_TRY(dng_prologue(file_host, file_dev, file_size, L, width, height, scratch, scratch_bytes, out, out_pitch, st, plan, b));
+    if (b.fast) return dng_launch_fast(file_dev, file_size, L, width, height, out, out_pitch, plan, b, nullptr, st);
+    return dng_sequential(file_dev, file_size, L, width, height, out, out_pitch, plan, b, false, st);
+}
+
+int isa_dng_decode_finish(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* L, int width, int height,
+                          void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream)
+{
+    g_dng_path = -1;
     ISA_REQ(file_host && file_dev && scratch && out, "NULL argument");
     ISA_TRY(isa_dng_check(L, width, height));
-    ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
+    cudaStream_t st = S(stream);
     DngPlan plan;
     if (L->compression == 7) ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));
-    const size_t need = dng_scratch_bytes(L, width, height, plan);
-    ISA_REQ(scratch_bytes >= need, "scratch too small (isa_dng_decode_scratch)");
-    cudaStream_t st = S(stream);
-    char* base = (char*)scratch;
-    size_t o = 0;
-    const auto take = [&](size_t bytes) { char* p = base + o; o += align256(bytes); return p; };
-    take((size_t)L->n * 16);
-    unsigned long long* d_offs = (unsigned long long*)take((size_t)L->n * 8);
-    unsigned long long* d_cnts = (unsigned long long*)take((size_t)L->n * 8);
-    int* d_err = (int*)take(64);
-    uint16_t* d_bh = (uint16_t*)take((size_t)width * 2);
-    uint16_t* d_bv = (uint16_t*)take((size_t)height * 2);
-    uint16_t* d_lin = (uint16_t*)take((size_t)std::max(L->nlin, 1) * 2);
-    std::vector<unsigned long long> offs(L->n), cnts(L->n);
-    for (int i = 0; i < L->n; i++) { offs[i] = L->offsets[i]; cnts[i] = L->byte_counts[i]; }
-    ISA_CK(cudaMemcpyAsync(d_offs, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(d_cnts, cnts.data(), cnts.size() * 8, cudaMemcpyHostToDevice, st));
-    const int err0 = 0x7fffffff;
-    ISA_CK(cudaMemcpyAsync(d_err, &err0, sizeof(int), cudaMemcpyHostToDevice, st));
-    if (L->black_h) ISA_CK(cudaMemcpyAsync(d_bh, L->black_h, (size_t)width * 2, cudaMemcpyHostToDevice, st));
-    if (L->black_v) ISA_CK(cudaMemcpyAsync(d_bv, L->black_v, (size_t)height * 2, cudaMemcpyHostToDevice, st));
-    if (L->linearization) ISA_CK(cudaMemcpyAsync(d_lin, L->linearization, (size_t)L->nlin * 2, cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemset2DAsync(out, out_pitch, 0, (size_t)width * 2, height, st));
-    const void* d_parts = nullptr;
-    const uint16_t* d_tables = nullptr;
-    uint16_t* d_rows = nullptr;
-    int nparts = L->n;
-    if (L->compression == 7) {
-        if ((size_t)4 * (4096 + 4 * (size_t)plan.jwide_max + 64) > 227 * 1024)
-            return fail(ISA_EINVAL, "rows of %d samples exceed the decoder's shared-memory row buffers", plan.jwide_max);
-        void* p = take(plan.parts.size());
-        uint16_t* tb = (uint16_t*)take(plan.tables.size() * 2 + 2);
-        d_rows = (uint16_t*)take(plan.row_samples * 2 + 16);
-        ISA_CK(cudaMemcpyAsync(p, plan.parts.data(), plan.parts.size(), cudaMemcpyHostToDevice, st));
-        if (!plan.tables.empty()) ISA_CK(cudaMemcpyAsync(tb, plan.tables.data(), plan.tables.size() * 2, cudaMemcpyHostToDevice, st));
-        d_parts = p;
-        d_tables = tb;
-        const size_t fast = isa_dngf_scratch(plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(), L->dng_version_large);
-        if (fast > 0) {
-            // the parallel decoder; its flag sends the frame to the per-part reader
-            void* fs = take(fast);
-            int anomaly = 1;
-            ISA_CK(isa_launch_dngf(file_dev, file_size, plan.parts.data(), plan.nparts, plan.tables.data(), plan.tables.size(),
-                                   L->linearization ? d_lin : nullptr, L->nlin, L->black_h ? d_bh : nullptr, L->black_v ? d_bv : nullptr, width,
-                                   height, L->dng_version_large, out, out_pitch, d_err, fs, fast, &anomaly, st));
-            ISA_CK(cudaStreamSynchronize(st));
-            if (anomaly == 0) {
-                int err = err0;
-                ISA_CK(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
-                g_dng_path = 1;
-                if (err != err0) return fail(ISA_EINVAL, "part %d: a decoded sample exceeds the frame's bit depth (the reference stops there)", err);
-                return ISA_OK;
-            }
-            ISA_CK(cudaMemcpyAsync(d_err, &err0, sizeof(int), cudaMemcpyHostToDevice, st));
-            ISA_CK(cudaMemset2DAsync(out, out_pitch, 0, (size_t)width * 2, height, st));
-        }
+    ISA_REQ(scratch_bytes >= dng_scratch_bytes(L, width, height, plan), "scratch too small (isa_dng_decode_scratch)");
+    const DngBuffers b = dng_buffers((char*)scratch, L, width, height, plan);
+    if (!b.fast) {  // isa_dng_decode_begin already decoded it with the per-part reader and waited
+        g_dng_path = L->compression == 7 ? 0 : -1;
+        return ISA_OK;
     }
-    g_dng_path = L->compression == 7 ? 0 : -1;
-    ISA_CK(isa_launch_dng(file_dev, file_size, L->compression, d_parts, nparts, d_tables, d_rows, d_offs, d_cnts, L->rows_per_strip, L->bit_depth,
-                          L->linearization ? d_lin : nullptr, L->nlin, L->black_h ? d_bh : nullptr, L->black_v ? d_bv : nullptr, width, height,
-                          L->dng_version_large, out, out_pitch, d_err, st, plan.jwide_max, (int)plan.tables.size()));
-    int err = err0;
-    ISA_CK(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    ISA_CK(cudaStreamSynchronize(st));
-    if (err != err0) return fail(ISA_EINVAL, "part %d: a decoded sample exceeds the frame's bit depth (the reference stops there)", err);
-    return ISA_OK;
+    return dng_settle(file_dev, file_size, L, width, height, out, out_pitch, plan, b, st);
 }

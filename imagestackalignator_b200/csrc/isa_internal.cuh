@@ -203,6 +203,8 @@ cudaError_t isa_launch_dng(const uint8_t* file, unsigned long long fsize, int co
                            cudaStream_t st, int jwide_max, int ntables);
 // the parallel decoder of predictor-1 parts: scratch bytes (0 = the frame does not qualify) and launch
 size_t isa_dngf_scratch(const void* parts, int nparts, const uint16_t* tables, size_t ntables, int large);
+size_t isa_dngf_flag_offset(const void* parts, int nparts, const uint16_t* tables, size_t ntables, int large);  // the hand-back flag in that scratch
 cudaError_t isa_launch_dngf(const uint8_t* file, unsigned long long fsize, const void* parts_host, int nparts, const uint16_t* tables_host,
                             size_t ntables, const uint16_t* lin, int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large,
-                            uint16_t* out, size_t out_pitch, int* error, void* scratch, size_t scratch_bytes, int* anomaly_host, cudaStream_t st);
+                            uint16_t* out, size_t out_pitch, int* error, void* scratch, size_t scratch_bytes, int* anomaly_host /* NULL: not read back */,
+                            cudaStream_t st);

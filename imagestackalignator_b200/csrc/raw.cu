@@ -1343,6 +1343,12 @@ size_t isa_dngf_scratch(const void* parts, int nparts, const uint16_t* tables, s
     return dngf_plan((const Lj92Part*)parts, nparts, tables, ntables, large, pl) ? pl.bytes : 0;
 }
 
+size_t isa_dngf_flag_offset(const void* parts, int nparts, const uint16_t* tables, size_t ntables, int large)
+{
+    DngfPlan pl;
+    return dngf_plan((const Lj92Part*)parts, nparts, tables, ntables, large, pl) ? pl.part[17] : 0;
+}
+
 cudaError_t isa_launch_dngf(const uint8_t* file, unsigned long long fsize, const void* parts_host, int nparts, const uint16_t* tables_host,
                             size_t ntables, const uint16_t* lin, int nlin, const uint16_t* bh, const uint16_t* bv, int W, int H, int large,
                             uint16_t* out, size_t out_pitch, int* error, void* scratch, size_t scratch_bytes, int* anomaly_host, cudaStream_t st)
@@ -1406,5 +1412,5 @@ cudaError_t isa_launch_dngf(const uint8_t* file, unsigned long long fsize, const
     DngArgs A{file, fsize, nullptr, nparts, nullptr, nullptr, lin, nlin, bh, bv, W, H, large, out, out_pitch, error};
     k_dngf_rows<<<dim3((max_high + 7) / 8, nparts), 256, 0, st>>>(A, d_parts, diff);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return cudaMemcpyAsync(anomaly_host, d_anomaly, sizeof(int), cudaMemcpyDeviceToHost, st);
+    return anomaly_host ? cudaMemcpyAsync(anomaly_host, d_anomaly, sizeof(int), cudaMemcpyDeviceToHost, st) : cudaSuccess;
 }

@@ -78,7 +78,7 @@ EXPORTS = [
     "isa_pef_huff_table", "isa_pef_decode_scratch", "isa_pef_decode", "isa_pef_unpack", "isa_pef_levels",
     "isa_dng_color_spec", "isa_pef_color_spec", "isa_dng_decode_scratch", "isa_dng_decode",
     "isa_dng_levels", "isa_noise_model", "isa_crop_window", "isa_profile_color_spec", "isa_dng_decode_path",
-    "isa_dng_open", "isa_dng_close", "isa_dng_file_info", "isa_dng_roll_angle", "isa_pef_open", "isa_pef_close", "isa_pef_file_info",
+    "isa_dng_open", "isa_dng_close", "isa_dng_file_info", "isa_dng_roll_angle", "isa_dng_decode_begin", "isa_dng_decode_finish", "isa_pef_open", "isa_pef_close", "isa_pef_file_info",
 ]
 
 _lib = None
@@ -576,11 +576,12 @@ class IsaDngLayout(ctypes.Structure):
 
 
 def dng_decode(file, width, height, offsets, counts, compression=7, tiled=True, tile_w=0, tile_h=0, rows_per_strip=0, bit_depth=16, large=True,
-               linearization=None, black_h=None, black_v=None, file_dev=None, stream=None, scratch=None, out=None):
+               linearization=None, black_h=None, black_v=None, file_dev=None, stream=None, scratch=None, out=None, phase=None):
     """isa_dng_decode of a DNG file image (host uint8 array; copied to the
     device unless file_dev is given); returns the frame (int16 tensor holding
     uint16). scratch / out: device buffers to reuse (scratch of at least
-    isa_dng_decode_scratch bytes)."""
+    isa_dng_decode_scratch bytes). phase "begin" / "finish": the two halves
+    (isa_dng_decode_begin / _finish), called with the same arguments."""
     import torch
     f = np.ascontiguousarray(file, np.uint8)
     keep = [np.ascontiguousarray(offsets, np.uint32), np.ascontiguousarray(counts, np.uint32)]
@@ -600,8 +601,9 @@ def dng_decode(file, width, height, offsets, counts, compression=7, tiled=True, 
         scratch = torch.empty(need, dtype=torch.uint8, device=dev.device)
     if out is None:
         out = torch.empty((height, width), dtype=torch.int16, device=dev.device)
-    check(lib().isa_dng_decode(fp, vp(dev), ctypes.c_size_t(f.size), ctypes.byref(L), width, height, vp(scratch), ctypes.c_size_t(scratch.numel()),
-                               vp(out), ctypes.c_size_t(out.stride(0) * 2), stream_ptr(stream)))
+    fn = {None: lib().isa_dng_decode, "begin": lib().isa_dng_decode_begin, "finish": lib().isa_dng_decode_finish}[phase]
+    check(fn(fp, vp(dev), ctypes.c_size_t(f.size), ctypes.byref(L), width, height, vp(scratch), ctypes.c_size_t(scratch.numel()),
+             vp(out), ctypes.c_size_t(out.stride(0) * 2), stream_ptr(stream)))
     return out
 
 

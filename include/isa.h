@@ -497,6 +497,17 @@ ISA_API size_t isa_dng_decode_scratch(const uint8_t* file_host, size_t file_size
  * stop (a sample above the frame's bit depth). */
 ISA_API int isa_dng_decode(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* layout, int width, int height,
                            void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream);
+/* isa_dng_decode in two halves, so that a host decodes many frames with one
+ * wait: begin does the checks, the uploads and, when the frame qualifies for
+ * the parallel decoder, enqueues it on `stream` and returns at once (other
+ * frames decode with the per-part reader inside begin, synchronised);
+ * finish, with the same arguments and the scratch untouched in between,
+ * waits for `stream`, reads the decoder's flags and decodes a handed-back
+ * frame with the per-part reader. The output is complete after finish. */
+ISA_API int isa_dng_decode_begin(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* layout, int width,
+                                 int height, void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream);
+ISA_API int isa_dng_decode_finish(const uint8_t* file_host, const uint8_t* file_dev, size_t file_size, const isa_dng_layout* layout, int width,
+                                  int height, void* scratch, size_t scratch_bytes, uint16_t* out, size_t out_pitch, void* stream);
 /* Which decoder the calling thread's last isa_dng_decode used: 1 = the
  * parallel one (lossless-JPEG parts with predictor 1, no restart inside a
  * part, one Huffman table: chunks decoded from every candidate start, as

@@ -257,3 +257,36 @@ def test_dng_files_to_tiff(cuda, tmp_path):
     d = np.abs(img.astype(np.int64) - want.astype(np.int64))
     assert d.max() <= 1 and (d > 0).sum() <= max(3, 2e-3 * d.size)
     assert img.std() > 100
+
+
+def test_begin_finish_over_many_frames(cuda):
+    """isa_dng_decode_begin for every frame, then isa_dng_decode_finish for every frame:
+    each output equals isa_dng_decode's, for frames of the parallel decoder, a frame it
+    hands back (a long 0xFF run) and a frame of the per-part reader (predictor 2)."""
+    import torch
+    rng = np.random.default_rng(17)
+    H, W = 80, 128
+    cases = []
+    for kind in ("parallel", "handback", "psv2", "parallel"):
+        img = rng.integers(0, 32768, (H, W)).astype(np.uint16)
+        f, offs, cnts = R.dng_tiles(img, 64, 40, clrs=2, bits=16, psv=2 if kind == "psv2" else 1)
+        if kind == "handback":
+            f, offs, cnts = _random_entropy(f, offs, cnts, 9, ff=0.05, ff_run=101)
+        cases.append((kind, f, offs, cnts))
+    kw = dict(tiled=True, tile_w=64, tile_h=40)
+    want = [run(f, W, H, o, c, **kw) for _, f, o, c in cases]
+    jobs = []
+    for kind, f, o, c in cases:
+        dev = torch.from_numpy(f).cuda()
+        scratch = torch.empty(isa.dng_decode_scratch(f, W, H, o, c, **kw), dtype=torch.uint8, device="cuda")
+        out = torch.full((H, W), -1, dtype=torch.int16, device="cuda")
+        isa.dng_decode(f, W, H, o, c, file_dev=dev, scratch=scratch, out=out, phase="begin", **kw)
+        jobs.append((f, o, c, dev, scratch, out))
+    paths = []
+    for f, o, c, dev, scratch, out in jobs:
+        isa.dng_decode(f, W, H, o, c, file_dev=dev, scratch=scratch, out=out, phase="finish", **kw)
+        paths.append(isa.dng_decode_path())
+    torch.cuda.synchronize()
+    assert paths == [1, 0, 0, 1]
+    for (f, o, c, dev, scratch, out), w in zip(jobs, want):
+        assert np.array_equal(out.cpu().numpy().view(np.uint16), w)
