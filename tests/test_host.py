@@ -115,3 +115,24 @@ def test_gauss_taps_follow_controller_rule(oracle):
     assert len(oracle.gauss_taps(2.0)) == 7
     assert len(oracle.gauss_taps(0.0)) == 9 and oracle.gauss_taps(0.0)[4] == 1
     assert abs(oracle.gauss_taps(1.0).sum() - 1) < 1e-12
+
+
+def test_dng_decode_halves_and_file_handles_check_their_arguments():
+    """isa_dng_decode_begin / _finish, isa_dng_roll_angle, isa_dng_file_info and
+    isa_pef_file_info refuse NULL and bad layouts before any CUDA call."""
+    lib = isa.lib()
+    fake = ctypes.c_void_p(256)
+    L = isa.IsaDngLayout()
+    for fn in (lib.isa_dng_decode_begin, lib.isa_dng_decode_finish):
+        assert fn(None, fake, ctypes.c_size_t(16), ctypes.byref(L), 8, 8, fake, ctypes.c_size_t(1 << 20), fake, ctypes.c_size_t(16),
+                  None) == isa.ISA_EINVAL
+        assert fn(fake, fake, ctypes.c_size_t(16), ctypes.byref(L), 8, 8, fake, ctypes.c_size_t(1 << 20), fake, ctypes.c_size_t(16),
+                  None) == isa.ISA_EINVAL   # n = 0: a bad layout
+    roll = ctypes.c_float()
+    assert lib.isa_dng_roll_angle(None, ctypes.byref(roll)) == isa.ISA_EINVAL
+    assert lib.isa_dng_file_info(None, None, None, None, None, None) == isa.ISA_EINVAL
+    assert lib.isa_pef_file_info(None, None) == isa.ISA_EINVAL
+    h = ctypes.c_void_p()
+    assert lib.isa_dng_open(None, ctypes.c_size_t(0), ctypes.byref(h)) == isa.ISA_EINVAL
+    assert lib.isa_pef_open(ctypes.c_char_p(b"II*\0"), ctypes.c_size_t(4), ctypes.byref(h)) == isa.ISA_EINVAL
+    assert lib.isa_dng_close(None) == isa.ISA_OK and lib.isa_pef_close(None) == isa.ISA_OK
