@@ -229,6 +229,9 @@ struct isa_ctx {
     cudaEvent_t ev_free = nullptr, ev_copied = nullptr;
     int ev_count = 0;
     long launches = 0;  // kernels of this library launched by the last merge
+    // caller-owned record of every level's tile search (isa_debug_track_record), or null
+    int* track_rec = nullptr;
+    size_t track_rec_bytes = 0;
     // last call
     int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0;
 };
@@ -474,6 +477,15 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     float2* grids_tmp = c->grids_tmp;
     ISA_CK(cudaMemsetAsync(grids, 0, gstride * strat.m, st));
     int tcx0 = 0, tcy0 = 0;
+    // record of the tile search per level (argmin, then block offsets), finest level first
+    std::vector<size_t> rec_off(L + 1, 0);
+    for (int li = 0; li < L; li++) {
+        int tx, ty;
+        if (level_tiles(p->levels[li], W, H, &tx, &ty) != ISA_OK) return fail(ISA_EINVAL, "level %d has no tiles for %dx%d", li, W, H);
+        rec_off[li + 1] = rec_off[li] + (size_t)3 * strat.m * tx * ty;
+    }
+    if (c->track_rec && c->track_rec_bytes < rec_off[L] * sizeof(int))
+        return fail(ISA_EINVAL, "tile-search record of %zu bytes < %zu needed", c->track_rec_bytes, rec_off[L] * sizeof(int));
     // levels with resize 2, 4 and 8 (the default pyramid) from one read of each tracking image
     int lv_of[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
     for (int li = 0; li < L; li++)
@@ -524,7 +536,8 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         ISA_CK(cudaMemcpyAsync(c->frame_tab + (size_t)li * c->max_n, fptr.data(), n * sizeof(float*), cudaMemcpyHostToDevice, st));
         ISA_LAUNCH(c, isa_launch_track(c->frame_tab + (size_t)li * c->max_n, lpitch, Wl, Hl, lv.tile_size, lv.max_shift, tcx, tcy,
                                 c->pair_desc + (size_t)li * c->max_pairs, strat.m, grids, gpitch, gstride, p->matching_threshold, nullptr,
-                                nullptr, st));
+                                c->track_rec ? c->track_rec + rec_off[li] : nullptr,
+                                c->track_rec ? c->track_rec + rec_off[li] + (size_t)strat.m * tcx * tcy : nullptr, st));
         ISA_LAUNCH(c, isa_launch_solve(c->row_a, c->row_b, c->row_sign, c->N0, strat.m, strat.n1, grids, gpitch, gstride, c->row_grid, tcx, tcy,
                                 c->x, c->status, st));
         otcx = tcx; otcy = tcy; olevel = lv.resize_level; oT = lv.tile_size;
@@ -1075,6 +1088,15 @@ int isa_debug_buffers(isa_ctx* c, int frame, const void** flow, size_t* flow_pit
     return ISA_OK;
 }
 
+int isa_debug_track_record(isa_ctx* c, int* record, size_t bytes)
+{
+    if (!c) return fail(ISA_EINVAL, "NULL context");
+    if (record && ((uintptr_t)record & 3)) return fail(ISA_EINVAL, "the record must be 4-byte aligned");
+    c->track_rec = record;
+    c->track_rec_bytes = record ? bytes : 0;
+    return ISA_OK;
+}
+
 int isa_debug_shifts(isa_ctx* c, const void** one_to_one, int* tx, int* ty)
 {
     if (!c || c->last_n == 0) return fail(ISA_EINVAL, "no merge has run on this context");
@@ -1205,7 +1227,7 @@ int isa_track_level(const float* const* frames, size_t frame_pitch, int W, int H
     ISA_REQ(grid_pitch >= (size_t)tcx * 8 && grid_stride >= grid_pitch * tcy, "grid pitch/stride too small");
     static_assert(sizeof(isa_track_pair) == sizeof(isa_pair_desc), "pair layout");
     cudaError_t e = isa_launch_track(frames, frame_pitch, W, H, T, Smax, tcx, tcy, (const isa_pair_desc*)pairs, npairs, (float2*)grids, grid_pitch,
-                                     grid_stride, threshold, scores, argmin, S(stream));
+                                     grid_stride, threshold, scores, argmin, nullptr, S(stream));
     if (e == cudaErrorInvalidValue) return fail(ISA_EINVAL, "tile size %d / max shift %d not supported", T, Smax);
     ISA_CK(e);
     return ISA_OK;

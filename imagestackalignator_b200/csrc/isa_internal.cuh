@@ -73,11 +73,12 @@ cudaError_t isa_launch_subsample(const uint16_t* raw, size_t raw_pitch, int W, i
 // track.cu
 cudaError_t isa_launch_track(const float* const* frames, size_t img_pitch, int Wl, int Hl, int T, int S, int tcx, int tcy,
                              const isa_pair_desc* pairs, int npairs, float2* grids, size_t grid_pitch, size_t grid_stride,
-                             float threshold, float* scores, int* argmin, cudaStream_t st);
+                             float threshold, float* scores, int* argmin, int* offsets, cudaStream_t st);
 cudaError_t isa_launch_upsample(const float2* in, size_t in_pitch, size_t in_stride, float2* out, size_t out_pitch,
                                 size_t out_stride, int ngrids, int oldLevel, int newLevel, int ocx, int ocy, int ncx, int ncy,
                                 int oldT, int newT, cudaStream_t st);
 size_t isa_solve_smem(int m, int n1);
+cudaError_t isa_solve_prepare();
 cudaError_t isa_launch_solve(const int* row_a, const int* row_b, const int* row_sign, const double* N0, int m, int n1,
                              float2* grids, size_t grid_pitch, size_t grid_stride, const int* row_grid, int tcx, int tcy,
                              float2* x_out, int* status, cudaStream_t st);

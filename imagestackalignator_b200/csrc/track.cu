@@ -65,7 +65,7 @@ template <int T, int S>
 __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* const* __restrict__ frames, size_t pitch, int Wl, int Hl, int tcx,
                                                                int tcy, const isa_pair_desc* __restrict__ pairs, float2* __restrict__ grids,
                                                                size_t grid_pitch, size_t grid_stride, float threshold, float* __restrict__ scores,
-                                                               int* __restrict__ argmin_out)
+                                                               int* __restrict__ argmin_out, int* __restrict__ offsets_out)
 {
     using L = TrackDims<T, S>;
     constexpr int B = L::B, D = L::D, TP2 = L::TP2, BP = L::BP, HP = L::HP;
@@ -217,6 +217,7 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
             if (mi == 0x7fffffff) mi = -1;
             size_t tix = (size_t)p * tcx * tcy + tile;
             if (argmin_out) argmin_out[tix] = mi;
+            if (offsets_out) { offsets_out[2 * tix] = oxt; offsets_out[2 * tix + 1] = oyt; }
             float cx = 0.f, cy = 0.f;
             if (mi >= 0) {
                 int iy = mi / D, ix = mi - iy * D;
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(TrackDims<T, S>::NT) k_track(const float* cons
 template <int T, int S>
 cudaError_t launch_track_ts(const float* const* frames, size_t pitch, int Wl, int Hl, int tcx, int tcy, const isa_pair_desc* pairs,
                             int npairs, float2* grids, size_t grid_pitch, size_t grid_stride, float thr, float* scores, int* argmin,
-                            cudaStream_t st)
+                            int* offsets, cudaStream_t st)
 {
     using L = TrackDims<T, S>;
     if (L::BYTES > 48 * 1024) {
@@ -269,7 +270,7 @@ cudaError_t launch_track_ts(const float* const* frames, size_t pitch, int Wl, in
         if (e != cudaSuccess) return e;
     }
     dim3 g(npairs, tcx * tcy);
-    k_track<T, S><<<g, L::NT, L::BYTES, st>>>(frames, pitch, Wl, Hl, tcx, tcy, pairs, grids, grid_pitch, grid_stride, thr, scores, argmin);
+    k_track<T, S><<<g, L::NT, L::BYTES, st>>>(frames, pitch, Wl, Hl, tcx, tcy, pairs, grids, grid_pitch, grid_stride, thr, scores, argmin, offsets);
     return cudaGetLastError();
 }
 
@@ -496,11 +497,11 @@ __global__ void k_optimal(const float2* __restrict__ x, int n1, int tcx, int tcy
 }  // namespace
 
 #define ISA_TRACK_CASE(TT, SS) \
-    if (T == TT && S == SS) return launch_track_ts<TT, SS>(frames, img_pitch, Wl, Hl, tcx, tcy, pairs, npairs, grids, grid_pitch, grid_stride, threshold, scores, argmin, st);
+    if (T == TT && S == SS) return launch_track_ts<TT, SS>(frames, img_pitch, Wl, Hl, tcx, tcy, pairs, npairs, grids, grid_pitch, grid_stride, threshold, scores, argmin, offsets, st);
 
 cudaError_t isa_launch_track(const float* const* frames, size_t img_pitch, int Wl, int Hl, int T, int S, int tcx, int tcy,
                              const isa_pair_desc* pairs, int npairs, float2* grids, size_t grid_pitch, size_t grid_stride, float threshold,
-                             float* scores, int* argmin, cudaStream_t st)
+                             float* scores, int* argmin, int* offsets, cudaStream_t st)
 {
     if (npairs <= 0 || tcx <= 0 || tcy <= 0) return cudaSuccess;
     ISA_TRACK_CASE(32, 1) ISA_TRACK_CASE(32, 2) ISA_TRACK_CASE(32, 3) ISA_TRACK_CASE(32, 4)
@@ -522,6 +523,14 @@ cudaError_t isa_launch_upsample(const float2* in, size_t in_pitch, size_t in_str
 }
 
 size_t isa_solve_smem(int m, int n1) { return solve_layout(m, n1).bytes; }
+
+// Loads the solver's device code on the current device (CUDA loads modules
+// lazily, at first use, and loading allocates the module's globals).
+cudaError_t isa_solve_prepare()
+{
+    cudaFuncAttributes a;
+    return cudaFuncGetAttributes(&a, k_solve);
+}
 
 cudaError_t isa_launch_solve(const int* row_a, const int* row_b, const int* row_sign, const double* N0, int m, int n1, float2* grids,
                              size_t grid_pitch, size_t grid_stride, const int* row_grid, int tcx, int tcy, float2* x_out, int* status,

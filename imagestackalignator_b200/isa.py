@@ -69,7 +69,7 @@ class IsaTrackPair(ctypes.Structure):
 EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
-    "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
@@ -307,6 +307,38 @@ class Merger:
         tx, ty = ctypes.c_int(), ctypes.c_int()
         check(lib().isa_debug_shifts(self.ctx, ctypes.byref(p), ctypes.byref(tx), ctypes.byref(ty)))
         return p.value, tx.value, ty.value
+
+    def set_track_record(self, record=None):
+        """Record every level's integer tile shifts and search-block offsets of
+        the following merges into `record` (a cuda int32 tensor; None stops)."""
+        if record is None:
+            check(lib().isa_debug_track_record(self.ctx, None, ctypes.c_size_t(0)))
+        else:
+            check(lib().isa_debug_track_record(self.ctx, vp(record), ctypes.c_size_t(record.numel() * record.element_size())))
+
+    def flows_masks(self, n, width, height, reference=0):
+        """Dense flows (H x W x 2) and eroded masks (H/2 x W/2 x 4) of the last
+        merge, as host float32 arrays keyed by frame (the reference excluded)."""
+        import torch
+        flows, masks = {}, {}
+        for i in range(n):
+            if i == reference:
+                continue
+            d = self.debug(i)
+            flows[i] = device_copy(d["flow"], (height, width, 2), torch.float32).cpu().numpy()
+            masks[i] = device_copy(d["mask"], (height // 2, width // 2, 4), torch.float32).cpu().numpy()
+        return flows, masks
+
+
+def track_record_ints(params: IsaParams, width, height, npairs):
+    """int32 entries of an isa_debug_track_record buffer for one merge."""
+    total = 0
+    for li in range(params.level_count):
+        lv = params.levels[li]
+        tcx = (width // lv.resize_level - 2 * lv.max_shift) // lv.tile_size
+        tcy = (height // lv.resize_level - 2 * lv.max_shift) // lv.tile_size
+        total += 3 * npairs * tcx * tcy
+    return total
 
 
 MAX_LUT = 512

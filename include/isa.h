@@ -211,6 +211,16 @@ ISA_API int isa_debug_buffers(isa_ctx* ctx, int frame, const void** flow, size_t
 /* Tile-alignment intermediates of the last isa_merge_burst: one-to-one shifts
  * of the finest level (tiles x (n-1) float2, device) and its tile counts. */
 ISA_API int isa_debug_shifts(isa_ctx* ctx, const void** one_to_one, int* tiles_x, int* tiles_y);
+/* Records every level's tile search of the following isa_merge_burst calls
+ * into `record` (device, caller-owned, 4-byte aligned; NULL stops recording):
+ * per level, finest first, m x tiles int32 first-minimum indices of the L2
+ * maps (findMinimum, kernel.cu:422-546; -1 when no minimum), then m x tiles
+ * int32 pairs (x, y) of the search block's integer offset (the rounded
+ * pre-shift, PatchTracker.cs:225-253); m = the strategy's pair count in
+ * isa_tracking_pairs order, tiles = tiles_x * tiles_y of the level. A merge
+ * whose record needs more than `bytes` fails with ISA_EINVAL. No counterpart
+ * in the reference: it exposes the integer tile shifts for parity checks. */
+ISA_API int isa_debug_track_record(isa_ctx* ctx, int* record, size_t bytes);
 
 /* ShiftCollection pair bookkeeping (ShiftCollection.cs:100-512), host only:
  * returns the pair count m; pairs (m x 2, optional) = (reference, toTrack)

@@ -292,7 +292,8 @@ static const real FIT_B2[9] = {-0.125, -0.25, -0.125, 0, 0, 0, 0.125, 0.25, 0.12
 
 /* The integer pixel offset of a tile: rotation about the image centre plus
  * the negated base shift, rounded (kernel.cu:203-221, 262-281). */
-static void tile_offset(int tx, int ty, int T, int Wl, int Hl, const real* base, real rot, real addx, real addy, int* ox, int* oy)
+static void tile_offset(int tx, int ty, int T, int Wl, int Hl, const real* base, real rot, real addx, real addy, int* ox, int* oy,
+                        real* unrounded)
 {
     real sf = sin(rot), cf = cos(rot);
     real sx = addx + cf * -base[0] - sf * -base[1];
@@ -302,13 +303,16 @@ static void tile_offset(int tx, int ty, int T, int Wl, int Hl, const real* base,
     sy += sf * pcx + cf * pcy - pcy;
     *ox = (int)round(sx);
     *oy = (int)round(sy);
+    if (unrounded) { unrounded[0] = sx; unrounded[1] = sy; }
 }
 
 /* scores (optional): tiles x (2S+1)^2 L2 maps; argmin (optional): index of
- * the first strict minimum per tile. preShift: tcy x tcx float pairs. */
+ * the first strict minimum per tile; offsets (optional): tiles x 2, the
+ * search block's offset before rounding (PatchTracker.cs:225-253).
+ * preShift: tcy x tcx float pairs. */
 EXPORT void orc_track_pair(const real* imgTrack, const real* imgRef, int Wl, int Hl, int T, int S, int tcx, int tcy,
                            real* preShift, const real* baseRef, real rotRef, const real* baseTrk, real rotTrk,
-                           real threshold, real* scores, int* argmin)
+                           real threshold, real* scores, int* argmin, real* offsets)
 {
     int B = T + 2 * S, D = 2 * S + 1;
     real* tpl = (real*)malloc((size_t)T * T * sizeof(real));
@@ -318,14 +322,14 @@ EXPORT void orc_track_pair(const real* imgTrack, const real* imgRef, int Wl, int
         for (int tx = 0; tx < tcx; tx++) {
             int t = ty * tcx + tx;
             int ox, oy;
-            tile_offset(tx, ty, T, Wl, Hl, baseRef, rotRef, 0, 0, &ox, &oy);
+            tile_offset(tx, ty, T, Wl, Hl, baseRef, rotRef, 0, 0, &ox, &oy, NULL);
             for (int y = 0; y < T; y++)
                 for (int x = 0; x < T; x++) {
                     int ix = clampi(tx * T + S + x + ox, 0, Wl - 1), iy = clampi(ty * T + S + y + oy, 0, Hl - 1);
                     tpl[y * T + x] = imgRef[(size_t)iy * Wl + ix];
                 }
             real* ps = preShift + (size_t)t * 2;
-            tile_offset(tx, ty, T, Wl, Hl, baseTrk, rotTrk, ps[0], ps[1], &ox, &oy);
+            tile_offset(tx, ty, T, Wl, Hl, baseTrk, rotTrk, ps[0], ps[1], &ox, &oy, offsets ? offsets + (size_t)t * 2 : NULL);
             for (int y = 0; y < B; y++)
                 for (int x = 0; x < B; x++) {
                     int ix = clampi(tx * T + x + ox, 0, Wl - 1), iy = clampi(ty * T + y + oy, 0, Hl - 1);

@@ -99,17 +99,25 @@ class StageLib:
         self.kf("fourier_filter_mask")(W, H, R(lp), R(hp), R(lps), R(hps), clear_axis, _p(m))
         return m
 
-    def track_pair(self, img_trk, img_ref, T, S, tcx, tcy, pre, base_ref, rot_ref, base_trk, rot_trk, thr, want_scores=False):
+    def track_pair(self, img_trk, img_ref, T, S, tcx, tcy, pre, base_ref, rot_ref, base_trk, rot_trk, thr, want_scores=False,
+                   want_offsets=False):
+        """Returns (pre + shift, L2 maps or None), plus the unrounded search
+        block offsets (tiles x 2) when want_offsets (restatement only)."""
         Hl, Wl = img_trk.shape
         pre = self.arr(pre).copy()
         D = 2 * S + 1
         scores = np.empty((tcy * tcx, D * D), self.dtype) if want_scores else None
+        offs = np.empty((tcy * tcx, 2), self.dtype) if want_offsets else None
         R = self.R
         args = [_p(self.arr(img_trk)), _p(self.arr(img_ref)), Wl, Hl, T, S, tcx, tcy, _p(pre), _p(self.vec(base_ref)), R(rot_ref),
                 _p(self.vec(base_trk)), R(rot_trk), R(thr), _p(scores)]
         if self.pfx == "orc_":
-            args.append(None)
+            args += [None, _p(offs)]
+        elif want_offsets:
+            raise ValueError("offsets come from the restatement only")
         self.kf("track_pair")(*args)
+        if want_offsets:
+            return pre, scores, offs
         return pre, scores
 
     def upsample_shifts(self, grid, old_level, new_level, ncx, ncy, old_t, new_t):
@@ -368,14 +376,18 @@ def track_patches(lib: StageLib, bw_track, pre: PreAlignment, p: P.MergeParams, 
             imgs = bw_track
         for (r, t) in pairs:
             k = idx[r, t]
-            g, sc = lib.track_pair(imgs[t], imgs[r], T, S, tcx, tcy, grids[k, :tcy, :tcx],
-                                   pre.shift(pre.reference, r) / np.float32(lvl.resize_level), pre.rotation(pre.reference, r),
-                                   pre.shift(pre.reference, t) / np.float32(lvl.resize_level), pre.rotation(pre.reference, t),
-                                   p.f32("matching_threshold"), want_scores=keep is not None)
+            want_offs = keep is not None and lib.pfx == "orc_"
+            res = lib.track_pair(imgs[t], imgs[r], T, S, tcx, tcy, grids[k, :tcy, :tcx],
+                                 pre.shift(pre.reference, r) / np.float32(lvl.resize_level), pre.rotation(pre.reference, r),
+                                 pre.shift(pre.reference, t) / np.float32(lvl.resize_level), pre.rotation(pre.reference, t),
+                                 p.f32("matching_threshold"), want_scores=keep is not None, want_offsets=want_offs)
+            g, sc = res[0], res[1]
             grids[k, :tcy, :tcx] = g
             if keep is not None:
                 keep.setdefault("scores", {})[(li, r, t)] = sc
                 keep.setdefault("measured", {})[(li, r, t)] = g.copy()
+                if want_offs:
+                    keep.setdefault("offsets", {})[(li, r, t)] = res[2]
         # MinimizeCUBLAS (ShiftCollection.cs:738-822)
         meas = np.stack([grids[idx[r, t], :tcy, :tcx].reshape(-1, 2) for (r, t) in
                          sorted(pairs, key=lambda rt: idx[rt[0], rt[1]])], axis=1)
