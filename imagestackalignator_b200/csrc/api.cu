@@ -184,6 +184,8 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 }  // namespace
 
+int isa_static_solve_setup();
+
 // ---------------------------------------------------------------------------
 struct isa_ctx {
     int max_w = 0, max_h = 0, max_n = 0;
@@ -207,10 +209,8 @@ struct isa_ctx {
     float *half_ref = nullptr, *half_mov = nullptr;
     float4 *ref_mr = nullptr, *ref_sr = nullptr, *mov_box = nullptr;  // robustness statistics (half resolution)
     float4* masks = nullptr;
-    // adjoint scratch (allocated by the first isa_merge_backward)
-    void* adj = nullptr;
-    float* adj_gkp = nullptr;
-    float4 *adj_gmask = nullptr, *adj_m = nullptr, *adj_aux = nullptr, *adj_gm = nullptr;
+    // adjoint sums (loss and the eight parameter gradients); the adjoint's image-sized scratch reuses buffers
+    // that the forward no longer needs (see isa_merge_backward)
     double* adj_acc = nullptr;
     float *st3 = nullptr, *kparam = nullptr;
     float *acc = nullptr, *wsum = nullptr, *out_stage = nullptr;
@@ -855,6 +855,7 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     add((void**)&c->wsum, (size_t)c->max_wo * c->max_ho * 12);
     add((void**)&c->out_stage, (size_t)c->max_wo * c->max_ho * 12);
     add((void**)&c->frame_in, (size_t)max_n * sizeof(isa_frame_in));
+    add((void**)&c->adj_acc, 16 * sizeof(double));
     size_t total = 0;
     for (auto& e : plan) total += e.second;
     if (cudaMalloc(&c->arena, total) != cudaSuccess) {
@@ -876,6 +877,9 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     if (!ok) { isa_ctx_destroy(c); return fail(ISA_ECUDA, "stream/event creation failed"); }
     int r = ensure_plans(c, max_w, max_h);
     if (r != ISA_OK) { isa_ctx_destroy(c); return r; }
+    // the static solve's set-up on this device (loads the solver's device code), so that it allocates nothing later
+    r = isa_static_solve_setup();
+    if (r != ISA_OK) { isa_ctx_destroy(c); return r; }
     *out = c;
     return ISA_OK;
 }
@@ -896,7 +900,6 @@ int isa_ctx_destroy(isa_ctx* c)
     if (c->ev_copied) cudaEventDestroy(c->ev_copied);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->arena) cudaFree(c->arena);
-    if (c->adj) cudaFree(c->adj);
     delete c;
     return ISA_OK;
 }
@@ -938,26 +941,21 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
     cudaStream_t st = S(stream);
     // forward (keeps flows, masks, kernel parameters, structure tensor, sums and the frame table)
     ISA_TRY(run_merge(c, raw, raw_pitch, frame_stride, n, info, pre, out, out_pitch, st));
-    const size_t fsz = (size_t)W * H, mw = (size_t)c->max_w, mh = (size_t)c->max_h;
+    const size_t fsz = (size_t)W * H;
     const int Wh = W / 2, Hh = H / 2;
     const size_t hsz = (size_t)Wh * Hh, hp4 = (size_t)Wh * 16, hp3 = (size_t)Wh * 12, fp = (size_t)W * sizeof(float2), p3 = (size_t)W * 12,
                  p4 = (size_t)W * 16, op = (size_t)g.Wo * 12;
-    if (!c->adj) {
-        const size_t hmax = (mw / 2) * (mh / 2);
-        const size_t b_gkp = mw * mh * 12, b_gmask = hmax * 16 * c->max_n, b_h = hmax * 16;
-        const size_t total = b_gkp + b_gmask + 3 * b_h + 16 * sizeof(double) + 4 * 256;
-        if (cudaMalloc(&c->adj, total) != cudaSuccess) { c->adj = nullptr; return fail(ISA_ENOMEM, "adjoint scratch of %.2f GB", total / 1e9); }
-        char* q = (char*)c->adj;
-        auto take = [&](size_t bytes) { char* r = q; q += (bytes + 255) / 256 * 256; return r; };
-        c->adj_gkp = (float*)take(b_gkp);
-        c->adj_gmask = (float4*)take(b_gmask);
-        c->adj_m = (float4*)take(b_h);
-        c->adj_aux = (float4*)take(b_h);
-        c->adj_gm = (float4*)take(b_h);
-        c->adj_acc = (double*)take(16 * sizeof(double));
-    }
-    ISA_CK(cudaMemsetAsync(c->adj_gkp, 0, fsz * 12, st));
-    ISA_CK(cudaMemsetAsync(c->adj_gmask, 0, hsz * 16 * n, st));
+    // scratch of the adjoint in buffers the forward has finished with: the FFT / Gauss scratch (fsz x 12 B) takes the
+    // kernel-parameter gradients, the tracking images (n x fsz x 4 B) the mask-certainty gradients of every frame, the
+    // LK ping-pong flow (fsz x 8 B) the recomputed mask and its auxiliaries, the accumulation images the routed
+    // gradient; none of them is read again before the next merge
+    float* adj_gkp = c->tmp;
+    float4* adj_gmask = (float4*)c->bw_track;
+    float4* adj_m = (float4*)c->flow_tmp;
+    float4* adj_aux = (float4*)((char*)c->flow_tmp + hsz * 16);
+    float4* adj_gm = (float4*)c->bw_acc;
+    ISA_CK(cudaMemsetAsync(adj_gkp, 0, fsz * 12, st));
+    ISA_CK(cudaMemsetAsync(adj_gmask, 0, hsz * 16 * n, st));
     ISA_CK(cudaMemsetAsync(c->adj_acc, 0, 16 * sizeof(double), st));
     float black[3], white[3], scale[3], divisor[3];
     color_consts(info, black, white, scale, divisor);
@@ -965,9 +963,9 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
     const int ref = pre ? pre->reference : 0;
     // output -> kernel parameters and mask certainties (all frames at once)
     ISA_LAUNCH(c, isa_launch_accumulate_bwd(g, cfa, c->frame_in, n, raw_pitch, fp, hp4, c->kparam, p4, white, black, out, out_pitch, c->wsum, op, target,
-                                            target_pitch, weight, weight_pitch, c->adj_gkp, c->adj_gmask, hsz, c->adj_acc + 8, st));
+                                            target_pitch, weight, weight_pitch, adj_gkp, adj_gmask, hsz, c->adj_acc + 8, st));
     // kernel parameters -> kDetail, kDenoise, Dth, Dtr, kStretch, kShrink
-    ISA_LAUNCH(c, isa_launch_kparam_bwd(c->st3, p3, W, H, c->adj_gkp, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
+    ISA_LAUNCH(c, isa_launch_kparam_bwd(c->st3, p3, W, H, adj_gkp, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
                                         c->adj_acc, st));
     // mask certainties -> erosion -> robustness s, t (per frame, recomputing the un-eroded mask)
     float maxv = 0.f;
@@ -980,10 +978,10 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
         ISA_LAUNCH(c, isa_launch_subsample(fr, raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
         ISA_LAUNCH(c, isa_launch_box3(c->half_mov, hp3, Wh, Hh, c->mov_box, hp4, st));
         ISA_LAUNCH(c, isa_launch_mask_store(c->ref_mr, c->ref_sr, c->mov_box, hp4, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha,
-                                            info->noise_beta, p->threshold_m, p->robust_s, p->robust_t, c->adj_m, c->adj_aux, st));
-        ISA_CK(cudaMemsetAsync(c->adj_gm, 0, hsz * 16, st));
-        ISA_LAUNCH(c, isa_launch_erode_route(c->adj_m, c->adj_gmask + (size_t)f * hsz, hp4, Wh, Hh, p->erode_size, c->adj_gm, st));
-        ISA_LAUNCH(c, isa_launch_mask_param_bwd(c->adj_m, c->adj_aux, c->adj_gm, hp4, Wh, Hh, p->robust_t, c->adj_acc + 6, st));
+                                            info->noise_beta, p->threshold_m, p->robust_s, p->robust_t, adj_m, adj_aux, st));
+        ISA_CK(cudaMemsetAsync(adj_gm, 0, hsz * 16, st));
+        ISA_LAUNCH(c, isa_launch_erode_route(adj_m, adj_gmask + (size_t)f * hsz, hp4, Wh, Hh, p->erode_size, adj_gm, st));
+        ISA_LAUNCH(c, isa_launch_mask_param_bwd(adj_m, adj_aux, adj_gm, hp4, Wh, Hh, p->robust_t, c->adj_acc + 6, st));
         f++;
     }
     double h[9];
@@ -1430,11 +1428,44 @@ struct StaticSolveTables {
 
 static __device__ __align__(256) unsigned char g_solve_scratch[sizeof(StaticSolveTables)];
 
-// Device address of g_solve_scratch per device. In host code the symbol is
-// only a handle, so the address is asked for once per device (with that
-// device current) and cached.
+// Device address of g_solve_scratch. In host code the symbol is only a
+// handle, so the address is asked for (with the device current) once per
+// device and CUDA context, and kept with the context's unique id: after a
+// cudaDeviceReset the device code is loaded again in a new context and the
+// array may move, so a new id triggers a new look-up. The same set-up loads
+// the solver's device code, so that a later call loads nothing.
+typedef int (*CtxGetCurrentFn)(void**);                     // CUresult cuCtxGetCurrent(CUcontext*)
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);      // CUresult cuCtxGetId(CUcontext, unsigned long long*)
+
+struct StaticScratchSlot {
+    unsigned long long ctx_id = 0;
+    StaticSolveTables* addr = nullptr;
+};
 std::mutex g_scratch_lock;
-StaticSolveTables* g_scratch_addr[64] = {};
+StaticScratchSlot g_scratch_slot[64];
+
+// The current context's unique id (cuCtxGetId through the runtime's driver
+// entry points, so the library needs no link to the driver library); 0 when
+// no context is current yet.
+int current_ctx_id(unsigned long long* id)
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        void *f1 = nullptr, *f2 = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) != cudaSuccess || !f1 ||
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) != cudaSuccess || !f2)
+            return fail(ISA_ECUDA, "the driver does not provide cuCtxGetCurrent / cuCtxGetId");
+        get_current = (CtxGetCurrentFn)f1;
+        get_id = (CtxGetIdFn)f2;
+    }
+    void* ctx = nullptr;
+    *id = 0;
+    if (get_current(&ctx) != 0) return fail(ISA_ECUDA, "cuCtxGetCurrent failed");
+    if (ctx && get_id(ctx, id) != 0) return fail(ISA_ECUDA, "cuCtxGetId failed");
+    return ISA_OK;
+}
 
 int static_tables(StaticSolveTables** out)
 {
@@ -1442,17 +1473,31 @@ int static_tables(StaticSolveTables** out)
     ISA_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(ISA_EINVAL, "device ordinal %d out of range", dev);
     std::lock_guard<std::mutex> lock(g_scratch_lock);
-    if (!g_scratch_addr[dev]) {
+    unsigned long long id = 0;
+    ISA_TRY(current_ctx_id(&id));
+    StaticScratchSlot& slot = g_scratch_slot[dev];
+    if (!slot.addr || id == 0 || id != slot.ctx_id) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_solve_scratch);  // loads this file's device code on the device
         if (e != cudaSuccess) return fail(ISA_ECUDA, "cudaGetSymbolAddress(g_solve_scratch): %s", cudaGetErrorString(e));
-        g_scratch_addr[dev] = (StaticSolveTables*)p;
+        e = isa_solve_prepare();
+        if (e != cudaSuccess) return fail(ISA_ECUDA, "loading the solver: %s", cudaGetErrorString(e));
+        ISA_TRY(current_ctx_id(&id));
+        slot.addr = (StaticSolveTables*)p;
+        slot.ctx_id = id;
     }
-    *out = g_scratch_addr[dev];
+    *out = slot.addr;
     return ISA_OK;
 }
 
 }  // namespace
+
+// The static solve's set-up on the current device, also run by isa_ctx_create.
+int isa_static_solve_setup()
+{
+    StaticSolveTables* t = nullptr;
+    return static_tables(&t);
+}
 
 extern "C" int isa_solve_shifts_static(int n, int ref, int strategy, int block, void* grids, size_t grid_pitch, size_t grid_stride, int tcx,
                                        int tcy, void* x, int* status, void* stream)
@@ -2727,6 +2772,7 @@ int isa_dng_decode_finish(const uint8_t* file_host, const uint8_t* file_dev, siz
     g_dng_path = -1;
     ISA_REQ(file_host && file_dev && scratch && out, "NULL argument");
     ISA_TRY(isa_dng_check(L, width, height));
+    ISA_REQ(out_pitch >= (size_t)width * 2 && out_pitch % 2 == 0, "bad output pitch");
     cudaStream_t st = S(stream);
     DngPlan plan;
     if (L->compression == 7) ISA_TRY(dng_plan(file_host, file_size, L, width, height, plan));

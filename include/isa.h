@@ -179,8 +179,10 @@ ISA_API int isa_merge_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch,
  * round(s * flow) and round(flow / 2) and the mask's flow term M only
  * switches the gain at a threshold -- so none is returned. Covers the
  * merge_scale and super-resolution modes (normalisation threshold 0) with
- * fused_accumulate; the first call allocates the adjoint scratch in the
- * context. */
+ * fused_accumulate. Allocates nothing: the adjoint's scratch is context
+ * memory the forward has finished with, so afterwards the tracking and
+ * accumulation images of isa_debug_buffers hold adjoint scratch, not the
+ * forward's images. */
 ISA_API int isa_merge_backward(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
                                const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch,
                                float* out, size_t out_pitch, double* loss, double* grad, void* stream);
@@ -301,11 +303,16 @@ ISA_API int isa_solve_shifts(isa_ctx* ctx, int n, int reference, int strategy, i
  * an allocation can cause). No counterpart in the reference: it replaces
  * isa_solve_shifts' context scratch by a library-owned static device array
  * that every GPU loading the library keeps until exit. Limits: at most 2048
- * frame pairs and 65 frames (ISA_EINVAL beyond). Allocates nothing; the
- * first call on a device looks up the array's address, so make it before any
- * stream capture. All calls share the array: calls that overlap on the GPU
- * (different streams, or several host threads) race and must be serialised
- * by the caller. Inputs and outputs as isa_solve_shifts. */
+ * frame pairs and 65 frames (ISA_EINVAL beyond). Allocates nothing once set
+ * up on a device. The set-up happens in the first call on each device (and
+ * CUDA context), or in isa_ctx_create on that device: it loads the library's
+ * device code there -- CUDA loads it lazily, and loading allocates the
+ * code's globals, this array among them, and can synchronise the device --
+ * and looks up the array's address. So make one call per device at
+ * initialisation, before any stream capture. All calls share the array:
+ * calls that overlap on the GPU (different streams, or several host
+ * threads) race and must be serialised by the caller. Inputs and outputs as
+ * isa_solve_shifts. */
 ISA_API int isa_solve_shifts_static(int n, int reference, int strategy, int block_size, void* grids, size_t grid_pitch, size_t grid_stride,
                                     int tiles_x, int tiles_y, void* one_to_one, int* status, void* stream);
 /* getOptimalShiftsKernel (ShiftMinimizerKernels.cs): shift of frame

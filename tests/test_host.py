@@ -128,6 +128,14 @@ def test_dng_decode_halves_and_file_handles_check_their_arguments():
                   None) == isa.ISA_EINVAL
         assert fn(fake, fake, ctypes.c_size_t(16), ctypes.byref(L), 8, 8, fake, ctypes.c_size_t(1 << 20), fake, ctypes.c_size_t(16),
                   None) == isa.ISA_EINVAL   # n = 0: a bad layout
+    # a valid uncompressed layout with an output pitch below one row: refused by both halves before any CUDA call
+    offs, cnts = (ctypes.c_uint32 * 1)(0), (ctypes.c_uint32 * 1)(128)
+    good = isa.IsaDngLayout(tiled=0, rows_per_strip=8, n=1, offsets=ctypes.cast(offs, ctypes.c_void_p),
+                            byte_counts=ctypes.cast(cnts, ctypes.c_void_p), compression=1, bit_depth=16)
+    for fn in (lib.isa_dng_decode_begin, lib.isa_dng_decode_finish):
+        assert fn(fake, fake, ctypes.c_size_t(128), ctypes.byref(good), 8, 8, fake, ctypes.c_size_t(1 << 20), fake, ctypes.c_size_t(15),
+                  None) == isa.ISA_EINVAL
+        assert b"output pitch" in lib.isa_last_error()
     roll = ctypes.c_float()
     assert lib.isa_dng_roll_angle(None, ctypes.byref(roll)) == isa.ISA_EINVAL
     assert lib.isa_dng_file_info(None, None, None, None, None, None) == isa.ISA_EINVAL

@@ -60,6 +60,27 @@ def test_static_solve_matches_context_solve(cuda, order):
     merger.close()
 
 
+def test_static_solve_allocates_nothing_after_set_up(cuda):
+    """After the set-up call on the device, a call leaves the device's free
+    memory unchanged (every buffer of the call is made beforehand)."""
+    import torch
+    lib = isa.lib()
+    rng = np.random.default_rng(5)
+    n, ref, strategy, block, tcx, tcy = 12, 0, P.FULL, 5, 31, 23
+    g = _case(rng, n, ref, strategy, block, tcx, tcy)
+    grids = torch.from_numpy(g).cuda()
+    x = torch.zeros((tcx * tcy, n - 1, 2), dtype=torch.float32, device="cuda")
+    st = torch.zeros(tcx * tcy, dtype=torch.int32, device="cuda")
+    args = [n, ref, strategy, block, isa.vp(grids), ctypes.c_size_t(tcx * 8), ctypes.c_size_t(tcx * tcy * 8), tcx, tcy, isa.vp(x), isa.vp(st),
+            None]
+    isa.check(lib.isa_solve_shifts_static(*args))  # set-up on this device
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    isa.check(lib.isa_solve_shifts_static(*args))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_static_solve_rejects_sizes_beyond_its_limit(cuda):
     import torch
     lib = isa.lib()
@@ -69,3 +90,7 @@ def test_static_solve_rejects_sizes_beyond_its_limit(cuda):
     rc = lib.isa_solve_shifts_static(70, 0, P.FULL, 5, isa.vp(grids), ctypes.c_size_t(8), ctypes.c_size_t(8), 1, 1, isa.vp(x), isa.vp(st), None)
     assert rc == isa.ISA_EINVAL
     assert b"static limit" in lib.isa_last_error()
+    # 65 frames are within the frame limit, but Full tracking makes 2080 pairs (> 2048)
+    rc = lib.isa_solve_shifts_static(65, 0, P.FULL, 5, isa.vp(grids), ctypes.c_size_t(8), ctypes.c_size_t(8), 1, 1, isa.vp(x), isa.vp(st), None)
+    assert rc == isa.ISA_EINVAL
+    assert b"frame pairs exceed the static limit" in lib.isa_last_error()
