@@ -330,6 +330,13 @@ class Merger:
         return flows, masks
 
 
+    def weight_sums(self, width, height):
+        """Per-channel weight sums of the last merge's accumulation (Ho x Wo x 3, host float32)."""
+        import torch
+        Wo, Ho = self.output_size(width, height)
+        return device_copy(self.debug(0)["wsum"], (Ho, Wo, 3), torch.float32).cpu().numpy()
+
+
 def track_record_ints(params: IsaParams, width, height, npairs):
     """int32 entries of an isa_debug_track_record buffer for one merge."""
     total = 0

@@ -88,10 +88,13 @@ def _out_coords(Wo, Ho, s, origin):
 
 
 def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry, erode_size, wsum_orc=None, ref=0,
-                 max_excluded=0.02, bar=IMAGE_BAR, maps=None):
+                 max_excluded=0.02, bar=IMAGE_BAR, maps=None, wsum_gpu=None):
     """got / want: Ho x Wo x 3 merged images (GPU, FP64 oracle). flows_*: dict
     frame -> H x W x 2; masks_*: dict frame -> H/2 x W/2 x 4 (eroded).
     geometry: (Wo, Ho, s, origin, crop, thr) as oracle/pipeline.out_geometry.
+    wsum_gpu / wsum_orc: Ho x Wo x 3 weight sums; ApplyWeighting's decision
+    w < thr is compared between them (with only wsum_orc, oracle sums within
+    a relative 1e-4 of thr count as undecided).
     Returns a dict of counts; raises AssertionError when the bar fails.
     maps (a dict, optional) receives the per-pixel |difference| and the
     excluded-pixel masks before the bar is checked."""
@@ -148,7 +151,11 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
                 excl_mask |= mdiff[np.clip(cy, 0, Hh - 1), np.clip(cx, 0, Wh - 1)]
     excl_w = np.zeros((Ho, Wo), bool)
     if thr > 0 and wsum_orc is not None:
-        excl_w = (np.abs(np.asarray(wsum_orc, np.float64) - thr) < 1e-5 * max(thr, 1.0)).any(axis=2)
+        wo = np.asarray(wsum_orc, np.float64)
+        if wsum_gpu is not None:
+            excl_w = ((np.asarray(wsum_gpu, np.float64) < thr) != (wo < thr)).any(axis=2)
+        else:
+            excl_w = (np.abs(wo - thr) < 1e-4 * max(thr, 1.0)).any(axis=2)
     excl = excl_shift | excl_mask | excl_w
     diff = np.abs(got - want).max(axis=2)
     keep = ~excl

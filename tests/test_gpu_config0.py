@@ -69,7 +69,7 @@ def test_config0_matches_oracle(cuda, case):
     # merged image over decision-matched pixels
     geom = PL.out_geometry(W, H, p)
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
-                             max_excluded=0.01)
+                             wsum_gpu=m.weight_sums(W, H), max_excluded=0.01)
     print("merged image:", st)
     m.set_track_record(None)
     m.close()

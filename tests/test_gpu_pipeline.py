@@ -47,7 +47,7 @@ def image_parity(m, burst, p, got, want, keep, reference=0):
     flows, masks = m.flows_masks(burst.n, burst.width, burst.height, reference=reference)
     geom = PL.out_geometry(burst.width, burst.height, p)
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
-                             ref=reference)
+                             wsum_gpu=m.weight_sums(burst.width, burst.height), ref=reference)
     print(st)
     return st
 

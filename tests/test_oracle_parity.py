@@ -98,3 +98,21 @@ def test_track_parity_on_the_oracles_own_record(merged):
     bad[j] = (bad[j] + 1) % sc.shape[1]
     with pytest.raises(AssertionError, match="integer shift"):
         parity.track_parity(bad, keep, pairs, p.levels, b.width, b.height)
+
+
+def test_weight_threshold_decision_is_identified(merged):
+    """ApplyWeighting's w < 1 (plain merge): a channel whose weight sum lies on
+    the other side of the threshold on the GPU is excluded, wherever it is."""
+    b, p, keep, res = merged
+    flows, masks, geom = _args(b, p, keep)
+    wg = res.wsum.copy()
+    y, x = 50, 90
+    wg[y, x, 1] = 0.99999 if res.wsum[y, x, 1] >= 1 else 1.00001
+    got = res.image.copy()
+    got[y, x, 1] += 1e-3
+    st = parity.merge_parity(got, res.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=res.wsum,
+                             wsum_gpu=wg)
+    assert st["excluded_weight"] == 1 and st["max_abs_matched"] == 0.0
+    got[y + 1, x, 1] += 1e-3
+    with pytest.raises(AssertionError, match="decision-matched"):
+        parity.merge_parity(got, res.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=res.wsum, wsum_gpu=wg)
