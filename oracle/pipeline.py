@@ -494,6 +494,35 @@ def merge_burst(burst, p: P.MergeParams = None, kind="oracle64", pre: Optional[P
     return MergeResult(image=image, acc=acc, wsum=wsum)
 
 
+def merge_tail(burst, p: P.MergeParams, flows, masks, kparam, lib: StageLib, reference=0):
+    """The accumulation and ApplyWeighting of a burst (PrepareAccumulation
+    :1894-1902, Accumulate :1978-1986, ApplyWeighting :1994-2002) on given
+    per-frame flows and eroded masks (dicts frame -> array, the reference
+    frame excluded) and kernel parameters, in the restatement's precision.
+    The parity checker feeds it the GPU's flows and masks to separate the
+    accumulation's own arithmetic from upstream FP32 differences."""
+    n, H, W = burst.raw.shape
+    white = np.asarray(burst.white, np.float64)
+    black = np.asarray(burst.black, np.float64)
+    Wo, Ho, s, origin, crop, thr = out_geometry(W, H, p)
+    acc = np.zeros((Ho, Wo, 3), lib.dtype)
+    wsum = np.zeros((Ho, Wo, 3), lib.dtype)
+    kparam = lib.arr(kparam)
+    lib.accumulate(burst.raw[reference], burst.cfa, acc, wsum, np.ones((H // 2, W // 2, 4), lib.dtype), kparam,
+                   np.zeros((H, W, 2), lib.dtype), white, black, s, origin, crop)
+    for i in range(n):
+        if i == reference:
+            continue
+        lib.accumulate(burst.raw[i], burst.cfa, acc, wsum, lib.arr(masks[i]), kparam, lib.arr(flows[i]), white, black, s, origin, crop)
+    if thr > 0:
+        cw = np.asarray(burst.camera_white, np.float64)
+        dec = lib.debayer_full(burst.raw[reference], burst.cfa, black, (1.0 / cw).astype(np.float32),
+                               (white.astype(np.float32) / cw.astype(np.float32)))
+    else:
+        dec = np.zeros((Ho, Wo, 3), lib.dtype)
+    return MergeResult(image=lib.apply_weighting(dec, acc, wsum, thr), acc=acc, wsum=wsum)
+
+
 def accumulate_canvas_ref(lib, raw, cfa, acc, wsum, mask, kp4, flow, white, black, s):
     """Full-frame 2x merge with the reference's central-crop kernel
     (accumulateImagesSuperRes, DeBayerKernels.cu:379-468): the frame is

@@ -11,7 +11,11 @@ one in a nearly rank-one window next to the 2-px black demosaic border, can
 decide the other way and change the pixel by up to the local contrast.
 oracle/parity.py identifies those pixels from both sides' flows, masks and
 weight sums, requires every differing mask value to be explained by a
-differing rounding decision, and bounds their count."""
+differing rounding decision, and bounds their count. The oracle's
+accumulation fed the GPU's own flows and masks must match the GPU to 1e-4
+on every pixel; where only it matches (a channel normalised by a tiny
+certainty-weighted sum amplifies 1e-8-level mask differences, at scales
+other than 1 and 2), the pixel is counted as carried in from upstream."""
 import ctypes
 
 import numpy as np
@@ -46,8 +50,9 @@ def image_parity(m, burst, p, got, want, keep, reference=0):
     """max |GPU - FP64| <= 1e-4 over the decision-matched pixels (oracle/parity.py)."""
     flows, masks = m.flows_masks(burst.n, burst.width, burst.height, reference=reference)
     geom = PL.out_geometry(burst.width, burst.height, p)
+    sub = PL.merge_tail(burst, p, flows, masks, keep["kparam"], PL.StageLib("oracle64"), reference=reference)
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
-                             wsum_gpu=m.weight_sums(burst.width, burst.height), ref=reference)
+                             wsum_gpu=m.weight_sums(burst.width, burst.height), want_sub=sub.image, ref=reference)
     print(st)
     return st
 

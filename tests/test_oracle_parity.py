@@ -116,3 +116,31 @@ def test_weight_threshold_decision_is_identified(merged):
     got[y + 1, x, 1] += 1e-3
     with pytest.raises(AssertionError, match="decision-matched"):
         parity.merge_parity(got, res.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=res.wsum, wsum_gpu=wg)
+
+
+
+def test_substituted_tail_explains_upstream_differences(merged, oracle):
+    """A pixel off by more than the bar is counted as carried in from upstream
+    when the oracle's accumulation fed the same flows and masks reproduces
+    it; an error of the accumulation itself still fails."""
+    b, p, keep, res = merged
+    flows, masks, geom = _args(b, p, keep)
+    masks[1][20, 30, 2] = max(masks[1][20, 30, 2] - 5e-6, 0.0)  # within the mask tolerance
+    sub = PL.merge_tail(b, p, flows, masks, keep["kparam"], oracle)
+    got = sub.image.copy()
+    y, x = 41, 61
+    got[y, x] = res.image[y, x] + 3e-4          # upstream: the substituted oracle moves with it
+    sub.image[y, x] = got[y, x]
+    st = parity.merge_parity(got, res.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=res.wsum,
+                             want_sub=sub.image)
+    assert st["excluded_conditioned"] >= 1 and st["tail_max_abs"] <= parity.IMAGE_BAR
+    got[y + 2, x] += 3e-4                        # not reproduced by the substituted oracle: the accumulation's own error
+    with pytest.raises(AssertionError, match="own flows and masks"):
+        parity.merge_parity(got, res.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=res.wsum,
+                            want_sub=sub.image)
+
+
+def test_merge_tail_reproduces_the_oracle(merged, oracle):
+    b, p, keep, res = merged
+    sub = PL.merge_tail(b, p, keep["flow"], keep["mask"], keep["kparam"], oracle)
+    np.testing.assert_array_equal(sub.image, res.image)
