@@ -91,7 +91,7 @@ def _out_coords(Wo, Ho, s, origin):
 
 
 def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry, erode_size, wsum_orc=None, ref=0,
-                 max_excluded=0.02, bar=IMAGE_BAR, maps=None, wsum_gpu=None, want_sub=None):
+                 max_excluded=0.02, bar=IMAGE_BAR, maps=None, wsum_gpu=None, want_sub=None, wsum_sub=None):
     """got / want: Ho x Wo x 3 merged images (GPU, FP64 oracle). flows_*: dict
     frame -> H x W x 2; masks_*: dict frame -> H/2 x W/2 x 4 (eroded).
     geometry: (Wo, Ho, s, origin, crop, thr) as oracle/pipeline.out_geometry.
@@ -102,7 +102,8 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
     GPU's flows and masks; it must match the GPU to the bar on every pixel
     whose shift the GPU's FP32 interpolation cannot round either way, and a
     pixel where it matches while the pure oracle does not is counted as
-    carried in from upstream FP32 inputs instead of failing.
+    carried in from upstream FP32 inputs instead of failing. wsum_sub: its
+    weight sums, for its own ApplyWeighting decision.
     Returns a dict of counts; raises AssertionError when the bar fails.
     maps (a dict, optional) receives the per-pixel |difference| and the
     excluded-pixel masks before the bar is checked."""
@@ -175,7 +176,9 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
         excl_cond = ~excl & (diff > bar) & (dsub <= bar)
         # the accumulation itself: same flows and masks -> the bar on every pixel but the GPU's own near-half
         # interpolated shifts (s != 1) and a flipped ApplyWeighting threshold
-        tail_skip = excl_w.copy() if wsum_gpu is not None else np.zeros((Ho, Wo), bool)
+        tail_skip = np.zeros((Ho, Wo), bool)
+        if thr > 0 and wsum_gpu is not None and wsum_sub is not None:
+            tail_skip = ((np.asarray(wsum_gpu, np.float64) < thr) != (np.asarray(wsum_sub, np.float64) < thr)).any(axis=2)
         if not exact_s:
             for i in sorted(flows_gpu):
                 if i != ref:

@@ -70,7 +70,7 @@ def test_config0_matches_oracle(cuda, case):
     geom = PL.out_geometry(W, H, p)
     sub = PL.merge_tail(burst, p, flows, masks, keep["kparam"], PL.StageLib("oracle64"))
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
-                             wsum_gpu=m.weight_sums(W, H), want_sub=sub.image, max_excluded=0.01)
+                             wsum_gpu=m.weight_sums(W, H), want_sub=sub.image, wsum_sub=sub.wsum, max_excluded=0.01)
     print("merged image:", st)
     m.set_track_record(None)
     m.close()

@@ -52,7 +52,7 @@ def image_parity(m, burst, p, got, want, keep, reference=0):
     geom = PL.out_geometry(burst.width, burst.height, p)
     sub = PL.merge_tail(burst, p, flows, masks, keep["kparam"], PL.StageLib("oracle64"), reference=reference)
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
-                             wsum_gpu=m.weight_sums(burst.width, burst.height), want_sub=sub.image, ref=reference)
+                             wsum_gpu=m.weight_sums(burst.width, burst.height), want_sub=sub.image, wsum_sub=sub.wsum, ref=reference)
     print(st)
     return st
 
