@@ -330,6 +330,11 @@ class Merger:
         return flows, masks
 
 
+    def kernel_params(self, width, height):
+        """Kernel parameters of the last merge's reference frame (H x W x 4, host float32)."""
+        import torch
+        return device_copy(self.debug(0)["kparam"], (height, width, 4), torch.float32).cpu().numpy()
+
     def weight_sums(self, width, height):
         """Per-channel weight sums of the last merge's accumulation (Ho x Wo x 3, host float32)."""
         import torch

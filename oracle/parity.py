@@ -14,10 +14,11 @@ other pixel must agree to 1e-4 of the white level (the whole-path bar).
 weight sums, excludes exactly the output pixels that read a differing
 decision, checks that every mask value that differs is explained by a
 differing rounding decision, and asserts max |GPU - FP64| <= 1e-4 over the
-rest. Given the oracle's accumulation fed the GPU's own flows and masks, it
-also holds the accumulation to the bar on every pixel, and counts the pixels
-whose difference from the pure oracle is carried in from those FP32 inputs
-(a channel normalised by a tiny certainty-weighted sum amplifies them). `track_parity` compares the integer tile shifts (the first minimum of
+rest. Given the oracle's accumulation fed the GPU's own flows, masks and
+kernel parameters, it also holds the accumulation to the bar on every pixel,
+and counts the pixels whose difference from the pure oracle is carried in
+from those FP32 inputs (the kernel's orientation is ill-conditioned where
+the structure tensor is nearly isotropic). `track_parity` compares the integer tile shifts (the first minimum of
 every tile's L2 map, kernel.cu:422-546) of every pair at every pyramid level.
 
 Only the tests and the smoke check import this module.
@@ -99,7 +100,7 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
     w < thr is compared between them (with only wsum_orc, oracle sums within
     a relative 1e-4 of thr count as undecided). want_sub (optional): the
     oracle's accumulation and ApplyWeighting (pipeline.merge_tail) fed the
-    GPU's flows and masks; it must match the GPU to the bar on every pixel
+    GPU's flows, masks and kernel parameters; it must match the GPU to the bar on every pixel
     whose shift the GPU's FP32 interpolation cannot round either way, and a
     pixel where it matches while the pure oracle does not is counted as
     carried in from upstream FP32 inputs instead of failing. wsum_sub: its
@@ -167,9 +168,12 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
             excl_w = (np.abs(wo - thr) < 1e-4 * max(thr, 1.0)).any(axis=2)
     excl = excl_shift | excl_mask | excl_w
     diff = np.abs(got - want).max(axis=2)
-    # upstream conditioning: where the pure oracle disagrees but the oracle's accumulation fed the GPU's own flows
-    # and masks agrees, the difference is carried in from FP32 inputs that are within their own tolerances (a
-    # channel normalised by a tiny certainty-weighted sum amplifies 1e-8-level certainty differences)
+    # upstream conditioning: where the pure oracle disagrees but the oracle's accumulation fed the GPU's own flows,
+    # masks and kernel parameters agrees, the difference is carried in from FP32 inputs. The kernel's orientation
+    # comes from the structure tensor's eigenvectors (kernel.cu:628-700), which are ill-defined where the tensor is
+    # nearly isotropic, while the kernel stays anisotropic (stretch / shrink); far taps' weights exp(-q / 2) then
+    # move with the FP32 rounding of the tensor, and a channel reached only by far taps (scales other than 1 and 2)
+    # or normalised by a tiny certainty-weighted sum carries that into the output
     excl_cond = np.zeros((Ho, Wo), bool)
     if want_sub is not None:
         dsub = np.abs(got - np.asarray(want_sub, np.float64)).max(axis=2)
@@ -184,7 +188,7 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
                 if i != ref:
                     tail_skip |= near_half(bilinear(np.asarray(flows_gpu[i], np.float64), xb, yb, True) * s, HALF_MARGIN).any(axis=2)
         stats["tail_max_abs"] = float(dsub[~tail_skip].max())
-        assert stats["tail_max_abs"] <= bar, (f"accumulation on the GPU's own flows and masks differs by {stats['tail_max_abs']:.3e}", stats)
+        assert stats["tail_max_abs"] <= bar, (f"accumulation on the GPU's own flows, masks and kernel parameters differs by {stats['tail_max_abs']:.3e}", stats)
     excl |= excl_cond
     keep = ~excl
     if maps is not None:

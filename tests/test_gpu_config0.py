@@ -68,7 +68,7 @@ def test_config0_matches_oracle(cuda, case):
         assert np.percentile(df, 99.9) < 1e-3, (i, np.percentile(df, 99.9))
     # merged image over decision-matched pixels
     geom = PL.out_geometry(W, H, p)
-    sub = PL.merge_tail(burst, p, flows, masks, keep["kparam"], PL.StageLib("oracle64"))
+    sub = PL.merge_tail(burst, p, flows, masks, m.kernel_params(W, H), PL.StageLib("oracle64"))
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
                              wsum_gpu=m.weight_sums(W, H), want_sub=sub.image, wsum_sub=sub.wsum, max_excluded=0.01)
     print("merged image:", st)

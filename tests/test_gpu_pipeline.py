@@ -12,10 +12,12 @@ decide the other way and change the pixel by up to the local contrast.
 oracle/parity.py identifies those pixels from both sides' flows, masks and
 weight sums, requires every differing mask value to be explained by a
 differing rounding decision, and bounds their count. The oracle's
-accumulation fed the GPU's own flows and masks must match the GPU to 1e-4
-on every pixel; where only it matches (a channel normalised by a tiny
-certainty-weighted sum amplifies 1e-8-level mask differences, at scales
-other than 1 and 2), the pixel is counted as carried in from upstream."""
+accumulation fed the GPU's own flows, masks and kernel parameters must
+match the GPU to 1e-4 on every pixel; where only it matches (the kernel's
+orientation is ill-conditioned where the structure tensor is nearly
+isotropic, and at scales other than 1 and 2 a channel may be reached only by
+far taps whose weights follow it), the pixel is counted as carried in from
+upstream FP32 inputs."""
 import ctypes
 
 import numpy as np
@@ -50,7 +52,7 @@ def image_parity(m, burst, p, got, want, keep, reference=0):
     """max |GPU - FP64| <= 1e-4 over the decision-matched pixels (oracle/parity.py)."""
     flows, masks = m.flows_masks(burst.n, burst.width, burst.height, reference=reference)
     geom = PL.out_geometry(burst.width, burst.height, p)
-    sub = PL.merge_tail(burst, p, flows, masks, keep["kparam"], PL.StageLib("oracle64"), reference=reference)
+    sub = PL.merge_tail(burst, p, flows, masks, m.kernel_params(burst.width, burst.height), PL.StageLib("oracle64"), reference=reference)
     st = parity.merge_parity(got, want.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=want.wsum,
                              wsum_gpu=m.weight_sums(burst.width, burst.height), want_sub=sub.image, wsum_sub=sub.wsum, ref=reference)
     print(st)

@@ -135,7 +135,7 @@ def test_substituted_tail_explains_upstream_differences(merged, oracle):
                              want_sub=sub.image, wsum_sub=sub.wsum)
     assert st["excluded_conditioned"] >= 1 and st["tail_max_abs"] <= parity.IMAGE_BAR
     got[y + 2, x] += 3e-4                        # not reproduced by the substituted oracle: the accumulation's own error
-    with pytest.raises(AssertionError, match="own flows and masks"):
+    with pytest.raises(AssertionError, match="own flows, masks and kernel parameters"):
         parity.merge_parity(got, res.image, flows, keep["flow"], masks, keep["mask"], geom, p.erode_size, wsum_orc=res.wsum,
                             want_sub=sub.image)
 
