@@ -188,6 +188,8 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
                 if i != ref:
                     tail_skip |= near_half(bilinear(np.asarray(flows_gpu[i], np.float64), xb, yb, True) * s, HALF_MARGIN).any(axis=2)
         stats["tail_max_abs"] = float(dsub[~tail_skip].max())
+        if maps is not None:
+            maps.update(tail_diff=dsub, tail_skip=tail_skip)
         assert stats["tail_max_abs"] <= bar, (f"accumulation on the GPU's own flows, masks and kernel parameters differs by {stats['tail_max_abs']:.3e}", stats)
     excl |= excl_cond
     keep = ~excl
