@@ -29,7 +29,6 @@ import numpy as np
 
 IMAGE_BAR = 1e-4      # max |GPU - FP64| in units of the white level, over decision-matched pixels
 MASK_DECISION = 1e-5  # an eroded-mask value differing by more than this was decided differently
-HALF_MARGIN = 1e-4    # a GPU value (FP32 interpolation) this close to a half-integer may round either way
 TIE_MARGIN = 1e-5     # relative L2 margin under which two shifts of a tile tie at FP32 resolution
 
 
@@ -39,7 +38,11 @@ def c_round(v):
 
 
 def near_half(v, margin):
+    """v within `margin` (scalar, or per point for the last axis of v) of a half-integer."""
     f = np.abs(v) - np.floor(np.abs(v))
+    margin = np.asarray(margin)
+    if margin.ndim and margin.ndim < np.ndim(v):
+        margin = margin[..., None]
     return np.abs(f - 0.5) < margin
 
 
@@ -71,6 +74,37 @@ def bilinear(img, xb, yb, mirror):
     return v
 
 
+def bilinear_f32(img, xb, yb, mirror):
+    """The GPU kernels' FP32 bilinear sample (isa::lerp2, zero-weight texels
+    skipped) at FP32 positions xb, yb, evaluated in float32 without fused
+    multiply-adds; returns float64."""
+    f = np.float32
+    xb = np.asarray(xb, f)
+    yb = np.asarray(yb, f)
+    H, W = img.shape[:2]
+    fx, fy = np.floor(xb), np.floor(yb)
+    i, j = fx.astype(np.int64), fy.astype(np.int64)
+    a, b = (xb - fx).astype(f), (yb - fy).astype(f)
+    if mirror:
+        i0, i1, j0, j1 = mirror_index(i, W), mirror_index(i + 1, W), mirror_index(j, H), mirror_index(j + 1, H)
+    else:
+        i0, i1 = np.clip(i, 0, W - 1), np.clip(i + 1, 0, W - 1)
+        j0, j1 = np.clip(j, 0, H - 1), np.clip(j + 1, 0, H - 1)
+    img = np.asarray(img, f)
+    a, b = a[..., None], b[..., None]
+    one = f(1)
+    v = ((one - a) * (one - b)) * img[j0, i0]
+    v = np.where(a != 0, v + (a * (one - b)) * img[j0, i1], v)
+    v = np.where(b != 0, v + ((one - a) * b) * img[j1, i0], v)
+    v = np.where((a != 0) & (b != 0), v + (a * b) * img[j1, i1], v)
+    return v.astype(np.float64)
+
+
+def f32_margin(v):
+    """Room for the kernels' fused multiply-adds in an FP32 value v: a few ulps."""
+    return 1e-6 + 8.0 * np.abs(v) * 2.0 ** -24
+
+
 def dilate(mask2d, r):
     """Binary dilation by a (2r+1) x (2r+1) square with the border replicated."""
     if r <= 0:
@@ -82,6 +116,15 @@ def dilate(mask2d, r):
         for dx in range(2 * r + 1):
             out |= p[dy:dy + H, dx:dx + W]
     return out
+
+
+def gpu_shift_values(flow, x, y, s, origin):
+    """s * flow as the accumulation kernels compute it in FP32 at output pixel
+    (x, y): position ((float)x + 0.5f + ox) / s - 0.5f, FP32 bilinear, times s."""
+    f = np.float32
+    gx = ((x.astype(f) + f(0.5) + f(origin[0])) / f(s) - f(0.5)).astype(f)
+    gy = ((y.astype(f) + f(0.5) + f(origin[1])) / f(s) - f(0.5)).astype(f)
+    return (bilinear_f32(flow, gx, gy, True).astype(f) * f(s)).astype(np.float64)
 
 
 def _out_coords(Wo, Ho, s, origin):
@@ -127,12 +170,12 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
         stats["frames"] += 1
         fg, fo = np.asarray(flows_gpu[i], np.float64), np.asarray(flows_orc[i], np.float64)
         H, W = fg.shape[:2]
-        # accumulation shift at each output pixel
-        vg = bilinear(fg, xb, yb, True) * s
+        # accumulation shift at each output pixel: the GPU's own FP32 sample (DeBayerKernels.cu:403-404 positions)
+        vg = gpu_shift_values(fg, x, y, s, origin)
         vo = bilinear(fo, xb, yb, True) * s
         d = (c_round(vg) != c_round(vo)).any(axis=2)
         if not exact_s:
-            d |= near_half(vg, HALF_MARGIN).any(axis=2)
+            d |= near_half(vg, f32_margin(vg)).any(axis=2)
         d[[0, -1], :] = False
         d[:, [0, -1]] = False
         stats["shift_decisions_differ"] += int(d.sum())
@@ -141,9 +184,21 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
         Hh, Wh = H // 2, W // 2
         hy, hx = np.mgrid[0:Hh, 0:Wh].astype(np.float64)
         cxb, cyb = (hx + 0.5) / Wh * W - 0.5, (hy + 0.5) / Hh * H - 0.5
-        hg = bilinear(fg, cxb, cyb, True) * 0.5
+        # the robustness kernel's position ((float)x + 0.5f) / Wh * Wf - 0.5f, rounded after the product or fused
+        # with the subtraction: a cell whose offset depends on which is undecided
+        f = np.float32
+        qx, qy = ((hx.astype(f) + f(0.5)) / f(Wh)).astype(f), ((hy.astype(f) + f(0.5)) / f(Hh)).astype(f)
+        hgs = []
+        for fused in (False, True):
+            if fused:
+                gxb, gyb = (qx.astype(np.float64) * W - 0.5).astype(f), (qy.astype(np.float64) * H - 0.5).astype(f)
+            else:
+                gxb, gyb = ((qx * f(W)).astype(f) - f(0.5)).astype(f), ((qy * f(H)).astype(f) - f(0.5)).astype(f)
+            hgs.append((bilinear_f32(fg, gxb, gyb, True).astype(f) * f(0.5)).astype(np.float64))
+        hg = hgs[0]
         ho = bilinear(fo, cxb, cyb, True) * 0.5
-        md = (c_round(hg) != c_round(ho)).any(axis=2) | near_half(hg, HALF_MARGIN).any(axis=2)
+        md = (c_round(hg) != c_round(ho)).any(axis=2) | (c_round(hgs[1]) != c_round(ho)).any(axis=2)
+        md |= near_half(hg, f32_margin(hg)).any(axis=2) | near_half(hgs[1], f32_margin(hgs[1])).any(axis=2)
         mg, mo = np.asarray(masks_gpu[i], np.float64), np.asarray(masks_orc[i], np.float64)
         mdiff = (np.abs(mg - mo)[..., :3] > MASK_DECISION).any(axis=2)
         # the erosion spreads a cell's decision over erode_size x erode_size cells; the mask's
@@ -186,7 +241,8 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
         if not exact_s:
             for i in sorted(flows_gpu):
                 if i != ref:
-                    tail_skip |= near_half(bilinear(np.asarray(flows_gpu[i], np.float64), xb, yb, True) * s, HALF_MARGIN).any(axis=2)
+                    vg = gpu_shift_values(np.asarray(flows_gpu[i], np.float64), x, y, s, origin)
+                    tail_skip |= near_half(vg, f32_margin(vg)).any(axis=2)
         stats["tail_max_abs"] = float(dsub[~tail_skip].max())
         if maps is not None:
             maps.update(tail_diff=dsub, tail_skip=tail_skip)
