@@ -233,16 +233,18 @@ def merge_parity(got, want, flows_gpu, flows_orc, masks_gpu, masks_orc, geometry
     if want_sub is not None:
         dsub = np.abs(got - np.asarray(want_sub, np.float64)).max(axis=2)
         excl_cond = ~excl & (diff > bar) & (dsub <= bar)
-        # the accumulation itself: same flows and masks -> the bar on every pixel but the GPU's own near-half
-        # interpolated shifts (s != 1) and a flipped ApplyWeighting threshold
+        # the accumulation itself: same flows and masks -> the bar on every pixel but those whose shift the GPU's FP32
+        # sample rounds otherwise than FP64 on the same flows (s != 1) and a flipped ApplyWeighting threshold
         tail_skip = np.zeros((Ho, Wo), bool)
         if thr > 0 and wsum_gpu is not None and wsum_sub is not None:
             tail_skip = ((np.asarray(wsum_gpu, np.float64) < thr) != (np.asarray(wsum_sub, np.float64) < thr)).any(axis=2)
         if not exact_s:
             for i in sorted(flows_gpu):
                 if i != ref:
-                    vg = gpu_shift_values(np.asarray(flows_gpu[i], np.float64), x, y, s, origin)
-                    tail_skip |= near_half(vg, f32_margin(vg)).any(axis=2)
+                    fgi = np.asarray(flows_gpu[i], np.float64)
+                    vg = gpu_shift_values(fgi, x, y, s, origin)
+                    v64 = bilinear(fgi, xb, yb, True) * s  # what the FP64 tail takes from the same flows
+                    tail_skip |= near_half(vg, f32_margin(vg)).any(axis=2) | (c_round(vg) != c_round(v64)).any(axis=2)
         stats["tail_max_abs"] = float(dsub[~tail_skip].max())
         if maps is not None:
             maps.update(tail_diff=dsub, tail_skip=tail_skip)
