@@ -293,6 +293,44 @@ def batch_throughput(args):
             "sequential_mp_s": mp / (seq / 1e3), "batched_mp_s": mp / (bat / 1e3), "batched_bursts_s": nb / (bat / 1e3)}
 
 
+LARGE = dict(width=6016, height=4000, frames=50, max_shift=32.0, max_rot_deg=0.5, moving_object=0.05, object_step=(2.0, 40.0))
+
+
+def large_motion_throughput(args):
+    """The large burst with local motion: 50 frames of 6016x4000 RGGB 14-bit,
+    global shifts of +-32 px, and a rigid textured object covering 5 % of the
+    frame that moves 2-40 px per frame on its own path; merged at 2x with the
+    Full strategy (1,225 frame pairs). Device time per merge, frames resident."""
+    import torch
+    from imagestackalignator_b200 import isa, synthetic
+    W, H, n = LARGE["width"], LARGE["height"], LARGE["frames"]
+    b = synthetic.make_burst(W, H, n, seed=4000, max_shift=LARGE["max_shift"], max_rot_deg=LARGE["max_rot_deg"], noise_a=WORKLOAD["noise_a"],
+                             noise_b=WORKLOAD["noise_b"], device="cuda", moving_object=LARGE["moving_object"], object_step=LARGE["object_step"])
+    raw = torch.from_numpy(b.raw.view(np.int16)).cuda()
+    info = isa.make_info(b)
+    m = isa.Merger(W, H, n, merge_params())
+    Wo, Ho = m.output_size(W, H)
+    out = torch.empty((Ho, Wo, 3), dtype=torch.float32, device="cuda")
+    main = torch.cuda.current_stream()
+    steps = max(1, min(args.steps, 3))
+    for _ in range(max(1, min(args.warmup, 2))):
+        m.merge(raw, info, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(main)
+    for _ in range(steps):
+        m.merge(raw, info, out)
+    e1.record(main)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    stages = m.stage_times()
+    m.close()
+    names = ["tracking_images", "tile_alignment", "kernel_params", "lk_and_robustness", "accumulation", "finalize"]
+    return {"workload": f"{n}x{W}x{H} RGGB, shifts +-{LARGE['max_shift']:.0f} px, a 5 % object moving 2-40 px per frame, merged at 2x",
+            "pairs": n * (n - 1) // 2, "steps": steps, "ms_per_burst": ms, "mp_s": Wo * Ho / 1e6 / (ms / 1e3),
+            "stages_ms": dict(zip(names, stages))}
+
+
 def post_throughput(args, merged):
     """Colour/tone post-processing (isa_postprocess, the SaveAs16BitTiff chain)
     of the merged image to uint16 RGB: device time per call, HBM roofline."""
@@ -586,6 +624,9 @@ def run_ours(args):
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = batch_throughput(args)
+    large = None
+    if rank == 0 and world == 1 and not args.no_large:
+        large = large_motion_throughput(args)
     names = ["tracking_images", "tile_alignment", "kernel_params", "lk_and_robustness", "accumulation", "finalize"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -597,7 +638,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint, "batch": batch, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec, "dng_files_e2e": files,
+        "fwd_adjoint": adjoint, "batch": batch, "large_local_motion": large, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec, "dng_files_e2e": files,
         "clocks": clocks,
     }
     if rank == 0:
@@ -620,6 +661,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
+    ap.add_argument("--no-large", action="store_true", help="skip the 50-frame burst with local motion")
     ap.add_argument("--no-post", action="store_true", help="skip the colour/tone post-processing timing")
     ap.add_argument("--no-raw", action="store_true", help="skip the PEF and DNG raw-decoding timings")
     ap.add_argument("--no-files", action="store_true", help="skip the DNG-files-to-image end-to-end timing")

@@ -36,6 +36,7 @@ class Burst:
     truth: Optional[np.ndarray] = None  # H x W x 3 clean linear scene of frame 0 (float64)
     camera_white: tuple = (1.0, 1.0, 1.0)
     meta: dict = field(default_factory=dict)
+    object_path: Optional[np.ndarray] = None  # n x 2 centre (frame px) of the independently moving object, if any
 
     @property
     def n(self):
@@ -111,8 +112,13 @@ def _render_scene(Wp, Hp, rng, torch, device, dtype):
 
 def make_burst(width=2048, height=1536, frames=8, seed=0, max_shift=6.0, max_rot_deg=0.2,
                noise_a=4e-4, noise_b=2e-6, black=512, white_max=16383, cfa="RGGB", device="cpu",
-               keep_truth=False, dtype=None) -> Burst:
-    """Seeded burst; frame 0 is the reference with zero motion."""
+               keep_truth=False, dtype=None, moving_object=0.0, object_step=(2.0, 40.0)) -> Burst:
+    """Seeded burst; frame 0 is the reference with zero motion.
+
+    moving_object > 0 adds a rigid textured disc covering that fraction of
+    the frame area, which moves independently of the camera: each frame it
+    steps object_step[0]..object_step[1] px in a random direction (reflected
+    at the frame edges), occluding the background."""
     import torch
     import torch.nn.functional as F
 
@@ -134,6 +140,24 @@ def make_burst(width=2048, height=1536, frames=8, seed=0, max_shift=6.0, max_rot
     raw = np.empty((frames, height, width), dtype=np.uint16)
     gen = torch.Generator(device=device).manual_seed(int(seed) * 7919 + 17)
     truth = None
+    obj = None
+    if moving_object > 0:
+        orng = np.random.default_rng(int(seed) * 104729 + 7)
+        rad = float(np.sqrt(moving_object * width * height / np.pi))
+        side = int(np.ceil(2 * rad)) + 8
+        tex = _render_scene(side, side, orng, torch, device, dtype)
+        pos = np.zeros((frames, 2))
+        lo = np.array([rad + 2, rad + 2])
+        hi = np.array([width - rad - 3, height - rad - 3])
+        pos[0] = orng.uniform(lo, hi)
+        for f in range(1, frames):
+            ang = orng.uniform(0, 2 * np.pi)
+            step = orng.uniform(*object_step)
+            p = pos[f - 1] + step * np.array([np.cos(ang), np.sin(ang)])
+            p = np.where(p < lo, 2 * lo - p, p)
+            p = np.where(p > hi, 2 * hi - p, p)
+            pos[f] = np.clip(p, lo, hi)
+        obj = (tex, rad, side, pos)
     for f in range(frames):
         th = np.deg2rad(rots[f])
         c, s = np.cos(th), np.sin(th)
@@ -144,6 +168,14 @@ def make_burst(width=2048, height=1536, frames=8, seed=0, max_shift=6.0, max_rot
         sy = s * dx + c * dy + cyf + shifts[f, 1] + margin
         grid = torch.stack([(sx + 0.5) / Wp * 2 - 1, (sy + 0.5) / Hp * 2 - 1], dim=-1)[None]
         frame = F.grid_sample(scene[None], grid, mode="bicubic", padding_mode="border", align_corners=False)[0]
+        if obj is not None:
+            tex, rad, side, pos = obj
+            ox, oy = xs - pos[f, 0] + side / 2.0, ys - pos[f, 1] + side / 2.0
+            inside = ((xs - pos[f, 0]) ** 2 + (ys - pos[f, 1]) ** 2) <= rad * rad
+            og = torch.stack([(ox + 0.5) / side * 2 - 1, (oy + 0.5) / side * 2 - 1], dim=-1)[None]
+            ocol = F.grid_sample(tex[None], og, mode="bilinear", padding_mode="border", align_corners=False)[0]
+            frame = torch.where(inside[None], ocol, frame)
+            del og, ocol, inside
         frame = frame.clamp(0, 1)
         if f == 0 and keep_truth:
             truth = frame.permute(1, 2, 0).double().cpu().numpy()
@@ -155,7 +187,7 @@ def make_burst(width=2048, height=1536, frames=8, seed=0, max_shift=6.0, max_rot
         del frame, mosaic, noise, noisy, q, grid
     w = float(white_max - black)
     return Burst(raw=raw, cfa=codes, black=(float(black),) * 3, white=(w, w, w), noise_a=noise_a, noise_b=noise_b,
-                 shifts=shifts, rotations=rots, truth=truth)
+                 shifts=shifts, rotations=rots, truth=truth, object_path=None if obj is None else obj[3])
 
 
 # ---- PEF-style compressed streams (inputs for isa_pef_decode) ----

@@ -92,10 +92,13 @@ def test_merge_matches_oracle(cuda, oracle, burst, mode):
     m.close()
 
 
-@pytest.mark.parametrize("case", ["onref", "refblock", "blocks", "ref2", "prealign", "bggr"])
+@pytest.mark.parametrize("case", ["onref", "refblock", "blocks", "ref2", "prealign", "bggr", "moving"])
 def test_merge_variants_match_oracle(cuda, oracle, case):
+    """Tracking strategies, reference choice, pre-alignment input, another
+    Bayer layout, and an independently moving object (5 % of the frame,
+    2-40 px per frame: the robustness mask rejects it where it occludes)."""
     cfa = "BGGR" if case == "bggr" else "RGGB"
-    b = synthetic.make_burst(512, 384, 6, seed=33, max_shift=5, max_rot_deg=0.2, cfa=cfa)
+    b = synthetic.make_burst(512, 384, 6, seed=33, max_shift=5, max_rot_deg=0.2, cfa=cfa, moving_object=0.05 if case == "moving" else 0.0)
     p = P.MergeParams()
     p.merge_scale = 2.0
     pre = PL.PreAlignment.zeros(b.n)

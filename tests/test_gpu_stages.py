@@ -195,8 +195,8 @@ def test_upsample(cuda, oracle, rng):
     close(host(out), want, atol=2e-6, what="upsample")
 
 
-@pytest.mark.parametrize("strategy,n,ref", [(P.FULL, 6, 0), (P.FULL, 20, 0), (P.ONLY_ON_REFERENCE, 5, 2), (P.ON_REFERENCE_BLOCK, 9, 6),
-                                            (P.BLOCKS, 7, 0)])
+@pytest.mark.parametrize("strategy,n,ref", [(P.FULL, 6, 0), (P.FULL, 20, 0), (P.FULL, 50, 0), (P.ONLY_ON_REFERENCE, 5, 2),
+                                            (P.ON_REFERENCE_BLOCK, 9, 6), (P.BLOCKS, 7, 0)])
 def test_solve_shifts(cuda, oracle, rng, strategy, n, ref):
     A = P.shift_matrix(n, ref, strategy, 3)
     m = A.shape[0]
