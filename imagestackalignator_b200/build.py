@@ -59,8 +59,7 @@ def build(force=False, verbose=False):
     if failed:
         raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
     tmp = LIB + ".tmp"
-    link = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft",
-            "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")]
+    link = [NVCC, *ARCH, "-shared", "-o", tmp, *objs]
     if verbose:
         print(" ".join(link))
     subprocess.run(link, check=True)

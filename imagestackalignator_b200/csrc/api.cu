@@ -6,7 +6,6 @@
 #include "isa.h"
 #include "isa_internal.cuh"
 
-#include <cufft.h>
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -50,11 +49,6 @@ namespace {
     do {                                                                                     \
         cudaError_t e_ = (call);                                                             \
         if (e_ != cudaSuccess) return fail(ISA_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
-#define ISA_FFT(call)                                                              \
-    do {                                                                           \
-        cufftResult r_ = (call);                                                   \
-        if (r_ != CUFFT_SUCCESS) return fail(ISA_ECUDA, "%s: cufft error %d", #call, (int)r_); \
     } while (0)
 #define ISA_LAUNCH(ctx, call) \
     do {                      \
@@ -215,11 +209,11 @@ struct isa_ctx {
     float *st3 = nullptr, *kparam = nullptr;
     float *acc = nullptr, *wsum = nullptr, *out_stage = nullptr;
     isa_frame_in* frame_in = nullptr;
-    // cuFFT plans for the current frame size
-    cufftHandle r2c = 0, c2r = 0;
-    int plan_w = 0, plan_h = 0;
-    void* fft_work = nullptr;
-    size_t fft_work_bytes = 0;
+    // full-frame transforms: plans (radices) and twiddle tables for the current frame size: rows of W / 2, the
+    // unpacking factors e^{-2 pi i k / W} (k <= W / 2), columns of H
+    isa_fft_plan fft_rows{}, fft_cols{};
+    float2 *tw_rows = nullptr, *tw_unpack = nullptr, *tw_cols = nullptr;
+    int fft_w = 0, fft_h = 0;
     cudaEvent_t ev[8] = {};
     // host entry point: frames copied in and the image copied out on a second stream, overlapped with the work
     static constexpr int kBands = 8;
@@ -293,30 +287,37 @@ void accum_geom(const isa_params* p, int W, int H, isa_accum_geom& g, float& thr
     g.yb1 = g.Ho;
 }
 
-int ensure_plans(isa_ctx* c, int W, int H)
+// Plans and twiddle tables of the W x H transforms (the tables are copied on
+// the caller's stream, ordered with the work that reads them).
+int ensure_fft(isa_ctx* c, int W, int H, cudaStream_t st)
 {
-    if (c->plan_w == W && c->plan_h == H) return ISA_OK;
-    if (c->r2c) { cufftDestroy(c->r2c); c->r2c = 0; }
-    if (c->c2r) { cufftDestroy(c->c2r); c->c2r = 0; }
-    size_t w1 = 0, w2 = 0;
-    ISA_FFT(cufftCreate(&c->r2c));
-    ISA_FFT(cufftCreate(&c->c2r));
-    ISA_FFT(cufftSetAutoAllocation(c->r2c, 0));
-    ISA_FFT(cufftSetAutoAllocation(c->c2r, 0));
-    ISA_FFT(cufftMakePlan2d(c->r2c, H, W, CUFFT_R2C, &w1));
-    ISA_FFT(cufftMakePlan2d(c->c2r, H, W, CUFFT_C2R, &w2));
-    size_t need = std::max(w1, w2);
-    if (need > c->fft_work_bytes) {
-        if (c->fft_work) cudaFree(c->fft_work);
-        c->fft_work = nullptr;
-        c->fft_work_bytes = 0;
-        if (cudaMalloc(&c->fft_work, need) != cudaSuccess) return fail(ISA_ENOMEM, "cuFFT work area of %zu bytes", need);
-        c->fft_work_bytes = need;
-    }
-    ISA_FFT(cufftSetWorkArea(c->r2c, c->fft_work));
-    ISA_FFT(cufftSetWorkArea(c->c2r, c->fft_work));
-    c->plan_w = W;
-    c->plan_h = H;
+    if (c->fft_w == W && c->fft_h == H) return ISA_OK;
+    if ((W & 1) || W > c->max_w || H > c->max_h) return fail(ISA_EINVAL, "transform size %dx%d", W, H);
+    isa_fft_plan pr, pc;
+    if (!isa_fft_plan_make(W / 2, pr) || !isa_fft_plan_make(H, pc)) return fail(ISA_EINVAL, "no FFT plan for %dx%d", W, H);
+    std::vector<float2> tr(W / 2), tu(W), tc(H);
+    isa_fft_twiddles(W / 2, tr.data());
+    isa_fft_twiddles(W, tu.data());
+    isa_fft_twiddles(H, tc.data());
+    ISA_CK(cudaMemcpyAsync(c->tw_rows, tr.data(), tr.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(c->tw_unpack, tu.data(), (W / 2 + 1) * sizeof(float2), cudaMemcpyHostToDevice, st));
+    ISA_CK(cudaMemcpyAsync(c->tw_cols, tc.data(), tc.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+    // pageable sources: the copies above are staged before returning
+    c->fft_rows = pr;
+    c->fft_cols = pc;
+    c->fft_w = W;
+    c->fft_h = H;
+    return ISA_OK;
+}
+
+// The forward half spectrum of a W x H real image into `spec` (pitch (W/2 + 1) * 8).
+int fft_forward(isa_ctx* c, const float* img, size_t pitch, float2* spec, int W, int H, cudaStream_t st)
+{
+    ISA_TRY(ensure_fft(c, W, H, st));
+    const size_t sp = (size_t)(W / 2 + 1) * sizeof(float2);
+    ISA_LAUNCH(c, isa_launch_fft_rows_r2c(img, pitch, spec, sp, W, H, c->fft_rows, c->tw_rows, c->tw_unpack, st));
+    isa_fft_filter none{};
+    ISA_LAUNCH(c, isa_launch_fft_cols(spec, sp, W, H, W / 2 + 1, c->fft_cols, c->tw_cols, ISA_FFT_COLS_FWD, none, nullptr, 0, st));
     return ISA_OK;
 }
 
@@ -348,17 +349,22 @@ int bw_frame(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H, co
     if (acc_out)
         ISA_LAUNCH(c, isa_launch_gauss(out, pitch, acc_out, pitch, c->tmp, pitch, W, H, 1, taps_acc.data(), (int)taps_acc.size(), 0, st));
     if (high_pass) {
-        ISA_TRY(ensure_plans(c, W, H));
-        ISA_FFT(cufftSetStream(c->r2c, st));
-        ISA_FFT(cufftSetStream(c->c2r, st));
-        ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)out, (cufftComplex*)c->spec));
-        ISA_LAUNCH(c, isa_launch_fourier_filter(c->spec, (size_t)(W / 2 + 1) * sizeof(float2), W, H, 1, 0, 1.0f, c->p.high_pass, 1.0f,
-                                         c->p.high_pass_sigma, c->p.clear_axis, 1.0f / ((float)W * (float)H), st));
+        // PreAlignment.FourierFilter: R2C rows, then per column the forward transform, fourierFilter (with the
+        // 1 / (W * H) of the inverse) and the inverse transform, then C2R rows
+        ISA_TRY(ensure_fft(c, W, H, st));
+        const size_t sp = (size_t)(W / 2 + 1) * sizeof(float2);
+        ISA_LAUNCH(c, isa_launch_fft_rows_r2c(out, pitch, c->spec, sp, W, H, c->fft_rows, c->tw_rows, c->tw_unpack, st));
+        const isa_fft_filter f{1.0f, c->p.high_pass, 1.0f, c->p.high_pass_sigma, c->p.clear_axis, 1.0f / ((float)W * (float)H)};
+        // columns from kf on have the coefficient 1 at every row: their forward and inverse transforms cancel (a
+        // factor H), so they skip the column pass and take post_scale * H in the inverse row pass
+        const int kf = isa_fft_filter_columns(W, f);
+        const float kscale = f.post_scale * (float)H;
+        ISA_LAUNCH(c, isa_launch_fft_cols(c->spec, sp, W, H, kf, c->fft_cols, c->tw_cols, ISA_FFT_COLS_FILTER, f, nullptr, 0, st));
         if (taps_hp.empty()) {
-            ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)out));
+            ISA_LAUNCH(c, isa_launch_fft_rows_c2r(c->spec, sp, out, pitch, W, H, c->fft_rows, c->tw_rows, c->tw_unpack, 1, kf, kscale, st));
         } else {
-            // inverse transform into scratch, then clamp + Gauss back into `out` in one pass
-            ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)c->spec, (cufftReal*)c->tmp));
+            // inverse rows into scratch, then clamp + Gauss back into `out` in one pass
+            ISA_LAUNCH(c, isa_launch_fft_rows_c2r(c->spec, sp, c->tmp, pitch, W, H, c->fft_rows, c->tw_rows, c->tw_unpack, 0, kf, kscale, st));
             ISA_LAUNCH(c, isa_launch_gauss(c->tmp, pitch, out, pitch, c->tmp + fsz_of(W, H), pitch, W, H, 1, taps_hp.data(), (int)taps_hp.size(), 1,
                                            st));
         }
@@ -665,8 +671,9 @@ int scan_angles(isa_ctx* c, const float* img, int W, int H, double incr, double 
     constexpr int kMaxAngles = 256;
     const float N = (float)W * (float)H;
     double maxVal = -DBL_MAX, maxAng = 0, maxX = 0, maxY = 0;
-    ISA_FFT(cufftSetStream(c->r2c, st));
-    ISA_FFT(cufftSetStream(c->c2r, st));
+    ISA_TRY(ensure_fft(c, W, H, st));
+    const size_t sp = hw * sizeof(float2);
+    const isa_fft_filter none{};
     for (int phase = 0; phase < 2; phase++) {
         // the reference's loops, in the same double arithmetic
         std::vector<double> angles;
@@ -677,9 +684,10 @@ int scan_angles(isa_ctx* c, const float* img, int W, int H, double incr, double 
         }
         for (size_t k = 0; k < angles.size(); k++) {
             ISA_LAUNCH(c, isa_launch_rotate_cubic(img, (size_t)W * 4, W, H, angles[k], rot, (size_t)W * 4, st));
-            ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)rot, (cufftComplex*)spec));
-            ISA_LAUNCH(c, isa_launch_conj_mul(c->spec, spec, hw * H, st));
-            ISA_FFT(cufftExecC2R(c->c2r, (cufftComplex*)spec, (cufftReal*)rot));
+            // R2C, conjugateComplexMulKernel against the reference spectrum, C2R (one column pass does the middle three)
+            ISA_LAUNCH(c, isa_launch_fft_rows_r2c(rot, (size_t)W * 4, spec, sp, W, H, c->fft_rows, c->tw_rows, c->tw_unpack, st));
+            ISA_LAUNCH(c, isa_launch_fft_cols(spec, sp, W, H, (int)hw, c->fft_cols, c->tw_cols, ISA_FFT_COLS_XCORR, none, c->spec, sp, st));
+            ISA_LAUNCH(c, isa_launch_fft_rows_c2r(spec, sp, rot, (size_t)W * 4, W, H, c->fft_rows, c->tw_rows, c->tw_unpack, 0, W, 1.0f, st));
             ISA_LAUNCH(c, isa_launch_argmax(rot, (int)fsz, scratch, res + k, st));
         }
         std::vector<ArgMax> h(angles.size());
@@ -795,6 +803,9 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     ISA_TRY(check_params(p));
     if (max_w < 16 || max_h < 16 || (max_w & 1) || (max_h & 1) || max_n < 2 || max_n > 65)
         return fail(ISA_EINVAL, "context size %dx%d x %d frames invalid", max_w, max_h, max_n);
+    // the full-frame transforms hold a row (W complex values) and at least one column (2 H) in shared memory
+    if ((size_t)max_w * 8 > 227 * 1024 || isa_fft_cols_per_cta(max_h) < 1)
+        return fail(ISA_EINVAL, "context size %dx%d exceeds the full-frame transform's limit (W <= 29056, H <= 12800)", max_w, max_h);
     isa_ctx* c = new isa_ctx();
     c->max_w = max_w; c->max_h = max_h; c->max_n = max_n; c->p = *p;
     // worst case pairs over strategies for max_n frames
@@ -856,6 +867,9 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     add((void**)&c->out_stage, (size_t)c->max_wo * c->max_ho * 12);
     add((void**)&c->frame_in, (size_t)max_n * sizeof(isa_frame_in));
     add((void**)&c->adj_acc, 16 * sizeof(double));
+    add((void**)&c->tw_rows, (size_t)(max_w / 2) * sizeof(float2));
+    add((void**)&c->tw_unpack, (size_t)(max_w / 2 + 1) * sizeof(float2));
+    add((void**)&c->tw_cols, (size_t)max_h * sizeof(float2));
     size_t total = 0;
     for (auto& e : plan) total += e.second;
     if (cudaMalloc(&c->arena, total) != cudaSuccess) {
@@ -875,8 +889,7 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     ok = ok && cudaEventCreateWithFlags(&c->ev_free, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) { isa_ctx_destroy(c); return fail(ISA_ECUDA, "stream/event creation failed"); }
-    int r = ensure_plans(c, max_w, max_h);
-    if (r != ISA_OK) { isa_ctx_destroy(c); return r; }
+    int r = ISA_OK;
     // the static solve's set-up on this device (loads the solver's device code), so that it allocates nothing later
     r = isa_static_solve_setup();
     if (r != ISA_OK) { isa_ctx_destroy(c); return r; }
@@ -887,9 +900,6 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
 int isa_ctx_destroy(isa_ctx* c)
 {
     if (!c) return ISA_OK;
-    if (c->r2c) cufftDestroy(c->r2c);
-    if (c->c2r) cufftDestroy(c->c2r);
-    if (c->fft_work) cudaFree(c->fft_work);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (cudaEvent_t e : c->ev_frame)
@@ -1153,6 +1163,7 @@ int isa_bw_image(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, int W, int H
     ISA_REQ(info->width == W && info->height == H, "info size differs from width/height");
     ISA_REQ(W <= c->max_w && H <= c->max_h, "frame exceeds the context");
     ISA_REQ(out_pitch == (size_t)W * 4 && raw_pitch >= (size_t)W * 2, "out pitch must be width * 4");
+    ISA_REQ(!high_pass || ((uintptr_t)out & 7) == 0, "out must be 8-byte aligned for the high-pass (rows are read as complex pairs)");
     std::vector<float> taps = gauss_taps(sigma), none;
     return bw_frame(c, raw, raw_pitch, W, H, info, high_pass != 0, out, taps, nullptr, none, S(stream));
 }
@@ -1175,9 +1186,7 @@ int isa_prealign_burst(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
         ISA_TRY(bw_frame(c, (const uint16_t*)((const char*)raw + (size_t)i * frame_stride), raw_pitch, W, H, info, true, c->bw_track + i * fsz, taps,
                          nullptr, none, st));
     // reference spectrum (SetReferenceImage, PreAlignment.cs:164-175): frame 0
-    ISA_TRY(ensure_plans(c, W, H));
-    ISA_FFT(cufftSetStream(c->r2c, st));
-    ISA_FFT(cufftExecR2C(c->r2c, (cufftReal*)c->bw_track, (cufftComplex*)c->spec));
+    ISA_TRY(fft_forward(c, c->bw_track, (size_t)W * 4, c->spec, W, H, st));
     std::vector<ScanResult> init(n, ScanResult{0, 0, 0, 0});
     const float roll0 = roll_deg ? -roll_deg[0] : 0.f;
     for (int i = 1; i < n; i++) {

@@ -179,30 +179,7 @@ __global__ void k_fourier_filter(float2* spec, size_t pitch, size_t batch_stride
 {
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W / 2 + 1 || y >= H) return;
-    float mx = (float)x, my = (float)y;
-    if (my > H * 0.5f) my = (H - my) * -1.0f;
-    mx /= W;
-    my /= H;
-    float dist = sqrtf(mx * mx + my * my);
-    float fil = 0;
-    lp = lp - lps;
-    hp = hp + hps;
-    if (lp > 0) { if (dist <= lp) fil = 1; }
-    else { if (dist <= 1.0f) fil = 1; }
-    if (lps > 0) {
-        float f2 = (-fil + 1.0f) * expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
-        if (f2 > 0.001f) fil = f2;
-    }
-    if (lps > 0 && lp == 0 && hp == 0 && hps == 0) fil = expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
-    if (hp > 0) {
-        float f2 = dist >= hp ? 1.0f : 0.0f;
-        fil *= f2;
-        if (hps > 0) {
-            float f3 = (-f2 + 1.0f) * expf(-((dist - hp) * (dist - hp) / (2 * hps * hps)));
-            if (f3 > 0.001f) fil = f3;
-        }
-    }
-    if (x < clear_axis || fabsf(my) * H < clear_axis) fil = 0;
+    float fil = isa::fourier_mask(x, y, W, H, lp, hp, lps, hps, clear_axis);
     fil *= post_scale;
     float2* p = (float2*)((char*)spec + blockIdx.z * batch_stride + (size_t)y * pitch) + x;
     float2 v = *p;

@@ -44,9 +44,60 @@ ISA_DEV float lerp2(float p00, float p10, float p01, float p11, float a, float b
 // CFA code at (x, y): cfa packed as 4 x 2 bits, (y&1)*2 + (x&1) selects.
 ISA_DEV int cfa_at(unsigned cfa, int x, int y) { return (cfa >> ((((y & 1) << 1) | (x & 1)) * 2)) & 3; }
 
+// fourierFilter's coefficient (kernel.cu:704-779) of half-spectrum bin (x, y) of a W x H transform.
+ISA_DEV float fourier_mask(int x, int y, int W, int H, float lp, float hp, float lps, float hps, int clear_axis)
+{
+    float mx = (float)x, my = (float)y;
+    if (my > H * 0.5f) my = (H - my) * -1.0f;
+    mx /= W;
+    my /= H;
+    float dist = sqrtf(mx * mx + my * my);
+    float fil = 0;
+    lp = lp - lps;
+    hp = hp + hps;
+    if (lp > 0) { if (dist <= lp) fil = 1; }
+    else { if (dist <= 1.0f) fil = 1; }
+    if (lps > 0) {
+        float f2 = (-fil + 1.0f) * expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
+        if (f2 > 0.001f) fil = f2;
+    }
+    if (lps > 0 && lp == 0 && hp == 0 && hps == 0) fil = expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
+    if (hp > 0) {
+        float f2 = dist >= hp ? 1.0f : 0.0f;
+        fil *= f2;
+        if (hps > 0) {
+            float f3 = (-f2 + 1.0f) * expf(-((dist - hp) * (dist - hp) / (2 * hps * hps)));
+            if (f3 > 0.001f) fil = f3;
+        }
+    }
+    if (x < clear_axis || fabsf(my) * H < clear_axis) fil = 0;
+    return fil;
+}
+
 }  // namespace isa
 
 // ---- launchers implemented in the .cu files (host side) -------------------
+// fft.cu: mixed-radix transforms in shared memory (plan = radices of the stages)
+constexpr int ISA_FFT_MAX_STAGES = 24;
+// radix[s]: the stage's radix; ns[s]: the product of the radices before it; mns[s]: 2^32 / ns + 1 (division by ns
+// as a multiply-high, exact for the sizes used: numerator and divisor below 2^15)
+struct isa_fft_plan { int n, nst; int radix[ISA_FFT_MAX_STAGES]; int ns[ISA_FFT_MAX_STAGES]; unsigned mns[ISA_FFT_MAX_STAGES]; };
+struct isa_fft_filter { float lp, hp, lps, hps; int clear_axis; float post_scale; };
+enum { ISA_FFT_COLS_FWD = 0, ISA_FFT_COLS_FILTER = 1, ISA_FFT_COLS_XCORR = 2 };
+bool isa_fft_plan_make(int n, isa_fft_plan& p);
+void isa_fft_twiddles(int n, float2* out);  // e^{-2 pi i k / n}, k < n, from double precision
+int isa_fft_cols_per_cta(int H);            // 0: H too long for one column in shared memory
+cudaError_t isa_launch_fft_rows_r2c(const float* in, size_t in_pitch, float2* spec, size_t spec_pitch, int W, int H, const isa_fft_plan& pn,
+                                    const float2* tw_n, const float2* tw_w, cudaStream_t st);
+// bins k >= kfrom are multiplied by kscale before the inverse (kfrom > W / 2: none)
+cudaError_t isa_launch_fft_rows_c2r(const float2* spec, size_t spec_pitch, float* out, size_t out_pitch, int W, int H, const isa_fft_plan& pn,
+                                    const float2* tw_n, const float2* tw_w, int clamp01, int kfrom, float kscale, cudaStream_t st);
+// columns [0, ncols) of the half spectrum
+cudaError_t isa_launch_fft_cols(float2* spec, size_t spec_pitch, int W, int H, int ncols, const isa_fft_plan& ph, const float2* tw_h, int mode,
+                                const isa_fft_filter& f, const float2* ref, size_t ref_pitch, cudaStream_t st);
+// the first bin column from which the filter is 1 at every row (W / 2 + 1: none)
+int isa_fft_filter_columns(int W, const isa_fft_filter& f);
+
 struct isa_pair_desc {
     int ref, trk;          // frame indices
     int grid;              // index of this pair's shift grid
