@@ -44,7 +44,7 @@ extern "C" {
 
 #define ISA_OK 0
 #define ISA_EINVAL (-1)      /* bad size, pointer or parameter */
-#define ISA_ECUDA (-2)       /* a CUDA runtime or cuFFT call failed */
+#define ISA_ECUDA (-2)       /* a CUDA runtime call or kernel launch failed */
 #define ISA_ESINGULAR (-3)   /* reported per tile in the solver status array, never returned */
 #define ISA_ETIMEDOUT (-4)   /* reserved for bounded waits */
 #define ISA_ENOMEM (-5)      /* device allocation failed (isa_ctx_create only) */
@@ -148,7 +148,7 @@ ISA_API int isa_output_size(const isa_params* p, int width, int height, int* out
  * finalize. Synchronises the context's events. Returns the count written. */
 ISA_API int isa_stage_times(isa_ctx* ctx, float* ms, int max_count);
 /* Number of this library's kernels the last isa_merge_burst launched
- * (cuFFT's own kernels are not counted). */
+ * (every kernel of the merge, the full-frame FFTs included). */
 ISA_API long isa_launch_count(isa_ctx* ctx);
 
 /* ---- fused pipeline ------------------------------------------------------ */
@@ -241,7 +241,8 @@ ISA_API int isa_debayer_full(const uint16_t* raw, size_t raw_pitch, int width, i
 ISA_API int isa_gamma_srgb(float* img, size_t pitch, int width, int height, void* stream);
 /* DeBayerBWGaussWB (controller :2384-2418) for one frame: demosaic, gamma,
  * gray, optional Fourier high-pass + clamp (PreAlignment.FourierFilter
- * PreAlignment.cs:268-281), Gaussian. Needs ctx for the FFT plan/scratch. */
+ * PreAlignment.cs:268-281), Gaussian. Needs ctx for the FFT tables and
+ * spectrum; with high_pass, out must be 8-byte aligned. */
 ISA_API int isa_bw_image(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, int width, int height, const isa_raw_info* info,
                  float sigma, int high_pass, float* out, size_t out_pitch, void* stream);
 /* Global pre-alignment of a burst (ComputePreAlignment, controller

@@ -122,8 +122,33 @@ def test_bw_image(cuda, oracle, small_burst, high_pass):
     info = isa.make_info(b)
     ok(lib().isa_bw_image(m.ctx, isa.vp(dev(b.raw[1])), sz(b.width * 2), b.width, b.height, ctypes.byref(info), ctypes.c_float(0.5),
                           high_pass, isa.vp(out), sz(b.width * 4), S0))
-    # FP32 demosaic + cuFFT (high-pass) against FP64 numpy FFT
+    # FP32 demosaic + the library's FFT high-pass against FP64 numpy FFT
     close(host(out), want, atol=2e-5 if high_pass else 2e-6, what="bw")
+    m.close()
+
+
+@pytest.mark.parametrize("W,H,params", [
+    (188, 250, {}),                                   # rows of 94 = 2 * 47, columns 2 * 5^3 (the 6016 x 4000 factors)
+    (134, 106, {}),                                   # rows of 67 (prime), columns 2 * 53 (prime)
+    (240, 162, {"high_pass": 0.05}),                 # radix 3 in both directions, a wider high-pass band
+    (160, 96, {"high_pass": 0.02, "clear_axis": 2}),  # axis clearing: every column through the column pass
+])
+def test_bw_image_fft_sizes(cuda, oracle, W, H, params):
+    """The full-frame high-pass (PreAlignment.FourierFilter) through the hand-written FFT at frame sizes whose
+    row and column lengths take every kind of stage (radix 8, 4, 2, 5, 3 and the paired prime stage), and with
+    filter parameters that send every column through the column pass, against numpy's FP64 FFT."""
+    import pipeline as PL
+    from imagestackalignator_b200 import synthetic
+    b = synthetic.make_burst(W, H, 2, seed=W + H, max_shift=2, max_rot_deg=0.1)
+    p = P.MergeParams()
+    for k, v in params.items():
+        setattr(p, k, v)
+    want = PL.bw_image(oracle, b, 1, 0.5, True, p)
+    m = isa.Merger(W, H, 2, p)
+    out = dev(np.zeros((H, W), np.float32))
+    info = isa.make_info(b)
+    ok(lib().isa_bw_image(m.ctx, isa.vp(dev(b.raw[1])), sz(W * 2), W, H, ctypes.byref(info), ctypes.c_float(0.5), 1, isa.vp(out), sz(W * 4), S0))
+    close(host(out), want, atol=2e-5, what=f"bw {W}x{H}")
     m.close()
 
 
