@@ -14,9 +14,9 @@ def test_calls_allocate_nothing(cuda):
     import torch
     p = P.MergeParams()
     p.merge_scale = 2.0
-    sizes = [(320, 240, 4), (256, 192, 3), (384, 256, 5)]
+    sizes = [(640, 480, 4), (512, 384, 3), (768, 512, 5)]  # every level of the default 4-level pyramid has tiles
     bursts = [synthetic.make_burst(w, h, n, seed=w + n, max_shift=3, max_rot_deg=0.1) for w, h, n in sizes]
-    m = isa.Merger(384, 256, 5, p)
+    m = isa.Merger(768, 512, 5, p)
     raws = [torch.from_numpy(np.ascontiguousarray(b.raw).view(np.int16)).cuda() for b in bursts]
     infos = [isa.make_info(b) for b in bursts]
     outs = [torch.empty((h * 2, w * 2, 3), dtype=torch.float32, device="cuda") for w, h, _ in sizes]
