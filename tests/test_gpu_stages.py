@@ -141,6 +141,7 @@ def test_bw_image_fft_sizes(cuda, oracle, W, H, params):
     from imagestackalignator_b200 import synthetic
     b = synthetic.make_burst(W, H, 2, seed=W + H, max_shift=2, max_rot_deg=0.1)
     p = P.MergeParams()
+    p.levels = P.default_levels(1)  # the context is only needed for the transforms' tables and spectrum
     for k, v in params.items():
         setattr(p, k, v)
     want = PL.bw_image(oracle, b, 1, 0.5, True, p)
