@@ -15,6 +15,9 @@
 // pseudo-inverse in FP64.
 #include "isa_internal.cuh"
 
+#include <algorithm>
+#include <type_traits>
+
 namespace {
 
 __device__ __forceinline__ float bilinear_mirror(const float* img, size_t pitch, int W, int H, int px, int py, float fx, float fy)
@@ -29,33 +32,33 @@ __device__ __forceinline__ float bilinear_mirror(const float* img, size_t pitch,
     return isa::lerp2(p00, p10, p01, p11, a, b);
 }
 
-// lucasKanadeOptim's pseudo-inverse (opticalFlow.cu:229-290) in FP64. For a
-// well-conditioned matrix (lambda2 > 1e-3 lambda1) the angle/singular-value
-// construction of the reference equals the closed-form inverse to ~1e-10
-// relative; below that the reference's own construction is evaluated.
-// Returns false where the reference leaves the pixel unchanged
-// (sigma1 < minDet; the reference tests min(sigma1, sigma1)).
-__device__ __forceinline__ bool lk_pinv(double a, double b, double d, double min_det, double (&M)[4])
+// lucasKanadeOptim's pseudo-inverse (opticalFlow.cu:229-290) in FP64 and the
+// flow update u = M (sxt, syt). For a well-conditioned matrix
+// (lambda2 > 1e-3 lambda1) the angle/singular-value construction of the
+// reference equals the closed-form inverse to ~1e-10 relative; below that the
+// reference's own construction is evaluated (lk_update_svd). The pixel is
+// left unchanged where sigma1 < minDet (the reference tests
+// min(sigma1, sigma1)).
+__device__ __forceinline__ float2 lk_apply(float2 f, double m0, double m1, double m2, double m3, double sxt, double syt)
 {
-    // the largest eigenvalue only steers two threshold tests, so a float
-    // square root is enough (the reference compares sigma1 with minDet and
-    // the branch point is a conditioning bound)
-    double hd = 0.5 * (a - d);
-    double l1 = 0.5 * (a + d) + (double)sqrtf((float)(hd * hd + b * b));
-    double det = a * d - b * b;
-    if (det > 1e-3 * l1 * l1) {
-        if (l1 < min_det) return false;
-        double inv = 1.0 / det;
-        M[0] = d * inv; M[1] = -b * inv; M[2] = -b * inv; M[3] = a * inv;
-        return true;
-    }
+    double u = m0 * sxt + m1 * syt, v = m2 * sxt + m3 * syt;
+    if (isnan(u)) u = 0;
+    if (isnan(v)) v = 0;
+    return make_float2((float)((double)f.x + u), (float)((double)f.y + v));
+}
+
+// The ill-conditioned branch: the reference's angle/singular-value
+// construction. Out of line: it is rarely taken, and inlined at every solve
+// it would multiply the code of the per-pixel kernels.
+__device__ __noinline__ float2 lk_update_svd(float2 f, double a, double b, double d, double sxt, double syt, double min_det)
+{
     const double c = b;
     double th = 0.5 * atan2(2 * a * c + 2 * b * d, a * a + b * b - c * c - d * d);
     double ct = cos(th), st = sin(th);
     double S1 = a * a + b * b + c * c + d * d;
     double S2 = sqrt((a * a + b * b - c * c - d * d) * (a * a + b * b - c * c - d * d) + 4 * (a * c + b * d) * (a * c + b * d));
     double s1 = sqrt((S1 + S2) / 2), s2 = sqrt((S1 - S2) / 2);
-    if (s1 < min_det) return false;
+    if (s1 < min_det) return f;
     s1 = s1 != 0 ? 1 / s1 : 0;
     s2 = s2 != 0 ? 1 / s2 : 0;
     double ep = 0.5 * atan2(2 * a * b + 2 * c * d, a * a - b * b + c * c - d * d);
@@ -66,21 +69,23 @@ __device__ __forceinline__ bool lk_pinv(double a, double b, double d, double min
     q22 = q22 > 0 ? 1 : (q22 < 0 ? -1 : 0);
     double V0 = q11 * ce, V1 = -q22 * se, V2 = q11 * se, V3 = q22 * ce;
     double m0 = s1 * ct, m1 = s1 * st, m2 = s2 * -st, m3 = s2 * ct;
-    M[0] = V0 * m0 + V1 * m2;
-    M[1] = V0 * m1 + V1 * m3;
-    M[2] = V2 * m0 + V3 * m2;
-    M[3] = V2 * m1 + V3 * m3;
-    return true;
+    return lk_apply(f, V0 * m0 + V1 * m2, V0 * m1 + V1 * m3, V2 * m0 + V3 * m2, V2 * m1 + V3 * m3, sxt, syt);
 }
 
-__device__ __forceinline__ float2 lk_update(float2 f, double sxx, double sxy, double syy, double sxt, double syt, double min_det)
+__device__ __forceinline__ float2 lk_update(float2 f, double a, double b, double d, double sxt, double syt, double min_det)
 {
-    double M[4];
-    if (!lk_pinv(sxx, sxy, syy, min_det, M)) return f;
-    double u = M[0] * sxt + M[1] * syt, v = M[2] * sxt + M[3] * syt;
-    if (isnan(u)) u = 0;
-    if (isnan(v)) v = 0;
-    return make_float2((float)((double)f.x + u), (float)((double)f.y + v));
+    // the largest eigenvalue only steers two threshold tests, so a float
+    // square root is enough (the reference compares sigma1 with minDet and
+    // the branch point is a conditioning bound)
+    double hd = 0.5 * (a - d);
+    double l1 = 0.5 * (a + d) + (double)sqrtf((float)(hd * hd + b * b));
+    double det = a * d - b * b;
+    if (det > 1e-3 * l1 * l1) {
+        if (l1 < min_det) return f;
+        double inv = 1.0 / det;
+        return lk_apply(f, d * inv, -b * inv, -b * inv, a * inv, sxt, syt);
+    }
+    return lk_update_svd(f, a, b, d, sxt, syt, min_det);
 }
 
 // c, s: cosine and sine of the pre-alignment rotation (uniform, computed once
@@ -192,145 +197,223 @@ __global__ void k_lk_sums(float2* flow, size_t flow_pitch, const float* __restri
 }
 
 // Streaming form of one reference iteration (warp, Set(0) x3, derivatives,
-// lucasKanadeOptim). A CTA of LKS_NT threads owns a vertical strip: thread t
-// owns image column x0 - R + t (R = h + 2, mirrored at the border) and walks
-// down the strip one row at a time:
-//   1. the warped source and the reference at (column, row) go into a
-//      six-row ring in shared memory (one row more than the derivatives
-//      read, so a slot is rewritten only after the next row's barrier and
-//      the step needs no barrier at its end); the global loads for the next
-//      rows are issued one and two rows ahead (flow, then the bilinear
-//      samples);
-//   2. five-tap derivatives at the ring's centre row (neighbouring columns
-//      from shared memory), FP32 products, and per-column vertical window
-//      sums in FP64 registers (the product leaving the window comes from a
-//      per-thread ring of the last 2h + 1 rows);
-//   3. every two output rows, the row window sums (sliding FP64 sums over
-//      2h + 1 columns, two pixels per thread) and the 2x2 solve.
+// lucasKanadeOptim). A CTA of LKS_NT threads owns a vertical strip of LKS_NT
+// columns (SW = LKS_NT - 2R output columns, R = h + 2) and `sh` output rows:
+// thread t owns image column x0 - R + t (mirrored at the border) and walks
+// down the strip two rows per step:
+//   1. the warped source and the reference of the two rows go into a ring of
+//      six rows of (warped, reference) pairs in shared memory; the global
+//      loads of the next two rows are issued one step ahead (bilinear
+//      samples) and two steps ahead (flow);
+//   2. after a barrier, five-tap derivatives at the two centre rows (own
+//      column and neighbours from the ring), FP32 products, and per-column
+//      vertical window sums in FP64 registers (the product leaving the
+//      window comes from a shared ring of the last 2h + 1 product rows that
+//      only its own thread touches);
+//   3. after a second barrier, the row window sums of the two output rows
+//      (2h + 1 columns, two pixels per thread, FP64) and the 2x2 solve.
 // The FP64 sums hold the FP32 products exactly enough that the order of
-// summation does not matter at FP32 output precision.
-constexpr int LKS_NT = 128, LKS_SH = 64;
+// summation does not matter at FP32 output precision. Threads at the strip's
+// edges (t < 2, t >= LKS_NT - 2) compute products from padding; their column
+// sums are never read.
+constexpr int LKS_NT = 128, LKS_PX = 2;
 
 template <int H>
 struct LkStream {
     static constexpr int R = H + 2, SW = LKS_NT - 2 * R, WIN = 2 * H + 1;
-    static constexpr int NSEG = (SW + 1) / 2;
-    static constexpr size_t E_BYTES = (size_t)2 * 6 * LKS_NT * 4;
-    static constexpr size_t P_BYTES = (size_t)WIN * 5 * LKS_NT * 4;
-    static constexpr size_t OFF_P = E_BYTES, OFF_C = (OFF_P + P_BYTES + 15) / 16 * 16;
+    static constexpr int PX = LKS_PX, NSEG = (SW + PX - 1) / PX;  // row-sum phase: PX output pixels per thread, NSEG threads per row
+    static_assert(SW > 0 && SW % 2 == 0 && PX % 2 == 0 && 2 * NSEG <= LKS_NT, "two output rows of PX-pixel segments per step");
+    static_assert(SW - 2 + WIN + PX <= LKS_NT, "the last segment's window stays inside its row of column sums");
+    static constexpr int EPAD = 2;  // float2 either side of the pair ring: the edge threads' taps stay in shared memory
+    static constexpr size_t OFF_P4 = (size_t)(6 * LKS_NT + 2 * EPAD) * 8;           // [WIN][NT] float4: products 0-3
+    static constexpr size_t OFF_P1 = OFF_P4 + (size_t)WIN * LKS_NT * 16;            // [WIN][NT] float: product 4
+    static constexpr size_t OFF_C = (OFF_P1 + (size_t)WIN * LKS_NT * 4 + 15) / 16 * 16;  // [2][5][NT] double: column sums
     static constexpr size_t TOTAL = OFF_C + (size_t)2 * 5 * LKS_NT * 8;
 };
 
+// Bilinear source samples of one row (mirror addressing) and the reference texel.
+struct LkTaps {
+    float s00, s10, s01, s11, a, b, r;
+};
+
 template <int H>
-__global__ void __launch_bounds__(LKS_NT) k_lk_stream(const float2* __restrict__ flow_in, float2* __restrict__ flow_out, size_t flow_pitch,
-                                                      const float* __restrict__ src, const float* __restrict__ ref, size_t img_pitch, int W,
-                                                      int Himg, float min_det)
+__global__ void __launch_bounds__(LKS_NT, 512 / LKS_NT) k_lk_stream(const float2* __restrict__ flow_in, float2* __restrict__ flow_out, size_t flow_pitch,
+                                                         const float* __restrict__ src, const float* __restrict__ ref, size_t img_pitch, int W,
+                                                         int Himg, int sh, float min_det)
 {
     using L = LkStream<H>;
-    constexpr int R = L::R, SW = L::SW, WIN = L::WIN, NT = LKS_NT;
+    constexpr int R = L::R, SW = L::SW, WIN = L::WIN, NT = LKS_NT, NSEG = L::NSEG, PX = L::PX;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* Ew = (float*)smem;            // [6][NT]
-    float* Er = Ew + 6 * NT;              // [6][NT]
-    float* Pr = (float*)(smem + L::OFF_P);    // [WIN][5][NT]
-    double* Cs = (double*)(smem + L::OFF_C);  // [2][5][NT]
+    float2* E = (float2*)smem + L::EPAD;              // [6][NT] (warped source, reference), three two-row slots
+    float4* P4 = (float4*)(smem + L::OFF_P4);
+    float* P1 = (float*)(smem + L::OFF_P1);
+    double* Cs = (double*)(smem + L::OFF_C);
     const int t = threadIdx.x;
-    const int x0 = blockIdx.x * SW, y0 = blockIdx.y * LKS_SH;
-    const int nout = min(LKS_SH, Himg - y0);
-    const int nE = nout + 2 * R;
+    const int x0 = blockIdx.x * SW, y0 = blockIdx.y * sh;
+    const int nout = min(sh, Himg - y0);
+    const int nsteps = (nout + 2 * R + 1) / 2;  // rows 0 .. 2 nsteps - 1 of the strip (one extra, mirrored, when nout is odd)
     const int col = isa::mirror(x0 - R + t, W);
-    // pipeline: flow two rows ahead, bilinear samples one row ahead
-    float2 fnext;
-    float s00, s10, s01, s11, sa, sb, sref;
+    const float* refc = ref + col;
+    const float2* flc = flow_in + col;
     const auto erow = [&](int e) { return isa::mirror(y0 - R + e, Himg); };
-    const auto issue_samples = [&](int row, float2 f) {
+    const auto flow_at = [&](int e) { return __ldg(isa::row_ptr(flc, flow_pitch, erow(e))); };
+    const auto sample = [&](int e, float2 f, LkTaps& q) {
+        const int row = erow(e);
         const float flx = floorf(f.x), fly = floorf(f.y);
         const int ix = col + (int)flx, iy = row + (int)fly;
-        sa = f.x - flx;
-        sb = f.y - fly;
-        const int xa = isa::mirror(ix, W), xb = isa::mirror(ix + 1, W);
-        const float* r0 = isa::row_ptr(src, img_pitch, isa::mirror(iy, Himg));
-        const float* r1 = isa::row_ptr(src, img_pitch, isa::mirror(iy + 1, Himg));
-        s00 = __ldg(r0 + xa); s10 = __ldg(r0 + xb); s01 = __ldg(r1 + xa); s11 = __ldg(r1 + xb);
-        sref = __ldg(isa::row_ptr(ref, img_pitch, row) + col);
-    };
-    issue_samples(erow(0), __ldg(isa::row_ptr(flow_in, flow_pitch, erow(0)) + col));
-    if (nE > 1) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(1)) + col);
-    double cs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    // ring slots of rows e, e-1, e-2, e-3, e-4 (mod 5) and of the product row (mod WIN), advanced incrementally
-    int r0 = 0, r1 = 5, r2 = 4, r3 = 3, r4 = 2, pw = 0;
-    for (int e = 0; e < nE; e++) {
-        Ew[r0 * NT + t] = isa::lerp2(s00, s10, s01, s11, sa, sb);
-        Er[r0 * NT + t] = sref;
-        if (e + 1 < nE) {
-            issue_samples(erow(e + 1), fnext);
-            if (e + 2 < nE) fnext = __ldg(isa::row_ptr(flow_in, flow_pitch, erow(e + 2)) + col);
+        q.a = f.x - flx;
+        q.b = f.y - fly;
+        if ((unsigned)ix < (unsigned)(W - 1) && (unsigned)iy < (unsigned)(Himg - 1)) {
+            const float* p0 = isa::row_ptr(src, img_pitch, iy) + ix;
+            const float* p1 = isa::row_ptr(p0, img_pitch, 1);
+            q.s00 = __ldg(p0); q.s10 = __ldg(p0 + 1); q.s01 = __ldg(p1); q.s11 = __ldg(p1 + 1);
+        } else {
+            const int xa = isa::mirror(ix, W), xb = isa::mirror(ix + 1, W);
+            const float* r0 = isa::row_ptr(src, img_pitch, isa::mirror(iy, Himg));
+            const float* r1 = isa::row_ptr(src, img_pitch, isa::mirror(iy + 1, Himg));
+            q.s00 = __ldg(r0 + xa); q.s10 = __ldg(r0 + xb); q.s01 = __ldg(r1 + xa); q.s11 = __ldg(r1 + xb);
         }
+        q.r = __ldg(isa::row_ptr(refc, img_pitch, row));
+    };
+    LkTaps qa, qb;
+    sample(0, flow_at(0), qa);
+    sample(1, flow_at(1), qb);
+    float2 fa = flow_at(2), fb = flow_at(3);
+    // the product ring starts at zero: the first 2h + 1 rows subtract nothing
+#pragma unroll 1
+    for (int k = 0; k < WIN; k++) {
+        P4[k * NT + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        P1[k * NT + t] = 0.f;
+    }
+    double cs[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    int pw = 0;                                 // product ring slot of the next product row
+    int sn = 0, s2 = 2 * NT, s1 = 4 * NT;       // pair slots: rows 2s, 2s+1 / 2s-4, 2s-3 / 2s-2, 2s-1
+    // row-sum phase: thread t < 2 NSEG sums output row (t / NSEG) of the step at columns j0 .. j0 + PX - 1
+    const int rr = t / NSEG, j0 = PX * (t - rr * NSEG);
+    const bool summer = t < 2 * NSEG;
+
+    // one product row: the centre row's pairs at c (neighbours in the ring) and above/below it in the own column
+    const auto product_row = [&](const float2* c, float2 vm2, float2 vm1, float2 vp1, float2 vp2) {
+        const float2 cm2 = c[-2], cm1 = c[-1], c0 = c[0], cp1 = c[1], cp2 = c[2];
+        // five-tap derivatives averaged over both images: ((8 (c[-1] - c[1]) + c[2] - c[-2]) / 12 of each) / 2
+        const float gx = (cp2.x - cm2.x) + (cp2.y - cm2.y) + 8.0f * ((cm1.x - cp1.x) + (cm1.y - cp1.y));
+        const float gy = (vp2.x - vm2.x) + (vp2.y - vm2.y) + 8.0f * ((vm1.x - vp1.x) + (vm1.y - vp1.y));
+        const float dx = gx * (1.0f / 24.0f), dy = gy * (1.0f / 24.0f);
+        const float dt = c0.x - c0.y;
+        const float p0 = dx * dx, p1 = dx * dy, p2 = dy * dy, p3 = dx * dt, p4 = dy * dt;
+        const float4 o4 = P4[pw * NT + t];
+        const float o1 = P1[pw * NT + t];
+        cs[0] += (double)p0 - (double)o4.x;
+        cs[1] += (double)p1 - (double)o4.y;
+        cs[2] += (double)p2 - (double)o4.z;
+        cs[3] += (double)p3 - (double)o4.w;
+        cs[4] += (double)p4 - (double)o1;
+        P4[pw * NT + t] = make_float4(p0, p1, p2, p3);
+        P1[pw * NT + t] = p4;
+        pw = pw + 1 == WIN ? 0 : pw + 1;
+    };
+    // one step: rows 2s, 2s+1 into the ring, then (DER) product rows of centres 2s-2, 2s-1, then (OUT) output rows 2s-4-2h, 2s-3-2h
+    const auto step = [&](int s, auto der, auto out) {
+        float2* en = E + sn;
+        en[t] = make_float2(isa::lerp2(qa.s00, qa.s10, qa.s01, qa.s11, qa.a, qa.b), qa.r);
+        en[NT + t] = make_float2(isa::lerp2(qb.s00, qb.s10, qb.s01, qb.s11, qb.a, qb.b), qb.r);
+        sample(2 * s + 2, fa, qa);
+        sample(2 * s + 3, fb, qb);
+        fa = flow_at(2 * s + 4);
+        fb = flow_at(2 * s + 5);
         __syncthreads();
-        if (e >= 4) {
-            const int gi = e - 4;  // product row: image row y0 - h + gi
-            if (t >= 2 && t < NT - 2) {
-                // five-tap derivatives averaged over both images: ((8 (c[-1] - c[1]) + c[2] - c[-2]) / 12 of each) / 2
-                const float* ew = Ew + r2 * NT + t;
-                const float* er = Er + r2 * NT + t;
-                const float gx = (ew[2] - ew[-2]) + (er[2] - er[-2]) + 8.0f * ((ew[-1] - ew[1]) + (er[-1] - er[1]));
-                const float gy = (Ew[r0 * NT + t] - Ew[r4 * NT + t]) + (Er[r0 * NT + t] - Er[r4 * NT + t]) +
-                                 8.0f * ((Ew[r3 * NT + t] - Ew[r1 * NT + t]) + (Er[r3 * NT + t] - Er[r1 * NT + t]));
-                const float dx = gx * (1.0f / 24.0f), dy = gy * (1.0f / 24.0f);
-                const float dt = ew[0] - er[0];
-                const float p[5] = {dx * dx, dx * dy, dy * dy, dx * dt, dy * dt};
-                float* pr = Pr + pw * 5 * NT + t;
+        if constexpr (decltype(der)::value) {
+            const float2* e2 = E + s2 + t;  // rows 2s-4, 2s-3
+            const float2* e1 = E + s1 + t;  // rows 2s-2, 2s-1 (the centres)
+            const float2 v0 = e2[0], v1 = e2[NT], v4 = en[t], v5 = en[NT + t];
+            const float2 v2 = e1[0], v3 = e1[NT];
+            product_row(e1, v0, v1, v3, v4);
+            if constexpr (decltype(out)::value) {
 #pragma unroll
-                for (int ch = 0; ch < 5; ch++) {
-                    const float old = gi >= WIN ? pr[ch * NT] : 0.f;
-                    cs[ch] += (double)p[ch] - (double)old;
-                    pr[ch * NT] = p[ch];
-                }
+                for (int ch = 0; ch < 5; ch++) Cs[ch * NT + t] = cs[ch];
             }
-            pw = pw + 1 == WIN ? 0 : pw + 1;
-            if (gi >= 2 * H) {
-                const int o = gi - 2 * H;  // output row y0 + o
-                if (t >= 2 && t < NT - 2) {
+            product_row(e1 + NT, v1, v2, v4, v5);
+            if constexpr (decltype(out)::value) {
 #pragma unroll
-                    for (int ch = 0; ch < 5; ch++) Cs[((o & 1) * 5 + ch) * NT + t] = cs[ch];
-                }
-                if ((o & 1) || o == nout - 1) {
-                    __syncthreads();
-                    const int rlo = o & ~1, nr = o - rlo + 1;
-                    if (t < nr * L::NSEG) {
-                        const int r = rlo + t / L::NSEG, j0 = 2 * (t % L::NSEG);
-                        const double* cr = Cs + (r & 1) * 5 * NT + j0 + 2;
-                        double v0[5], v1[5];
+                for (int ch = 0; ch < 5; ch++) Cs[(5 + ch) * NT + t] = cs[ch];
+                __syncthreads();
+                const int y = y0 + 2 * s - 4 - 2 * H + rr;  // output row
+                const int x = x0 + j0;
+                if (summer && y < y0 + nout && x < W) {
+                    const float2* irow = isa::row_ptr(flow_in, flow_pitch, y) + x;
+                    float2 fin[PX];
 #pragma unroll
-                        for (int ch = 0; ch < 5; ch++) {
-                            const double* c = cr + ch * NT;
-                            double s = 0.0;
+                    for (int k = 0; k < PX; k++) fin[k] = j0 + k < SW && x + k < W ? __ldg(irow + k) : make_float2(0.f, 0.f);
+                    // window sums of pixel j0 (2h + 1 columns from j0 + 2), then sliding by one column per pixel
+                    const double* cr = Cs + rr * 5 * NT + j0 + 2;
+                    double v[PX][5];
 #pragma unroll
-                            for (int d = 0; d < WIN; d++) s += c[d];
-                            v0[ch] = s;
-                            v1[ch] = s + (c[WIN] - c[0]);
-                        }
-                        const int y = y0 + r;
-                        const bool yin = y >= H && y < Himg - H;
-                        float2* orow = isa::row_ptr(flow_out, flow_pitch, y);
-                        const float2* irow = isa::row_ptr(flow_in, flow_pitch, y);
-                        int x = x0 + j0;
-                        if (j0 < SW && x < W) {
-                            float2 f = __ldg(irow + x);
-                            if (yin && x >= H && x < W - H) f = lk_update(f, v0[0], v0[1], v0[2], v0[3], v0[4], min_det);
-                            orow[x] = f;
-                        }
-                        x++;
-                        if (j0 + 1 < SW && x < W) {
-                            float2 f = __ldg(irow + x);
-                            if (yin && x >= H && x < W - H) f = lk_update(f, v1[0], v1[1], v1[2], v1[3], v1[4], min_det);
-                            orow[x] = f;
-                        }
+                    for (int ch = 0; ch < 5; ch++) {
+                        const double* c = cr + ch * NT;
+                        double sum = 0.0;
+#pragma unroll
+                        for (int d = 0; d < WIN; d++) sum += c[d];
+                        v[0][ch] = sum;
+#pragma unroll
+                        for (int k = 1; k < PX; k++) v[k][ch] = sum = sum + (c[WIN + k - 1] - c[k - 1]);
+                    }
+                    const bool yin = y >= H && y < Himg - H;
+                    float2* orow = isa::row_ptr(flow_out, flow_pitch, y) + x;
+#pragma unroll
+                    for (int k = 0; k < PX; k++) {
+                        const int xk = x + k;
+                        if (j0 + k < SW && xk < W)
+                            orow[k] = yin && xk >= H && xk < W - H ? lk_update(fin[k], v[k][0], v[k][1], v[k][2], v[k][3], v[k][4], min_det) : fin[k];
                     }
                 }
+            } else {
+                __syncthreads();  // the next step overwrites rows 2s-4, 2s-3
             }
         }
-        r4 = r3; r3 = r2; r2 = r1; r1 = r0; r0 = r0 + 1 == 6 ? 0 : r0 + 1;
+        const int tmp = s2;
+        s2 = s1;
+        s1 = sn;
+        sn = tmp;
+    };
+    using T_ = std::true_type;
+    using F_ = std::false_type;
+    int s = 0;
+#pragma unroll 1
+    for (; s < 2; s++) step(s, F_{}, F_{});
+#pragma unroll 1
+    for (; s < R; s++) step(s, T_{}, F_{});
+#pragma unroll 1
+    for (; s < nsteps; s++) step(s, T_{}, T_{});
+}
+
+// Strip height: the grid of (column strips x row strips) CTAs should fill
+// whole waves of the CTAs resident on the device; a CTA's time grows with its
+// rows plus the 2R halo rows.
+template <int H>
+int lk_strip_rows(int W, int Himg)
+{
+    using L = LkStream<H>;
+    static int slots_by_dev[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 64;
+    int slots = slots_by_dev[dev];
+    if (slots <= 0) {
+        int nsm = 0, occ = 0;
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_lk_stream<H>, LKS_NT, L::TOTAL) != cudaSuccess || nsm * occ <= 0)
+            return 64;
+        slots = slots_by_dev[dev] = nsm * occ;
     }
+    const long nx = (W + L::SW - 1) / L::SW;
+    int best = 64;
+    long best_cost = -1;
+    for (int sh = 32; sh <= 192; sh += 2) {
+        const long ny = (Himg + sh - 1) / sh;
+        const long waves = (nx * ny + slots - 1) / slots;
+        const long cost = waves * (std::min(sh, Himg) + 2 * L::R);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = sh; }
+    }
+    return best;
 }
 
 template <int H>
@@ -340,8 +423,9 @@ cudaError_t launch_lk(const float2* flow_in, float2* flow_out, size_t flow_pitch
     using L = LkStream<H>;
     cudaError_t e = cudaFuncSetAttribute(k_lk_stream<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL);
     if (e != cudaSuccess) return e;
-    dim3 g((W + L::SW - 1) / L::SW, (Himg + LKS_SH - 1) / LKS_SH);
-    k_lk_stream<H><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, min_det);
+    const int sh = lk_strip_rows<H>(W, Himg);
+    dim3 g((W + L::SW - 1) / L::SW, (Himg + sh - 1) / sh);
+    k_lk_stream<H><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, sh, min_det);
     return cudaGetLastError();
 }
 

@@ -23,7 +23,7 @@ ISA_DEV int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : 
 // Mirror addressing of a CUDA texture: reflect the texel index with the
 // edge texel repeated (period 2n).
 ISA_DEV int mirror(int i, int n) {
-    if (i >= 0 && i < n) return i;
+    if ((unsigned)i < (unsigned)n) return i;
     int p = 2 * n;
     int j = i % p;
     if (j < 0) j += p;
