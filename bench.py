@@ -205,7 +205,7 @@ def adjoint_ratio(args):
     the differentiable-merge workload, device time per call, same warm-up and
     step counts as the main measurement."""
     import torch
-    from imagestackalignator_b200 import isa, synthetic
+    from imagestackalignator_b200 import isa, params as P, synthetic
     W, H, n = ADJ["width"], ADJ["height"], ADJ["frames"]
     b = synthetic.make_burst(W, H, n, seed=2000, max_shift=WORKLOAD["max_shift"], max_rot_deg=WORKLOAD["max_rot_deg"],
                              noise_a=WORKLOAD["noise_a"], noise_b=WORKLOAD["noise_b"], device="cuda")
@@ -233,8 +233,18 @@ def adjoint_ratio(args):
     fwd = timed(lambda: m.merge(raw, info, out))
     both = timed(lambda: m.backward(raw, info, target, out=out))
     m.close()
+    # sample mode BILINEAR: the same, plus the gradient of every frame's tile flow (isa_merge_backward_tiles)
+    pb = merge_params()
+    pb.merge_scale = ADJ["scale"]
+    pb.sample_mode = P.SAMPLE_BILINEAR
+    mb = isa.Merger(W, H, n, pb)
+    fwd_b = timed(lambda: mb.merge(raw, info, out))
+    both_b = timed(lambda: mb.backward_tiles(raw, info, target, out=out))
+    mb.close()
     return {"workload": f"{n}x{W}x{H} merged at {ADJ['scale']}x, L2 loss, gradients of the 8 merge parameters", "fwd_ms": fwd,
-            "fwd_adj_ms": both, "ratio": both / fwd}
+            "fwd_adj_ms": both, "ratio": both / fwd,
+            "bilinear": {"workload": "sample mode BILINEAR, gradients of the 8 merge parameters and of every frame's tile flow",
+                         "fwd_ms": fwd_b, "fwd_adj_tiles_ms": both_b, "ratio": both_b / fwd_b}}
 
 
 BATCH = dict(width=2048, height=1536, frames=8, bursts=16, contexts=4)  # many small bursts (phone-sized) merged at 2x

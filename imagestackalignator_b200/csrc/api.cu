@@ -226,13 +226,22 @@ struct isa_ctx {
     // caller-owned record of every level's tile search (isa_debug_track_record), or null
     int* track_rec = nullptr;
     size_t track_rec_bytes = 0;
+    // caller-owned per-frame tile flows that replace the solved ones (isa_set_tile_flow), or null
+    const float2* tile_override = nullptr;
+    // sample mode BILINEAR only: scratch of the flow adjoint (isa_merge_backward_tiles), 25 floats per frame pixel
+    float* adj_flow = nullptr;
     // last call
-    int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0;
+    int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0, last_ref = 0;
 };
 
 namespace {
 
 size_t bw_pitch(int W) { return (size_t)W * sizeof(float); }
+
+// floats per frame pixel of the flow adjoint's scratch: the recomputed flows of the LK iterations before the last (3 x 2), the
+// warped source (1), the window-sum gradients and their box sums (5 + 5), the derivative gradients (3), the flow gradient
+// ping-pong (2 x 2) and the half-res mask gradient (4 per half-res pixel = 1 per frame pixel)
+constexpr size_t kAdjFlowFloats = 25;
 
 int level_tiles(const isa_level& l, int W, int H, int* tcx, int* tcy)
 {
@@ -257,6 +266,7 @@ int check_params(const isa_params* p)
     if (p->iterations_lk < 0) return fail(ISA_EINVAL, "iterations_lk < 0");
     if (p->tracking_strategy < 0 || p->tracking_strategy > 3) return fail(ISA_EINVAL, "tracking_strategy %d", p->tracking_strategy);
     if (p->merge_scale < 0 || p->merge_scale > 8) return fail(ISA_EINVAL, "merge_scale %g out of range", p->merge_scale);
+    if (p->sample_mode != ISA_SAMPLE_ROUND && p->sample_mode != ISA_SAMPLE_BILINEAR) return fail(ISA_EINVAL, "sample_mode %d", p->sample_mode);
     return ISA_OK;
 }
 
@@ -265,6 +275,7 @@ void accum_geom(const isa_params* p, int W, int H, isa_accum_geom& g, float& thr
 {
     g.W = W; g.H = H;
     g.masks_finite = 0;
+    g.bilinear = p->sample_mode == ISA_SAMPLE_BILINEAR;
     if (p->merge_scale > 0) {
         g.s = p->merge_scale;
         g.Wo = (int)std::lround(W * (double)p->merge_scale);
@@ -571,13 +582,17 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         if (i == ref) continue;
         float2* flow = c->flows + (size_t)i * fsz;
         ISA_LAUNCH(c, isa_launch_subsample(frame(i), raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
-        ISA_LAUNCH(c, isa_launch_optimal(c->x, strat.n1, tcx0, tcy0, ref, i, c->tiles_opt, (size_t)tcx0 * sizeof(float2), st));
+        const float2* tiles = c->tiles_opt;
+        if (c->tile_override)
+            tiles = c->tile_override + (size_t)i * tcx0 * tcy0;
+        else
+            ISA_LAUNCH(c, isa_launch_optimal(c->x, strat.n1, tcx0, tcy0, ref, i, c->tiles_opt, (size_t)tcx0 * sizeof(float2), st));
         float bs[2];
         prealign_shift(pre, ref, i, bs);
         // ping-pong so that the last iteration lands in `flow`
         float2* a = (p->iterations_lk & 1) ? c->flow_tmp : flow;
         float2* b = (p->iterations_lk & 1) ? flow : c->flow_tmp;
-        ISA_LAUNCH(c, isa_launch_flow_from_tiles(c->tiles_opt, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1], prealign_rot(pre, ref, i),
+        ISA_LAUNCH(c, isa_launch_flow_from_tiles(tiles, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1], prealign_rot(pre, ref, i),
                                           a, fp, st));
         for (int it = 0; it < p->iterations_lk; it++) {
             ISA_LAUNCH(c, isa_launch_lk_iteration(a, b, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, pitch, W, H, half, p->min_det_lk, st));
@@ -587,7 +602,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         ISA_LAUNCH(c, isa_launch_box3(c->half_mov, hp3, Wh, Hh, c->mov_box, hp4, st));
         ISA_LAUNCH(c, isa_launch_robustness_erode_tabs(c->ref_mr, c->ref_sr, c->mov_box, hp4, c->half_mov, hp3, Wh, Hh, flow, fp, W, H,
                                                        info->noise_alpha, info->noise_beta, p->threshold_m, p->robust_s, p->robust_t,
-                                                       p->erode_size, mask, hp4, st));
+                                                       p->erode_size, mask, hp4, p->sample_mode == ISA_SAMPLE_BILINEAR, st));
         fin.push_back({frame(i), flow, mask});
     }
     ISA_TRY(mark());
@@ -629,7 +644,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         // the caller's stream completes only when the image has left the device
         ISA_CK(cudaEventRecord(c->ev_copied, c->copy_stream));
         ISA_CK(cudaStreamWaitEvent(st, c->ev_copied, 0));
-        c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1;
+        c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1; c->last_ref = ref;
         return ISA_OK;
     }
     if (p->fused_accumulate) {
@@ -648,7 +663,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         ISA_LAUNCH(c, isa_launch_demosaic_gray(frame(ref), raw_pitch, W, H, cfa, black, scale, divisor, nullptr, 0, nullptr, 0, out, out_pitch, st));
     ISA_LAUNCH(c, isa_launch_apply_weighting(out, out_pitch, c->acc, c->wsum, op, g.Wo, g.Ho, thr, st));
     ISA_TRY(mark());
-    c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1;
+    c->last_w = W; c->last_h = H; c->last_n = n; c->last_tcx0 = tcx0; c->last_tcy0 = tcy0; c->last_n1 = strat.n1; c->last_ref = ref;
     return ISA_OK;
 }
 
@@ -783,6 +798,7 @@ void isa_params_default(isa_params* p)
     p->robust_s = 1.5f;
     p->robust_t = 0.12f;
     p->fused_accumulate = 1;
+    p->sample_mode = ISA_SAMPLE_ROUND;
 }
 
 int isa_output_size(const isa_params* p, int width, int height, int* ow, int* oh)
@@ -870,6 +886,7 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     add((void**)&c->tw_rows, (size_t)(max_w / 2) * sizeof(float2));
     add((void**)&c->tw_unpack, (size_t)(max_w / 2 + 1) * sizeof(float2));
     add((void**)&c->tw_cols, (size_t)max_h * sizeof(float2));
+    if (p->sample_mode == ISA_SAMPLE_BILINEAR) add((void**)&c->adj_flow, fsz * kAdjFlowFloats * sizeof(float));
     size_t total = 0;
     for (auto& e : plan) total += e.second;
     if (cudaMalloc(&c->arena, total) != cudaSuccess) {
@@ -933,9 +950,13 @@ int isa_merge_burst(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t fr
     return run_merge(c, raw, raw_pitch, frame_stride, n, info, pre, out, out_pitch, S(stream));
 }
 
-int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
-                       const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch, float* out,
-                       size_t out_pitch, double* loss, double* grad, void* stream)
+namespace {
+
+// Forward merge, then the adjoint of the weighted L2 loss: the eight parameter gradients, and with tile_grad (sample
+// mode BILINEAR) the gradient of every frame's tile flow.
+int merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                   const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch, float* out,
+                   size_t out_pitch, double* loss, double* grad, float* tile_grad, cudaStream_t st)
 {
     if (!c || !raw || !target || !out || !loss || !grad) return fail(ISA_EINVAL, "NULL argument");
     ISA_TRY(check_info(info));
@@ -948,7 +969,12 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
     if (!p->fused_accumulate) return fail(ISA_EINVAL, "the adjoint needs fused_accumulate");
     if (target_pitch < (size_t)g.Wo * 12) return fail(ISA_EINVAL, "target pitch %zu < %d", target_pitch, g.Wo * 12);
     if (weight && weight_pitch < (size_t)g.Wo * 4) return fail(ISA_EINVAL, "weight pitch %zu < %d", weight_pitch, g.Wo * 4);
-    cudaStream_t st = S(stream);
+    if (tile_grad) {
+        if (p->sample_mode != ISA_SAMPLE_BILINEAR || !c->adj_flow)
+            return fail(ISA_EINVAL, "the tile-flow gradient needs a context created with sample_mode ISA_SAMPLE_BILINEAR");
+        if (p->iterations_lk > 3) return fail(ISA_EINVAL, "the tile-flow gradient covers up to 3 LK iterations (%d)", p->iterations_lk);
+        if (((uintptr_t)tile_grad & 7) != 0) return fail(ISA_EINVAL, "tile_grad must be 8-byte aligned");
+    }
     // forward (keeps flows, masks, kernel parameters, structure tensor, sums and the frame table)
     ISA_TRY(run_merge(c, raw, raw_pitch, frame_stride, n, info, pre, out, out_pitch, st));
     const size_t fsz = (size_t)W * H;
@@ -957,13 +983,23 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
                  p4 = (size_t)W * 16, op = (size_t)g.Wo * 12;
     // scratch of the adjoint in buffers the forward has finished with: the FFT / Gauss scratch (fsz x 12 B) takes the
     // kernel-parameter gradients, the tracking images (n x fsz x 4 B) the mask-certainty gradients of every frame, the
-    // LK ping-pong flow (fsz x 8 B) the recomputed mask and its auxiliaries, the accumulation images the routed
-    // gradient; none of them is read again before the next merge
+    // LK ping-pong flow (fsz x 8 B) the recomputed mask and its auxiliaries, the accumulation images (or, for the
+    // tile-flow gradient, whose LK recomputation reads them, the flow adjoint's scratch) the routed gradient; none of
+    // them is read again before the next merge
     float* adj_gkp = c->tmp;
     float4* adj_gmask = (float4*)c->bw_track;
     float4* adj_m = (float4*)c->flow_tmp;
     float4* adj_aux = (float4*)((char*)c->flow_tmp + hsz * 16);
-    float4* adj_gm = (float4*)c->bw_acc;
+    // flow adjoint scratch (floats per frame pixel, kAdjFlowFloats in all)
+    float* sc = c->adj_flow;
+    float2* F[3] = {(float2*)sc, (float2*)(sc + 2 * fsz), (float2*)(sc + 4 * fsz)};
+    float* wplane = sc + 6 * fsz;
+    float* a5 = sc + 7 * fsz;
+    float* A5 = sc + 12 * fsz;
+    float* gd3 = sc + 17 * fsz;
+    float2* gA = (float2*)(sc + 20 * fsz);
+    float2* gB = (float2*)(sc + 22 * fsz);
+    float4* adj_gm = tile_grad ? (float4*)(sc + 24 * fsz) : (float4*)c->bw_acc;
     ISA_CK(cudaMemsetAsync(adj_gkp, 0, fsz * 12, st));
     ISA_CK(cudaMemsetAsync(adj_gmask, 0, hsz * 16 * n, st));
     ISA_CK(cudaMemsetAsync(c->adj_acc, 0, 16 * sizeof(double), st));
@@ -971,35 +1007,95 @@ int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t
     color_consts(info, black, white, scale, divisor);
     const unsigned cfa = pack_cfa(info->cfa);
     const int ref = pre ? pre->reference : 0;
-    // output -> kernel parameters and mask certainties (all frames at once)
-    ISA_LAUNCH(c, isa_launch_accumulate_bwd(g, cfa, c->frame_in, n, raw_pitch, fp, hp4, c->kparam, p4, white, black, out, out_pitch, c->wsum, op, target,
-                                            target_pitch, weight, weight_pitch, adj_gkp, adj_gmask, hsz, c->adj_acc + 8, st));
-    // kernel parameters -> kDetail, kDenoise, Dth, Dtr, kStretch, kShrink
-    ISA_LAUNCH(c, isa_launch_kparam_bwd(c->st3, p3, W, H, adj_gkp, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
-                                        c->adj_acc, st));
-    // mask certainties -> erosion -> robustness s, t (per frame, recomputing the un-eroded mask)
+    const int tcx0 = c->last_tcx0, tcy0 = c->last_tcy0;
+    const size_t tsz = (size_t)tcx0 * tcy0;
+    // output -> kernel parameters and mask certainties; with the tile-flow gradient frame by frame (below), each
+    // launch adding its flow gradient to gA, the reference frame's here with the loss
+    ISA_LAUNCH(c, isa_launch_accumulate_bwd(g, cfa, c->frame_in, tile_grad ? 1 : n, raw_pitch, fp, hp4, c->kparam, p4, white, black, out, out_pitch,
+                                            c->wsum, op, target, target_pitch, weight, weight_pitch, adj_gkp, adj_gmask, hsz, c->adj_acc + 8, nullptr,
+                                            st));
+    if (tile_grad) ISA_CK(cudaMemsetAsync(tile_grad + 2 * ref * tsz, 0, tsz * sizeof(float2), st));
+    // mask certainties -> erosion -> robustness s, t (per frame, recomputing the un-eroded mask); with the tile-flow
+    // gradient also the flow: accumulation and mask -> final flow -> LK iterations (recomputed) -> tile flow
     float maxv = 0.f;
     for (int ch = 0; ch < 3; ch++) maxv = std::max(maxv, white[ch] + black[ch]);
+    const int half = p->window_size_lk / 2;
+    const int bil = p->sample_mode == ISA_SAMPLE_BILINEAR;
     int f = 1;
     for (int i = 0; i < n; i++) {
         if (i == ref) continue;
         const uint16_t* fr = (const uint16_t*)((const char*)raw + (size_t)i * frame_stride);
         const float2* flow = c->flows + (size_t)i * fsz;
+        if (tile_grad) {
+            ISA_CK(cudaMemsetAsync(gA, 0, fsz * sizeof(float2), st));
+            ISA_LAUNCH(c, isa_launch_accumulate_bwd(g, cfa, c->frame_in + f, 1, raw_pitch, fp, hp4, c->kparam, p4, white, black, out, out_pitch, c->wsum,
+                                                    op, target, target_pitch, weight, weight_pitch, adj_gkp, adj_gmask + (size_t)f * hsz, hsz, nullptr,
+                                                    gA, st));
+        }
         ISA_LAUNCH(c, isa_launch_subsample(fr, raw_pitch, W, H, cfa, maxv, c->half_mov, hp3, st));
         ISA_LAUNCH(c, isa_launch_box3(c->half_mov, hp3, Wh, Hh, c->mov_box, hp4, st));
         ISA_LAUNCH(c, isa_launch_mask_store(c->ref_mr, c->ref_sr, c->mov_box, hp4, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha,
-                                            info->noise_beta, p->threshold_m, p->robust_s, p->robust_t, adj_m, adj_aux, st));
+                                            info->noise_beta, p->threshold_m, p->robust_s, p->robust_t, adj_m, adj_aux, bil, st));
         ISA_CK(cudaMemsetAsync(adj_gm, 0, hsz * 16, st));
         ISA_LAUNCH(c, isa_launch_erode_route(adj_m, adj_gmask + (size_t)f * hsz, hp4, Wh, Hh, p->erode_size, adj_gm, st));
         ISA_LAUNCH(c, isa_launch_mask_param_bwd(adj_m, adj_aux, adj_gm, hp4, Wh, Hh, p->robust_t, c->adj_acc + 6, st));
+        if (tile_grad) {
+            ISA_LAUNCH(c, isa_launch_mask_flow_bwd(c->ref_mr, c->ref_sr, c->mov_box, hp4, c->half_mov, hp3, Wh, Hh, flow, fp, W, H, info->noise_alpha,
+                                                   info->noise_beta, p->robust_t, adj_aux, adj_gm, gA, st));
+            // the flows before each LK iteration, as the forward made them
+            const float2* tiles = c->tiles_opt;
+            if (c->tile_override)
+                tiles = c->tile_override + (size_t)i * tsz;
+            else
+                ISA_LAUNCH(c, isa_launch_optimal(c->x, c->last_n1, tcx0, tcy0, ref, i, c->tiles_opt, (size_t)tcx0 * sizeof(float2), st));
+            float bs[2];
+            prealign_shift(pre, ref, i, bs);
+            const int K = p->iterations_lk;
+            if (K > 0)
+                ISA_LAUNCH(c, isa_launch_flow_from_tiles(tiles, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1],
+                                                         prealign_rot(pre, ref, i), F[0], fp, st));
+            for (int k = 1; k < K; k++)
+                ISA_LAUNCH(c, isa_launch_lk_iteration(F[k - 1], F[k], fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, bw_pitch(W), W, H, half,
+                                                      p->min_det_lk, st));
+            float2* gcur = gA;
+            float2* gnext = gB;
+            for (int k = K - 1; k >= 0; k--) {
+                ISA_LAUNCH(c, isa_launch_lk_adjoint(F[k], gcur, gnext, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, bw_pitch(W), W, H, half,
+                                                    p->min_det_lk, wplane, a5, A5, gd3, st));
+                std::swap(gcur, gnext);
+            }
+            ISA_LAUNCH(c, isa_launch_tiles_bwd(gcur, fp, W, H, tcx0, tcy0, (float2*)tile_grad + (size_t)i * tsz, (size_t)tcx0 * sizeof(float2), st));
+        }
         f++;
     }
+    // kernel parameters -> kDetail, kDenoise, Dth, Dtr, kStretch, kShrink (after every frame's accumulation adjoint)
+    ISA_LAUNCH(c, isa_launch_kparam_bwd(c->st3, p3, W, H, adj_gkp, p->dth, p->dtr, p->k_detail, p->k_denoise, p->k_stretch, p->k_shrink,
+                                        c->adj_acc, st));
     double h[9];
     ISA_CK(cudaMemcpyAsync(h, c->adj_acc, sizeof(h), cudaMemcpyDeviceToHost, st));
     ISA_CK(cudaStreamSynchronize(st));
     *loss = h[8];
     for (int k = 0; k < 8; k++) grad[k] = h[k];
     return ISA_OK;
+}
+
+}  // namespace
+
+int isa_merge_backward(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                       const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch, float* out,
+                       size_t out_pitch, double* loss, double* grad, void* stream)
+{
+    return merge_backward(c, raw, raw_pitch, frame_stride, n, info, pre, target, target_pitch, weight, weight_pitch, out, out_pitch, loss, grad,
+                          nullptr, S(stream));
+}
+
+int isa_merge_backward_tiles(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                             const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch,
+                             float* out, size_t out_pitch, double* loss, double* grad, float* tile_grad, void* stream)
+{
+    if (!tile_grad) return fail(ISA_EINVAL, "tile_grad is NULL");
+    return merge_backward(c, raw, raw_pitch, frame_stride, n, info, pre, target, target_pitch, weight, weight_pitch, out, out_pitch, loss, grad,
+                          tile_grad, S(stream));
 }
 
 int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, int* status)
@@ -1111,6 +1207,36 @@ int isa_debug_shifts(isa_ctx* c, const void** one_to_one, int* tx, int* ty)
     if (one_to_one) *one_to_one = c->x;
     if (tx) *tx = c->last_tcx0;
     if (ty) *ty = c->last_tcy0;
+    return ISA_OK;
+}
+
+int isa_set_tile_flow(isa_ctx* c, const float* tiles)
+{
+    if (!c) return fail(ISA_EINVAL, "ctx is NULL");
+    if (((uintptr_t)tiles & 7) != 0) return fail(ISA_EINVAL, "tile flows must be 8-byte aligned");
+    c->tile_override = (const float2*)tiles;
+    return ISA_OK;
+}
+
+int isa_tile_flow(isa_ctx* c, float* tiles, int* tcx, int* tcy, void* stream)
+{
+    if (!c || c->last_n == 0) return fail(ISA_EINVAL, "no merge has run on this context");
+    if (tcx) *tcx = c->last_tcx0;
+    if (tcy) *tcy = c->last_tcy0;
+    if (!tiles) return ISA_OK;
+    if (((uintptr_t)tiles & 7) != 0) return fail(ISA_EINVAL, "tile flows must be 8-byte aligned");
+    cudaStream_t st = S(stream);
+    const size_t tsz = (size_t)c->last_tcx0 * c->last_tcy0;
+    float2* out = (float2*)tiles;
+    for (int i = 0; i < c->last_n; i++) {
+        if (i == c->last_ref)
+            ISA_CK(cudaMemsetAsync(out + i * tsz, 0, tsz * sizeof(float2), st));
+        else if (c->tile_override)
+            ISA_CK(cudaMemcpyAsync(out + i * tsz, c->tile_override + i * tsz, tsz * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        else
+            ISA_CK(isa_launch_optimal(c->x, c->last_n1, c->last_tcx0, c->last_tcy0, c->last_ref, i, out + i * tsz,
+                                      (size_t)c->last_tcx0 * sizeof(float2), st));
+    }
     return ISA_OK;
 }
 
@@ -1397,6 +1523,7 @@ int isa_accumulate(const uint16_t* raw, size_t raw_pitch, int W, int H, const in
     g.W = W; g.H = H; g.Wo = Wo; g.Ho = Ho; g.s = scale; g.ox = ox; g.oy = oy;
     g.cx0 = crop[0]; g.cy0 = crop[1]; g.cx1 = crop[2]; g.cy1 = crop[3];
     g.masks_finite = 0;
+    g.bilinear = 0;
     g.yb0 = 0;
     g.yb1 = Ho;
     float r = std::round(scale);

@@ -36,7 +36,7 @@ __device__ __forceinline__ float bilinear_mirror(const float* img, size_t pitch,
 // flow update u = M (sxt, syt). For a well-conditioned matrix
 // (lambda2 > 1e-3 lambda1) the angle/singular-value construction of the
 // reference equals the closed-form inverse to ~1e-10 relative; below that the
-// reference's own construction is evaluated (lk_update_svd). The pixel is
+// reference's own construction is evaluated (lk_svd). The pixel is
 // left unchanged where sigma1 < minDet (the reference tests
 // min(sigma1, sigma1)).
 __device__ __forceinline__ float2 lk_apply(float2 f, double m0, double m1, double m2, double m3, double sxt, double syt)
@@ -48,17 +48,24 @@ __device__ __forceinline__ float2 lk_apply(float2 f, double m0, double m1, doubl
 }
 
 // The ill-conditioned branch: the reference's angle/singular-value
-// construction. Out of line: it is rarely taken, and inlined at every solve
-// it would multiply the code of the per-pixel kernels.
-__device__ __noinline__ float2 lk_update_svd(float2 f, double a, double b, double d, double sxt, double syt, double min_det)
+// construction of the pseudo-inverse. Out of line: it is rarely taken, and
+// inlined at every solve it would multiply the code of the per-pixel
+// kernels. ok = false where sigma1 < minDet (no update).
+struct LkM {
+    double m0, m1, m2, m3;
+    bool ok;
+};
+
+__device__ __noinline__ LkM lk_svd(double a, double b, double d, double min_det)
 {
+    LkM r{0.0, 0.0, 0.0, 0.0, false};
     const double c = b;
     double th = 0.5 * atan2(2 * a * c + 2 * b * d, a * a + b * b - c * c - d * d);
     double ct = cos(th), st = sin(th);
     double S1 = a * a + b * b + c * c + d * d;
     double S2 = sqrt((a * a + b * b - c * c - d * d) * (a * a + b * b - c * c - d * d) + 4 * (a * c + b * d) * (a * c + b * d));
     double s1 = sqrt((S1 + S2) / 2), s2 = sqrt((S1 - S2) / 2);
-    if (s1 < min_det) return f;
+    if (s1 < min_det) return r;
     s1 = s1 != 0 ? 1 / s1 : 0;
     s2 = s2 != 0 ? 1 / s2 : 0;
     double ep = 0.5 * atan2(2 * a * b + 2 * c * d, a * a - b * b + c * c - d * d);
@@ -69,10 +76,17 @@ __device__ __noinline__ float2 lk_update_svd(float2 f, double a, double b, doubl
     q22 = q22 > 0 ? 1 : (q22 < 0 ? -1 : 0);
     double V0 = q11 * ce, V1 = -q22 * se, V2 = q11 * se, V3 = q22 * ce;
     double m0 = s1 * ct, m1 = s1 * st, m2 = s2 * -st, m3 = s2 * ct;
-    return lk_apply(f, V0 * m0 + V1 * m2, V0 * m1 + V1 * m3, V2 * m0 + V3 * m2, V2 * m1 + V3 * m3, sxt, syt);
+    r.m0 = V0 * m0 + V1 * m2;
+    r.m1 = V0 * m1 + V1 * m3;
+    r.m2 = V2 * m0 + V3 * m2;
+    r.m3 = V2 * m1 + V3 * m3;
+    r.ok = true;
+    return r;
 }
 
-__device__ __forceinline__ float2 lk_update(float2 f, double a, double b, double d, double sxt, double syt, double min_det)
+// The pseudo-inverse M of the window matrix [a b; b d], as the forward
+// chooses it; false where the reference leaves the pixel unchanged.
+__device__ __forceinline__ bool lk_matrix(double a, double b, double d, double min_det, double& m0, double& m1, double& m2, double& m3)
 {
     // the largest eigenvalue only steers two threshold tests, so a float
     // square root is enough (the reference compares sigma1 with minDet and
@@ -81,11 +95,44 @@ __device__ __forceinline__ float2 lk_update(float2 f, double a, double b, double
     double l1 = 0.5 * (a + d) + (double)sqrtf((float)(hd * hd + b * b));
     double det = a * d - b * b;
     if (det > 1e-3 * l1 * l1) {
-        if (l1 < min_det) return f;
+        if (l1 < min_det) return false;
         double inv = 1.0 / det;
-        return lk_apply(f, d * inv, -b * inv, -b * inv, a * inv, sxt, syt);
+        m0 = d * inv; m1 = -b * inv; m2 = -b * inv; m3 = a * inv;
+        return true;
     }
-    return lk_update_svd(f, a, b, d, sxt, syt, min_det);
+    const LkM r = lk_svd(a, b, d, min_det);
+    m0 = r.m0; m1 = r.m1; m2 = r.m2; m3 = r.m3;
+    return r.ok;
+}
+
+__device__ __forceinline__ float2 lk_update(float2 f, double a, double b, double d, double sxt, double syt, double min_det)
+{
+    double m0, m1, m2, m3;
+    if (!lk_matrix(a, b, d, min_det, m0, m1, m2, m3)) return f;
+    return lk_apply(f, m0, m1, m2, m3, sxt, syt);
+}
+
+// Adjoint of lk_update at one pixel for the upstream gradient g of the
+// updated flow: with delta = M c (c = (sxt, syt)) and gamma = M^T g, the
+// window sums get dL/dsxx = -gamma_x delta_x, dL/dsxy = -(gamma_x delta_y +
+// gamma_y delta_x), dL/dsyy = -gamma_y delta_y, dL/dsxt = gamma_x,
+// dL/dsyt = gamma_y (d(M c) = -M dM M c). A component the forward sets to 0
+// (NaN) passes no gradient; a pixel it leaves unchanged gets zeros.
+__device__ __forceinline__ void lk_coeffs(float2 g, double a, double b, double d, double sxt, double syt, double min_det, float co[5])
+{
+    co[0] = co[1] = co[2] = co[3] = co[4] = 0.f;
+    double m0, m1, m2, m3;
+    if (!lk_matrix(a, b, d, min_det, m0, m1, m2, m3)) return;
+    double u = m0 * sxt + m1 * syt, v = m2 * sxt + m3 * syt;
+    const double gx = isnan(u) ? 0.0 : (double)g.x, gy = isnan(v) ? 0.0 : (double)g.y;
+    if (isnan(u)) u = 0;
+    if (isnan(v)) v = 0;
+    const double c0 = m0 * gx + m2 * gy, c1 = m1 * gx + m3 * gy;
+    co[0] = (float)(-c0 * u);
+    co[1] = (float)(-(c0 * v + c1 * u));
+    co[2] = (float)(-c1 * v);
+    co[3] = (float)c0;
+    co[4] = (float)c1;
 }
 
 // c, s: cosine and sine of the pre-alignment rotation (uniform, computed once
@@ -236,10 +283,16 @@ struct LkTaps {
     float s00, s10, s01, s11, a, b, r;
 };
 
-template <int H>
+// ADJ: the adjoint-coefficient form. The same window sums at the flow
+// flow_in; instead of the update, each pixel writes lk_coeffs of the
+// upstream gradient gin (float2, rows at flow_pitch) to five float planes
+// (aout, rows at a_pitch, planes a_plane bytes apart): dL/d(sxx, sxy, syy,
+// sxt, syt), zero where the forward leaves the pixel unchanged.
+template <int H, bool ADJ>
 __global__ void __launch_bounds__(LKS_NT, 512 / LKS_NT) k_lk_stream(const float2* __restrict__ flow_in, float2* __restrict__ flow_out, size_t flow_pitch,
                                                          const float* __restrict__ src, const float* __restrict__ ref, size_t img_pitch, int W,
-                                                         int Himg, int sh, float min_det)
+                                                         int Himg, int sh, float min_det, const float2* __restrict__ gin, float* __restrict__ aout,
+                                                         size_t a_pitch, size_t a_plane)
 {
     using L = LkStream<H>;
     constexpr int R = L::R, SW = L::SW, WIN = L::WIN, NT = LKS_NT, NSEG = L::NSEG, PX = L::PX;
@@ -340,7 +393,7 @@ __global__ void __launch_bounds__(LKS_NT, 512 / LKS_NT) k_lk_stream(const float2
                 const int y = y0 + 2 * s - 4 - 2 * H + rr;  // output row
                 const int x = x0 + j0;
                 if (summer && y < y0 + nout && x < W) {
-                    const float2* irow = isa::row_ptr(flow_in, flow_pitch, y) + x;
+                    const float2* irow = isa::row_ptr(ADJ ? gin : flow_in, flow_pitch, y) + x;
                     float2 fin[PX];
 #pragma unroll
                     for (int k = 0; k < PX; k++) fin[k] = j0 + k < SW && x + k < W ? __ldg(irow + k) : make_float2(0.f, 0.f);
@@ -358,12 +411,26 @@ __global__ void __launch_bounds__(LKS_NT, 512 / LKS_NT) k_lk_stream(const float2
                         for (int k = 1; k < PX; k++) v[k][ch] = sum = sum + (c[WIN + k - 1] - c[k - 1]);
                     }
                     const bool yin = y >= H && y < Himg - H;
-                    float2* orow = isa::row_ptr(flow_out, flow_pitch, y) + x;
+                    if constexpr (ADJ) {
+                        float* arow = isa::row_ptr(aout, a_pitch, y) + x;
 #pragma unroll
-                    for (int k = 0; k < PX; k++) {
-                        const int xk = x + k;
-                        if (j0 + k < SW && xk < W)
-                            orow[k] = yin && xk >= H && xk < W - H ? lk_update(fin[k], v[k][0], v[k][1], v[k][2], v[k][3], v[k][4], min_det) : fin[k];
+                        for (int k = 0; k < PX; k++) {
+                            const int xk = x + k;
+                            if (j0 + k < SW && xk < W) {
+                                float co[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+                                if (yin && xk >= H && xk < W - H) lk_coeffs(fin[k], v[k][0], v[k][1], v[k][2], v[k][3], v[k][4], min_det, co);
+#pragma unroll
+                                for (int ch = 0; ch < 5; ch++) ((float*)((char*)arow + ch * a_plane))[k] = co[ch];
+                            }
+                        }
+                    } else {
+                        float2* orow = isa::row_ptr(flow_out, flow_pitch, y) + x;
+#pragma unroll
+                        for (int k = 0; k < PX; k++) {
+                            const int xk = x + k;
+                            if (j0 + k < SW && xk < W)
+                                orow[k] = yin && xk >= H && xk < W - H ? lk_update(fin[k], v[k][0], v[k][1], v[k][2], v[k][3], v[k][4], min_det) : fin[k];
+                        }
                     }
                 }
             } else {
@@ -400,7 +467,7 @@ int lk_strip_rows(int W, int Himg)
     if (slots <= 0) {
         int nsm = 0, occ = 0;
         if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_lk_stream<H>, LKS_NT, L::TOTAL) != cudaSuccess || nsm * occ <= 0)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_lk_stream<H, false>, LKS_NT, L::TOTAL) != cudaSuccess || nsm * occ <= 0)
             return 64;
         slots = slots_by_dev[dev] = nsm * occ;
     }
@@ -418,15 +485,181 @@ int lk_strip_rows(int W, int Himg)
 
 template <int H>
 cudaError_t launch_lk(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref, size_t img_pitch, int W, int Himg,
-                      float min_det, cudaStream_t st)
+                      float min_det, const float2* gin, float* aout, size_t a_pitch, size_t a_plane, cudaStream_t st)
 {
     using L = LkStream<H>;
-    cudaError_t e = cudaFuncSetAttribute(k_lk_stream<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::TOTAL);
+    const bool adj = aout != nullptr;
+    cudaError_t e = cudaFuncSetAttribute(adj ? k_lk_stream<H, true> : k_lk_stream<H, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)L::TOTAL);
     if (e != cudaSuccess) return e;
     const int sh = lk_strip_rows<H>(W, Himg);
     dim3 g((W + L::SW - 1) / L::SW, (Himg + sh - 1) / sh);
-    k_lk_stream<H><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, sh, min_det);
+    if (adj)
+        k_lk_stream<H, true><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, nullptr, flow_pitch, src, ref, img_pitch, W, Himg, sh, min_det, gin, aout, a_pitch,
+                                                          a_plane);
+    else
+        k_lk_stream<H, false><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, Himg, sh, min_det, nullptr, nullptr, 0,
+                                                           0);
     return cudaGetLastError();
+}
+
+// ---- adjoint of one LK iteration --------------------------------------------
+// f_out(p) = f_in(p) + M(p) c(p) where M, c come from the (2h+1)^2 window
+// sums of the products of dx, dy, dt at q, which are five-tap derivatives
+// (mirror addressing) of the warped source w(q) = src(q + f_in(q)) and the
+// reference. Given g = dL/df_out: k_lk_stream<h, true> writes the window
+// sums' gradients a(p); k_box5 sums them over the window around each q
+// (A(q)); k_lk_adj_deriv turns A into gradients of dx, dy, dt at q;
+// k_lk_adj_flow applies the transposed derivative taps to get dL/dw and,
+// through the bilinear warp, dL/df_in = g + dL/dw grad(w).
+
+// Sum of five float planes over the (2h+1)^2 window around each pixel, zero
+// outside the frame. CTA tile BX_TX x BX_TY plus the halo in shared memory:
+// row sums, then column sums.
+constexpr int BX_TX = 32, BX_TY = 16;
+
+__global__ void __launch_bounds__(256) k_box5(const float* __restrict__ a, size_t pitch, size_t plane, int W, int Himg, int h, float* __restrict__ out)
+{
+    extern __shared__ float bsm[];
+    const int SWp = BX_TX + 2 * h, SHp = BX_TY + 2 * h, win = 2 * h + 1;
+    float* t0 = bsm;
+    float* t1 = bsm + SWp * SHp;
+    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * BX_TY, tid = threadIdx.x;
+    for (int ch = 0; ch < 5; ch++) {
+        const float* ap = (const float*)((const char*)a + ch * plane);
+        float* op = (float*)((char*)out + ch * plane);
+        for (int i = tid; i < SWp * SHp; i += 256) {
+            const int sy = i / SWp, sx = i - sy * SWp;
+            const int gx = x0 + sx - h, gy = y0 + sy - h;
+            t0[i] = (unsigned)gx < (unsigned)W && (unsigned)gy < (unsigned)Himg ? __ldg(isa::row_ptr(ap, pitch, gy) + gx) : 0.f;
+        }
+        __syncthreads();
+        for (int i = tid; i < SHp * BX_TX; i += 256) {
+            const int sy = i / BX_TX, x = i - sy * BX_TX;
+            float v = 0.f;
+            for (int k = 0; k < win; k++) v += t0[sy * SWp + x + k];
+            t1[i] = v;
+        }
+        __syncthreads();
+        for (int i = tid; i < BX_TY * BX_TX; i += 256) {
+            const int ly = i / BX_TX, lx = i - ly * BX_TX;
+            const int x = x0 + lx, y = y0 + ly;
+            if (x >= W || y >= Himg) continue;
+            float v = 0.f;
+            for (int k = 0; k < win; k++) v += t1[(ly + k) * BX_TX + lx];
+            isa::row_ptr(op, pitch, y)[x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// dL/d(dx, dy, dt) at q from the window-summed gradients A(q) of the
+// products (dx^2, dx dy, dy^2, dx dt, dy dt); dx, dy, dt recomputed from the
+// warped source w and the reference as the forward computes them.
+__global__ void k_lk_adj_deriv(const float* __restrict__ w, size_t w_pitch, const float* __restrict__ ref, size_t r_pitch, int W, int Himg,
+                               const float* __restrict__ A, size_t pitch, size_t plane, float* __restrict__ gd)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= Himg) return;
+    const auto wv = [&](int xx, int yy) { return __ldg(isa::row_ptr(w, w_pitch, isa::mirror(yy, Himg)) + isa::mirror(xx, W)); };
+    const auto rv = [&](int xx, int yy) { return __ldg(isa::row_ptr(ref, r_pitch, isa::mirror(yy, Himg)) + isa::mirror(xx, W)); };
+    const float gx = (wv(x + 2, y) - wv(x - 2, y)) + (rv(x + 2, y) - rv(x - 2, y)) + 8.0f * ((wv(x - 1, y) - wv(x + 1, y)) + (rv(x - 1, y) - rv(x + 1, y)));
+    const float gy = (wv(x, y + 2) - wv(x, y - 2)) + (rv(x, y + 2) - rv(x, y - 2)) + 8.0f * ((wv(x, y - 1) - wv(x, y + 1)) + (rv(x, y - 1) - rv(x, y + 1)));
+    const float dx = gx * (1.0f / 24.0f), dy = gy * (1.0f / 24.0f), dt = wv(x, y) - rv(x, y);
+    float a[5];
+#pragma unroll
+    for (int ch = 0; ch < 5; ch++) a[ch] = __ldg(isa::row_ptr((const float*)((const char*)A + ch * plane), pitch, y) + x);
+    isa::row_ptr(gd, pitch, y)[x] = 2.f * dx * a[0] + dy * a[1] + dt * a[3];
+    isa::row_ptr((float*)((char*)gd + plane), pitch, y)[x] = dx * a[1] + 2.f * dy * a[2] + dt * a[4];
+    isa::row_ptr((float*)((char*)gd + 2 * plane), pitch, y)[x] = dx * a[3] + dy * a[4];
+}
+
+// dL/dw(x) = dL/ddt(x) + the transposed five-tap filters of dL/ddx and
+// dL/ddy: w(x) enters 24 dx(q) with coefficient c_k wherever
+// mirror(q + k) = x (c_2 = 1, c_-2 = -1, c_-1 = 8, c_1 = -8), which happens
+// only for q within 2 of x. Then dL/df_in(x) = g(x) + dL/dw(x) times the
+// gradient of the bilinear (mirror) sample of src at x + f_in(x).
+__global__ void k_lk_adj_flow(const float* __restrict__ gd, size_t pitch, size_t plane, const float* __restrict__ src, size_t s_pitch,
+                              const float2* __restrict__ f, const float2* __restrict__ gout, float2* __restrict__ gin, size_t fpitch, int W, int Himg)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= Himg) return;
+    const float* gdx = gd;
+    const float* gdy = (const float*)((const char*)gd + plane);
+    const float* gdt = (const float*)((const char*)gd + 2 * plane);
+    const int ks[4] = {2, -2, -1, 1};
+    const float cs[4] = {1.f / 24.f, -1.f / 24.f, 8.f / 24.f, -8.f / 24.f};
+    float gw = __ldg(isa::row_ptr(gdt, pitch, y) + x);
+#pragma unroll
+    for (int dq = -2; dq <= 2; dq++) {
+        const int qx = x + dq, qy = y + dq;
+        if ((unsigned)qx < (unsigned)W) {
+            const float g = __ldg(isa::row_ptr(gdx, pitch, y) + qx);
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if (isa::mirror(qx + ks[t], W) == x) gw += cs[t] * g;
+        }
+        if ((unsigned)qy < (unsigned)Himg) {
+            const float g = __ldg(isa::row_ptr(gdy, pitch, qy) + x);
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if (isa::mirror(qy + ks[t], Himg) == y) gw += cs[t] * g;
+        }
+    }
+    const float2 fl = __ldg(isa::row_ptr(f, fpitch, y) + x);
+    const float flx = floorf(fl.x), fly = floorf(fl.y);
+    const int ix = x + (int)flx, iy = y + (int)fly;
+    const float a = fl.x - flx, b = fl.y - fly;
+    const int xa = isa::mirror(ix, W), xb = isa::mirror(ix + 1, W);
+    const float* r0 = isa::row_ptr(src, s_pitch, isa::mirror(iy, Himg));
+    const float* r1 = isa::row_ptr(src, s_pitch, isa::mirror(iy + 1, Himg));
+    const float s00 = __ldg(r0 + xa), s10 = __ldg(r0 + xb), s01 = __ldg(r1 + xa), s11 = __ldg(r1 + xb);
+    const float dwx = (1.f - b) * (s10 - s00) + b * (s11 - s01);
+    const float dwy = (1.f - a) * (s01 - s00) + a * (s11 - s10);
+    const float2 go = __ldg(isa::row_ptr(gout, fpitch, y) + x);
+    isa::row_ptr(gin, fpitch, y)[x] = make_float2(go.x + gw * dwx, go.y + gw * dwy);
+}
+
+// Transpose of the tile term of k_flow_from_tiles: one warp per tile (i, j)
+// sums weight x g over the pixels whose bilinear (clamp) lookup reads the
+// tile, with the forward's own sample positions and weights.
+__global__ void k_tiles_bwd(const float2* __restrict__ g, size_t fpitch, int W, int H, int tcx, int tcy, float2* __restrict__ gt, size_t tpitch)
+{
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (wid >= tcx * tcy) return;
+    const int i = wid % tcx, j = wid / tcx;
+    const int ylo = j == 0 ? 0 : max(0, (int)floorf((j - 0.5f) * H / tcy - 0.5f) - 1);
+    const int yhi = j == tcy - 1 ? H - 1 : min(H - 1, (int)ceilf((j + 1.5f) * H / tcy - 0.5f) + 1);
+    const int xlo = i == 0 ? 0 : max(0, (int)floorf((i - 0.5f) * W / tcx - 0.5f) - 1);
+    const int xhi = i == tcx - 1 ? W - 1 : min(W - 1, (int)ceilf((i + 1.5f) * W / tcx - 0.5f) + 1);
+    float sx = 0.f, sy = 0.f;
+    for (int y = ylo; y <= yhi; y++) {
+        const float yb = ((float)y + 0.5f) / (float)H * tcy - 0.5f;
+        const float fly = floorf(yb);
+        const int jj = (int)fly;
+        const float b = yb - fly;
+        const int j0 = isa::clampi(jj, 0, tcy - 1), j1 = isa::clampi(jj + 1, 0, tcy - 1);
+        const float wy = (j0 == j ? 1.f - b : 0.f) + (j1 == j ? b : 0.f);
+        if (wy == 0.f) continue;
+        const float2* gr = isa::row_ptr(g, fpitch, y);
+        for (int x = xlo + lane; x <= xhi; x += 32) {
+            const float xb = ((float)x + 0.5f) / (float)W * tcx - 0.5f;
+            const float flx = floorf(xb);
+            const int ii = (int)flx;
+            const float a = xb - flx;
+            const int i0 = isa::clampi(ii, 0, tcx - 1), i1 = isa::clampi(ii + 1, 0, tcx - 1);
+            const float wx = (i0 == i ? 1.f - a : 0.f) + (i1 == i ? a : 0.f);
+            if (wx == 0.f) continue;
+            const float2 v = __ldg(gr + x);
+            sx += wx * wy * v.x;
+            sy += wx * wy * v.y;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (lane == 0) isa::row_ptr(gt, tpitch, j)[i] = make_float2(sx, sy);
 }
 
 inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
@@ -477,10 +710,39 @@ cudaError_t isa_launch_lk_iteration(const float2* flow_in, float2* flow_out, siz
                                     size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st)
 {
     switch (half) {
-#define ISA_LK_CASE(h) case h: return launch_lk<h>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, H, min_det, st);
+#define ISA_LK_CASE(h) case h: return launch_lk<h>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, H, min_det, nullptr, nullptr, 0, 0, st);
     ISA_LK_CASE(0) ISA_LK_CASE(1) ISA_LK_CASE(2) ISA_LK_CASE(3) ISA_LK_CASE(4) ISA_LK_CASE(5) ISA_LK_CASE(6) ISA_LK_CASE(7) ISA_LK_CASE(8)
     ISA_LK_CASE(9) ISA_LK_CASE(10) ISA_LK_CASE(11) ISA_LK_CASE(12) ISA_LK_CASE(13) ISA_LK_CASE(14) ISA_LK_CASE(15)
 #undef ISA_LK_CASE
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t isa_launch_lk_adjoint(const float2* f, const float2* gout, float2* gin, size_t fpitch, const float* src, const float* ref, size_t img_pitch,
+                                  int W, int H, int half, float min_det, float* wplane, float* a5, float* A5, float* gd3, cudaStream_t st)
+{
+    if (half < 0 || half > 15) return cudaErrorInvalidValue;
+    const size_t sp = (size_t)W * 4, plane = sp * H;
+    cudaError_t e = isa_launch_warp(src, img_pitch, W, H, f, fpitch, wplane, sp, st);
+    if (e != cudaSuccess) return e;
+    switch (half) {
+#define ISA_LK_CASE(h) case h: e = launch_lk<h>(f, nullptr, fpitch, src, ref, img_pitch, W, H, min_det, gout, a5, sp, plane, st); break;
+    ISA_LK_CASE(0) ISA_LK_CASE(1) ISA_LK_CASE(2) ISA_LK_CASE(3) ISA_LK_CASE(4) ISA_LK_CASE(5) ISA_LK_CASE(6) ISA_LK_CASE(7) ISA_LK_CASE(8)
+    ISA_LK_CASE(9) ISA_LK_CASE(10) ISA_LK_CASE(11) ISA_LK_CASE(12) ISA_LK_CASE(13) ISA_LK_CASE(14) ISA_LK_CASE(15)
+#undef ISA_LK_CASE
+    }
+    if (e != cudaSuccess) return e;
+    const size_t bsmem = (size_t)((BX_TX + 2 * half) * (BX_TY + 2 * half) + (BX_TY + 2 * half) * BX_TX) * sizeof(float);
+    k_box5<<<dim3((W + BX_TX - 1) / BX_TX, (H + BX_TY - 1) / BX_TY), 256, bsmem, st>>>(a5, sp, plane, W, H, half, A5);
+    dim3 b(32, 8);
+    k_lk_adj_deriv<<<grid2(W, H, b), b, 0, st>>>(wplane, sp, ref, img_pitch, W, H, A5, sp, plane, gd3);
+    k_lk_adj_flow<<<grid2(W, H, b), b, 0, st>>>(gd3, sp, plane, src, img_pitch, f, gout, gin, fpitch, W, H);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_tiles_bwd(const float2* g, size_t fpitch, int W, int H, int tcx, int tcy, float2* gt, size_t tpitch, cudaStream_t st)
+{
+    const long warps = (long)tcx * tcy;
+    k_tiles_bwd<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(g, fpitch, W, H, tcx, tcy, gt, tpitch);
+    return cudaGetLastError();
 }

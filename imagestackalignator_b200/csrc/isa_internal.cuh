@@ -149,6 +149,11 @@ cudaError_t isa_launch_lk_sums(float2* flow, size_t flow_pitch, const float* ix,
                                int H, int half, float min_det, cudaStream_t st);
 cudaError_t isa_launch_lk_iteration(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref,
                                     size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st);
+// adjoint of one LK iteration (scratch: wplane one float plane, a5 and A5 five planes, gd3 three planes, all W x H floats at
+// pitch W * 4) and of the tile term of the flow from tiles
+cudaError_t isa_launch_lk_adjoint(const float2* f, const float2* gout, float2* gin, size_t fpitch, const float* src, const float* ref, size_t img_pitch,
+                                  int W, int H, int half, float min_det, float* wplane, float* a5, float* A5, float* gd3, cudaStream_t st);
+cudaError_t isa_launch_tiles_bwd(const float2* g, size_t fpitch, int W, int H, int tcx, int tcy, float2* gt, size_t tpitch, cudaStream_t st);
 
 // robust.cu
 cudaError_t isa_launch_robustness(const float* ref3, const float* mov3, size_t img_pitch, float4* mask, size_t mask_pitch, int Wh,
@@ -165,7 +170,7 @@ cudaError_t isa_launch_ref_stats(const float* ref3, size_t img_pitch, int Wh, in
 cudaError_t isa_launch_box3(const float* mov3, size_t img_pitch, int Wh, int Hh, float4* box, size_t sp, cudaStream_t st);
 cudaError_t isa_launch_robustness_erode_tabs(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch,
                                              int Wh, int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
-                                             float thr_m, float s, float t, int size, float4* out, size_t out_pitch, cudaStream_t st);
+                                             float thr_m, float s, float t, int size, float4* out, size_t out_pitch, int bil, cudaStream_t st);
 
 // prealign.cu
 cudaError_t isa_launch_rotate_cubic(const float* src, size_t pitch, int W, int H, double angle_deg, float* dst, size_t dst_pitch, cudaStream_t st);
@@ -176,7 +181,10 @@ cudaError_t isa_launch_argmax(const float* img, int n, void* scratch, void* out,
 // adjoint of the merge (robust.cu, merge.cu)
 cudaError_t isa_launch_mask_store(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch, int Wh,
                                   int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s,
-                                  float t, float4* m_out, float4* aux_out, cudaStream_t st);
+                                  float t, float4* m_out, float4* aux_out, int bil, cudaStream_t st);
+cudaError_t isa_launch_mask_flow_bwd(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch, int Wh,
+                                     int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float t,
+                                     const float4* aux, const float4* g_mask, float2* gflow, cudaStream_t st);
 cudaError_t isa_launch_erode_route(const float4* m, const float4* g_eroded, size_t sp, int Wh, int Hh, int size, float4* g_mask, cudaStream_t st);
 cudaError_t isa_launch_mask_param_bwd(const float4* m, const float4* aux, const float4* g_mask, size_t sp, int Wh, int Hh, float t, double* grad2,
                                       cudaStream_t st);
@@ -190,6 +198,7 @@ struct isa_accum_geom {
     int ox, oy;        // output-grid origin
     int cx0, cy0, cx1, cy1;  // inclusive source crop
     int masks_finite;  // 1: every mask value is finite (masks made by this library)
+    int bilinear;      // 1: sample mode BILINEAR (the four integer shifts around s * flow, blended)
     int yb0, yb1;      // output rows [yb0, yb1) computed by this launch (yb0 a multiple of 32)
 };
 struct isa_frame_in {
@@ -217,7 +226,7 @@ cudaError_t isa_launch_accumulate_bwd(const isa_accum_geom& g, unsigned cfa, con
                                       size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch, const float* white,
                                       const float* black, const float* out, size_t out_pitch, const float* wsum, size_t ws_pitch, const float* target,
                                       size_t tg_pitch, const float* weight, size_t wt_pitch, float* gkp, float4* gmask, size_t gmask_stride, double* loss,
-                                      cudaStream_t st);
+                                      float2* gflow, cudaStream_t st);
 cudaError_t isa_launch_kparam_bwd(const float* st3, size_t st_pitch, int W, int H, const float* gkp, float Dth, float Dtr, float kDetail,
                                   float kDenoise, float kStretch, float kShrink, double* grad6, cudaStream_t st);
 

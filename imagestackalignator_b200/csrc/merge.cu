@@ -113,7 +113,11 @@ __device__ __forceinline__ float2 flow_sample(const float2* fl, size_t pitch, in
     return make_float2(isa::lerp2(p00.x, p10.x, p01.x, p11.x, a, b), isa::lerp2(p00.y, p10.y, p01.y, p11.y, a, b));
 }
 
-template <int KC>
+// BIL (sample mode BILINEAR): each frame contributes at the four integer
+// shifts around s * flow with the bilinear weights of its fractional part
+// (the certainty of a tap is scaled by the corner's weight); corners of
+// weight zero are skipped, so at integer flow the sums are ROUND's.
+template <int KC, bool BIL>
 __global__ void __launch_bounds__(256) k_accumulate(isa_accum_geom g, unsigned cfa, const isa_frame_in* __restrict__ frames, int nframes,
                                                    isa_frame_in single, size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* __restrict__ kparam,
                                                    size_t kp_pitch, F3 white, F3 black, float* __restrict__ acc, float* __restrict__ wsum,
@@ -155,33 +159,48 @@ __global__ void __launch_bounds__(256) k_accumulate(isa_accum_geom g, unsigned c
     }
     for (int f = 0; f < nframes; f++) {
         const isa_frame_in fr = frames ? frames[f] : single;
-        int sx = 0, sy = 0;
+        int sx0 = 0, sy0 = 0;
+        float bx = 0.f, by = 0.f;
         if (fr.flow) {
             float2 fl = flow_sample(fr.flow, flow_pitch, g.W, g.H, xb, yb);
-            sx = (int)roundf(fl.x * g.s);
-            sy = (int)roundf(fl.y * g.s);
+            if constexpr (BIL) {
+                const float hx = fl.x * g.s, hy = fl.y * g.s;
+                const float fx = floorf(hx), fy = floorf(hy);
+                sx0 = (int)fx; sy0 = (int)fy;
+                bx = hx - fx; by = hy - fy;
+            } else {
+                sx0 = (int)roundf(fl.x * g.s);
+                sy0 = (int)roundf(fl.y * g.s);
+            }
         }
+#pragma unroll 1
+        for (int corner = 0; corner < (BIL ? 4 : 1); corner++) {
+            const int sx = sx0 + (corner & 1), sy = sy0 + (corner >> 1);
+            const float wk = BIL ? ((corner & 1) ? bx : 1.f - bx) * ((corner >> 1) ? by : 1.f - by) : 1.f;
+            if (BIL && wk == 0.f) continue;
 #pragma unroll
-        for (int py = 0; py < 5; py++) {
-            const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
-            const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
-            const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
+            for (int py = 0; py < 5; py++) {
+                const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
+                const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
+                const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
 #pragma unroll
-            for (int px = 0; px < 5; px++) {
-                const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
-                const int c = isa::cfa_at(cfa, qx, qy);
-                if (c > 2) continue;
-                float raw = (float)__ldg(rr + qx);
-                raw = (raw - black.v[c]) / white.v[c];
-                float cert = 1.f;
-                if (mr) {
-                    float4 m = __ldg(mr + ux[px]);
-                    cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
-                    if (!isfinite(cert)) cert = 0.f;
+                for (int px = 0; px < 5; px++) {
+                    const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
+                    const int c = isa::cfa_at(cfa, qx, qy);
+                    if (c > 2) continue;
+                    float raw = (float)__ldg(rr + qx);
+                    raw = (raw - black.v[c]) / white.v[c];
+                    float cert = 1.f;
+                    if (mr) {
+                        float4 m = __ldg(mr + ux[px]);
+                        cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
+                        if (!isfinite(cert)) cert = 0.f;
+                    }
+                    if constexpr (BIL) cert *= wk;
+                    const float ww = wt[py * 5 + px];
+                    a[c] += raw * ww * cert;
+                    w[c] += ww * cert;
                 }
-                const float ww = wt[py * 5 + px];
-                a[c] += raw * ww * cert;
-                w[c] += ww * cert;
             }
         }
     }
@@ -213,14 +232,42 @@ __global__ void k_apply_weighting(float* img, size_t img_pitch, const float* __r
 // the weights w_t = exp(-q_t / 2) of the kernel parameters k give
 // dL/dk = sum_t dL/dw_t dw_t/dk, and the bilinear lookup of k scatters it to
 // the kernel-parameter image. Certainty gradients are scattered to the
-// frame's mask cell (atomic adds; their order is not fixed).
-template <int KC>
+// frame's mask cell (atomic adds; their order is not fixed). loss may be null
+// (a launch over some of the frames of a merge whose loss another adds).
+//
+// BIL: a frame's contribution is sum_k beta_k T_k over the four integer
+// shifts k around s * flow, beta the bilinear weights of its fractional part
+// (bx, by). With D_k = dL/dbeta_k = sum over k's taps of w c h_c (v - out_c),
+// dL/dbx = (1 - by)(D_1 - D_0) + by (D_3 - D_2) and
+// dL/dby = (1 - bx)(D_2 - D_0) + bx (D_3 - D_1); times s, they go to the
+// four flow texels of the bilinear (mirror) flow lookup in gflow (atomic
+// adds). A corner of weight zero still gives its D (the one-sided
+// derivative) but nothing to the kernel-parameter and mask gradients.
+__device__ __forceinline__ void flow_scatter(float2* gflow, size_t pitch, int W, int H, float xb, float yb, float gx, float gy)
+{
+    const float fx = floorf(xb), fy = floorf(yb);
+    const int i = (int)fx, j = (int)fy;
+    const float a = xb - fx, b = yb - fy;
+    const int i0 = isa::mirror(i, W), i1 = isa::mirror(i + 1, W), j0 = isa::mirror(j, H), j1 = isa::mirror(j + 1, H);
+    const float w[4] = {(1.f - a) * (1.f - b), a * (1.f - b), (1.f - a) * b, a * b};
+    const int xs[4] = {i0, i1, i0, i1}, ys[4] = {j0, j0, j1, j1};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (w[k] == 0.f) continue;
+        float* d = (float*)(isa::row_ptr(gflow, pitch, ys[k]) + xs[k]);
+        atomicAdd(d, w[k] * gx);
+        atomicAdd(d + 1, w[k] * gy);
+    }
+}
+
+template <int KC, bool BIL>
 __global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsigned cfa, const isa_frame_in* __restrict__ frames, int nframes,
                                                        size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* __restrict__ kparam,
                                                        size_t kp_pitch, F3 white, F3 black, const float* __restrict__ out, size_t out_pitch,
                                                        const float* __restrict__ wsum, size_t ws_pitch, const float* __restrict__ target,
                                                        size_t tg_pitch, const float* __restrict__ weight, size_t wt_pitch, float* __restrict__ gkp,
-                                                       float4* __restrict__ gmask, size_t gmask_stride, double* __restrict__ loss)
+                                                       float4* __restrict__ gmask, size_t gmask_stride, double* __restrict__ loss,
+                                                       float2* __restrict__ gflow)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     double lsum = 0.0;
@@ -264,40 +311,67 @@ __global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsign
             }
             for (int f = 0; f < nframes; f++) {
                 const isa_frame_in fr = frames[f];
-                int sx = 0, sy = 0;
+                int sx0 = 0, sy0 = 0;
+                float bx = 0.f, by = 0.f;
                 if (fr.flow) {
                     float2 fl = flow_sample(fr.flow, flow_pitch, g.W, g.H, xb, yb);
-                    sx = (int)roundf(fl.x * g.s);
-                    sy = (int)roundf(fl.y * g.s);
+                    if constexpr (BIL) {
+                        const float hx = fl.x * g.s, hy = fl.y * g.s;
+                        const float fx = floorf(hx), fy = floorf(hy);
+                        sx0 = (int)fx; sy0 = (int)fy;
+                        bx = hx - fx; by = hy - fy;
+                    } else {
+                        sx0 = (int)roundf(fl.x * g.s);
+                        sy0 = (int)roundf(fl.y * g.s);
+                    }
                 }
                 float4* gm = gmask + (size_t)f * gmask_stride;
+                float D[4] = {0.f, 0.f, 0.f, 0.f};
+                const int ncorner = BIL && fr.flow ? 4 : 1;
+#pragma unroll 1
+                for (int corner = 0; corner < ncorner; corner++) {
+                    const int sx = sx0 + (corner & 1), sy = sy0 + (corner >> 1);
+                    const float wk = BIL ? ((corner & 1) ? bx : 1.f - bx) * ((corner >> 1) ? by : 1.f - by) : 1.f;
+                    float dk = 0.f;
 #pragma unroll
-                for (int py = 0; py < 5; py++) {
-                    const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
-                    const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
-                    const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
+                    for (int py = 0; py < 5; py++) {
+                        const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
+                        const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
+                        const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
 #pragma unroll
-                    for (int px = 0; px < 5; px++) {
-                        const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
-                        const int c = isa::cfa_at(cfa, qx, qy);
-                        if (c > 2) continue;
-                        float raw = (float)__ldg(rr + qx);
-                        raw = (raw - black.v[c]) / white.v[c];
-                        const float hc = c == 0 ? h[0] : (c == 1 ? h[1] : h[2]);
-                        const float oc = c == 0 ? o[0] : (c == 1 ? o[1] : o[2]);
-                        const float r = hc * (raw - oc);
-                        float cert = 1.f;
-                        if (mr) {
-                            const float4 m = __ldg(mr + ux[px]);
-                            cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
-                            if (!isfinite(cert)) cert = 0.f;
-                            else {
-                                float* dst = (float*)(isa::row_ptr(gm, mask_pitch, uy[py]) + ux[px]) + c;
-                                atomicAdd(dst, wt[py * 5 + px] * r);
+                        for (int px = 0; px < 5; px++) {
+                            const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
+                            const int c = isa::cfa_at(cfa, qx, qy);
+                            if (c > 2) continue;
+                            float raw = (float)__ldg(rr + qx);
+                            raw = (raw - black.v[c]) / white.v[c];
+                            const float hc = c == 0 ? h[0] : (c == 1 ? h[1] : h[2]);
+                            const float oc = c == 0 ? o[0] : (c == 1 ? o[1] : o[2]);
+                            const float r = hc * (raw - oc);
+                            float cert = 1.f;
+                            if (mr) {
+                                const float4 m = __ldg(mr + ux[px]);
+                                cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
+                                if (!isfinite(cert)) cert = 0.f;
+                                else if (!BIL || wk != 0.f) {
+                                    float* dst = (float*)(isa::row_ptr(gm, mask_pitch, uy[py]) + ux[px]) + c;
+                                    atomicAdd(dst, BIL ? wt[py * 5 + px] * r * wk : wt[py * 5 + px] * r);
+                                }
+                            }
+                            if constexpr (BIL) {
+                                dk += wt[py * 5 + px] * cert * r;
+                                G[py * 5 + px] += cert * r * wk;
+                            } else {
+                                G[py * 5 + px] += cert * r;
                             }
                         }
-                        G[py * 5 + px] += cert * r;
                     }
+                    D[corner] = dk;
+                }
+                if (BIL && fr.flow && gflow) {
+                    const float dbx = (1.f - by) * (D[1] - D[0]) + by * (D[3] - D[2]);
+                    const float dby = (1.f - bx) * (D[2] - D[0]) + bx * (D[3] - D[1]);
+                    flow_scatter(gflow, flow_pitch, g.W, g.H, xb, yb, dbx * g.s, dby * g.s);
                 }
             }
             // dL/dk, then the transpose of the bilinear lookup (clamp addressing, zero weights skipped as in lerp2)
@@ -333,7 +407,7 @@ __global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsign
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     if ((tid & 31) == 0) sl[tid >> 5] = lsum;
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && loss) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; w++) t += sl[w];
         atomicAdd(loss, t);
@@ -433,7 +507,7 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
                                   const float* white, const float* black, float* acc, float* wsum, size_t out_pitch, int accumulate_into,
                                   cudaStream_t st)
 {
-    if (g.s_int == 2 && kparam_channels == 4 && isa_accumulate_x2_supported(cfa))
+    if (!g.bilinear && g.s_int == 2 && kparam_channels == 4 && isa_accumulate_x2_supported(cfa))
         return isa_launch_accumulate_x2(g, cfa, frames, nframes, single, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, white, black, acc,
                                         wsum, out_pitch, accumulate_into, st);
     F3 wh, bl;
@@ -441,12 +515,18 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
     isa_frame_in one = single ? *single : isa_frame_in{nullptr, nullptr, nullptr};
     if (g.yb0 < 0 || g.yb1 > g.Ho || g.yb1 <= g.yb0) return cudaErrorInvalidValue;
     dim3 b(32, 8), grd = grid2(g.Wo, g.yb1 - g.yb0, b);
-    if (kparam_channels == 4)
-        k_accumulate<4><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc, wsum,
-                                           out_pitch, accumulate_into);
+    if (kparam_channels == 4 && g.bilinear)
+        k_accumulate<4, true><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc,
+                                                 wsum, out_pitch, accumulate_into);
+    else if (kparam_channels == 4)
+        k_accumulate<4, false><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc,
+                                                  wsum, out_pitch, accumulate_into);
+    else if (kparam_channels == 3 && g.bilinear)
+        k_accumulate<3, true><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc,
+                                                 wsum, out_pitch, accumulate_into);
     else if (kparam_channels == 3)
-        k_accumulate<3><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc, wsum,
-                                           out_pitch, accumulate_into);
+        k_accumulate<3, false><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc,
+                                                  wsum, out_pitch, accumulate_into);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -464,13 +544,19 @@ cudaError_t isa_launch_accumulate_bwd(const isa_accum_geom& g, unsigned cfa, con
                                       size_t flow_pitch, size_t mask_pitch, const float* kparam, size_t kparam_pitch, const float* white,
                                       const float* black, const float* out, size_t out_pitch, const float* wsum, size_t ws_pitch, const float* target,
                                       size_t tg_pitch, const float* weight, size_t wt_pitch, float* gkp, float4* gmask, size_t gmask_stride, double* loss,
-                                      cudaStream_t st)
+                                      float2* gflow, cudaStream_t st)
 {
     F3 wh, bl;
     for (int c = 0; c < 3; c++) { wh.v[c] = white[c]; bl.v[c] = black[c]; }
     dim3 b(32, 8), grd = grid2(g.Wo, g.Ho, b);
-    k_accumulate_bwd<4><<<grd, b, 0, st>>>(g, cfa, frames, nframes, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, out, out_pitch,
-                                           wsum, ws_pitch, target, tg_pitch, weight, wt_pitch, gkp, gmask, gmask_stride, loss);
+    if (g.bilinear)
+        k_accumulate_bwd<4, true><<<grd, b, 0, st>>>(g, cfa, frames, nframes, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, out,
+                                                     out_pitch, wsum, ws_pitch, target, tg_pitch, weight, wt_pitch, gkp, gmask, gmask_stride, loss,
+                                                     gflow);
+    else
+        k_accumulate_bwd<4, false><<<grd, b, 0, st>>>(g, cfa, frames, nframes, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, out,
+                                                      out_pitch, wsum, ws_pitch, target, tg_pitch, weight, wt_pitch, gkp, gmask, gmask_stride, loss,
+                                                      nullptr);
     return cudaGetLastError();
 }
 

@@ -189,19 +189,11 @@ struct RobustTabs {
 // M exceeds the threshold), so that mask_c = clamp(sg E_c - t, 0, 1).
 struct MaskTerms { float m[3]; float M; float E[3]; float sg; };
 
-__device__ __forceinline__ MaskTerms mask_terms(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
-                                                const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
-                                                float thr_m, float s_lit, float t_lit, int x, int y)
+// 3x3 mean of the moving half-res image around (cx, cy): the table entry, or
+// (a centre outside the image) the clamped taps summed directly.
+__device__ __forceinline__ void moved_mean(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh, int cx, int cy,
+                                           float mm[3])
 {
-    float2 sf = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x, y);
-    float2 sl = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x + 2, y + 2);
-    float mxx = fmaxf(sl.x, sf.x), mxy = fmaxf(sl.y, sf.y);
-    float mnx = fminf(sl.x, sf.x), mny = fminf(sl.y, sf.y);
-    int shx = (int)roundf(sf.x * 0.5f), shy = (int)roundf(sf.y * 0.5f);
-    const float4 r4 = __ldg(isa::row_ptr(tb.mr, tb.sp, y) + x), s4 = __ldg(isa::row_ptr(tb.sr, tb.sp, y) + x);
-    const float mr[3] = {r4.x, r4.y, r4.z}, sr3[3] = {s4.x, s4.y, s4.z};
-    float mm[3];
-    const int cx = x + shx, cy = y + shy;
     if ((unsigned)cx < (unsigned)Wh && (unsigned)cy < (unsigned)Hh) {
         const float4 b4 = __ldg(isa::row_ptr(tb.box, tb.sp, cy) + cx);
         mm[0] = b4.x; mm[1] = b4.y; mm[2] = b4.z;
@@ -213,6 +205,55 @@ __device__ __forceinline__ MaskTerms mask_terms(const RobustTabs& tb, const floa
                 for (int c = 0; c < 3; c++) mm[c] += __ldg(q + c);
             }
         for (int c = 0; c < 3; c++) mm[c] /= 9.0f;
+    }
+}
+
+// Offset of the moved 3x3 mean for the flow sample sf at a half-res pixel:
+// ROUND, round(sf / 2); BIL (sample mode BILINEAR), floor(sf / 2) and the
+// fractional part (bx, by) that blends the four means around it.
+template <bool BIL>
+__device__ __forceinline__ void moved_offset(float2 sf, int& shx, int& shy, float& bx, float& by)
+{
+    if constexpr (BIL) {
+        const float hx = sf.x * 0.5f, hy = sf.y * 0.5f;
+        const float fx = floorf(hx), fy = floorf(hy);
+        shx = (int)fx; shy = (int)fy;
+        bx = hx - fx; by = hy - fy;
+    } else {
+        shx = (int)roundf(sf.x * 0.5f); shy = (int)roundf(sf.y * 0.5f);
+        bx = by = 0.f;
+    }
+}
+
+template <bool BIL>
+__device__ __forceinline__ MaskTerms mask_terms(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                                                const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
+                                                float thr_m, float s_lit, float t_lit, int x, int y)
+{
+    float2 sf = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x, y);
+    float2 sl = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x + 2, y + 2);
+    float mxx = fmaxf(sl.x, sf.x), mxy = fmaxf(sl.y, sf.y);
+    float mnx = fminf(sl.x, sf.x), mny = fminf(sl.y, sf.y);
+    int shx, shy;
+    float bx, by;
+    moved_offset<BIL>(sf, shx, shy, bx, by);
+    const float4 r4 = __ldg(isa::row_ptr(tb.mr, tb.sp, y) + x), s4 = __ldg(isa::row_ptr(tb.sr, tb.sp, y) + x);
+    const float mr[3] = {r4.x, r4.y, r4.z}, sr3[3] = {s4.x, s4.y, s4.z};
+    float mm[3];
+    moved_mean(tb, mov3, img_pitch, Wh, Hh, x + shx, y + shy, mm);
+    if constexpr (BIL) {
+        const float w0 = (1.f - bx) * (1.f - by);
+#pragma unroll
+        for (int c = 0; c < 3; c++) mm[c] *= w0;
+#pragma unroll
+        for (int k = 1; k < 4; k++) {
+            const float wk = ((k & 1) ? bx : 1.f - bx) * ((k >> 1) ? by : 1.f - by);
+            if (wk == 0.f) continue;
+            float mk[3];
+            moved_mean(tb, mov3, img_pitch, Wh, Hh, x + shx + (k & 1), y + shy + (k >> 1), mk);
+#pragma unroll
+            for (int c = 0; c < 3; c++) mm[c] += wk * mk[c];
+        }
     }
     float md = fabsf(mr[0] - mm[0]) + fabsf(mr[1] - mm[1]) + fabsf(mr[2] - mm[2]);
     md /= 3.0f;
@@ -234,17 +275,19 @@ __device__ __forceinline__ MaskTerms mask_terms(const RobustTabs& tb, const floa
     return r;
 }
 
+template <bool BIL>
 __device__ __forceinline__ float4 mask_fast(const RobustTabs& tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
                                             const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m,
                                             float s_lit, float t_lit, int x, int y)
 {
-    const MaskTerms r = mask_terms(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s_lit, t_lit, x, y);
+    const MaskTerms r = mask_terms<BIL>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s_lit, t_lit, x, y);
     return make_float4(r.m[0], r.m[1], r.m[2], r.M);
 }
 
 // Adjoint support: the un-eroded mask of every half-res pixel (border 1, as
 // in the forward) and its exponentials and gain (zero on the border, whose
 // value does not depend on s and t).
+template <bool BIL>
 __global__ void k_mask_store(RobustTabs tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh, const float2* __restrict__ flow,
                              size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s, float t, float4* __restrict__ m_out,
                              float4* __restrict__ aux_out, size_t sp)
@@ -253,7 +296,7 @@ __global__ void k_mask_store(RobustTabs tb, const float* __restrict__ mov3, size
     if (x >= Wh || y >= Hh) return;
     float4 m = make_float4(1.f, 1.f, 1.f, 1.f), aux = make_float4(0.f, 0.f, 0.f, 0.f);
     if (x >= 1 && x < Wh - 1 && y >= 1 && y < Hh - 1) {
-        const MaskTerms r = mask_terms(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, x, y);
+        const MaskTerms r = mask_terms<BIL>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, x, y);
         m = make_float4(r.m[0], r.m[1], r.m[2], r.M);
         aux = make_float4(r.E[0], r.E[1], r.E[2], r.sg);
     }
@@ -266,6 +309,7 @@ __global__ void k_mask_store(RobustTabs tb, const float* __restrict__ mov3, size
 // separable min filter: rows, then columns.
 constexpr int RF_T = 32;
 
+template <bool BIL>
 __global__ void __launch_bounds__(256) k_robustness_erode_fast(RobustTabs tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
                                                               const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha,
                                                               float beta, float thr_m, float s, float t, int size, float4* __restrict__ out,
@@ -282,7 +326,7 @@ __global__ void __launch_bounds__(256) k_robustness_erode_fast(RobustTabs tb, co
         const int qx = isa::clampi(x0 + sx - a, 0, Wh - 1), qy = isa::clampi(y0 + sy - a, 0, Hh - 1);
         float4 v = make_float4(1.f, 1.f, 1.f, 1.f);
         if (qx >= 1 && qx < Wh - 1 && qy >= 1 && qy < Hh - 1)
-            v = mask_fast(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, qx, qy);
+            v = mask_fast<BIL>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, qx, qy);
         sm[i] = v;
     }
     __syncthreads();
@@ -372,6 +416,79 @@ __global__ void __launch_bounds__(256) k_mask_param_bwd(const float4* __restrict
     }
 }
 
+// dL/dflow of the mask in sample mode BILINEAR, from the un-eroded mask's
+// gradient g_mask: mask_c = clamp(sg E_c - t, 0, 1), E_c = exp(-dist_c^2 /
+// sig_c^2), dist_c = |mr_c - mm_c| k_c with k_c = sr_c^2 / (sr_c^2 + smd_c^2),
+// and mm_c the blend of the four moved 3x3 means B_k around sf / 2 (sf the
+// flow sample of the half-res pixel):
+//   dmm/dbx = (1 - by)(B_1 - B_0) + by (B_3 - B_2),
+//   dmm/dby = (1 - bx)(B_2 - B_0) + bx (B_3 - B_1),
+// and d(sf / 2)/dsf = 1/2. The flow also enters M, which only switches sg at
+// a threshold (zero derivative almost everywhere). The gradient of sf goes to
+// the four full-res flow texels of its bilinear (mirror) lookup (atomic adds).
+__global__ void __launch_bounds__(256) k_mask_flow_bwd(RobustTabs tb, const float* __restrict__ mov3, size_t img_pitch, int Wh, int Hh,
+                                                      const float2* __restrict__ flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
+                                                      float t_lit, const float4* __restrict__ aux, const float4* __restrict__ g_mask,
+                                                      float2* __restrict__ gflow)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x < 1 || x >= Wh - 1 || y < 1 || y >= Hh - 1) return;
+    const float4 gm = __ldg(isa::row_ptr(g_mask, tb.sp, y) + x);
+    const float4 ax = __ldg(isa::row_ptr(aux, tb.sp, y) + x);
+    if (ax.w == 0.f || (gm.x == 0.f && gm.y == 0.f && gm.z == 0.f)) return;
+    const float2 sf = flow_sample(flow, flow_pitch, Wf, Hf, Wh, Hh, x, y);
+    int shx, shy;
+    float bx, by;
+    moved_offset<true>(sf, shx, shy, bx, by);
+    float B[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; k++) moved_mean(tb, mov3, img_pitch, Wh, Hh, x + shx + (k & 1), y + shy + (k >> 1), B[k]);
+    float mm[3];
+    const float w0 = (1.f - bx) * (1.f - by);
+#pragma unroll
+    for (int c = 0; c < 3; c++) mm[c] = B[0][c] * w0;
+#pragma unroll
+    for (int k = 1; k < 4; k++) {
+        const float wk = ((k & 1) ? bx : 1.f - bx) * ((k >> 1) ? by : 1.f - by);
+        if (wk == 0.f) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++) mm[c] += wk * B[k][c];
+    }
+    const float4 r4 = __ldg(isa::row_ptr(tb.mr, tb.sp, y) + x), s4 = __ldg(isa::row_ptr(tb.sr, tb.sp, y) + x);
+    const float mr[3] = {r4.x, r4.y, r4.z}, sr3[3] = {s4.x, s4.y, s4.z}, g[3] = {gm.x, gm.y, gm.z}, E[3] = {ax.x, ax.y, ax.z};
+    float ghx = 0.f, ghy = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float raw = ax.w * E[c] - t_lit;
+        if (g[c] == 0.f || !(raw > 0.f && raw < 1.f)) continue;
+        const float sr = sr3[c];
+        float smd = sqrtf(alpha * mr[c] + beta);
+        if (c == 1) smd /= sqrtf(2.0f);
+        const float sig = fmaxf(smd, sr);
+        const float kc = sr * sr / (sr * sr + smd * smd);
+        const float dist = fabsf(mr[c] - mm[c]) * kc;
+        const float sgn = mm[c] > mr[c] ? 1.f : (mm[c] < mr[c] ? -1.f : 0.f);
+        const float gmm = g[c] * ax.w * E[c] * (-2.f * dist / (sig * sig)) * kc * sgn;
+        ghx += gmm * ((1.f - by) * (B[1][c] - B[0][c]) + by * (B[3][c] - B[2][c]));
+        ghy += gmm * ((1.f - bx) * (B[2][c] - B[0][c]) + bx * (B[3][c] - B[1][c]));
+    }
+    // the transpose of flow_sample at the half-res pixel
+    const float xb = ((float)x + 0.5f) / (float)Wh * Wf - 0.5f, yb = ((float)y + 0.5f) / (float)Hh * Hf - 0.5f;
+    const float fx = floorf(xb), fy = floorf(yb);
+    const int i = (int)fx, j = (int)fy;
+    const float a = xb - fx, b = yb - fy;
+    const int i0 = isa::mirror(i, Wf), i1 = isa::mirror(i + 1, Wf), j0 = isa::mirror(j, Hf), j1 = isa::mirror(j + 1, Hf);
+    const float w[4] = {(1.f - a) * (1.f - b), a * (1.f - b), (1.f - a) * b, a * b};
+    const int xs[4] = {i0, i1, i0, i1}, ys[4] = {j0, j0, j1, j1};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (w[k] == 0.f) continue;
+        float* d = (float*)(isa::row_ptr(gflow, flow_pitch, ys[k]) + xs[k]);
+        atomicAdd(d, w[k] * 0.5f * ghx);
+        atomicAdd(d + 1, w[k] * 0.5f * ghy);
+    }
+}
+
 inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
 
 }  // namespace
@@ -421,23 +538,42 @@ cudaError_t isa_launch_box3(const float* mov3, size_t img_pitch, int Wh, int Hh,
 
 cudaError_t isa_launch_robustness_erode_tabs(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch,
                                              int Wh, int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta,
-                                             float thr_m, float s, float t, int size, float4* out, size_t out_pitch, cudaStream_t st)
+                                             float thr_m, float s, float t, int size, float4* out, size_t out_pitch, int bil, cudaStream_t st)
 {
     if (size < 1 || size / 2 > RB_MAXA) return cudaErrorInvalidValue;
     RobustTabs tb{mr, sr, box, sp};
     dim3 g((Wh + RF_T - 1) / RF_T, (Hh + RF_T - 1) / RF_T);
-    k_robustness_erode_fast<<<g, 256, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size, out,
-                                               out_pitch);
+    if (bil)
+        k_robustness_erode_fast<true><<<g, 256, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size, out,
+                                                         out_pitch);
+    else
+        k_robustness_erode_fast<false><<<g, 256, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, size, out,
+                                                          out_pitch);
     return cudaGetLastError();
 }
 
 cudaError_t isa_launch_mask_store(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch, int Wh,
                                   int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float thr_m, float s,
-                                  float t, float4* m_out, float4* aux_out, cudaStream_t st)
+                                  float t, float4* m_out, float4* aux_out, int bil, cudaStream_t st)
 {
     RobustTabs tb{mr, sr, box, sp};
     dim3 b(32, 8);
-    k_mask_store<<<grid2(Wh, Hh, b), b, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, m_out, aux_out, sp);
+    if (bil)
+        k_mask_store<true><<<grid2(Wh, Hh, b), b, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, m_out,
+                                                           aux_out, sp);
+    else
+        k_mask_store<false><<<grid2(Wh, Hh, b), b, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, thr_m, s, t, m_out,
+                                                            aux_out, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t isa_launch_mask_flow_bwd(const float4* mr, const float4* sr, const float4* box, size_t sp, const float* mov3, size_t img_pitch, int Wh,
+                                     int Hh, const float2* flow, size_t flow_pitch, int Wf, int Hf, float alpha, float beta, float t,
+                                     const float4* aux, const float4* g_mask, float2* gflow, cudaStream_t st)
+{
+    RobustTabs tb{mr, sr, box, sp};
+    dim3 b(32, 8);
+    k_mask_flow_bwd<<<grid2(Wh, Hh, b), b, 0, st>>>(tb, mov3, img_pitch, Wh, Hh, flow, flow_pitch, Wf, Hf, alpha, beta, t, aux, g_mask, gflow);
     return cudaGetLastError();
 }
 

@@ -44,7 +44,7 @@ class IsaParams(ctypes.Structure):
         ("threshold_m", ctypes.c_float), ("tracking_strategy", ctypes.c_int), ("tracking_block_size", ctypes.c_int),
         ("green_channel_only", ctypes.c_int), ("level_count", ctypes.c_int), ("levels", IsaLevel * MAX_LEVELS),
         ("super_resolution", ctypes.c_int), ("merge_scale", ctypes.c_float), ("robust_s", ctypes.c_float),
-        ("robust_t", ctypes.c_float), ("fused_accumulate", ctypes.c_int),
+        ("robust_t", ctypes.c_float), ("fused_accumulate", ctypes.c_int), ("sample_mode", ctypes.c_int),
     ]
 
 
@@ -69,7 +69,8 @@ class IsaTrackPair(ctypes.Structure):
 EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
-    "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record",
+    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
@@ -137,7 +138,7 @@ def make_params(p: Optional[P.MergeParams] = None, fused_accumulate=True) -> Isa
                  "sigma_structure_tensor", "dth", "dtr", "k_detail", "k_denoise", "k_stretch", "k_shrink", "min_det_lk", "threshold_m",
                  "merge_scale", "robust_s", "robust_t"):
         setattr(c, name, float(getattr(p, name)))
-    for name in ("clear_axis", "iterations_lk", "window_size_lk", "erode_size", "tracking_strategy", "tracking_block_size"):
+    for name in ("clear_axis", "iterations_lk", "window_size_lk", "erode_size", "tracking_strategy", "tracking_block_size", "sample_mode"):
         setattr(c, name, int(getattr(p, name)))
     c.green_channel_only = int(bool(p.green_channel_only))
     c.super_resolution = int(bool(p.super_resolution))
@@ -248,6 +249,48 @@ class Merger:
                                        ctypes.c_size_t(Wo * 4), vp(out), ctypes.c_size_t(Wo * 12),
                                        ctypes.byref(loss), grad.ctypes.data_as(ctypes.c_void_p), stream_ptr(stream)))
         return out, loss.value, grad
+
+    def backward_tiles(self, raw, info: IsaRawInfo, target, weight=None, out=None, shifts=None, rotations=None, reference=0, stream=None):
+        """isa_merge_backward_tiles: (out, loss, grad, tile_grad) with tile_grad
+        = d loss / d (tile flow), a cuda float32 tensor n x tiles_y x tiles_x x 2
+        (the context must use sample_mode SAMPLE_BILINEAR)."""
+        import torch
+        n, H, W = raw.shape
+        Wo, Ho = self.output_size(W, H)
+        if out is None:
+            out = torch.empty((Ho, Wo, 3), dtype=torch.float32, device=raw.device)
+        tx, ty = self.tile_grid(W, H)
+        tg = torch.empty((n, ty, tx, 2), dtype=torch.float32, device=raw.device)
+        pre, keep = self._pre(n, shifts, rotations, reference)
+        loss = ctypes.c_double()
+        grad = np.zeros(8, np.float64)
+        check(lib().isa_merge_backward_tiles(self.ctx, vp(raw), ctypes.c_size_t(W * 2), ctypes.c_size_t(W * H * 2), n, ctypes.byref(info),
+                                             ctypes.byref(pre), vp(target), ctypes.c_size_t(Wo * 12),
+                                             vp(weight) if weight is not None else None, ctypes.c_size_t(Wo * 4), vp(out),
+                                             ctypes.c_size_t(Wo * 12), ctypes.byref(loss), grad.ctypes.data_as(ctypes.c_void_p), vp(tg),
+                                             stream_ptr(stream)))
+        return out, loss.value, grad, tg
+
+    def tile_grid(self, width, height):
+        """Tile counts (tiles_x, tiles_y) of the finest tracking level for a width x height frame."""
+        lv = self.params.levels[0]
+        return ((width // lv.resize_level - 2 * lv.max_shift) // lv.tile_size, (height // lv.resize_level - 2 * lv.max_shift) // lv.tile_size)
+
+    def set_tile_flow(self, tiles=None):
+        """Merge at the given per-frame tile flows (cuda float32 n x tiles_y x
+        tiles_x x 2, kept alive by the caller) instead of the solved ones; None
+        returns to the solved flows (isa_set_tile_flow)."""
+        self._tile_override = tiles
+        check(lib().isa_set_tile_flow(self.ctx, vp(tiles) if tiles is not None else None))
+
+    def tile_flow(self, n, stream=None):
+        """The last merge's per-frame tile flows (isa_tile_flow) as a cuda tensor n x tiles_y x tiles_x x 2."""
+        import torch
+        tx, ty = ctypes.c_int(), ctypes.c_int()
+        check(lib().isa_tile_flow(self.ctx, None, ctypes.byref(tx), ctypes.byref(ty), stream_ptr(stream)))
+        t = torch.empty((n, ty.value, tx.value, 2), dtype=torch.float32, device="cuda")
+        check(lib().isa_tile_flow(self.ctx, vp(t), None, None, stream_ptr(stream)))
+        return t
 
     def merge_host(self, raw_host, info: IsaRawInfo, out_host=None, shifts=None, rotations=None, reference=0, stream=None):
         """raw_host: host uint16 array/tensor (pinned for full speed); returns host float32 Ho x Wo x 3."""

@@ -21,6 +21,7 @@ from typing import List, Tuple
 import numpy as np
 
 FULL, ONLY_ON_REFERENCE, ON_REFERENCE_BLOCK, BLOCKS = 0, 1, 2, 3
+SAMPLE_ROUND, SAMPLE_BILINEAR = 0, 1  # how the accumulation and the mask read a frame at the flow
 MAX_LEVELS = 8
 
 
@@ -68,6 +69,7 @@ class MergeParams:
     merge_scale: float = 0.0         # 0: reference mode (1x plain, or 2x crop when super_resolution)
     robust_s: float = 1.5            # RobustnessModell.cu:472 literal
     robust_t: float = 0.12           # RobustnessModell.cu:476 literal
+    sample_mode: int = SAMPLE_ROUND  # SAMPLE_BILINEAR: blend of the four integer shifts, continuous in the flow
 
     def f32(self, name):
         return float(np.float32(getattr(self, name)))

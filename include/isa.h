@@ -57,6 +57,18 @@ extern "C" {
 #define ISA_TRACK_ON_REFERENCE_BLOCK 2
 #define ISA_TRACK_BLOCKS 3
 
+/* How the accumulation and the robustness mask read a frame at the flow.
+ * ROUND: at the integer shift round(s * flow) and round(flow / 2), as the
+ * reference does (DeBayerKernels.cu:310-311, 403-404; RobustnessModell.cu:
+ * 401-402); the merge is piecewise constant in the flow. BILINEAR: the
+ * contributions at the four integer shifts around the flow, blended with
+ * the bilinear weights of its fractional part (equal to ROUND at integer
+ * flow); the merge is continuous in the flow and isa_merge_backward_tiles
+ * returns its gradient with respect to the tile flow. No counterpart in the
+ * reference. */
+#define ISA_SAMPLE_ROUND 0
+#define ISA_SAMPLE_BILINEAR 1
+
 /* PatchTrackingLevel (PatchTrackingLevel.cs:27-63). */
 typedef struct isa_level {
     int resize_level;
@@ -97,6 +109,7 @@ typedef struct isa_params {
     float robust_s;                   /* 1.5, literal at RobustnessModell.cu:472 */
     float robust_t;                   /* 0.12, literal at RobustnessModell.cu:476 */
     int fused_accumulate;             /* 1: all frames in one accumulation pass (same sums, same order) */
+    int sample_mode;                  /* ISA_SAMPLE_ROUND (reference) or ISA_SAMPLE_BILINEAR (differentiable in the flow) */
 } isa_params;
 
 /* RawFile metadata the merge uses (PefFile/RawFile.cs:94-119). white excludes black. */
@@ -186,6 +199,38 @@ ISA_API int isa_merge_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch,
 ISA_API int isa_merge_backward(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
                                const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch,
                                float* out, size_t out_pitch, double* loss, double* grad, void* stream);
+/* isa_merge_backward plus the gradient of the loss with respect to every
+ * frame's tile flow (the per-tile shifts of the finest level that
+ * CreateFlowFieldFromTiles, opticalFlow.cu:48-95, spreads over the frame):
+ * tile_grad (device, 8-byte aligned) receives n x tiles_y x tiles_x float2,
+ * frame i at tile_grad + 2 i tiles_x tiles_y, zero for the reference frame
+ * (isa_tile_flow gives tiles_x, tiles_y). The chain is the adjoint of the
+ * accumulation (DeBayerKernels.cu:290-468) and of the robustness mask
+ * (RobustnessModell.cu:29-157) with respect to the final flow, of each LK
+ * iteration (warp, derivatives, window sums and 2x2 solve,
+ * opticalFlow.cu:28-325; the flows before each iteration are recomputed
+ * from the tile flow) and of the flow from tiles. Needs a context created
+ * with sample_mode ISA_SAMPLE_BILINEAR (the merge is then continuous in the
+ * flow; its scratch, 100 B per frame pixel, is allocated with the context)
+ * and at most 3 LK iterations. The mask's flow term M only switches its gain
+ * at a threshold and the LK solve leaves a pixel unchanged below minDet:
+ * the gradient is that of the smooth piece. No counterpart in the reference. */
+ISA_API int isa_merge_backward_tiles(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
+                                     const isa_prealign* pre, const float* target, size_t target_pitch, const float* weight, size_t weight_pitch,
+                                     float* out, size_t out_pitch, double* loss, double* grad, float* tile_grad, void* stream);
+/* Tile flows in place of the solved ones: while `tiles` (device, caller-owned,
+ * 8-byte aligned; n x tiles_y x tiles_x float2, frame i at tiles + 2 i
+ * tiles_x tiles_y, the reference frame's entry unused) is set, each merge
+ * spreads these over the frame instead of the tile alignment's
+ * (isa_optimal_shifts) result; the tile alignment still runs. NULL returns
+ * to the solved flows. Used to evaluate the merge at chosen tile flows
+ * (finite differences, fits). No counterpart in the reference. */
+ISA_API int isa_set_tile_flow(isa_ctx* ctx, const float* tiles);
+/* The tile flows of the last merge (the solved ones, or those set with
+ * isa_set_tile_flow), in isa_set_tile_flow's layout, into `tiles` (device,
+ * 8-byte aligned; NULL: only the grid size) on `stream`; tiles_x, tiles_y:
+ * the finest level's tile counts. */
+ISA_API int isa_tile_flow(isa_ctx* ctx, float* tiles, int* tiles_x, int* tiles_y, void* stream);
 /* Many bursts of different sizes, frame counts, CFA layouts, bit depths and
  * merge scales (no counterpart in the reference, whose controller merges one
  * burst). Each burst goes to the context with the least work queued so far

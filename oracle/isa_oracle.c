@@ -681,8 +681,13 @@ EXPORT void orc_debayer_subsample(const uint16_t* raw, int W, int H, const int* 
  * The running max/min of the reference compares each tap with the centre
  * only, so M depends on the last tap; kept as is. s and t are the literals
  * 1.5 and 0.12 of the reference. */
-EXPORT void orc_robustness_mask(const real* ref, const real* mov, int Wh, int Hh, const real* flow, int Wf, int Hf,
-                                real alpha, real beta, real thresholdM, real s_lit, real t_lit, real* mask)
+/* bil = 0: the moved 3x3 mean at round(flow / 2) (RobustnessModell.cu:401-402);
+ * bil = 1 (sample mode BILINEAR, no counterpart in the reference): the
+ * moved means at the four integer offsets around flow / 2, blended with the
+ * bilinear weights of its fractional part, so that the mask is continuous in
+ * the flow. */
+static void robustness_mask_mode(const real* ref, const real* mov, int Wh, int Hh, const real* flow, int Wf, int Hf,
+                                 real alpha, real beta, real thresholdM, real s_lit, real t_lit, real* mask, int bil)
 {
     for (int y = 1; y < Hh - 1; y++)
         for (int x = 1; x < Wh - 1; x++) {
@@ -696,16 +701,36 @@ EXPORT void orc_robustness_mask(const real* ref, const real* mov, int Wh, int Hh
                     mxx = fmax(sx, fx); mxy = fmax(sy, fy);
                     mnx = fmin(sx, fx); mny = fmin(sy, fy);
                 }
-            int shx = (int)round(fx * 0.5), shy = (int)round(fy * 0.5);
             real mr[3] = {0, 0, 0}, mm[3] = {0, 0, 0}, sd[3] = {0, 0, 0};
             for (int j = -1; j <= 1; j++)
                 for (int i = -1; i <= 1; i++) {
                     const real* p = ref + ((size_t)(y + j) * Wh + x + i) * 3;
-                    int qy = clampi(y + shy + j, 0, Hh - 1), qx = clampi(x + shx + i, 0, Wh - 1);
-                    const real* q = mov + ((size_t)qy * Wh + qx) * 3;
-                    for (int c = 0; c < 3; c++) { mr[c] += p[c]; mm[c] += q[c]; }
+                    for (int c = 0; c < 3; c++) mr[c] += p[c];
                 }
-            for (int c = 0; c < 3; c++) { mr[c] /= 9; mm[c] /= 9; }
+            int shx, shy, nc;
+            real bx = 0, by = 0;
+            if (bil) {
+                real hx = fx * 0.5, hy = fy * 0.5;
+                shx = (int)floor(hx); shy = (int)floor(hy);
+                bx = hx - shx; by = hy - shy;
+                nc = 4;
+            } else {
+                shx = (int)round(fx * 0.5); shy = (int)round(fy * 0.5);
+                nc = 1;
+            }
+            for (int k = 0; k < nc; k++) {
+                int dx = k & 1, dy = k >> 1;
+                real wk = bil ? (dx ? bx : 1 - bx) * (dy ? by : 1 - by) : 1;
+                real box[3] = {0, 0, 0};
+                for (int j = -1; j <= 1; j++)
+                    for (int i = -1; i <= 1; i++) {
+                        int qy = clampi(y + shy + dy + j, 0, Hh - 1), qx = clampi(x + shx + dx + i, 0, Wh - 1);
+                        const real* q = mov + ((size_t)qy * Wh + qx) * 3;
+                        for (int c = 0; c < 3; c++) box[c] += q[c];
+                    }
+                for (int c = 0; c < 3; c++) mm[c] += wk * (box[c] / 9);
+            }
+            for (int c = 0; c < 3; c++) mr[c] /= 9;
             real md = (fabs(mr[0] - mm[0]) + fabs(mr[1] - mm[1]) + fabs(mr[2] - mm[2])) / 3;
             mxx *= 0.5 * md; mxy *= 0.5 * md; mnx *= 0.5 * md; mny *= 0.5 * md;
             real M = sqrt((mxx - mnx) * (mxx - mnx) + (mxy - mny) * (mxy - mny));
@@ -727,6 +752,18 @@ EXPORT void orc_robustness_mask(const real* ref, const real* mov, int Wh, int Hh
             }
             o[3] = M;
         }
+}
+
+EXPORT void orc_robustness_mask(const real* ref, const real* mov, int Wh, int Hh, const real* flow, int Wf, int Hf,
+                                real alpha, real beta, real thresholdM, real s_lit, real t_lit, real* mask)
+{
+    robustness_mask_mode(ref, mov, Wh, Hh, flow, Wf, Hf, alpha, beta, thresholdM, s_lit, t_lit, mask, 0);
+}
+
+EXPORT void orc_robustness_mask_bil(const real* ref, const real* mov, int Wh, int Hh, const real* flow, int Wf, int Hf,
+                                    real alpha, real beta, real thresholdM, real s_lit, real t_lit, real* mask)
+{
+    robustness_mask_mode(ref, mov, Wh, Hh, flow, Wf, Hf, alpha, beta, thresholdM, s_lit, t_lit, mask, 1);
 }
 
 /* NPP ErodeBorder with an all-ones size x size mask, anchor size/2 and
@@ -798,11 +835,16 @@ EXPORT void orc_kernel_param(real* st, int W, int H, real Dth, real Dtr, real kD
 /* kparam: H x W x kc (kc = 3 or 4); flow: H x W x 2.                        */
 /* crop: x0, y0, x1, y1 inclusive.                                           */
 /* ------------------------------------------------------------------------ */
-EXPORT void orc_accumulate(const uint16_t* raw, int W, int H, const int* cfa, real* acc, real* wsum, int Wo, int Ho,
-                           const real* mask, const real* kparam, int kc, const real* flow,
-                           const real* white, const real* black, real s, int ox, int oy, const int* crop)
+/* bil = 0: the frame is read at the integer shift round(s * flow)
+ * (DeBayerKernels.cu:310-311, 403-404); bil = 1 (sample mode BILINEAR, no
+ * counterpart in the reference): the contributions at the four integer
+ * shifts around s * flow, blended with the bilinear weights of its
+ * fractional part, so that the merge is continuous in the flow. */
+static void accumulate_mode(const uint16_t* raw, int W, int H, const int* cfa, real* acc, real* wsum, int Wo, int Ho,
+                            const real* mask, const real* kparam, int kc, const real* flow,
+                            const real* white, const real* black, real s, int ox, int oy, const int* crop, int bil)
 {
-    int Wm = W / 2, Hm = H / 2;
+    int Wm = W / 2;
     for (int y = 1; y < Ho - 1; y++)
         for (int x = 1; x < Wo - 1; x++) {
             real xb = (x + 0.5 + ox) / s - 0.5, yb = (y + 0.5 + oy) / s - 0.5;
@@ -810,28 +852,57 @@ EXPORT void orc_accumulate(const uint16_t* raw, int W, int H, const int* cfa, re
             real k1 = bilinear(kparam, W, H, kc, 1, xb, yb, 0);
             real k2 = bilinear(kparam, W, H, kc, 2, xb, yb, 0);
             real fx = bilinear(flow, W, H, 2, 0, xb, yb, 1), fy = bilinear(flow, W, H, 2, 1, xb, yb, 1);
-            int sx = (int)round(fx * s), sy = (int)round(fy * s);
+            int sx0, sy0, nc;
+            real bx = 0, by = 0;
+            if (bil) {
+                real hx = fx * s, hy = fy * s;
+                sx0 = (int)floor(hx); sy0 = (int)floor(hy);
+                bx = hx - sx0; by = hy - sy0;
+                nc = 4;
+            } else {
+                sx0 = (int)round(fx * s); sy0 = (int)round(fy * s);
+                nc = 1;
+            }
             real* a = acc + ((size_t)y * Wo + x) * 3;
             real* w = wsum + ((size_t)y * Wo + x) * 3;
-            for (int py = -2; py <= 2; py++)
-                for (int px = -2; px <= 2; px++) {
-                    int qx = clampi((int)floor((x + px + sx + ox) / s), crop[0], crop[2]);
-                    int qy = clampi((int)floor((y + py + sy + oy) / s), crop[1], crop[3]);
-                    int ux = clampi((int)floor((x + px + ox) / s), crop[0], crop[2]);
-                    int uy = clampi((int)floor((y + py + oy) / s), crop[1], crop[3]);
-                    int col = cfa[(qy & 1) * 2 + (qx & 1)];
-                    real q = px * px * k0 + 2 * px * py * k2 + py * py * k1;
-                    real wt = exp(-0.5 * q);
-                    if (!isfinite(wt)) wt = px * py == 0 ? 1 : 0;
-                    if (col < 0 || col > 2) continue;
-                    real v = ((real)raw[(size_t)qy * W + qx] - black[col]) / white[col];
-                    real cert = mask[((size_t)(uy / 2) * Wm + ux / 2) * 4 + col];
-                    if (!isfinite(cert)) cert = 0;
-                    a[col] += v * wt * cert;
-                    w[col] += wt * cert;
-                }
-            (void)Hm;
+            for (int k = 0; k < nc; k++) {
+                int sx = sx0 + (k & 1), sy = sy0 + (k >> 1);
+                real wk = bil ? ((k & 1) ? bx : 1 - bx) * ((k >> 1) ? by : 1 - by) : 1;
+                if (wk == 0) continue;
+                for (int py = -2; py <= 2; py++)
+                    for (int px = -2; px <= 2; px++) {
+                        int qx = clampi((int)floor((x + px + sx + ox) / s), crop[0], crop[2]);
+                        int qy = clampi((int)floor((y + py + sy + oy) / s), crop[1], crop[3]);
+                        int ux = clampi((int)floor((x + px + ox) / s), crop[0], crop[2]);
+                        int uy = clampi((int)floor((y + py + oy) / s), crop[1], crop[3]);
+                        int col = cfa[(qy & 1) * 2 + (qx & 1)];
+                        real q = px * px * k0 + 2 * px * py * k2 + py * py * k1;
+                        real wt = exp(-0.5 * q);
+                        if (!isfinite(wt)) wt = px * py == 0 ? 1 : 0;
+                        if (col < 0 || col > 2) continue;
+                        real v = ((real)raw[(size_t)qy * W + qx] - black[col]) / white[col];
+                        real cert = mask[((size_t)(uy / 2) * Wm + ux / 2) * 4 + col];
+                        if (!isfinite(cert)) cert = 0;
+                        if (bil) cert *= wk;
+                        a[col] += v * wt * cert;
+                        w[col] += wt * cert;
+                    }
+            }
         }
+}
+
+EXPORT void orc_accumulate(const uint16_t* raw, int W, int H, const int* cfa, real* acc, real* wsum, int Wo, int Ho,
+                           const real* mask, const real* kparam, int kc, const real* flow,
+                           const real* white, const real* black, real s, int ox, int oy, const int* crop)
+{
+    accumulate_mode(raw, W, H, cfa, acc, wsum, Wo, Ho, mask, kparam, kc, flow, white, black, s, ox, oy, crop, 0);
+}
+
+EXPORT void orc_accumulate_bil(const uint16_t* raw, int W, int H, const int* cfa, real* acc, real* wsum, int Wo, int Ho,
+                               const real* mask, const real* kparam, int kc, const real* flow,
+                               const real* white, const real* black, real s, int ox, int oy, const int* crop)
+{
+    accumulate_mode(raw, W, H, cfa, acc, wsum, Wo, Ho, mask, kparam, kc, flow, white, black, s, ox, oy, crop, 1);
 }
 
 /* A10: ApplyWeighting (kernel.cu:336-391): per channel, where w < thr the

@@ -185,7 +185,7 @@ class StageLib:
         self.kf("debayer_subsample")(_p(np.ascontiguousarray(raw)), W, H, _p(c), self.R(max_val), _p(out))
         return out
 
-    def robustness_mask(self, ref, mov, flow, alpha, beta, thr_m, mask, s=1.5, t=float(np.float32(0.12))):
+    def robustness_mask(self, ref, mov, flow, alpha, beta, thr_m, mask, s=1.5, t=float(np.float32(0.12)), bilinear=False):
         Hh, Wh, _ = ref.shape
         Hf, Wf, _ = flow.shape
         mask = self.arr(mask).copy()
@@ -194,8 +194,8 @@ class StageLib:
             self.k.ref_robustness_mask(_p(self.arr(ref)), _p(self.arr(mov)), Wh, Hh, _p(self.arr(flow)), Wf, Hf, R(alpha), R(beta),
                                        R(thr_m), _p(mask))
         else:
-            self.k.orc_robustness_mask(_p(self.arr(ref)), _p(self.arr(mov)), Wh, Hh, _p(self.arr(flow)), Wf, Hf, R(alpha), R(beta),
-                                       R(thr_m), R(s), R(t), _p(mask))
+            fn = self.k.orc_robustness_mask_bil if bilinear else self.k.orc_robustness_mask
+            fn(_p(self.arr(ref)), _p(self.arr(mov)), Wh, Hh, _p(self.arr(flow)), Wf, Hf, R(alpha), R(beta), R(thr_m), R(s), R(t), _p(mask))
         return mask
 
     def structure_tensor(self, dx, dy):
@@ -218,16 +218,16 @@ class StageLib:
         self.kf("apply_weighting")(_p(img), _p(self.arr(acc)), _p(self.arr(wsum)), W, H, self.R(thr))
         return img
 
-    def accumulate(self, raw, cfa, acc, wsum, mask, kparam, flow, white, black, scale, origin, crop):
-        """Generalised scale-s accumulation (restatement only)."""
+    def accumulate(self, raw, cfa, acc, wsum, mask, kparam, flow, white, black, scale, origin, crop, bilinear=False):
+        """Generalised scale-s accumulation (restatement only); bilinear: sample mode BILINEAR."""
         H, W = raw.shape
         Ho, Wo, _ = acc.shape
         c = np.ascontiguousarray(cfa, dtype=np.int32)
         cr = np.ascontiguousarray(crop, dtype=np.int32)
         kparam = self.arr(kparam)
-        self.k.orc_accumulate(_p(np.ascontiguousarray(raw)), W, H, _p(c), _p(acc), _p(wsum), Wo, Ho, _p(self.arr(mask)), _p(kparam),
-                              kparam.shape[2], _p(self.arr(flow)), _p(self.vec(white)), _p(self.vec(black)), self.R(scale),
-                              origin[0], origin[1], _p(cr))
+        fn = self.k.orc_accumulate_bil if bilinear else self.k.orc_accumulate
+        fn(_p(np.ascontiguousarray(raw)), W, H, _p(c), _p(acc), _p(wsum), Wo, Ho, _p(self.arr(mask)), _p(kparam), kparam.shape[2],
+           _p(self.arr(flow)), _p(self.vec(white)), _p(self.vec(black)), self.R(scale), origin[0], origin[1], _p(cr))
 
     def accumulate_ref(self, raw, cfa, acc, wsum, mask, kparam, flow, white, black, superres):
         H, W = raw.shape
@@ -417,11 +417,17 @@ def out_geometry(W, H, p: P.MergeParams):
 
 
 def merge_burst(burst, p: P.MergeParams = None, kind="oracle64", pre: Optional[PreAlignment] = None,
-                keep: Optional[dict] = None, threads=0, lib: Optional[StageLib] = None):
+                keep: Optional[dict] = None, threads=0, lib: Optional[StageLib] = None, tiles: Optional[dict] = None):
     """Whole forward merge of one burst. Returns MergeResult (FP arrays of the
-    backend's precision). `keep`, when a dict, receives intermediates."""
+    backend's precision). `keep`, when a dict, receives intermediates.
+    `tiles` (frame -> tiles_y x tiles_x x 2) replaces the solved tile flows,
+    as isa_set_tile_flow does; p.sample_mode SAMPLE_BILINEAR selects the
+    blended accumulation and mask (restatement only)."""
     p = p or P.MergeParams()
     lib = lib or StageLib(kind)
+    bil = p.sample_mode == P.SAMPLE_BILINEAR
+    if bil and lib.pfx != "orc_":
+        raise ValueError("sample mode BILINEAR has no counterpart in the reference's kernels")
     if threads:
         lib.set_threads(threads)
     n, H, W = burst.raw.shape
@@ -450,7 +456,7 @@ def merge_burst(burst, p: P.MergeParams = None, kind="oracle64", pre: Optional[P
 
     def accumulate(raw_i, mask_i, flow_i):
         if lib.pfx == "orc_":
-            lib.accumulate(raw_i, burst.cfa, acc, wsum, mask_i, kparam, flow_i, white, black, s, origin, crop)
+            lib.accumulate(raw_i, burst.cfa, acc, wsum, mask_i, kparam, flow_i, white, black, s, origin, crop, bilinear=bil)
         elif not use_canvas:
             lib.accumulate_ref(raw_i, burst.cfa, acc, wsum, mask_i, kp4 if p.super_resolution else kparam, flow_i, white, black,
                                p.super_resolution)
@@ -465,19 +471,19 @@ def merge_burst(burst, p: P.MergeParams = None, kind="oracle64", pre: Optional[P
         if i == ref:
             continue
         mov_half = lib.debayer_subsample(burst.raw[i], burst.cfa, max_val)
-        tiles = lib.optimal_shifts(x, tcx0, tcy0, ref, i)
-        flow = lib.flow_from_tiles(tiles, W, H, pre.shift(ref, i), pre.rotation(ref, i), lv0.tile_size)
+        tiles_i = lib.arr(tiles[i]) if tiles is not None else lib.optimal_shifts(x, tcx0, tcy0, ref, i)
+        flow = lib.flow_from_tiles(tiles_i, W, H, pre.shift(ref, i), pre.rotation(ref, i), lv0.tile_size)
         for _ in range(p.iterations_lk):
             warped = lib.warp(bw_acc[i], flow)
             ix, iy, it = lib.derivatives(warped, bw_acc[ref])
             flow = lib.lucas_kanade(flow, ix, iy, it, p.window_size_lk // 2, p.f32("min_det_lk"))
         mask = lib.robustness_mask(ref_half, mov_half, flow, float(np.float32(burst.noise_a)), float(np.float32(burst.noise_b)),
-                                   p.f32("threshold_m"), mask, p.f32("robust_s"), p.f32("robust_t"))
+                                   p.f32("threshold_m"), mask, p.f32("robust_s"), p.f32("robust_t"), bilinear=bil)
         eroded = lib.erode(mask, p.erode_size)
         if keep is not None:
             keep.setdefault("flow", {})[i] = flow
             keep.setdefault("mask", {})[i] = eroded
-            keep.setdefault("tiles", {})[i] = tiles
+            keep.setdefault("tiles", {})[i] = tiles_i
         accumulate(burst.raw[i], eroded, flow)
     if thr > 0:
         cw = np.asarray(burst.camera_white, np.float64)
@@ -508,12 +514,14 @@ def merge_tail(burst, p: P.MergeParams, flows, masks, kparam, lib: StageLib, ref
     acc = np.zeros((Ho, Wo, 3), lib.dtype)
     wsum = np.zeros((Ho, Wo, 3), lib.dtype)
     kparam = lib.arr(kparam)
+    bil = p.sample_mode == P.SAMPLE_BILINEAR
     lib.accumulate(burst.raw[reference], burst.cfa, acc, wsum, np.ones((H // 2, W // 2, 4), lib.dtype), kparam,
-                   np.zeros((H, W, 2), lib.dtype), white, black, s, origin, crop)
+                   np.zeros((H, W, 2), lib.dtype), white, black, s, origin, crop, bilinear=bil)
     for i in range(n):
         if i == reference:
             continue
-        lib.accumulate(burst.raw[i], burst.cfa, acc, wsum, lib.arr(masks[i]), kparam, lib.arr(flows[i]), white, black, s, origin, crop)
+        lib.accumulate(burst.raw[i], burst.cfa, acc, wsum, lib.arr(masks[i]), kparam, lib.arr(flows[i]), white, black, s, origin, crop,
+                       bilinear=bil)
     if thr > 0:
         cw = np.asarray(burst.camera_white, np.float64)
         dec = lib.debayer_full(burst.raw[reference], burst.cfa, black, (1.0 / cw).astype(np.float32),
@@ -521,6 +529,41 @@ def merge_tail(burst, p: P.MergeParams, flows, masks, kparam, lib: StageLib, ref
     else:
         dec = np.zeros((Ho, Wo, 3), lib.dtype)
     return MergeResult(image=lib.apply_weighting(dec, acc, wsum, thr), acc=acc, wsum=wsum)
+
+
+def merge_from_tiles(burst, p: P.MergeParams, tiles, keep, lib: StageLib, pre: Optional[PreAlignment] = None):
+    """The merge from given per-frame tile flows on (frame -> tiles_y x
+    tiles_x x 2): flow from tiles, LK, robustness mask and erosion (Accumulate
+    :1961-1977), accumulation and ApplyWeighting, reusing the intermediates of
+    an earlier merge_burst of the same burst and parameters that do not
+    depend on the tile flows (keep["bw_acc"], keep["kparam"]). Equal to
+    merge_burst(..., tiles=tiles) without its tile alignment; the finite
+    differences of the tile-flow gradient evaluate it."""
+    n, H, W = burst.raw.shape
+    pre = pre or PreAlignment.zeros(n)
+    ref = pre.reference
+    bw_acc, kparam = keep["bw_acc"], keep["kparam"]
+    white = np.asarray(burst.white, np.float64)
+    black = np.asarray(burst.black, np.float64)
+    max_val = float(np.max(np.float32(white) + np.float32(black)))
+    ref_half = lib.debayer_subsample(burst.raw[ref], burst.cfa, max_val)
+    bil = p.sample_mode == P.SAMPLE_BILINEAR
+    flows, masks = {}, {}
+    mask = np.ones((H // 2, W // 2, 4), lib.dtype)
+    for i in range(n):
+        if i == ref:
+            continue
+        mov_half = lib.debayer_subsample(burst.raw[i], burst.cfa, max_val)
+        flow = lib.flow_from_tiles(lib.arr(tiles[i]), W, H, pre.shift(ref, i), pre.rotation(ref, i), p.levels[0].tile_size)
+        for _ in range(p.iterations_lk):
+            warped = lib.warp(bw_acc[i], flow)
+            ix, iy, it = lib.derivatives(warped, bw_acc[ref])
+            flow = lib.lucas_kanade(flow, ix, iy, it, p.window_size_lk // 2, p.f32("min_det_lk"))
+        mask = lib.robustness_mask(ref_half, mov_half, flow, float(np.float32(burst.noise_a)), float(np.float32(burst.noise_b)),
+                                   p.f32("threshold_m"), mask, p.f32("robust_s"), p.f32("robust_t"), bilinear=bil)
+        flows[i] = flow
+        masks[i] = lib.erode(mask, p.erode_size)
+    return merge_tail(burst, p, flows, masks, kparam, lib, reference=ref)
 
 
 def accumulate_canvas_ref(lib, raw, cfa, acc, wsum, mask, kp4, flow, white, black, s):
