@@ -247,6 +247,73 @@ def adjoint_ratio(args):
                          "fwd_ms": fwd_b, "fwd_adj_tiles_ms": both_b, "ratio": both_b / fwd_b}}
 
 
+FIT_NAMES = ("k_detail", "k_denoise", "dth", "dtr", "k_stretch", "k_shrink", "robust_s", "robust_t")
+
+
+def param_fit(width, height, frames, steps, moving_object=0.0, max_shift=None, seed=3000):
+    """Adam on the eight merge parameters (isa_merge_backward), in log space
+    from the reference defaults, fitting the merge at scale 1 to the clean
+    scene of the reference frame (the synthetic generator keeps it). Loss and
+    PSNR over the output pixels inside a 32 px margin whose smallest weight
+    sum is at least 0.05; PSNR against the scene before and after the fit."""
+    import torch
+    from imagestackalignator_b200 import isa, params as P, synthetic
+    b = synthetic.make_burst(width, height, frames, seed=seed, max_shift=max_shift or WORKLOAD["max_shift"],
+                             max_rot_deg=WORKLOAD["max_rot_deg"], noise_a=WORKLOAD["noise_a"], noise_b=WORKLOAD["noise_b"], device="cuda",
+                             keep_truth=True, moving_object=moving_object)
+    p = P.MergeParams()
+    p.merge_scale = 1.0
+    m = isa.Merger(width, height, frames, p)
+    info = isa.make_info(b)
+    raw = torch.from_numpy(b.raw.view(np.int16)).cuda()
+    truth = torch.from_numpy(b.truth.astype(np.float32)).cuda().contiguous()
+    out = m.merge(raw, info).clone()
+    wsum = isa.device_copy(m.debug(0)["wsum"], (height, width, 3), torch.float32)
+    om = (wsum.min(dim=2).values >= 0.05).float()
+    om[:32] = 0
+    om[-32:] = 0
+    om[:, :32] = 0
+    om[:, -32:] = 0
+    om = om.contiguous()
+    npx = float(om.sum())
+
+    def psnr(img):
+        mse = float((om[..., None] * (img - truth) ** 2).sum()) / (3 * npx)
+        return 10 * np.log10(1.0 / mse)
+
+    base = np.array([getattr(p, k) for k in FIT_NAMES], np.float64)
+    u = np.zeros(8)
+    mom, vel = np.zeros(8), np.zeros(8)
+    lr, b1, b2 = 0.02, 0.9, 0.999
+    losses = []
+    psnr0 = psnr(out)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for step in range(1, steps + 1):
+        q = P.MergeParams(**vars(p))
+        for k, v in zip(FIT_NAMES, base * np.exp(u)):
+            setattr(q, k, float(v))
+        m.set_params(q)
+        _, loss, g = m.backward(raw, info, truth, weight=om, out=out)
+        losses.append(loss)
+        gu = g * base * np.exp(u)  # d loss / d log(theta)
+        mom = b1 * mom + (1 - b1) * gu
+        vel = b2 * vel + (1 - b2) * gu * gu
+        u -= lr * (mom / (1 - b1 ** step)) / (np.sqrt(vel / (1 - b2 ** step)) + 1e-12)
+    q = P.MergeParams(**vars(p))
+    for k, v in zip(FIT_NAMES, base * np.exp(u)):
+        setattr(q, k, float(v))
+    m.set_params(q)
+    fitted = m.merge(raw, info, out).clone()
+    torch.cuda.synchronize()
+    dt = time.time() - t0
+    res = {"workload": f"{frames}x{width}x{height} merged at 1x" + (f", moving object {moving_object:.0%} of the frame" if moving_object else ""),
+           "steps": steps, "loss_first": losses[0], "loss_last": losses[-1], "psnr_before_db": psnr0, "psnr_after_db": psnr(fitted),
+           "ms_per_step": 1000 * dt / steps, "params_after": {k: float(v) for k, v in zip(FIT_NAMES, base * np.exp(u))}}
+    m.close()
+    return res
+
+
 BATCH = dict(width=2048, height=1536, frames=8, bursts=16, contexts=4)  # many small bursts (phone-sized) merged at 2x
 
 
@@ -616,6 +683,13 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = adjoint_ratio(args)
+    fit = None
+    if rank == 0 and world == 1 and not args.no_fit:
+        fit = param_fit(ADJ["width"], ADJ["height"], ADJ["frames"], 200)
+    fit_large = None
+    if rank == 0 and world == 1 and args.fit_large:
+        fit_large = param_fit(LARGE["width"], LARGE["height"], LARGE["frames"], args.fit_large, moving_object=LARGE["moving_object"],
+                              max_shift=LARGE["max_shift"], seed=4000)
     post = None
     if rank == 0 and world == 1 and not args.no_post:
         post = post_throughput(args, out)
@@ -648,7 +722,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint, "batch": batch, "large_local_motion": large, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec, "dng_files_e2e": files,
+        "fwd_adjoint": adjoint, "param_fit": fit, "param_fit_large": fit_large, "batch": batch, "large_local_motion": large, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec, "dng_files_e2e": files,
         "clocks": clocks,
     }
     if rank == 0:
@@ -670,6 +744,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
+    ap.add_argument("--no-fit", action="store_true", help="skip the 200-step parameter fit on the differentiable-merge burst")
+    ap.add_argument("--fit-large", type=int, default=0, help="Adam steps of the parameter fit on the 50-frame burst with local motion (0: none)")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
     ap.add_argument("--no-large", action="store_true", help="skip the 50-frame burst with local motion")
     ap.add_argument("--no-post", action="store_true", help="skip the colour/tone post-processing timing")

@@ -1210,6 +1210,24 @@ int isa_debug_shifts(isa_ctx* c, const void** one_to_one, int* tx, int* ty)
     return ISA_OK;
 }
 
+int isa_ctx_set_params(isa_ctx* c, const isa_params* q)
+{
+    if (!c) return fail(ISA_EINVAL, "ctx is NULL");
+    ISA_TRY(check_params(q));
+    const isa_params& o = c->p;
+    bool same = q->level_count == o.level_count && q->tracking_strategy == o.tracking_strategy && q->tracking_block_size == o.tracking_block_size;
+    for (int l = 0; same && l < q->level_count; l++)
+        same = q->levels[l].resize_level == o.levels[l].resize_level && q->levels[l].tile_size == o.levels[l].tile_size &&
+               q->levels[l].max_shift == o.levels[l].max_shift;
+    if (!same) return fail(ISA_EINVAL, "the parameters change the pyramid levels or the tracking strategy of the context");
+    isa_accum_geom g;
+    float thr;
+    accum_geom(q, c->max_w, c->max_h, g, thr);
+    if (g.Wo > c->max_wo || g.Ho > c->max_ho) return fail(ISA_EINVAL, "output %dx%d exceeds the context's %dx%d", g.Wo, g.Ho, c->max_wo, c->max_ho);
+    c->p = *q;
+    return ISA_OK;
+}
+
 int isa_set_tile_flow(isa_ctx* c, const float* tiles)
 {
     if (!c) return fail(ISA_EINVAL, "ctx is NULL");

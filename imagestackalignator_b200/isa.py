@@ -70,7 +70,7 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record",
-    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
@@ -275,6 +275,12 @@ class Merger:
         """Tile counts (tiles_x, tiles_y) of the finest tracking level for a width x height frame."""
         lv = self.params.levels[0]
         return ((width // lv.resize_level - 2 * lv.max_shift) // lv.tile_size, (height // lv.resize_level - 2 * lv.max_shift) // lv.tile_size)
+
+    def set_params(self, params: P.MergeParams):
+        """Replace the context's parameters (isa_ctx_set_params): same levels and tracking, output within the context."""
+        c = make_params(params, bool(self.params.fused_accumulate))
+        check(lib().isa_ctx_set_params(self.ctx, ctypes.byref(c)))
+        self.params = c
 
     def set_tile_flow(self, tiles=None):
         """Merge at the given per-frame tile flows (cuda float32 n x tiles_y x

@@ -154,6 +154,13 @@ ISA_API const char* isa_version(void);
  * the controller buffers :1832-1849). */
 ISA_API int isa_ctx_create(isa_ctx** ctx, int max_width, int max_height, int max_frames, const isa_params* p);
 ISA_API int isa_ctx_destroy(isa_ctx* ctx);
+/* Replaces the context's parameters between calls (a parameter fit, for
+ * instance). The pyramid levels, the tracking strategy and block size must
+ * stay those of isa_ctx_create, and the output of a max_width x max_height
+ * frame must still fit the context; else ISA_EINVAL and the parameters are
+ * unchanged. Allocates nothing. No counterpart in the reference, whose
+ * controller reads its properties at each run. */
+ISA_API int isa_ctx_set_params(isa_ctx* ctx, const isa_params* p);
 /* Output size of the merge for a frame size under p. */
 ISA_API int isa_output_size(const isa_params* p, int width, int height, int* out_width, int* out_height);
 /* Stage times (ms) of the last isa_merge_burst call, in order: tracking

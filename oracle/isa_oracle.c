@@ -865,6 +865,14 @@ static void accumulate_mode(const uint16_t* raw, int W, int H, const int* cfa, r
             }
             real* a = acc + ((size_t)y * Wo + x) * 3;
             real* w = wsum + ((size_t)y * Wo + x) * 3;
+            real wts[25];
+            for (int py = -2; py <= 2; py++)
+                for (int px = -2; px <= 2; px++) {
+                    real q = px * px * k0 + 2 * px * py * k2 + py * py * k1;
+                    real wt = exp(-0.5 * q);
+                    if (!isfinite(wt)) wt = px * py == 0 ? 1 : 0;
+                    wts[(py + 2) * 5 + px + 2] = wt;
+                }
             for (int k = 0; k < nc; k++) {
                 int sx = sx0 + (k & 1), sy = sy0 + (k >> 1);
                 real wk = bil ? ((k & 1) ? bx : 1 - bx) * ((k >> 1) ? by : 1 - by) : 1;
@@ -876,9 +884,7 @@ static void accumulate_mode(const uint16_t* raw, int W, int H, const int* cfa, r
                         int ux = clampi((int)floor((x + px + ox) / s), crop[0], crop[2]);
                         int uy = clampi((int)floor((y + py + oy) / s), crop[1], crop[3]);
                         int col = cfa[(qy & 1) * 2 + (qx & 1)];
-                        real q = px * px * k0 + 2 * px * py * k2 + py * py * k1;
-                        real wt = exp(-0.5 * q);
-                        if (!isfinite(wt)) wt = px * py == 0 ? 1 : 0;
+                        real wt = wts[(py + 2) * 5 + px + 2];
                         if (col < 0 || col > 2) continue;
                         real v = ((real)raw[(size_t)qy * W + qx] - black[col]) / white[col];
                         real cert = mask[((size_t)(uy / 2) * Wm + ux / 2) * 4 + col];

@@ -484,6 +484,7 @@ def merge_burst(burst, p: P.MergeParams = None, kind="oracle64", pre: Optional[P
             keep.setdefault("flow", {})[i] = flow
             keep.setdefault("mask", {})[i] = eroded
             keep.setdefault("tiles", {})[i] = tiles_i
+            keep.setdefault("tail_flow", {}).setdefault(i, (np.array(tiles_i, copy=True), flow))
         accumulate(burst.raw[i], eroded, flow)
     if thr > 0:
         cw = np.asarray(burst.camera_white, np.float64)
@@ -534,36 +535,82 @@ def merge_tail(burst, p: P.MergeParams, flows, masks, kparam, lib: StageLib, ref
 def merge_from_tiles(burst, p: P.MergeParams, tiles, keep, lib: StageLib, pre: Optional[PreAlignment] = None):
     """The merge from given per-frame tile flows on (frame -> tiles_y x
     tiles_x x 2): flow from tiles, LK, robustness mask and erosion (Accumulate
-    :1961-1977), accumulation and ApplyWeighting, reusing the intermediates of
-    an earlier merge_burst of the same burst and parameters that do not
-    depend on the tile flows (keep["bw_acc"], keep["kparam"]). Equal to
-    merge_burst(..., tiles=tiles) without its tile alignment; the finite
-    differences of the tile-flow gradient evaluate it."""
+    :1961-1977), kernel parameters, accumulation and ApplyWeighting, reusing
+    the reference frame's accumulation image of an earlier merge_burst of the
+    same burst (keep["bw_acc"]). Equal to merge_burst(..., tiles=tiles)
+    without its tile alignment; the finite differences of the tile-flow and
+    parameter gradients evaluate it.
+
+    Each frame's flow (which depends on its tile flow), mask (also on
+    robust_s, robust_t) and accumulation sums (also on the kernel parameters)
+    of the first call are cached in keep, so that a call that changes one
+    frame's tile flow, or only the mask or kernel parameters, recomputes only
+    what depends on the change. The frames' sums are added in frame order
+    (merge_burst's running sums up to FP64 rounding)."""
     n, H, W = burst.raw.shape
     pre = pre or PreAlignment.zeros(n)
     ref = pre.reference
-    bw_acc, kparam = keep["bw_acc"], keep["kparam"]
+    bw_acc = keep["bw_acc"]
     white = np.asarray(burst.white, np.float64)
     black = np.asarray(burst.black, np.float64)
     max_val = float(np.max(np.float32(white) + np.float32(black)))
-    ref_half = lib.debayer_subsample(burst.raw[ref], burst.cfa, max_val)
     bil = p.sample_mode == P.SAMPLE_BILINEAR
-    flows, masks = {}, {}
-    mask = np.ones((H // 2, W // 2, 4), lib.dtype)
-    for i in range(n):
-        if i == ref:
-            continue
-        mov_half = lib.debayer_subsample(burst.raw[i], burst.cfa, max_val)
-        flow = lib.flow_from_tiles(lib.arr(tiles[i]), W, H, pre.shift(ref, i), pre.rotation(ref, i), p.levels[0].tile_size)
-        for _ in range(p.iterations_lk):
-            warped = lib.warp(bw_acc[i], flow)
-            ix, iy, it = lib.derivatives(warped, bw_acc[ref])
-            flow = lib.lucas_kanade(flow, ix, iy, it, p.window_size_lk // 2, p.f32("min_det_lk"))
-        mask = lib.robustness_mask(ref_half, mov_half, flow, float(np.float32(burst.noise_a)), float(np.float32(burst.noise_b)),
-                                   p.f32("threshold_m"), mask, p.f32("robust_s"), p.f32("robust_t"), bilinear=bil)
-        flows[i] = flow
-        masks[i] = lib.erode(mask, p.erode_size)
-    return merge_tail(burst, p, flows, masks, kparam, lib, reference=ref)
+    Wo, Ho, s, origin, crop, thr = out_geometry(W, H, p)
+    if thr > 0:
+        raise ValueError("merge_from_tiles covers the merge_scale and super-resolution modes (normalisation threshold 0)")
+    kkey = tuple(p.f32(k) for k in ("dth", "dtr", "k_detail", "k_denoise", "k_stretch", "k_shrink")) + (p.sigma_structure_tensor,)
+    mkey = (p.f32("robust_s"), p.f32("robust_t"))
+    kp = keep.setdefault("tail_kparam", {})
+    if kkey not in kp:
+        if len(kp) >= 2:
+            kp.pop(next(k for k in kp if k != next(iter(kp))))  # keep the first entry and one more
+        dx, dy = lib.derivatives2(bw_acc[ref])
+        st = lib.gauss_filter(lib.structure_tensor(dx, dy), lib.gauss_taps(p.sigma_structure_tensor))
+        kp[kkey] = lib.kernel_param(st, p)
+    kparam = kp[kkey]
+    fc = keep.setdefault("tail_flow", {})
+    mc = keep.setdefault("tail_mask", {})
+    sc = keep.setdefault("tail_sums", {})
+    if "ref_half" not in keep:
+        keep["ref_half"] = lib.debayer_subsample(burst.raw[ref], burst.cfa, max_val)
+    ref_half = keep["ref_half"]
+    acc = np.zeros((Ho, Wo, 3), lib.dtype)
+    wsum = np.zeros((Ho, Wo, 3), lib.dtype)
+    for i in [ref] + [k for k in range(n) if k != ref]:
+        ti = None if i == ref else np.asarray(tiles[i])
+        if i in sc and sc[i][0] == mkey and sc[i][1] == kkey and (i == ref or np.array_equal(sc[i][2], ti)):
+            a_i, w_i = sc[i][3], sc[i][4]
+        else:
+            a_i = np.zeros((Ho, Wo, 3), lib.dtype)
+            w_i = np.zeros((Ho, Wo, 3), lib.dtype)
+            if i == ref:
+                lib.accumulate(burst.raw[ref], burst.cfa, a_i, w_i, np.ones((H // 2, W // 2, 4), lib.dtype), kparam,
+                               np.zeros((H, W, 2), lib.dtype), white, black, s, origin, crop, bilinear=bil)
+            else:
+                if i in fc and np.array_equal(fc[i][0], ti):
+                    flow = fc[i][1]
+                else:
+                    flow = lib.flow_from_tiles(lib.arr(ti), W, H, pre.shift(ref, i), pre.rotation(ref, i), p.levels[0].tile_size)
+                    for _ in range(p.iterations_lk):
+                        warped = lib.warp(bw_acc[i], flow)
+                        ix, iy, it = lib.derivatives(warped, bw_acc[ref])
+                        flow = lib.lucas_kanade(flow, ix, iy, it, p.window_size_lk // 2, p.f32("min_det_lk"))
+                    fc.setdefault(i, (ti.copy(), flow))
+                if i in mc and mc[i][0] == mkey and np.array_equal(mc[i][1], ti):
+                    eroded = mc[i][2]
+                else:
+                    mov_half = lib.debayer_subsample(burst.raw[i], burst.cfa, max_val)
+                    mask = lib.robustness_mask(ref_half, mov_half, flow, float(np.float32(burst.noise_a)), float(np.float32(burst.noise_b)),
+                                               p.f32("threshold_m"), np.ones((H // 2, W // 2, 4), lib.dtype), mkey[0], mkey[1], bilinear=bil)
+                    eroded = lib.erode(mask, p.erode_size)
+                    mc.setdefault(i, (mkey, ti.copy(), eroded))
+                lib.accumulate(burst.raw[i], burst.cfa, a_i, w_i, lib.arr(eroded), kparam, lib.arr(flow), white, black, s, origin, crop,
+                               bilinear=bil)
+            sc.setdefault(i, (mkey, kkey, None if ti is None else ti.copy(), a_i, w_i))
+        acc += a_i
+        wsum += w_i
+    image = lib.apply_weighting(np.zeros((Ho, Wo, 3), lib.dtype), acc, wsum, thr)
+    return MergeResult(image=image, acc=acc, wsum=wsum)
 
 
 def accumulate_canvas_ref(lib, raw, cfa, acc, wsum, mask, kp4, flow, white, black, s):

@@ -1,7 +1,8 @@
 """Sample mode BILINEAR in the FP64 oracle (oracle/isa_oracle.c accumulate_mode
 and robustness_mask_mode, oracle/pipeline.py): equal to ROUND where the flow
 puts every frame on an integer shift, continuous in the tile flow elsewhere,
-and merge_from_tiles reproduces merge_burst at the same tile flows."""
+and merge_from_tiles reproduces merge_burst at the same tile flows (to FP64
+rounding: it adds the frames' sums in frame order)."""
 import numpy as np
 import pytest
 
@@ -25,7 +26,9 @@ def bil(oracle):
 def test_merge_from_tiles_reproduces_merge_burst(bil, oracle):
     b, p, keep, res = bil
     again = PL.merge_from_tiles(b, p, keep["tiles"], keep, oracle)
-    np.testing.assert_array_equal(again.image, res.image)
+    np.testing.assert_allclose(again.image, res.image, rtol=0, atol=1e-12)
+    twice = PL.merge_from_tiles(b, p, keep["tiles"], keep, oracle)  # from the cache
+    np.testing.assert_array_equal(twice.image, again.image)
 
 
 def test_bilinear_equals_round_at_integer_shifts(bil, oracle):
