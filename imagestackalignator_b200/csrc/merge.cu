@@ -173,19 +173,53 @@ __global__ void __launch_bounds__(256) k_accumulate(isa_accum_geom g, unsigned c
                 sy0 = (int)roundf(fl.y * g.s);
             }
         }
-#pragma unroll 1
-        for (int corner = 0; corner < (BIL ? 4 : 1); corner++) {
-            const int sx = sx0 + (corner & 1), sy = sy0 + (corner >> 1);
-            const float wk = BIL ? ((corner & 1) ? bx : 1.f - bx) * ((corner >> 1) ? by : 1.f - by) : 1.f;
-            if (BIL && wk == 0.f) continue;
+        if constexpr (BIL) {
+            // the four corners' taps fall on 6 x 6 output-grid positions: their source rows, columns and CFA
+            // colours once; each tap's mask cell (the unshifted tap's) is shared by the corners
+            const float wk[4] = {(1.f - bx) * (1.f - by), bx * (1.f - by), (1.f - bx) * by, bx * by};
+            int qxs[6];
+            const uint16_t* rrs[6];
+            int qys[6];
+#pragma unroll
+            for (int d = 0; d < 6; d++) {
+                qxs[d] = isa::clampi(floor_div_s(x + d - 2 + sx0 + g.ox, g), g.cx0, g.cx1);
+                qys[d] = isa::clampi(floor_div_s(y + d - 2 + sy0 + g.oy, g), g.cy0, g.cy1);
+                rrs[d] = isa::row_ptr(fr.raw, raw_pitch, qys[d]);
+            }
 #pragma unroll
             for (int py = 0; py < 5; py++) {
-                const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
+                const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
+#pragma unroll
+                for (int px = 0; px < 5; px++) {
+                    float4 m = make_float4(1.f, 1.f, 1.f, 1.f);
+                    if (mr) m = __ldg(mr + ux[px]);
+                    const float ww = wt[py * 5 + px];
+#pragma unroll
+                    for (int corner = 0; corner < 4; corner++) {
+                        if (wk[corner] == 0.f) continue;
+                        const int dx = corner & 1, dy = corner >> 1;
+                        const int qx = qxs[px + dx], qy = qys[py + dy];
+                        const int c = isa::cfa_at(cfa, qx, qy);
+                        if (c > 2) continue;
+                        float raw = (float)__ldg(rrs[py + dy] + qx);
+                        raw = (raw - black.v[c]) / white.v[c];
+                        float cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
+                        if (!isfinite(cert)) cert = 0.f;
+                        cert *= wk[corner];
+                        a[c] += raw * ww * cert;
+                        w[c] += ww * cert;
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int py = 0; py < 5; py++) {
+                const int qy = isa::clampi(floor_div_s(y + py - 2 + sy0 + g.oy, g), g.cy0, g.cy1);
                 const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
                 const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
 #pragma unroll
                 for (int px = 0; px < 5; px++) {
-                    const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
+                    const int qx = isa::clampi(floor_div_s(x + px - 2 + sx0 + g.ox, g), g.cx0, g.cx1);
                     const int c = isa::cfa_at(cfa, qx, qy);
                     if (c > 2) continue;
                     float raw = (float)__ldg(rr + qx);
@@ -196,7 +230,6 @@ __global__ void __launch_bounds__(256) k_accumulate(isa_accum_geom g, unsigned c
                         cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
                         if (!isfinite(cert)) cert = 0.f;
                     }
-                    if constexpr (BIL) cert *= wk;
                     const float ww = wt[py * 5 + px];
                     a[c] += raw * ww * cert;
                     w[c] += ww * cert;
@@ -261,7 +294,7 @@ __device__ __forceinline__ void flow_scatter(float2* gflow, size_t pitch, int W,
 }
 
 template <int KC, bool BIL>
-__global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsigned cfa, const isa_frame_in* __restrict__ frames, int nframes,
+__global__ void __launch_bounds__(256, 2) k_accumulate_bwd(isa_accum_geom g, unsigned cfa, const isa_frame_in* __restrict__ frames, int nframes,
                                                        size_t raw_pitch, size_t flow_pitch, size_t mask_pitch, const float* __restrict__ kparam,
                                                        size_t kp_pitch, F3 white, F3 black, const float* __restrict__ out, size_t out_pitch,
                                                        const float* __restrict__ wsum, size_t ws_pitch, const float* __restrict__ target,
@@ -327,20 +360,66 @@ __global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsign
                 }
                 float4* gm = gmask + (size_t)f * gmask_stride;
                 float D[4] = {0.f, 0.f, 0.f, 0.f};
-                const int ncorner = BIL && fr.flow ? 4 : 1;
-#pragma unroll 1
-                for (int corner = 0; corner < ncorner; corner++) {
-                    const int sx = sx0 + (corner & 1), sy = sy0 + (corner >> 1);
-                    const float wk = BIL ? ((corner & 1) ? bx : 1.f - bx) * ((corner >> 1) ? by : 1.f - by) : 1.f;
-                    float dk = 0.f;
+                if constexpr (BIL) {
+                    // taps outer, corners inner (as the forward): the 6 x 6 positions once, the tap's mask cell and
+                    // its gradient (per channel, summed over the corners) once per tap
+                    const float wk[4] = {(1.f - bx) * (1.f - by), bx * (1.f - by), (1.f - bx) * by, bx * by};
+                    const bool need_d = fr.flow != nullptr;
+                    int qxs[6], qys[6];
+                    const uint16_t* rrs[6];
+#pragma unroll
+                    for (int d = 0; d < 6; d++) {
+                        qxs[d] = isa::clampi(floor_div_s(x + d - 2 + sx0 + g.ox, g), g.cx0, g.cx1);
+                        qys[d] = isa::clampi(floor_div_s(y + d - 2 + sy0 + g.oy, g), g.cy0, g.cy1);
+                        rrs[d] = isa::row_ptr(fr.raw, raw_pitch, qys[d]);
+                    }
 #pragma unroll
                     for (int py = 0; py < 5; py++) {
-                        const int qy = isa::clampi(floor_div_s(y + py - 2 + sy + g.oy, g), g.cy0, g.cy1);
+                        const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
+#pragma unroll
+                        for (int px = 0; px < 5; px++) {
+                            float4 m = make_float4(1.f, 1.f, 1.f, 1.f);
+                            if (mr) m = __ldg(mr + ux[px]);
+                            const float ww = wt[py * 5 + px];
+                            float gc[3] = {0.f, 0.f, 0.f}, Gt = 0.f;
+#pragma unroll
+                            for (int corner = 0; corner < 4; corner++) {
+                                if (wk[corner] == 0.f && !need_d) continue;
+                                const int dx = corner & 1, dy = corner >> 1;
+                                const int qx = qxs[px + dx], qy = qys[py + dy];
+                                const int c = isa::cfa_at(cfa, qx, qy);
+                                if (c > 2) continue;
+                                float raw = (float)__ldg(rrs[py + dy] + qx);
+                                raw = (raw - black.v[c]) / white.v[c];
+                                const float hc = c == 0 ? h[0] : (c == 1 ? h[1] : h[2]);
+                                const float oc = c == 0 ? o[0] : (c == 1 ? o[1] : o[2]);
+                                const float r = hc * (raw - oc);
+                                float cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
+                                if (!isfinite(cert)) cert = 0.f;
+                                else if (c == 0) gc[0] += ww * r * wk[corner];
+                                else if (c == 1) gc[1] += ww * r * wk[corner];
+                                else gc[2] += ww * r * wk[corner];
+                                D[corner] += ww * cert * r;
+                                Gt += cert * r * wk[corner];
+                            }
+                            G[py * 5 + px] += Gt;
+                            if (mr) {
+                                float* dst = (float*)(isa::row_ptr(gm, mask_pitch, uy[py]) + ux[px]);
+#pragma unroll
+                                for (int c = 0; c < 3; c++)
+                                    if (gc[c] != 0.f) atomicAdd(dst + c, gc[c]);
+                            }
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int py = 0; py < 5; py++) {
+                        const int qy = isa::clampi(floor_div_s(y + py - 2 + sy0 + g.oy, g), g.cy0, g.cy1);
                         const uint16_t* rr = isa::row_ptr(fr.raw, raw_pitch, qy);
                         const float4* mr = fr.mask ? isa::row_ptr(fr.mask, mask_pitch, uy[py]) : nullptr;
 #pragma unroll
                         for (int px = 0; px < 5; px++) {
-                            const int qx = isa::clampi(floor_div_s(x + px - 2 + sx + g.ox, g), g.cx0, g.cx1);
+                            const int qx = isa::clampi(floor_div_s(x + px - 2 + sx0 + g.ox, g), g.cx0, g.cx1);
                             const int c = isa::cfa_at(cfa, qx, qy);
                             if (c > 2) continue;
                             float raw = (float)__ldg(rr + qx);
@@ -353,20 +432,14 @@ __global__ void __launch_bounds__(256) k_accumulate_bwd(isa_accum_geom g, unsign
                                 const float4 m = __ldg(mr + ux[px]);
                                 cert = c == 0 ? m.x : (c == 1 ? m.y : m.z);
                                 if (!isfinite(cert)) cert = 0.f;
-                                else if (!BIL || wk != 0.f) {
+                                else {
                                     float* dst = (float*)(isa::row_ptr(gm, mask_pitch, uy[py]) + ux[px]) + c;
-                                    atomicAdd(dst, BIL ? wt[py * 5 + px] * r * wk : wt[py * 5 + px] * r);
+                                    atomicAdd(dst, wt[py * 5 + px] * r);
                                 }
                             }
-                            if constexpr (BIL) {
-                                dk += wt[py * 5 + px] * cert * r;
-                                G[py * 5 + px] += cert * r * wk;
-                            } else {
-                                G[py * 5 + px] += cert * r;
-                            }
+                            G[py * 5 + px] += cert * r;
                         }
                     }
-                    D[corner] = dk;
                 }
                 if (BIL && fr.flow && gflow) {
                     const float dbx = (1.f - by) * (D[1] - D[0]) + by * (D[3] - D[2]);
