@@ -182,6 +182,7 @@ int isa_static_solve_setup();
 
 // ---------------------------------------------------------------------------
 struct isa_ctx {
+    int device = 0;  // current device at isa_ctx_create; the context's memory, events and streams live there
     int max_w = 0, max_h = 0, max_n = 0;
     isa_params p{};
     int max_pairs = 0, max_rows = 0, max_tiles = 0, maxcx = 0, maxcy = 0;
@@ -823,6 +824,7 @@ int isa_ctx_create(isa_ctx** out, int max_w, int max_h, int max_n, const isa_par
     if ((size_t)max_w * 8 > 227 * 1024 || isa_fft_cols_per_cta(max_h) < 1)
         return fail(ISA_EINVAL, "context size %dx%d exceeds the full-frame transform's limit (W <= 29056, H <= 12800)", max_w, max_h);
     isa_ctx* c = new isa_ctx();
+    if (cudaGetDevice(&c->device) != cudaSuccess) { cudaGetLastError(); delete c; return fail(ISA_ECUDA, "cudaGetDevice failed"); }
     c->max_w = max_w; c->max_h = max_h; c->max_n = max_n; c->p = *p;
     // worst case pairs over strategies for max_n frames
     c->max_rows = 0;
@@ -1098,41 +1100,94 @@ int isa_merge_backward_tiles(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, 
                           tile_grad, S(stream));
 }
 
+int isa_batch_plan(const double* work, const int* burst_device, int nbursts, const int* ctx_device, int nctx, int* assignment)
+{
+    if (nbursts < 0 || nctx < 1 || !ctx_device || (nbursts > 0 && (!work || !burst_device || !assignment))) return fail(ISA_EINVAL, "bad plan arguments");
+    std::vector<double> load(nctx, 0.0);
+    int unassigned = 0;
+    for (int b = 0; b < nbursts; b++) {
+        int k = -1;
+        for (int i = 0; i < nctx; i++)
+            if ((burst_device[b] < 0 || ctx_device[i] == burst_device[b]) && (k < 0 || load[i] < load[k])) k = i;
+        assignment[b] = k;
+        if (k < 0)
+            unassigned++;
+        else
+            load[k] += work[b] > 0 ? work[b] : 0.0;
+    }
+    return unassigned;
+}
+
+namespace {
+
+// Device of a device pointer (-1: managed memory, which every device reaches); ISA_EINVAL for host memory.
+int pointer_device(const void* ptr, int* dev)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ISA_EINVAL, "not a CUDA pointer");
+    }
+    if (a.type == cudaMemoryTypeManaged) { *dev = -1; return ISA_OK; }
+    if (a.type != cudaMemoryTypeDevice) return fail(ISA_EINVAL, "burst frames and outputs must be device memory");
+    *dev = a.device;
+    return ISA_OK;
+}
+
+}  // namespace
+
 int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, int* status)
 {
     if (!ctxs || nctx < 1 || (!bursts && nbursts > 0) || nbursts < 0) return fail(ISA_EINVAL, "bad batch arguments");
     for (int i = 0; i < nctx; i++)
         if (!ctxs[i]) return fail(ISA_EINVAL, "context %d is NULL", i);
-    std::vector<double> load(nctx, 0.0);
+    int caller_dev = 0;
+    ISA_CK(cudaGetDevice(&caller_dev));
+    // the plan: each burst to the least-loaded context on the device of its frames
+    std::vector<double> work(nbursts, 0.0);
+    std::vector<int> bdev(nbursts, -1), cdev(nctx), assign(nbursts, -1), pre_rc(nbursts, ISA_OK);
+    for (int i = 0; i < nctx; i++) cdev[i] = ctxs[i]->device;
+    for (int b = 0; b < nbursts; b++) {
+        const isa_burst& u = bursts[b];
+        if (!u.info || !u.raw || !u.out) { pre_rc[b] = fail(ISA_EINVAL, "burst %d: NULL argument", b); continue; }
+        int od = -1;
+        if (pointer_device(u.raw, &bdev[b]) != ISA_OK || pointer_device(u.out, &od) != ISA_OK) { pre_rc[b] = ISA_EINVAL; continue; }
+        if (od >= 0 && bdev[b] >= 0 && od != bdev[b]) { pre_rc[b] = fail(ISA_EINVAL, "burst %d: frames and output on different devices", b); continue; }
+        if (bdev[b] < 0) bdev[b] = od;
+        work[b] = (double)u.info->width * u.info->height * u.n;
+    }
+    isa_batch_plan(work.data(), bdev.data(), nbursts, cdev.data(), nctx, assign.data());
     int first = ISA_OK;
     for (int b = 0; b < nbursts; b++) {
         const isa_burst& u = bursts[b];
-        int rc = ISA_OK;
-        if (!u.info || !u.raw || !u.out) rc = fail(ISA_EINVAL, "burst %d: NULL argument", b);
-        int k = 0;
-        for (int i = 1; i < nctx; i++)
-            if (load[i] < load[k]) k = i;
-        isa_ctx* c = ctxs[k];
-        const isa_params saved = c->p;
-        if (rc == ISA_OK && u.params) {
-            const isa_params& q = *u.params;
-            rc = check_params(&q);
-            bool same = rc == ISA_OK && q.level_count == saved.level_count && q.tracking_strategy == saved.tracking_strategy &&
-                        q.tracking_block_size == saved.tracking_block_size;
-            for (int l = 0; same && l < q.level_count; l++)
-                same = q.levels[l].resize_level == saved.levels[l].resize_level && q.levels[l].tile_size == saved.levels[l].tile_size &&
-                       q.levels[l].max_shift == saved.levels[l].max_shift;
-            if (rc == ISA_OK && !same) rc = fail(ISA_EINVAL, "burst %d: params change the pyramid levels or the tracking strategy", b);
-            if (rc == ISA_OK) c->p = q;
-        }
+        int rc = pre_rc[b];
+        if (rc == ISA_OK && assign[b] < 0) rc = fail(ISA_EINVAL, "burst %d: no context on device %d", b, bdev[b]);
         if (rc == ISA_OK) {
-            rc = run_merge(c, u.raw, u.raw_pitch, u.frame_stride, u.n, u.info, u.pre, u.out, u.out_pitch, S(streams ? streams[k] : nullptr));
-            load[k] += (double)u.info->width * u.info->height * u.n;
+            const int k = assign[b];
+            isa_ctx* c = ctxs[k];
+            const isa_params saved = c->p;
+            if (u.params) {
+                const isa_params& q = *u.params;
+                rc = check_params(&q);
+                bool same = rc == ISA_OK && q.level_count == saved.level_count && q.tracking_strategy == saved.tracking_strategy &&
+                            q.tracking_block_size == saved.tracking_block_size;
+                for (int l = 0; same && l < q.level_count; l++)
+                    same = q.levels[l].resize_level == saved.levels[l].resize_level && q.levels[l].tile_size == saved.levels[l].tile_size &&
+                           q.levels[l].max_shift == saved.levels[l].max_shift;
+                if (rc == ISA_OK && !same) rc = fail(ISA_EINVAL, "burst %d: params change the pyramid levels or the tracking strategy", b);
+                if (rc == ISA_OK) c->p = q;
+            }
+            if (rc == ISA_OK && cudaSetDevice(c->device) != cudaSuccess) {
+                cudaGetLastError();
+                rc = fail(ISA_ECUDA, "cudaSetDevice(%d) failed", c->device);
+            }
+            if (rc == ISA_OK) rc = run_merge(c, u.raw, u.raw_pitch, u.frame_stride, u.n, u.info, u.pre, u.out, u.out_pitch, S(streams ? streams[k] : nullptr));
+            c->p = saved;
         }
-        c->p = saved;
         if (status) status[b] = rc;
         if (rc != ISA_OK && first == ISA_OK) first = rc;
     }
+    cudaSetDevice(caller_dev);
     return first;
 }
 

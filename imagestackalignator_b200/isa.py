@@ -70,7 +70,7 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record",
-    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_batch_plan", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
@@ -816,6 +816,31 @@ def merge_batch(mergers, bursts, streams=None):
     status = (ctypes.c_int * max(1, len(bursts)))()
     lib().isa_merge_batch(ctxs, sts, len(mergers), arr, len(bursts), status)
     return [status[i] for i in range(len(bursts))]
+
+
+def batch_plan(work, burst_device, ctx_device):
+    """isa_batch_plan: the context index isa_merge_batch gives each burst (the
+    least-loaded context, by W*H*n work in burst order, among those on the
+    burst's device; -1 in burst_device = any device), -1 where none fits.
+    Host only."""
+    n, k = len(work), len(ctx_device)
+    w = (ctypes.c_double * max(n, 1))(*[float(v) for v in work])
+    bd = (ctypes.c_int * max(n, 1))(*[int(v) for v in burst_device])
+    cd = (ctypes.c_int * k)(*[int(v) for v in ctx_device])
+    out = (ctypes.c_int * max(n, 1))()
+    r = lib().isa_batch_plan(w, bd, n, cd, k, out)
+    if r < 0:
+        check(r)
+    return [out[i] for i in range(n)]
+
+
+def rank_bursts(work, world):
+    """Bursts of a batch shared out over `world` ranks (one process per GPU,
+    each merging its own bursts, no collective on the data path): the same
+    rule as isa_batch_plan with one context per rank, so every rank computes
+    the same split from the same list. Returns, per rank, its burst indices."""
+    plan = batch_plan(work, [-1] * len(work), list(range(world)))
+    return [[b for b, r in enumerate(plan) if r == k] for k in range(world)]
 
 
 def device_copy(ptr, shape, dtype, device="cuda"):

@@ -240,17 +240,30 @@ ISA_API int isa_set_tile_flow(isa_ctx* ctx, const float* tiles);
 ISA_API int isa_tile_flow(isa_ctx* ctx, float* tiles, int* tiles_x, int* tiles_y, void* stream);
 /* Many bursts of different sizes, frame counts, CFA layouts, bit depths and
  * merge scales (no counterpart in the reference, whose controller merges one
- * burst). Each burst goes to the context with the least work queued so far
- * (W * H * n, in burst order, deterministic) and is merged on that context's
- * stream (streams[i] for ctxs[i]); contexts run concurrently, so small
- * bursts that cannot fill the GPU alone overlap. Returns after enqueuing all
- * bursts; the caller synchronises the streams. A burst's params may differ
- * from its context's in the merge mode and scale and in the scalar
- * parameters, but must keep the context's pyramid levels and tracking
- * strategy, and its frames and output must fit the context. status[b]
- * (optional, host) receives each burst's result; the return value is the
- * first failure, or ISA_OK. */
+ * burst). The contexts may live on different devices (each on the device
+ * that was current at its isa_ctx_create; streams[i], or the legacy default
+ * stream when streams is NULL, must belong to ctxs[i]'s device). Each burst
+ * goes to the context with the least work queued so far (W * H * n, in burst
+ * order, deterministic; isa_batch_plan) among those on the device that holds
+ * its frames, and is merged on that context's stream with that device
+ * current; contexts run concurrently, so small bursts that cannot fill a GPU
+ * alone overlap, and several GPUs share one batch. Returns after enqueuing
+ * all bursts, with the caller's current device restored; the caller
+ * synchronises the streams. A burst's params may differ from its context's
+ * in the merge mode and scale and in the scalar parameters, but must keep
+ * the context's pyramid levels and tracking strategy, and its frames and
+ * output (on the same device) must fit the context. status[b] (optional,
+ * host) receives each burst's result; the return value is the first
+ * failure, or ISA_OK. */
 ISA_API int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, int* status);
+/* The assignment isa_merge_batch makes, on the host alone: burst b (work
+ * work[b] > 0, data on device burst_device[b], or -1 for memory every
+ * device reaches) goes to the context k with the least work assigned so far
+ * among those with ctx_device[k] == burst_device[b] (any context for -1);
+ * ties go to the lowest index. assignment[b] receives k, or -1 when no
+ * context is on the burst's device. Returns the number of unassigned
+ * bursts, or ISA_EINVAL for bad arguments. */
+ISA_API int isa_batch_plan(const double* work, const int* burst_device, int nbursts, const int* ctx_device, int nctx, int* assignment);
 /* The same with host buffers: frames are copied in and the image copied out
  * on `stream` (pinned host memory gives full PCIe speed). */
 ISA_API int isa_merge_burst_host(isa_ctx* ctx, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre,
