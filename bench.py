@@ -370,6 +370,93 @@ def batch_throughput(args):
             "sequential_mp_s": mp / (seq / 1e3), "batched_mp_s": mp / (bat / 1e3), "batched_bursts_s": nb / (bat / 1e3)}
 
 
+UNEVEN = dict(bursts=64, contexts=4, frames=(4, 30), mp=(2.0, 12.0), seed=5000)  # the uneven batch: sizes, counts, CFA, depth, scale
+
+
+def uneven_specs():
+    """64 bursts: frame counts uniform 4-30, frame areas uniform 2-12 MP at 4:3
+    or 3:2 (sides multiples of 16), CFA RGGB / BGGR / GRBG, 12 or 14 bits,
+    merge scale 1 or 2; seeded."""
+    rng = np.random.default_rng(UNEVEN["seed"])
+    specs = []
+    for i in range(UNEVEN["bursts"]):
+        n = int(rng.integers(UNEVEN["frames"][0], UNEVEN["frames"][1] + 1))
+        area = rng.uniform(*UNEVEN["mp"]) * 1e6
+        aspect = (4 / 3, 3 / 2)[int(rng.integers(2))]
+        H = max(64, int(round(np.sqrt(area / aspect) / 16)) * 16)
+        W = max(64, int(round(H * aspect / 16)) * 16)
+        specs.append(dict(n=n, W=W, H=H, cfa=("RGGB", "BGGR", "GRBG")[int(rng.integers(3))], bits=(12, 14)[int(rng.integers(2))],
+                          scale=(1.0, 2.0)[int(rng.integers(2))], seed=UNEVEN["seed"] + i))
+    return specs
+
+
+def uneven_batch(args):
+    """The uneven batch: 64 bursts of uneven sizes, frame counts, CFA layouts,
+    bit depths and merge scales. Sequential (one context, one stream, burst by
+    burst) against isa_merge_batch over several contexts and streams, both
+    with the launch shapes of the project's autotuner (imagestackalignator_b200
+    .tune, JSON cache), and the batch without them; device time for the set."""
+    import torch
+    from imagestackalignator_b200 import isa, params as P, synthetic, tune
+    specs = uneven_specs()
+    mw, mh, mn = max(s["W"] for s in specs), max(s["H"] for s in specs), max(s["n"] for s in specs)
+    p = merge_params()
+    p.merge_scale = 2.0
+    mergers = [isa.Merger(mw, mh, mn, p) for _ in range(UNEVEN["contexts"])]
+    items, mp = [], 0.0
+    for sp in specs:
+        white = (1 << sp["bits"]) - 1
+        b = synthetic.make_burst(sp["W"], sp["H"], sp["n"], seed=sp["seed"], max_shift=WORKLOAD["max_shift"], max_rot_deg=WORKLOAD["max_rot_deg"],
+                                 noise_a=WORKLOAD["noise_a"], noise_b=WORKLOAD["noise_b"], black=white // 32, white_max=white, cfa=sp["cfa"],
+                                 device="cuda")
+        q = P.MergeParams(**vars(p))
+        q.merge_scale = sp["scale"]
+        Wo, Ho = isa.output_size(isa.make_params(q), sp["W"], sp["H"])
+        items.append(dict(raw=torch.from_numpy(b.raw.view(np.int16)).cuda(), info=isa.make_info(b), params=q,
+                          out=torch.empty((Ho, Wo, 3), dtype=torch.float32, device="cuda")))
+        mp += Wo * Ho / 1e6
+    main = torch.cuda.current_stream()
+    streams = [torch.cuda.Stream() for _ in mergers]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run(ms, sts):
+        for s in sts:
+            s.wait_stream(main)
+        st = isa.merge_batch(ms, items, sts)
+        if any(st):
+            raise RuntimeError(f"isa_merge_batch status {st}")
+        for s in sts:
+            main.wait_stream(s)
+
+    def timed(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(main)
+        for _ in range(args.steps):
+            fn()
+        e1.record(main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    untuned = timed(lambda: run(mergers, streams))
+    t0 = time.time()
+    entries = tune.tune(mergers[0], items)
+    tune_s = time.time() - t0
+    for m in mergers:
+        m.set_tuning(entries)
+    seq = timed(lambda: run(mergers[:1], [main]))
+    bat = timed(lambda: run(mergers, streams))
+    for m in mergers:
+        m.close()
+    frames = sum(s["n"] for s in specs)
+    return {"workload": f"{len(specs)} bursts, {frames} frames of 2-12 MP (4:3, 3:2), 4-30 frames, RGGB/BGGR/GRBG, 12/14-bit, scale 1 or 2",
+            "output_mp": mp, "contexts": len(mergers), "sequential_ms": seq, "batched_ms": bat, "batched_untuned_ms": untuned,
+            "sequential_mp_s": mp / (seq / 1e3), "batched_mp_s": mp / (bat / 1e3), "batched_bursts_s": len(specs) / (bat / 1e3),
+            "sequential_bursts_s": len(specs) / (seq / 1e3), "tuning_classes": len({tune.burst_class(e["width"], e["height"], 0) for e in entries}),
+            "tuning_s": tune_s}
+
+
 LARGE = dict(width=6016, height=4000, frames=50, max_shift=32.0, max_rot_deg=0.5, moving_object=0.05, object_step=(2.0, 40.0))
 
 
@@ -683,6 +770,9 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = adjoint_ratio(args)
+    uneven = None
+    if rank == 0 and world == 1 and not args.no_uneven:
+        uneven = uneven_batch(args)
     fit = None
     if rank == 0 and world == 1 and not args.no_fit:
         fit = param_fit(ADJ["width"], ADJ["height"], ADJ["frames"], 200)
@@ -722,7 +812,7 @@ def run_ours(args):
                    "l2": f"inputs larger than L2 (raw frames {burst.raw.nbytes / 1e6:.0f} MB, 126 MB L2)",
                    "parallelism": f"{world} independent bursts" if world > 1 else "single GPU"},
         "stages_ms": dict(zip(names, stages)), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "fwd_adjoint": adjoint, "param_fit": fit, "param_fit_large": fit_large, "batch": batch, "large_local_motion": large, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec, "dng_files_e2e": files,
+        "fwd_adjoint": adjoint, "param_fit": fit, "param_fit_large": fit_large, "uneven_batch": uneven, "batch": batch, "large_local_motion": large, "postprocess": post, "raw_decode": rawdec, "dng_decode": dngdec, "dng_files_e2e": files,
         "clocks": clocks,
     }
     if rank == 0:
@@ -745,6 +835,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--no-fit", action="store_true", help="skip the 200-step parameter fit on the differentiable-merge burst")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the 64 uneven bursts (sequential vs batched, autotuned shapes)")
     ap.add_argument("--fit-large", type=int, default=0, help="Adam steps of the parameter fit on the 50-frame burst with local motion (0: none)")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-small-bursts timing")
     ap.add_argument("--no-large", action="store_true", help="skip the 50-frame burst with local motion")

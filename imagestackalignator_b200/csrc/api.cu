@@ -231,6 +231,8 @@ struct isa_ctx {
     const float2* tile_override = nullptr;
     // sample mode BILINEAR only: scratch of the flow adjoint (isa_merge_backward_tiles), 25 floats per frame pixel
     float* adj_flow = nullptr;
+    // launch shapes per frame size (isa_ctx_set_tuning)
+    std::vector<isa_tuning> tuning;
     // last call
     int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0, last_ref = 0;
 };
@@ -444,6 +446,17 @@ struct HostIo {
     float* host_out;    // when set: the output is copied out band by band (rows of 12 * Wo bytes)
 };
 
+// The tuning entry for W x H frames: its own, else the 0 x 0 entry, else none.
+const isa_tuning* tuning_for(const isa_ctx* c, int W, int H)
+{
+    const isa_tuning* any = nullptr;
+    for (const isa_tuning& t : c->tuning) {
+        if (t.width == W && t.height == H) return &t;
+        if (t.width == 0 && t.height == 0) any = &t;
+    }
+    return any;
+}
+
 int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_stride, int n, const isa_raw_info* info,
               const isa_prealign* pre, float* out, size_t out_pitch, cudaStream_t st, const HostIo* hio = nullptr)
 {
@@ -459,6 +472,9 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     isa_accum_geom g;
     float thr;
     accum_geom(p, W, H, g, thr);
+    const isa_tuning* tune = tuning_for(c, W, H);
+    const int lk_rows = tune ? tune->lk_strip_rows : 0;
+    if (tune) { g.bx = tune->acc_block_x; g.by = tune->acc_block_y; }
     if (out_pitch < (size_t)g.Wo * 12) return fail(ISA_EINVAL, "output pitch %zu < %d", out_pitch, g.Wo * 12);
     if (g.Wo > c->max_wo || g.Ho > c->max_ho) return fail(ISA_EINVAL, "output exceeds the context");
     Strategy strat;
@@ -596,7 +612,8 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
         ISA_LAUNCH(c, isa_launch_flow_from_tiles(tiles, (size_t)tcx0 * sizeof(float2), tcx0, tcy0, W, H, bs[0], bs[1], prealign_rot(pre, ref, i),
                                           a, fp, st));
         for (int it = 0; it < p->iterations_lk; it++) {
-            ISA_LAUNCH(c, isa_launch_lk_iteration(a, b, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, pitch, W, H, half, p->min_det_lk, st));
+            ISA_LAUNCH(c, isa_launch_lk_iteration(a, b, fp, c->bw_acc + i * fsz, c->bw_acc + ref * fsz, pitch, W, H, half, p->min_det_lk, st,
+                                                  lk_rows));
             std::swap(a, b);
         }
         float4* mask = c->masks + (size_t)i * Wh * Hh;
@@ -1280,6 +1297,20 @@ int isa_ctx_set_params(isa_ctx* c, const isa_params* q)
     accum_geom(q, c->max_w, c->max_h, g, thr);
     if (g.Wo > c->max_wo || g.Ho > c->max_ho) return fail(ISA_EINVAL, "output %dx%d exceeds the context's %dx%d", g.Wo, g.Ho, c->max_wo, c->max_ho);
     c->p = *q;
+    return ISA_OK;
+}
+
+int isa_ctx_set_tuning(isa_ctx* c, const isa_tuning* e, int count)
+{
+    if (!c || count < 0 || (count > 0 && !e)) return fail(ISA_EINVAL, "bad tuning arguments");
+    for (int i = 0; i < count; i++) {
+        const isa_tuning& t = e[i];
+        if (t.lk_strip_rows < 0 || t.lk_strip_rows > 4096) return fail(ISA_EINVAL, "tuning %d: lk_strip_rows %d", i, t.lk_strip_rows);
+        const bool block0 = t.acc_block_x == 0 && t.acc_block_y == 0;
+        if (!block0 && (t.acc_block_x < 1 || t.acc_block_y < 1 || t.acc_block_x * t.acc_block_y > 256 || (t.acc_block_x * t.acc_block_y) % 32 != 0))
+            return fail(ISA_EINVAL, "tuning %d: accumulation block %d x %d", i, t.acc_block_x, t.acc_block_y);
+    }
+    c->tuning.assign(e, e + count);
     return ISA_OK;
 }
 

@@ -485,14 +485,14 @@ int lk_strip_rows(int W, int Himg)
 
 template <int H>
 cudaError_t launch_lk(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref, size_t img_pitch, int W, int Himg,
-                      float min_det, const float2* gin, float* aout, size_t a_pitch, size_t a_plane, cudaStream_t st)
+                      float min_det, const float2* gin, float* aout, size_t a_pitch, size_t a_plane, cudaStream_t st, int strip_rows = 0)
 {
     using L = LkStream<H>;
     const bool adj = aout != nullptr;
     cudaError_t e = cudaFuncSetAttribute(adj ? k_lk_stream<H, true> : k_lk_stream<H, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)L::TOTAL);
     if (e != cudaSuccess) return e;
-    const int sh = lk_strip_rows<H>(W, Himg);
+    const int sh = strip_rows > 0 ? strip_rows : lk_strip_rows<H>(W, Himg);
     dim3 g((W + L::SW - 1) / L::SW, (Himg + sh - 1) / sh);
     if (adj)
         k_lk_stream<H, true><<<g, LKS_NT, L::TOTAL, st>>>(flow_in, nullptr, flow_pitch, src, ref, img_pitch, W, Himg, sh, min_det, gin, aout, a_pitch,
@@ -707,10 +707,10 @@ cudaError_t isa_launch_lk_sums(float2* flow, size_t flow_pitch, const float* ix,
 }
 
 cudaError_t isa_launch_lk_iteration(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref,
-                                    size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st)
+                                    size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st, int strip_rows)
 {
     switch (half) {
-#define ISA_LK_CASE(h) case h: return launch_lk<h>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, H, min_det, nullptr, nullptr, 0, 0, st);
+#define ISA_LK_CASE(h) case h: return launch_lk<h>(flow_in, flow_out, flow_pitch, src, ref, img_pitch, W, H, min_det, nullptr, nullptr, 0, 0, st, strip_rows);
     ISA_LK_CASE(0) ISA_LK_CASE(1) ISA_LK_CASE(2) ISA_LK_CASE(3) ISA_LK_CASE(4) ISA_LK_CASE(5) ISA_LK_CASE(6) ISA_LK_CASE(7) ISA_LK_CASE(8)
     ISA_LK_CASE(9) ISA_LK_CASE(10) ISA_LK_CASE(11) ISA_LK_CASE(12) ISA_LK_CASE(13) ISA_LK_CASE(14) ISA_LK_CASE(15)
 #undef ISA_LK_CASE

@@ -148,7 +148,7 @@ cudaError_t isa_launch_derivatives2(const float* img, size_t pitch, int W, int H
 cudaError_t isa_launch_lk_sums(float2* flow, size_t flow_pitch, const float* ix, const float* iy, const float* it, size_t pitch, int W,
                                int H, int half, float min_det, cudaStream_t st);
 cudaError_t isa_launch_lk_iteration(const float2* flow_in, float2* flow_out, size_t flow_pitch, const float* src, const float* ref,
-                                    size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st);
+                                    size_t img_pitch, int W, int H, int half, float min_det, cudaStream_t st, int strip_rows = 0);
 // adjoint of one LK iteration (scratch: wplane one float plane, a5 and A5 five planes, gd3 three planes, all W x H floats at
 // pitch W * 4) and of the tile term of the flow from tiles
 cudaError_t isa_launch_lk_adjoint(const float2* f, const float2* gout, float2* gin, size_t fpitch, const float* src, const float* ref, size_t img_pitch,
@@ -199,6 +199,7 @@ struct isa_accum_geom {
     int cx0, cy0, cx1, cy1;  // inclusive source crop
     int masks_finite;  // 1: every mask value is finite (masks made by this library)
     int bilinear;      // 1: sample mode BILINEAR (the four integer shifts around s * flow, blended)
+    int bx = 0, by = 0;  // thread block of the generic accumulation (0: 32 x 8)
     int yb0, yb1;      // output rows [yb0, yb1) computed by this launch (yb0 a multiple of 32)
 };
 struct isa_frame_in {

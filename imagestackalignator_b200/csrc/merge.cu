@@ -587,7 +587,8 @@ cudaError_t isa_launch_accumulate(const isa_accum_geom& g, unsigned cfa, const i
     for (int c = 0; c < 3; c++) { wh.v[c] = white[c]; bl.v[c] = black[c]; }
     isa_frame_in one = single ? *single : isa_frame_in{nullptr, nullptr, nullptr};
     if (g.yb0 < 0 || g.yb1 > g.Ho || g.yb1 <= g.yb0) return cudaErrorInvalidValue;
-    dim3 b(32, 8), grd = grid2(g.Wo, g.yb1 - g.yb0, b);
+    dim3 b(g.bx > 0 ? g.bx : 32, g.by > 0 ? g.by : 8), grd = grid2(g.Wo, g.yb1 - g.yb0, b);
+    if (b.x * b.y > 256) return cudaErrorInvalidValue;
     if (kparam_channels == 4 && g.bilinear)
         k_accumulate<4, true><<<grd, b, 0, st>>>(g, cfa, frames, nframes, one, raw_pitch, flow_pitch, mask_pitch, kparam, kparam_pitch, wh, bl, acc,
                                                  wsum, out_pitch, accumulate_into);

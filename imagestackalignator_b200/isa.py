@@ -33,6 +33,11 @@ class IsaLevel(ctypes.Structure):
     _fields_ = [("resize_level", ctypes.c_int), ("tile_size", ctypes.c_int), ("max_shift", ctypes.c_int)]
 
 
+class IsaTuning(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("lk_strip_rows", ctypes.c_int), ("acc_block_x", ctypes.c_int),
+                ("acc_block_y", ctypes.c_int)]
+
+
 class IsaParams(ctypes.Structure):
     _fields_ = [
         ("sigma_debayer_tracking", ctypes.c_float), ("sigma_debayer_accumulation", ctypes.c_float),
@@ -70,7 +75,7 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record",
-    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_batch_plan", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_batch_plan", "isa_ctx_set_tuning", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
@@ -281,6 +286,15 @@ class Merger:
         c = make_params(params, bool(self.params.fused_accumulate))
         check(lib().isa_ctx_set_params(self.ctx, ctypes.byref(c)))
         self.params = c
+
+    def set_tuning(self, entries=()):
+        """isa_ctx_set_tuning: launch shapes per frame size, each entry a dict with width, height (0, 0: any size),
+        lk_strip_rows, acc_block_x, acc_block_y (0: the library's choice)."""
+        arr = (IsaTuning * max(1, len(entries)))()
+        for i, e in enumerate(entries):
+            arr[i] = IsaTuning(int(e.get("width", 0)), int(e.get("height", 0)), int(e.get("lk_strip_rows", 0)), int(e.get("acc_block_x", 0)),
+                               int(e.get("acc_block_y", 0)))
+        check(lib().isa_ctx_set_tuning(self.ctx, arr, len(entries)))
 
     def set_tile_flow(self, tiles=None):
         """Merge at the given per-frame tile flows (cuda float32 n x tiles_y x

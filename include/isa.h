@@ -161,6 +161,23 @@ ISA_API int isa_ctx_destroy(isa_ctx* ctx);
  * unchanged. Allocates nothing. No counterpart in the reference, whose
  * controller reads its properties at each run. */
 ISA_API int isa_ctx_set_params(isa_ctx* ctx, const isa_params* p);
+/* Launch shapes chosen by a tuner for frames of width x height (0 x 0: any
+ * size without an entry of its own); 0 in a field keeps the library's
+ * choice. lk_strip_rows: rows per CTA strip of the LK iteration (else the
+ * wave-filling choice); acc_block_x, acc_block_y: thread block of the
+ * accumulation at scales other than 2 and in sample mode BILINEAR (else
+ * 32 x 8; x y <= 256). */
+typedef struct isa_tuning {
+    int width, height;
+    int lk_strip_rows;
+    int acc_block_x, acc_block_y;
+} isa_tuning;
+/* Sets the context's tuning table (copied; count 0 clears it). Each merge
+ * uses the entry of its frame size, else the 0 x 0 entry, else the
+ * library's choices. The shapes change the order of no sum: results do not
+ * depend on them. ISA_EINVAL for a shape out of range. No counterpart in the
+ * reference. */
+ISA_API int isa_ctx_set_tuning(isa_ctx* ctx, const isa_tuning* entries, int count);
 /* Output size of the merge for a frame size under p. */
 ISA_API int isa_output_size(const isa_params* p, int width, int height, int* out_width, int* out_height);
 /* Stage times (ms) of the last isa_merge_burst call, in order: tracking
