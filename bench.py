@@ -447,11 +447,23 @@ def uneven_batch(args):
         m.set_tuning(entries)
     seq = timed(lambda: run(mergers[:1], [main]))
     bat = timed(lambda: run(mergers, streams))
+    # the same batch captured once as a CUDA graph and replayed (one host launch per batch)
+    origin = torch.cuda.Stream()
+    graph = isa.BatchGraph(mergers, items, streams, origin)
+
+    def replay():
+        origin.wait_stream(main)
+        graph.launch(origin)
+        main.wait_stream(origin)
+
+    gr = timed(replay)
+    graph.close()
     for m in mergers:
         m.close()
     frames = sum(s["n"] for s in specs)
     return {"workload": f"{len(specs)} bursts, {frames} frames of 2-12 MP (4:3, 3:2), 4-30 frames, RGGB/BGGR/GRBG, 12/14-bit, scale 1 or 2",
             "output_mp": mp, "contexts": len(mergers), "sequential_ms": seq, "batched_ms": bat, "batched_untuned_ms": untuned,
+            "graph_ms": gr, "graph_mp_s": mp / (gr / 1e3), "graph_bursts_s": len(specs) / (gr / 1e3),
             "sequential_mp_s": mp / (seq / 1e3), "batched_mp_s": mp / (bat / 1e3), "batched_bursts_s": len(specs) / (bat / 1e3),
             "sequential_bursts_s": len(specs) / (seq / 1e3), "tuning_classes": len({tune.burst_class(e["width"], e["height"], 0) for e in entries}),
             "tuning_s": tune_s}

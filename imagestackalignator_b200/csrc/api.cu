@@ -233,6 +233,8 @@ struct isa_ctx {
     float* adj_flow = nullptr;
     // launch shapes per frame size (isa_ctx_set_tuning)
     std::vector<isa_tuning> tuning;
+    // set while isa_batch_graph_create captures a batch: no stage-time events, transform twiddles uploaded per burst
+    bool capturing = false;
     // last call
     int last_w = 0, last_h = 0, last_n = 0, last_tcx0 = 0, last_tcy0 = 0, last_n1 = 0, last_ref = 0;
 };
@@ -245,6 +247,27 @@ size_t bw_pitch(int W) { return (size_t)W * sizeof(float); }
 // warped source (1), the window-sum gradients and their box sums (5 + 5), the derivative gradients (3), the flow gradient
 // ping-pong (2 x 2) and the half-res mask gradient (4 per half-res pixel = 1 per frame pixel)
 constexpr size_t kAdjFlowFloats = 25;
+
+// Host-to-device copies of the merge's small tables (pair and frame tables, solver rows, transform twiddles). Outside a
+// graph capture they copy from the caller's host vectors; while isa_batch_graph_create captures a batch, they go
+// through the graph's pinned arena, so that the captured copy nodes read memory that stays valid and unchanged for
+// every replay.
+struct HostStage {
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+};
+thread_local HostStage* g_stage = nullptr;
+
+cudaError_t h2d(void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+    if (bytes == 0) return cudaSuccess;
+    if (!g_stage) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    const size_t at = (g_stage->used + 15) / 16 * 16;
+    if (at + bytes > g_stage->cap) return cudaErrorMemoryAllocation;
+    memcpy(g_stage->base + at, src, bytes);
+    g_stage->used = at + bytes;
+    return cudaMemcpyAsync(dst, g_stage->base + at, bytes, cudaMemcpyHostToDevice, st);
+}
 
 int level_tiles(const isa_level& l, int W, int H, int* tcx, int* tcy)
 {
@@ -313,9 +336,9 @@ int ensure_fft(isa_ctx* c, int W, int H, cudaStream_t st)
     isa_fft_twiddles(W / 2, tr.data());
     isa_fft_twiddles(W, tu.data());
     isa_fft_twiddles(H, tc.data());
-    ISA_CK(cudaMemcpyAsync(c->tw_rows, tr.data(), tr.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(c->tw_unpack, tu.data(), (W / 2 + 1) * sizeof(float2), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(c->tw_cols, tc.data(), tc.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+    ISA_CK(h2d(c->tw_rows, tr.data(), tr.size() * sizeof(float2), st));
+    ISA_CK(h2d(c->tw_unpack, tu.data(), (W / 2 + 1) * sizeof(float2), st));
+    ISA_CK(h2d(c->tw_cols, tc.data(), tc.size() * sizeof(float2), st));
     // pageable sources: the copies above are staged before returning
     c->fft_rows = pr;
     c->fft_cols = pc;
@@ -425,11 +448,11 @@ int upload_rows(int* d_a, int* d_b, int* d_sign, int* d_grid, double* d_N0, cons
             for (int j = s.a[k]; j < s.b[k]; j++) N0[(size_t)i * s.n1 + j] += 1.0;
     std::vector<int> rg(s.m);
     for (int k = 0; k < s.m; k++) rg[k] = k;  // grid k holds measurement row k
-    ISA_CK(cudaMemcpyAsync(d_a, s.a.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(d_b, s.b.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(d_sign, s.sign.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(d_grid, rg.data(), s.m * sizeof(int), cudaMemcpyHostToDevice, st));
-    ISA_CK(cudaMemcpyAsync(d_N0, N0.data(), N0.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    ISA_CK(h2d(d_a, s.a.data(), s.m * sizeof(int), st));
+    ISA_CK(h2d(d_b, s.b.data(), s.m * sizeof(int), st));
+    ISA_CK(h2d(d_sign, s.sign.data(), s.m * sizeof(int), st));
+    ISA_CK(h2d(d_grid, rg.data(), s.m * sizeof(int), st));
+    ISA_CK(h2d(d_N0, N0.data(), N0.size() * sizeof(double), st));
     // pageable sources: the copies above complete before returning
     return ISA_OK;
 }
@@ -491,9 +514,11 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     c->ev_count = 0;
     c->launches = 0;
     auto mark = [&]() -> int {
+        if (c->capturing) return ISA_OK;
         ISA_CK(cudaEventRecord(c->ev[c->ev_count++], st));
         return ISA_OK;
     };
+    if (c->capturing) c->fft_w = c->fft_h = 0;
     ISA_TRY(mark());
     // 1. tracking (high-pass) and accumulation images of every frame
     const std::vector<float> taps_trk = gauss_taps(p->sigma_debayer_tracking), taps_acc = gauss_taps(p->sigma_debayer_accumulation);
@@ -565,9 +590,8 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
             d.base_ref_x = br[0] / lv.resize_level; d.base_ref_y = br[1] / lv.resize_level; d.rot_ref = prealign_rot(pre, ref, r);
             d.base_trk_x = bt[0] / lv.resize_level; d.base_trk_y = bt[1] / lv.resize_level; d.rot_trk = prealign_rot(pre, ref, t);
         }
-        ISA_CK(cudaMemcpyAsync(c->pair_desc + (size_t)li * c->max_pairs, pd.data(), pd.size() * sizeof(isa_pair_desc),
-                               cudaMemcpyHostToDevice, st));
-        ISA_CK(cudaMemcpyAsync(c->frame_tab + (size_t)li * c->max_n, fptr.data(), n * sizeof(float*), cudaMemcpyHostToDevice, st));
+        ISA_CK(h2d(c->pair_desc + (size_t)li * c->max_pairs, pd.data(), pd.size() * sizeof(isa_pair_desc), st));
+        ISA_CK(h2d(c->frame_tab + (size_t)li * c->max_n, fptr.data(), n * sizeof(float*), st));
         ISA_LAUNCH(c, isa_launch_track(c->frame_tab + (size_t)li * c->max_n, lpitch, Wl, Hl, lv.tile_size, lv.max_shift, tcx, tcy,
                                 c->pair_desc + (size_t)li * c->max_pairs, strat.m, grids, gpitch, gstride, p->matching_threshold, nullptr,
                                 c->track_rec ? c->track_rec + rec_off[li] : nullptr,
@@ -627,7 +651,7 @@ int run_merge(isa_ctx* c, const uint16_t* raw, size_t raw_pitch, size_t frame_st
     // 5. accumulation: reference frame first (PrepareAccumulation :1894-1902), then the others in order
     const size_t op = (size_t)g.Wo * 12;
     g.masks_finite = 1;  // the masks come from isa_launch_robustness_erode_tabs, whose values are clamped to [0, 1]
-    ISA_CK(cudaMemcpyAsync(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), cudaMemcpyHostToDevice, st));
+    ISA_CK(h2d(c->frame_in, fin.data(), fin.size() * sizeof(isa_frame_in), st));
     if (hio && hio->host_out) {
         // bands of output rows: accumulate, normalise, then copy out on the copy stream while the next band runs
         if (thr > 0)
@@ -1206,6 +1230,118 @@ int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx, const 
     }
     cudaSetDevice(caller_dev);
     return first;
+}
+
+struct isa_batch_graph {
+    int device = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void* pinned = nullptr;  // the staged tables the graph's copy nodes read
+    std::vector<isa_ctx*> ctxs;
+};
+
+int isa_batch_graph_destroy(isa_batch_graph* gr)
+{
+    if (!gr) return ISA_OK;
+    if (gr->exec) cudaGraphExecDestroy(gr->exec);
+    if (gr->graph) cudaGraphDestroy(gr->graph);
+    if (gr->pinned) cudaFreeHost(gr->pinned);
+    delete gr;
+    return ISA_OK;
+}
+
+int isa_batch_graph_create(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, void* origin,
+                           isa_batch_graph** out)
+{
+    if (!out) return fail(ISA_EINVAL, "graph out pointer is NULL");
+    *out = nullptr;
+    if (!ctxs || !streams || nctx < 1 || !bursts || nbursts < 1 || !origin) return fail(ISA_EINVAL, "bad graph arguments");
+    int dev = 0;
+    ISA_CK(cudaGetDevice(&dev));
+    for (int i = 0; i < nctx; i++) {
+        if (!ctxs[i] || !streams[i]) return fail(ISA_EINVAL, "context or stream %d is NULL", i);
+        if (ctxs[i]->device != dev) return fail(ISA_EINVAL, "context %d is on device %d, not the current device %d", i, ctxs[i]->device, dev);
+        if (streams[i] == origin) return fail(ISA_EINVAL, "stream %d is the origin stream", i);
+        for (int j = 0; j < i; j++)
+            if (streams[j] == streams[i]) return fail(ISA_EINVAL, "streams %d and %d are the same", j, i);
+    }
+    // the pinned arena: per burst at most the tables of its context's maxima (twiddles, solver rows, N0, per level the
+    // pair and frame tables, the frame table of the accumulation), with 16-byte alignment slack per copy
+    size_t per = 0;
+    for (int i = 0; i < nctx; i++) {
+        const isa_ctx* c = ctxs[i];
+        size_t b = ((size_t)c->max_w / 2 + (size_t)c->max_w / 2 + 1 + (size_t)c->max_h) * sizeof(float2);
+        b += (size_t)c->max_rows * 4 * sizeof(int) + (size_t)(c->max_n - 1) * (c->max_n - 1) * sizeof(double);
+        b += (size_t)ISA_MAX_LEVELS * ((size_t)c->max_pairs * sizeof(isa_pair_desc) + (size_t)c->max_n * sizeof(float*));
+        b += (size_t)c->max_n * sizeof(isa_frame_in) + 32 * 16;
+        per = std::max(per, b);
+    }
+    isa_batch_graph* gr = new isa_batch_graph();
+    gr->device = dev;
+    gr->ctxs.assign(ctxs, ctxs + nctx);
+    HostStage stage;
+    stage.cap = per * (size_t)nbursts;
+    if (cudaHostAlloc(&gr->pinned, stage.cap, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        delete gr;
+        return fail(ISA_ENOMEM, "pinned staging of %zu bytes", stage.cap);
+    }
+    stage.base = (char*)gr->pinned;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join(nctx, nullptr);
+    bool ok = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < nctx && ok; i++) ok = cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming) == cudaSuccess;
+    int rc = ok ? ISA_OK : fail(ISA_ECUDA, "event creation failed");
+    cudaStream_t os = (cudaStream_t)origin;
+    bool capturing = false;
+    if (rc == ISA_OK) {
+        if (cudaStreamBeginCapture(os, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            rc = fail(ISA_ECUDA, "cudaStreamBeginCapture failed");
+        else
+            capturing = true;
+    }
+    if (rc == ISA_OK && cudaEventRecord(fork, os) != cudaSuccess) rc = fail(ISA_ECUDA, "fork record failed");
+    for (int i = 0; i < nctx && rc == ISA_OK; i++)
+        if (cudaStreamWaitEvent((cudaStream_t)streams[i], fork, 0) != cudaSuccess) rc = fail(ISA_ECUDA, "fork wait failed");
+    std::vector<int> status(nbursts, ISA_OK);
+    if (rc == ISA_OK) {
+        g_stage = &stage;
+        for (int i = 0; i < nctx; i++) ctxs[i]->capturing = true;
+        rc = isa_merge_batch(ctxs, streams, nctx, bursts, nbursts, status.data());
+        for (int i = 0; i < nctx; i++) ctxs[i]->capturing = false;
+        g_stage = nullptr;
+    }
+    for (int i = 0; i < nctx && capturing; i++) {
+        if (cudaEventRecord(join[i], (cudaStream_t)streams[i]) != cudaSuccess || cudaStreamWaitEvent(os, join[i], 0) != cudaSuccess)
+            if (rc == ISA_OK) rc = fail(ISA_ECUDA, "join failed");
+    }
+    if (capturing) {
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(os, &graph);
+        gr->graph = graph;
+        if (e != cudaSuccess && rc == ISA_OK) rc = fail(ISA_ECUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == ISA_OK && cudaGraphInstantiate(&gr->exec, gr->graph, 0) != cudaSuccess) rc = fail(ISA_ECUDA, "cudaGraphInstantiate failed");
+    if (fork) cudaEventDestroy(fork);
+    for (cudaEvent_t e : join)
+        if (e) cudaEventDestroy(e);
+    if (rc != ISA_OK) {
+        cudaGetLastError();
+        isa_batch_graph_destroy(gr);
+        return rc;
+    }
+    *out = gr;
+    return ISA_OK;
+}
+
+int isa_batch_graph_launch(isa_batch_graph* gr, void* stream)
+{
+    if (!gr || !gr->exec) return fail(ISA_EINVAL, "graph is NULL");
+    int dev = 0;
+    ISA_CK(cudaGetDevice(&dev));
+    if (dev != gr->device) return fail(ISA_EINVAL, "the graph belongs to device %d, the current device is %d", gr->device, dev);
+    ISA_CK(cudaGraphLaunch(gr->exec, S(stream)));
+    return ISA_OK;
 }
 
 int isa_merge_burst_host(isa_ctx* c, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre, float* host_out,

@@ -75,7 +75,8 @@ EXPORTS = [
     "isa_params_default", "isa_last_error", "isa_version", "isa_ctx_create", "isa_ctx_destroy", "isa_output_size", "isa_stage_times",
     "isa_launch_count", "isa_tracking_pairs",
     "isa_merge_burst", "isa_merge_burst_host", "isa_debug_buffers", "isa_debug_shifts", "isa_debug_track_record",
-    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_batch_plan", "isa_ctx_set_tuning", "isa_debayer_full", "isa_gamma_srgb",
+    "isa_merge_backward_tiles", "isa_set_tile_flow", "isa_tile_flow", "isa_ctx_set_params", "isa_batch_plan", "isa_ctx_set_tuning",
+    "isa_batch_graph_create", "isa_batch_graph_launch", "isa_batch_graph_destroy", "isa_debayer_full", "isa_gamma_srgb",
     "isa_bw_image", "isa_prealign_burst", "isa_merge_backward", "isa_merge_batch", "isa_fourier_filter", "isa_gauss_filter", "isa_resize_box", "isa_track_level", "isa_upsample_shifts",
     "isa_solve_shifts", "isa_solve_shifts_static", "isa_optimal_shifts", "isa_flow_from_tiles", "isa_warp", "isa_derivatives", "isa_derivatives2",
     "isa_lucas_kanade", "isa_lk_iteration", "isa_lk_refine", "isa_debayer_subsample", "isa_robustness_mask", "isa_erode",
@@ -830,6 +831,51 @@ def merge_batch(mergers, bursts, streams=None):
     status = (ctypes.c_int * max(1, len(bursts)))()
     lib().isa_merge_batch(ctxs, sts, len(mergers), arr, len(bursts), status)
     return [status[i] for i in range(len(bursts))]
+
+
+def _burst_array(bursts, keep):
+    arr = (IsaBurst * len(bursts))()
+    for i, b in enumerate(bursts):
+        raw, info, out = b["raw"], b["info"], b["out"]
+        n, H, W = raw.shape
+        pp = None
+        if b.get("params") is not None:
+            pp = make_params(b["params"])
+            keep.append(pp)
+        keep.append(info)
+        arr[i] = IsaBurst(raw.data_ptr(), W * 2, W * H * 2, n, ctypes.addressof(info), None,
+                          ctypes.addressof(pp) if pp is not None else None, out.data_ptr(), out.shape[1] * 12)
+    return arr
+
+
+class BatchGraph:
+    """A batch captured once as a CUDA graph (isa_batch_graph_create) and
+    replayed with one host launch (isa_batch_graph_launch). `bursts` as for
+    merge_batch; `streams`: one non-default torch stream per merger; the
+    capture forks from and joins back to `origin` (a torch stream)."""
+
+    def __init__(self, mergers, bursts, streams, origin):
+        self._keep = []
+        arr = _burst_array(bursts, self._keep)
+        ctxs = (ctypes.c_void_p * len(mergers))(*[m.ctx for m in mergers])
+        sts = (ctypes.c_void_p * len(mergers))(*[stream_ptr(s) for s in streams])
+        self.g = ctypes.c_void_p()
+        check(lib().isa_batch_graph_create(ctxs, sts, len(mergers), arr, len(bursts), stream_ptr(origin), ctypes.byref(self.g)))
+        self._refs = (mergers, bursts, streams)
+
+    def launch(self, stream=None):
+        check(lib().isa_batch_graph_launch(self.g, stream_ptr(stream)))
+
+    def close(self):
+        if self.g:
+            lib().isa_batch_graph_destroy(self.g)
+            self.g = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def batch_plan(work, burst_device, ctx_device):

@@ -281,6 +281,24 @@ ISA_API int isa_merge_batch(isa_ctx* const* ctxs, void* const* streams, int nctx
  * context is on the burst's device. Returns the number of unassigned
  * bursts, or ISA_EINVAL for bad arguments. */
 ISA_API int isa_batch_plan(const double* work, const int* burst_device, int nbursts, const int* ctx_device, int nctx, int* assignment);
+/* A batch captured once as a CUDA graph and replayed (no counterpart in the
+ * reference). isa_batch_graph_create captures what isa_merge_batch would
+ * enqueue for `bursts` on ctxs / streams (all on the current device; the
+ * streams distinct, not the legacy default stream, and not `origin`),
+ * forked from and joined back to the `origin` stream, into a graph whose
+ * host-to-device table copies read a pinned arena the graph owns; it runs
+ * nothing. isa_batch_graph_launch replays the whole batch on `stream`: the
+ * same frames and outputs (the bursts' device buffers must stay allocated;
+ * their contents may change between replays), with one launch on the host.
+ * While a graph runs, its contexts must not be used by other calls; merging
+ * other bursts on them between replays is fine (every table the graph reads
+ * is copied in by the graph itself). Stage times (isa_stage_times) are not
+ * recorded by replays. */
+typedef struct isa_batch_graph isa_batch_graph;
+ISA_API int isa_batch_graph_create(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, void* origin,
+                                   isa_batch_graph** graph);
+ISA_API int isa_batch_graph_launch(isa_batch_graph* graph, void* stream);
+ISA_API int isa_batch_graph_destroy(isa_batch_graph* graph);
 /* The same with host buffers: frames are copied in and the image copied out
  * on `stream` (pinned host memory gives full PCIe speed). */
 ISA_API int isa_merge_burst_host(isa_ctx* ctx, const uint16_t* host_raw, int n, const isa_raw_info* info, const isa_prealign* pre,
