@@ -55,6 +55,7 @@ void ComputeKernelParam(float3*, int, int, int, float, float, float, float, floa
 void fourierFilter(float2*, size_t, int, int, float, float, float, float, int);
 void checkForOutliers(float2*, const float*, float*, int*, int*, int, int, int);
 void getOptimalShifts(float2*, const float2*, int, int, int, int, int, int);
+void conjugateComplexMulKernel(const float2*, float2*, int);
 }
 
 typedef float real;  // `float` is `double` in the -DISA_REF_FP64 build
@@ -136,6 +137,14 @@ void ref_fourier_filter_mask(int W, int H, real lp, real hp, real lps, real hps,
         fourierFilter(spec.data(), (size_t)Wc * sizeof(float2), W, H, lp, hp, lps, hps, clearAxis);
     });
     for (size_t i = 0; i < spec.size(); i++) mask[i] = spec[i].x;
+}
+
+// conjugateComplexMulKernel.RunSafe (BasicKernels.cs:65-81): b = conj(a) * b
+// elementwise, block 128 (PreAlignment.cs:200 passes the reference spectrum
+// as a and the rotated frame's as b).
+void ref_conj_mul(const real* a, real* b, int n)
+{
+    run_grid(dim3{128, 1, 1}, (unsigned)n, 1, 1, [&] { conjugateComplexMulKernel((const float2*)a, (float2*)b, n); });
 }
 
 // PatchTracker.Track (PatchTracker.cs:317-360) for one pair. Tiles are cut

@@ -44,3 +44,29 @@ def test_rotation_by_zero_is_identity():
     rng = np.random.default_rng(1)
     img = rng.uniform(0, 1, (20, 30))
     np.testing.assert_allclose(PL.rotate_cubic(img, 0.0), img, atol=1e-12)
+
+
+def test_cross_correlation_product_is_the_reference_kernel():
+    """The scan's cross-correlation product conj(R) * T (oracle scan_angles, and
+    the fused multiply of the GPU's column transforms that test_gpu_prealign
+    checks against it) is the reference's own conjugateComplexMulKernel
+    (kernel.cu:395-411), which PreAlignment.cs:200 calls with the reference
+    spectrum as its first, conjugated operand; run through its host build."""
+    import ctypes
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libref64.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref not built here (no reference checkout)")
+    lib = ctypes.CDLL(path)
+    rng = np.random.default_rng(3)
+    n = 4099
+    R = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    T = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    a = np.ascontiguousarray(np.stack([R.real, R.imag], -1))
+    b = np.ascontiguousarray(np.stack([T.real, T.imag], -1))
+    lib.ref_conj_mul(a.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(n))
+    got = b[:, 0] + 1j * b[:, 1]
+    # numpy's complex product rounds differently from the kernel's four scalar products (an ulp): the convention
+    # (which spectrum is conjugated) is what is pinned; the other one is far off
+    np.testing.assert_allclose(got, np.conj(R) * T, rtol=1e-12, atol=0)
+    assert np.abs(got - np.conj(T) * R).max() > 1.0
