@@ -247,9 +247,6 @@ def adjoint_ratio(args):
                          "fwd_ms": fwd_b, "fwd_adj_tiles_ms": both_b, "ratio": both_b / fwd_b}}
 
 
-FIT_NAMES = ("k_detail", "k_denoise", "dth", "dtr", "k_stretch", "k_shrink", "robust_s", "robust_t")
-
-
 def param_fit(width, height, frames, steps, moving_object=0.0, max_shift=None, seed=3000):
     """Adam on the eight merge parameters (isa_merge_backward), in log space
     from the reference defaults, fitting the merge at scale 1 to the clean
@@ -257,7 +254,7 @@ def param_fit(width, height, frames, steps, moving_object=0.0, max_shift=None, s
     PSNR over the output pixels inside a 32 px margin whose smallest weight
     sum is at least 0.05; PSNR against the scene before and after the fit."""
     import torch
-    from imagestackalignator_b200 import isa, params as P, synthetic
+    from imagestackalignator_b200 import fit, isa, params as P, synthetic
     b = synthetic.make_burst(width, height, frames, seed=seed, max_shift=max_shift or WORKLOAD["max_shift"],
                              max_rot_deg=WORKLOAD["max_rot_deg"], noise_a=WORKLOAD["noise_a"], noise_b=WORKLOAD["noise_b"], device="cuda",
                              keep_truth=True, moving_object=moving_object)
@@ -281,35 +278,18 @@ def param_fit(width, height, frames, steps, moving_object=0.0, max_shift=None, s
         mse = float((om[..., None] * (img - truth) ** 2).sum()) / (3 * npx)
         return 10 * np.log10(1.0 / mse)
 
-    base = np.array([getattr(p, k) for k in FIT_NAMES], np.float64)
-    u = np.zeros(8)
-    mom, vel = np.zeros(8), np.zeros(8)
-    lr, b1, b2 = 0.02, 0.9, 0.999
-    losses = []
+    base = np.array([getattr(p, k) for k in fit.NAMES], np.float64)
     psnr0 = psnr(out)
     torch.cuda.synchronize()
     t0 = time.time()
-    for step in range(1, steps + 1):
-        q = P.MergeParams(**vars(p))
-        for k, v in zip(FIT_NAMES, base * np.exp(u)):
-            setattr(q, k, float(v))
-        m.set_params(q)
-        _, loss, g = m.backward(raw, info, truth, weight=om, out=out)
-        losses.append(loss)
-        gu = g * base * np.exp(u)  # d loss / d log(theta)
-        mom = b1 * mom + (1 - b1) * gu
-        vel = b2 * vel + (1 - b2) * gu * gu
-        u -= lr * (mom / (1 - b1 ** step)) / (np.sqrt(vel / (1 - b2 ** step)) + 1e-12)
-    q = P.MergeParams(**vars(p))
-    for k, v in zip(FIT_NAMES, base * np.exp(u)):
-        setattr(q, k, float(v))
-    m.set_params(q)
+    theta, losses = fit.adam_fit(fit.merger_grad_fn(m, p, raw, info, truth, weight=om, out=out), base, steps)
+    m.set_params(fit.params_of(p, theta))
     fitted = m.merge(raw, info, out).clone()
     torch.cuda.synchronize()
     dt = time.time() - t0
     res = {"workload": f"{frames}x{width}x{height} merged at 1x" + (f", moving object {moving_object:.0%} of the frame" if moving_object else ""),
            "steps": steps, "loss_first": losses[0], "loss_last": losses[-1], "psnr_before_db": psnr0, "psnr_after_db": psnr(fitted),
-           "ms_per_step": 1000 * dt / steps, "params_after": {k: float(v) for k, v in zip(FIT_NAMES, base * np.exp(u))}}
+           "ms_per_step": 1000 * dt / steps, "params_after": {k: float(v) for k, v in zip(fit.NAMES, theta)}}
     m.close()
     return res
 
