@@ -26,6 +26,7 @@ STRUCTS = {
     "isa_raw_levels": isa.IsaRawLevels,
     "isa_pef_info": isa.IsaPefInfo,
     "isa_burst": isa.IsaBurst,
+    "isa_tuning": isa.IsaTuning,
 }
 
 
