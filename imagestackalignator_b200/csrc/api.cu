@@ -1315,6 +1315,9 @@ int isa_batch_graph_create(isa_ctx* const* ctxs, void* const* streams, int nctx,
         if (cudaEventRecord(join[i], (cudaStream_t)streams[i]) != cudaSuccess || cudaStreamWaitEvent(os, join[i], 0) != cudaSuccess)
             if (rc == ISA_OK) rc = fail(ISA_ECUDA, "join failed");
     }
+    // the capture ran the host side of every merge but none of its copies: the contexts' transform tables are
+    // whatever they were before, so the size they record is forgotten and the next merge uploads its own
+    for (int i = 0; i < nctx; i++) ctxs[i]->fft_w = ctxs[i]->fft_h = 0;
     if (capturing) {
         cudaGraph_t graph = nullptr;
         const cudaError_t e = cudaStreamEndCapture(os, &graph);

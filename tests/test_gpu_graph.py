@@ -61,6 +61,30 @@ def test_graph_replays_equal_the_direct_batch(batch):
     g.close()
 
 
+def test_merges_after_a_capture_use_their_own_tables(batch):
+    """The capture runs the host side of the merges but none of their copies:
+    a direct merge right after it, of the size captured last, must still
+    upload its own transform tables (the context held another size before)."""
+    import torch
+    items, mergers = batch
+    m0 = mergers[0]
+    s0, origin = torch.cuda.Stream(), torch.cuda.Stream()
+    want = []
+    for it in items:
+        one = dict(it, out=torch.empty_like(it["out"]))
+        assert not any(isa.merge_batch([m0], [one]))
+        want.append(one["out"])
+    other = synthetic.make_burst(600, 400, 5, seed=98, max_shift=3.0)
+    o_out = torch.empty(m0.output_size(600, 400)[::-1] + (3,), dtype=torch.float32, device="cuda")
+    m0.merge(torch.from_numpy(np.ascontiguousarray(other.raw).view(np.int16)).cuda(), isa.make_info(other), o_out)
+    g = isa.BatchGraph([m0], items, [s0], origin)
+    last = dict(items[-1], out=torch.empty_like(items[-1]["out"]))
+    assert not any(isa.merge_batch([m0], [last]))
+    torch.cuda.synchronize()
+    assert torch.equal(last["out"], want[-1])
+    g.close()
+
+
 def test_graph_arguments_are_checked(batch):
     import torch
     items, mergers = batch
