@@ -1317,7 +1317,11 @@ int isa_batch_graph_create(isa_ctx* const* ctxs, void* const* streams, int nctx,
     }
     // the capture ran the host side of every merge but none of its copies: the contexts' transform tables are
     // whatever they were before, so the size they record is forgotten and the next merge uploads its own
-    for (int i = 0; i < nctx; i++) ctxs[i]->fft_w = ctxs[i]->fft_h = 0;
+    // (and the last merge the debug entry points describe did not run)
+    for (int i = 0; i < nctx; i++) {
+        ctxs[i]->fft_w = ctxs[i]->fft_h = 0;
+        ctxs[i]->last_n = 0;
+    }
     if (capturing) {
         cudaGraph_t graph = nullptr;
         const cudaError_t e = cudaStreamEndCapture(os, &graph);

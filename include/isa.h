@@ -293,7 +293,9 @@ ISA_API int isa_batch_plan(const double* work, const int* burst_device, int nbur
  * While a graph runs, its contexts must not be used by other calls; merging
  * other bursts on them between replays is fine (every table the graph reads
  * is copied in by the graph itself). Stage times (isa_stage_times) are not
- * recorded by replays. */
+ * recorded by replays, and after isa_batch_graph_create the debug entry
+ * points (isa_debug_buffers, isa_debug_shifts, isa_tile_flow) report no
+ * merge until the next direct merge. */
 typedef struct isa_batch_graph isa_batch_graph;
 ISA_API int isa_batch_graph_create(isa_ctx* const* ctxs, void* const* streams, int nctx, const isa_burst* bursts, int nbursts, void* origin,
                                    isa_batch_graph** graph);
