@@ -82,3 +82,17 @@ def test_bilinear_loss_is_continuous_in_the_tile_flow(bil, oracle):
         agree += abs(d[0] - d[1]) <= 1e-3 * max(abs(d[0]), 1e-12)
         nonzero += d[0] != 0.0
     assert agree >= 3 and nonzero >= 3
+
+
+def test_merge_from_tiles_follows_parameter_changes(bil, oracle):
+    """Its caches are keyed on what each step depends on: a change of the
+    kernel-shape or robustness parameters gives the full merge's image."""
+    b, p, keep, res = bil
+    PL.merge_from_tiles(b, p, keep["tiles"], keep, oracle)  # fill the caches at p
+    for name, factor in (("k_detail", 1.2), ("robust_t", 0.8)):
+        q = P.MergeParams(**vars(p))
+        setattr(q, name, float(np.float32(getattr(p, name) * factor)))
+        want = PL.merge_burst(b, q, lib=oracle, tiles=keep["tiles"]).image
+        got = PL.merge_from_tiles(b, q, keep["tiles"], keep, oracle).image
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+        assert np.abs(got - res.image).max() > 1e-6  # the change is visible
