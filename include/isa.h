@@ -211,10 +211,11 @@ ISA_API int isa_merge_burst(isa_ctx* ctx, const uint16_t* raw, size_t raw_pitch,
  * weight sum reaches exactly zero is set to 0 (ApplyWeighting), a jump, and
  * the mask clamps and the erosion's minimum have kinks; the gradient is
  * that of the smooth piece at the parameters (a zero weight excludes pixels
- * near such jumps). The gradient with respect to the flow is zero almost
- * everywhere -- the accumulation and the mask read the frames at
- * round(s * flow) and round(flow / 2) and the mask's flow term M only
- * switches the gain at a threshold -- so none is returned. Covers the
+ * near such jumps). No flow gradient is returned here: in sample mode
+ * ROUND it is zero almost everywhere (the accumulation and the mask read
+ * the frames at round(s * flow) and round(flow / 2), and the mask's flow
+ * term M only switches the gain at a threshold); in sample mode BILINEAR
+ * isa_merge_backward_tiles returns it. Covers the
  * merge_scale and super-resolution modes (normalisation threshold 0) with
  * fused_accumulate. Allocates nothing: the adjoint's scratch is context
  * memory the forward has finished with, so afterwards the tracking and
